@@ -1,0 +1,238 @@
+/* minipic_cuda.h -- C ABI of the B200 (sm_100a) implementation of mini-pic's
+ * per-step hot path: particle push + barycentric tet walk + node-density
+ * scatter (MoveParticles), the per-element E-field gather (FESolver::updateEf)
+ * and FESolver's Poisson-Boltzmann Newton step (computePhi).
+ *
+ * Plain pointers and sizes only.  Every call returns an int status (MP_OK or
+ * an MP_ERR_* code); mp_last_error() gives the message of the last failure on
+ * a context.  One context per host thread; a context owns one CUDA stream and
+ * all of its device buffers.  There is no CPU fallback: without a usable
+ * sm_100 device mp_create returns MP_ERR_NO_DEVICE.
+ *
+ * Reference interfaces each entry point replaces (paths in the reference
+ * project AD1641/mini-fem-pic-main):
+ *   mp_create / mp_destroy        DeviceData ctor/dtor, src/mini-pic.cpp:322-345
+ *   mp_particles_append           InjectIons' push_back + the per-step H2D copy,
+ *                                 src/mini-pic.cpp:257-260, 274-275
+ *   mp_push_scatter               MoveParticles, src/mini-pic.cpp:268-320
+ *   mp_particles_download         the per-step D2H copy, src/mini-pic.cpp:311
+ *   mp_density_download           src/mini-pic.cpp:312
+ *   mp_fe_setup                   FESolver ctor + preAssembly, src/FESolver.cpp:48-127, 434-485
+ *   mp_compute_phi                FESolver::computePhi, src/FESolver.cpp:604-619
+ *   mp_fe_build_f1                FESolver::buildF1Vector, src/FESolver.cpp:488-526
+ *   mp_fe_residual                G = K d - F0 - F1, src/FESolver.cpp:333-335
+ *   mp_fe_build_j                 FESolver::buildJmatrix, src/FESolver.cpp:367-431
+ *   mp_fe_solve_linear            FESolver::solveLinear / solveLinearLapack,
+ *                                 src/FESolver.cpp:561-601 / 528-558
+ *   mp_update_ef                  FESolver::updateEf, src/FESolver.cpp:622-636
+ *   mp_field_download             reads of FESolver::d, uh, ef (src/FESolver.h:45-49)
+ *   mp_mesh_geometry              LoadVolumeMesh geometry precompute, src/meshes.cpp:87-251
+ *   mp_fe_geometry                FESolver::computeNX + ID/LM, src/FESolver.cpp:108-118, 207-287
+ *   mp_injector_*                 InjectIons, src/mini-pic.cpp:208-265
+ */
+#ifndef MINIPIC_CUDA_H
+#define MINIPIC_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------- */
+enum {
+    MP_OK = 0,
+    MP_ERR_ARG = 1,           /* bad argument (null pointer, size, index) */
+    MP_ERR_OOM = 2,           /* device or pinned-host allocation failed */
+    MP_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+    MP_ERR_WALK_LIMIT = 4,    /* a particle's tet walk exceeded the hop limit */
+    MP_ERR_NOT_CONVERGED = 5, /* Newton (NonLinear method) did not converge */
+    MP_ERR_SINGULAR = 6,      /* factorization met a zero/non-finite pivot */
+    MP_ERR_STATE = 7,         /* call out of order (e.g. no FE setup yet) */
+    MP_ERR_NO_DEVICE = 8,     /* no usable sm_100 device */
+    MP_ERR_TIMEOUT = 9        /* a bounded device-side wait gave up */
+};
+
+/* FESolver::Method, src/FESolver.h:26 */
+enum { MP_METHOD_NONLINEAR = 0, MP_METHOD_GAUSS_SEIDEL = 1, MP_METHOD_LAPACK = 2 };
+
+/* Arithmetic forms. FP64 is the reference's method bit for bit on the particle
+ * side; MIXED stores particles as FP32 offsets from the owning tet's vertex 0
+ * (FP64 near-face re-test, FP64 density accumulators) and factors the Newton
+ * Jacobian in TF32 on the tensor cores with FP64 iterative refinement. */
+enum { MP_FORM_FP64 = 0, MP_FORM_MIXED = 1 };
+
+/* Density accumulation: FP64 atomics (order-dependent rounding, like the
+ * reference's atomic_ref) or 64-bit fixed point (run-to-run deterministic). */
+enum { MP_SCATTER_FP64_ATOMIC = 0, MP_SCATTER_FIXED64 = 1 };
+
+/* Particle order for mp_particles_download. */
+enum { MP_ORDER_STORAGE = 0, MP_ORDER_ID = 1 };
+
+/* Vector/matrix names for mp_fe_download / mp_fe_upload. */
+enum {
+    MP_VEC_F0 = 0, MP_VEC_F1 = 1, MP_VEC_D = 2, MP_VEC_G = 3, MP_VEC_UH = 4,
+    MP_VEC_DEN = 5, MP_VEC_EF = 6, MP_VEC_RESIDUAL = 7, MP_VEC_Y = 8,
+    MP_MAT_K = 16, MP_MAT_J = 17
+};
+
+typedef struct mp_ctx mp_ctx;
+
+/* Mesh description.  Every per-tet field is given by the address of tet 0's
+ * field and the byte stride between consecutive tets, so a caller can point
+ * straight into an array of the reference's Tetra records (stride 168) or
+ * into packed arrays.  Same for per-node fields (the reference's Node is 40 B). */
+typedef struct mp_mesh_desc {
+    int32_t n_nodes;
+    int32_t n_tets;
+    const int32_t *con;      int64_t con_stride;      /* 4 node ids, src/meshes.h:34 */
+    const double *volume;    int64_t volume_stride;   /* src/meshes.h:35 */
+    const double *alpha;     int64_t alpha_stride;    /* 4 each, src/meshes.h:39 */
+    const double *beta;      int64_t beta_stride;
+    const double *gamma;     int64_t gamma_stride;
+    const double *delta;     int64_t delta_stride;
+    const int32_t *cell_con; int64_t cell_con_stride; /* 4 neighbours, -1 = none, src/meshes.h:42 */
+    const double *node_pos;  int64_t node_pos_stride; /* 3 coords, src/meshes.h:27 */
+    const double *node_volume; int64_t node_volume_stride; /* src/meshes.h:29 */
+} mp_mesh_desc;
+
+/* FE description (FESolver's public members, src/FESolver.h:27-51). */
+typedef struct mp_fe_desc {
+    int32_t neq;
+    const int32_t *ID;        /* [n_nodes] equation of each node, -1 = Dirichlet */
+    const double *nx;         /* [n_tets][4][3] dN_a/dx (FESolver::NX) */
+    const double *detJ;       /* [n_tets] */
+    const double *g;          /* [n_nodes] Dirichlet values */
+    const double *const *K_rows; /* optional: neq row pointers of K; NULL = assemble on the device */
+    const double *K_dense;    /* optional alternative: row-major neq x neq */
+    const double *F0;         /* optional [neq]; NULL = assemble on the device */
+    double n0, phi0, kTe;     /* Boltzmann reference values */
+} mp_fe_desc;
+
+typedef struct mp_step_stats {
+    int64_t n_before;         /* particles pushed */
+    int64_t n_after;          /* particles kept */
+    int64_t total_hops;       /* tet-to-tet moves of all particles this step */
+    int32_t max_hops;         /* longest walk this step */
+    int32_t near_face_fp64;   /* mixed form: FP64 re-tests taken */
+} mp_step_stats;
+
+typedef struct mp_newton_stats {
+    int32_t newton_iterations;
+    int32_t linear_iterations;   /* GS sweeps of the last solve / refinement steps */
+    double l2;                   /* ||y|| / neq of the last Newton update */
+    double linear_residual;      /* ||b - J y|| / neq of the last linear solve */
+    double ms_total;             /* device time of the call, ms */
+    double ms_factor;            /* device time of the factorization, ms */
+} mp_newton_stats;
+
+/* ---- context ---------------------------------------------------------------- */
+const char *mp_error_string(int status);
+const char *mp_last_error(const mp_ctx *ctx);
+int mp_version(void);
+
+int mp_create(int device, const mp_mesh_desc *mesh, mp_ctx **out);
+int mp_destroy(mp_ctx *ctx);
+int mp_synchronize(mp_ctx *ctx);
+int mp_get_stream(mp_ctx *ctx, void **cuda_stream);
+/* Options: hop limit of the tet walk (default 4096), density accumulation mode,
+ * particle-ID tracking (default on), tet re-sort period in steps (0 = never). */
+int mp_set_walk_limit(mp_ctx *ctx, int32_t max_hops);
+int mp_set_scatter_mode(mp_ctx *ctx, int mode);
+int mp_set_sort_period(mp_ctx *ctx, int32_t steps);
+int mp_set_particle_form(mp_ctx *ctx, int form);
+
+/* ---- particles ---------------------------------------------------------------- */
+int mp_particles_reserve(mp_ctx *ctx, int64_t capacity);
+/* Appends n particles from host memory (strided like the reference's Particle,
+ * 88 B).  If rewind != 0 the device applies InjectIons' half-step velocity
+ * rewind with the current device E field: vel -= (q_over_m*ef[cell])*half_dt
+ * (src/mini-pic.cpp:253-257).  New particles get consecutive IDs. */
+int mp_particles_append(mp_ctx *ctx, int64_t n,
+                        const double *pos, int64_t pos_stride,
+                        const double *vel, int64_t vel_stride,
+                        const int32_t *cell, int64_t cell_stride,
+                        int rewind, double q_over_m, double half_dt);
+/* Appends from device memory: SoA arrays pos[3][n], vel[3][n], cell[n]. */
+int mp_particles_append_device(mp_ctx *ctx, int64_t n, const double *pos_soa, const double *vel_soa,
+                               const int32_t *cell, int rewind, double q_over_m, double half_dt);
+int mp_particles_count(mp_ctx *ctx, int64_t *n);
+/* Copies all particles to host memory, strided; any output may be NULL.  lc
+ * gets the barycentric weights in the current tet (recomputed exactly as the
+ * walk computes them).  order = MP_ORDER_ID returns injection order. */
+int mp_particles_download(mp_ctx *ctx, int64_t n_max,
+                          double *pos, int64_t pos_stride,
+                          double *vel, int64_t vel_stride,
+                          int32_t *cell, int64_t cell_stride,
+                          double *lc, int64_t lc_stride,
+                          int64_t *id, int order);
+int mp_particles_clear(mp_ctx *ctx);
+
+/* ---- MoveParticles -------------------------------------------------------------- */
+/* One push: E gather + kick + drift + tet walk + density scatter for every
+ * particle, stable removal of the particles that left the domain, and the
+ * normalisation den[n] *= spwt / node_volume[n].  The density stays on the
+ * device for mp_compute_phi; den_out (host, nullable) receives a copy. */
+int mp_push_scatter(mp_ctx *ctx, double q_over_m, double dt, double spwt,
+                    double *den_out, mp_step_stats *stats);
+int mp_density_download(mp_ctx *ctx, double *den);
+int mp_sort_by_tet(mp_ctx *ctx);
+
+/* ---- field solve ------------------------------------------------------------------ */
+int mp_fe_setup(mp_ctx *ctx, const mp_fe_desc *fe);
+int mp_fe_upload(mp_ctx *ctx, int which, const double *values);
+int mp_fe_download(mp_ctx *ctx, int which, double *out);
+/* FESolver::computePhi: ion_den (host, nullable = the device density of the last
+ * push) -> Newton step(s) by `method` -> uh = g + d. */
+int mp_compute_phi(mp_ctx *ctx, const double *ion_den, int method, int form, mp_newton_stats *stats);
+int mp_fe_build_f1(mp_ctx *ctx, const double *ion_den);
+int mp_fe_residual(mp_ctx *ctx);
+int mp_fe_build_j(mp_ctx *ctx, int method);
+/* Solves J y = G (G from mp_fe_residual, or b if non-NULL); y stays on the device
+ * (MP_VEC_Y).  method MP_METHOD_GAUSS_SEIDEL or MP_METHOD_LAPACK. */
+int mp_fe_solve_linear(mp_ctx *ctx, int method, int form, const double *b, mp_newton_stats *stats);
+/* FESolver::updateEf from the device uh (or uh_host if non-NULL). */
+int mp_update_ef(mp_ctx *ctx, const double *uh_host);
+int mp_field_download(mp_ctx *ctx, double *d, double *uh, double *ef);
+
+/* ---- host-side setup helpers (no device needed) ----------------------------------- */
+/* LoadVolumeMesh's geometry (src/meshes.cpp:80-262) from node positions in metres
+ * and 0-based tet connectivity.  con is fixed in place for negative volumes.
+ * Outputs: volume[n_tets], alpha/beta/gamma/delta[n_tets][4], cell_con[n_tets][4],
+ * node_volume[n_nodes], node_open[n_nodes] (1 where the reference marks OPEN). */
+int mp_mesh_geometry(int32_t n_nodes, const double *node_pos, int32_t n_tets, int32_t *con,
+                     double *volume, double *alpha, double *beta, double *gamma, double *delta,
+                     int32_t *cell_con, double *node_volume, int32_t *node_open);
+/* FESolver ctor bookkeeping (src/FESolver.cpp:48-127): ID from node types
+ * (0 NORMAL, 1 OPEN, 2 INLET, 3 FIXED), NX and detJ.  Returns neq in *neq. */
+int mp_fe_geometry(int32_t n_nodes, const double *node_pos, const int32_t *node_type,
+                   int32_t n_tets, const int32_t *con, int32_t *ID, double *nx, double *detJ, int32_t *neq);
+/* LoadSurfaceMesh's inlet face data (src/meshes.cpp:290-353): owning tet, u, v,
+ * unit normal and area of each inlet triangle (0-based node ids). */
+int mp_inlet_faces(int32_t n_nodes, const double *node_pos, int32_t n_tets, const int32_t *con,
+                   int32_t n_faces, const int32_t *face_con, int invert_normals,
+                   int32_t *cell_con, double *u, double *v, double *normal, double *area);
+
+/* InjectIons (src/mini-pic.cpp:208-265) with the reference's RNG stream
+ * (std::mt19937 seeded 0, uniform_real_distribution<double>(0,1)). */
+typedef struct mp_injector mp_injector;
+int mp_injector_create(int32_t n_faces, const int32_t *face_con, const double *u, const double *v,
+                       const double *normal, const double *area, const int32_t *cell_con,
+                       const double *node_pos, uint32_t seed, mp_injector **out);
+int mp_injector_destroy(mp_injector *inj);
+/* Samples one step's particles into caller buffers (capacity max_n, SoA-strided
+ * like mp_particles_append).  The velocity rewind is not applied (pass rewind=1
+ * to mp_particles_append).  *n_out = particles written. */
+int mp_injector_sample(mp_injector *inj, double plasma_den, double ion_velocity, double dt, double spwt,
+                       int64_t max_n, double *pos, int64_t pos_stride, double *vel, int64_t vel_stride,
+                       int32_t *cell, int64_t cell_stride, int64_t *n_out);
+int mp_injector_count(mp_injector *inj, double plasma_den, double ion_velocity, double dt, double spwt,
+                      int64_t *n_next);
+int mp_injector_get_rem(mp_injector *inj, double *rem);
+int mp_injector_set_rem(mp_injector *inj, double rem);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MINIPIC_CUDA_H */

@@ -1,0 +1,759 @@
+// Particle push: E gather + kick + drift + barycentric tet walk + node-density
+// scatter + stable removal of exited particles, in one pass over the particle
+// arrays (MoveParticles, src/mini-pic.cpp:268-320; walk XtoLtet,
+// src/meshes.h:75-100).
+//
+// One persistent grid; each CTA takes 256-particle tiles from a ticket counter.
+// Survivors are written to the other particle buffer at their global rank,
+// found by a decoupled look-back over the tiles' running counts, so the
+// removal is stable (the reference's std::erase_if order) and particle data
+// crosses HBM once per step: read 52 B, write 52 B (FP64) or 28 B + 28 B (mixed).
+#include <cuda/atomic>
+
+#include "mp_internal.h"
+
+namespace mp {
+
+constexpr int PUSH_THREADS = 256;
+constexpr double ONE_SIXTH = 1.0 / 6.0;
+constexpr unsigned long long ST_AGG = 1ull << 62;
+constexpr unsigned long long ST_PREFIX = 2ull << 62;
+constexpr unsigned long long ST_VALUE = (1ull << 62) - 1;
+constexpr long long LOOKBACK_SPIN_LIMIT = 1ll << 24;
+constexpr double FIXED_SCALE = 1099511627776.0;  // 2^40
+constexpr double NEAR_FACE = 1e-5;
+
+struct PushF64Args {
+    PartsF64 in, out;
+    const TetRec *__restrict__ tets;
+    double *den;
+    unsigned long long *den_fixed;
+    unsigned long long *counters;
+    unsigned long long *status;
+    double qm, dt;
+    int walk_limit;
+    int fixed;
+    int track_ids;
+};
+
+struct PushF32Args {
+    PartsF32 in, out;
+    const TetRec32 *__restrict__ tets32;
+    const TetRec *__restrict__ tets;
+    const double *__restrict__ x0;   // [n_tets][4]
+    double *den;
+    unsigned long long *den_fixed;
+    unsigned long long *counters;
+    unsigned long long *status;
+    float qm_dt;                     // q/m * dt
+    float dt;
+    int walk_limit;
+    int fixed;
+    int track_ids;
+};
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Position of the n-th (0-based) set bit of m; m must have more than n bits set.
+__device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
+    int base = 0;
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1) {
+        unsigned low = m & ((1u << w) - 1u);
+        int c = __popc(low);
+        if (n >= c) {
+            n -= c;
+            m >>= w;
+            base += w;
+        } else {
+            m = low;
+        }
+    }
+    return base;
+}
+
+// Sums v[0..3] over the lanes that share `key` (one tet), leaving the sums in
+// the group's lowest lane.  All 32 lanes must call it.  Returns true for the
+// lanes that hold a group sum.
+template <typename T>
+__device__ __forceinline__ bool group_sum4(int key, T v[4]) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    unsigned peers = __match_any_sync(FULL, key);
+    int r = __popc(peers & lanemask_lt());
+    int gsize = __popc(peers);
+    int maxg = __reduce_max_sync(FULL, gsize);
+    for (int s = 1; s < maxg; s <<= 1) {
+        int pr = r + s;
+        int src = pr < gsize ? nth_set_bit(peers, pr) : lane;
+        T t[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) t[i] = __shfl_sync(FULL, v[i], src);
+        if ((r & (2 * s - 1)) == 0 && pr < gsize) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) v[i] += t[i];
+        }
+    }
+    return r == 0;
+}
+
+__device__ __forceinline__ void store_release(unsigned long long *p, unsigned long long v) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(*p);
+    a.store(v, cuda::memory_order_release);
+}
+__device__ __forceinline__ unsigned long long load_acquire(unsigned long long *p) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(*p);
+    return a.load(cuda::memory_order_acquire);
+}
+
+// Exclusive prefix of tile `tile` given its own count (called by one thread).
+__device__ long long lookback(unsigned long long *status, long long tile, long long count,
+                              unsigned long long *counters) {
+    if (tile == 0) {
+        store_release(&status[0], ST_PREFIX | (unsigned long long)count);
+        return 0;
+    }
+    store_release(&status[tile], ST_AGG | (unsigned long long)count);
+    long long excl = 0;
+    long long p = tile - 1;
+    long long spins = 0;
+    while (p >= 0) {
+        unsigned long long s = load_acquire(&status[p]);
+        unsigned long long flag = s & ~ST_VALUE;
+        if (flag == 0) {
+            if (++spins > LOOKBACK_SPIN_LIMIT) {
+                atomicOr(&counters[C_FLAGS], FLAG_LOOKBACK_TIMEOUT);
+                break;
+            }
+            continue;
+        }
+        excl += (long long)(s & ST_VALUE);
+        if (flag == ST_PREFIX) break;
+        p--;
+    }
+    store_release(&status[tile], ST_PREFIX | (unsigned long long)(excl + count));
+    return excl;
+}
+
+// Barycentric weight i of point (x,y,z) in tet t, the reference's expression
+// (1.0/6.0)*(alpha - x*beta + y*gamma - z*delta)/volume in its order, unfused.
+__device__ __forceinline__ void lambdas_fp64(const TetRec *__restrict__ t, double x, double y, double z,
+                                             double lc[4]) {
+    const double2 *a2 = reinterpret_cast<const double2 *>(t->alpha);
+    const double2 *b2 = reinterpret_cast<const double2 *>(t->beta);
+    const double2 *g2 = reinterpret_cast<const double2 *>(t->gamma);
+    const double2 *d2 = reinterpret_cast<const double2 *>(t->delta);
+    double vol = __ldg(&t->volume);
+    double al[4], be[4], ga[4], de[4];
+    double2 q;
+    q = __ldg(a2); al[0] = q.x; al[1] = q.y; q = __ldg(a2 + 1); al[2] = q.x; al[3] = q.y;
+    q = __ldg(b2); be[0] = q.x; be[1] = q.y; q = __ldg(b2 + 1); be[2] = q.x; be[3] = q.y;
+    q = __ldg(g2); ga[0] = q.x; ga[1] = q.y; q = __ldg(g2 + 1); ga[2] = q.x; ga[3] = q.y;
+    q = __ldg(d2); de[0] = q.x; de[1] = q.y; q = __ldg(d2 + 1); de[2] = q.x; de[3] = q.y;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        double v = __dsub_rn(al[i], __dmul_rn(x, be[i]));
+        v = __dadd_rn(v, __dmul_rn(y, ga[i]));
+        v = __dsub_rn(v, __dmul_rn(z, de[i]));
+        v = __dmul_rn(ONE_SIXTH, v);
+        lc[i] = __ddiv_rn(v, vol);
+    }
+}
+
+// XtoLtet (src/meshes.h:75-100) with a hop limit.  Returns 1 inside, 0 left the
+// domain, -1 hop limit reached (cell is then the last tet visited).
+__device__ __forceinline__ int walk_fp64(const TetRec *__restrict__ tets, int &cell, double x, double y, double z,
+                                         double lc[4], int limit, int &hops) {
+    for (;;) {
+        const TetRec *t = tets + cell;
+        lambdas_fp64(t, x, y, z, lc);
+        bool inside = true;
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            if (lc[i] < 0 || lc[i] > 1.0) inside = false;
+        if (inside) return 1;
+        int min_i = 0;
+        double min_lc = lc[0];
+#pragma unroll
+        for (int i = 1; i < 4; i++)
+            if (lc[i] < min_lc) {
+                min_lc = lc[i];
+                min_i = i;
+            }
+        int nb = __ldg(&t->cell_con[min_i]);
+        if (nb < 0) return 0;
+        if (hops >= limit) return -1;
+        cell = nb;
+        hops++;
+    }
+}
+
+// Shared tail of both push kernels: scatter, block scan, look-back.  Returns the
+// output index of this thread's particle (or -1 if it is removed).
+template <typename Lc>
+__device__ __forceinline__ long long scatter_and_rank(int keep_state, int cell, const int con[4], Lc lcv[4],
+                                                      double *den, unsigned long long *den_fixed, int fixed,
+                                                      long long tile, unsigned long long *status,
+                                                      unsigned long long *counters, int hops,
+                                                      long long n_tiles, int *s_wc, long long *s_base) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    __syncwarp();
+    // density scatter, aggregated over the lanes of a warp that sit in one tet
+    int key = keep_state == 1 ? cell : -2 - lane;
+    if (fixed) {
+        unsigned long long q[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            q[i] = keep_state == 1 ? (unsigned long long)__double2ll_rn((double)lcv[i] * FIXED_SCALE) : 0ull;
+        bool leader = group_sum4<unsigned long long>(key, q);
+        if (leader && keep_state == 1) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) atomicAdd(&den_fixed[con[i]], q[i]);
+        }
+    } else {
+        double s[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) s[i] = keep_state == 1 ? (double)lcv[i] : 0.0;
+        bool leader = group_sum4<double>(key, s);
+        if (leader && keep_state == 1) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) atomicAdd(&den[con[i]], s[i]);
+        }
+    }
+    // walk statistics
+    int hsum = __reduce_add_sync(0xffffffffu, hops);
+    int hmax = __reduce_max_sync(0xffffffffu, hops);
+    if (lane == 0 && hsum) {
+        atomicAdd(&counters[C_HOPS], (unsigned long long)hsum);
+        atomicMax(&counters[C_MAX_HOPS], (unsigned long long)hmax);
+    }
+    // stable rank of the kept particles
+    bool keep = keep_state != 0;
+    unsigned kb = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) s_wc[warp] = __popc(kb);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long run = 0;
+        for (int w = 0; w < PUSH_THREADS / 32; w++) {
+            int c = s_wc[w];
+            s_wc[w] = (int)run;
+            run += c;
+        }
+        long long excl = lookback(status, tile, run, counters);
+        *s_base = excl;
+        if (tile == n_tiles - 1) counters[C_N_OUT] = (unsigned long long)(excl + run);
+    }
+    __syncthreads();
+    long long idx = keep ? *s_base + s_wc[warp] + __popc(kb & lanemask_lt()) : -1;
+    return idx;
+}
+
+__global__ void __launch_bounds__(PUSH_THREADS) k_push_fp64(PushF64Args a) {
+    __shared__ long long s_tile;
+    __shared__ int s_wc[PUSH_THREADS / 32];
+    __shared__ long long s_base;
+    const long long n = (long long)a.counters[C_N];
+    const long long n_tiles = (n + PUSH_THREADS - 1) / PUSH_THREADS;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(&a.counters[C_TILE], 1ull);
+        __syncthreads();
+        const long long tile = s_tile;
+        if (tile >= n_tiles) break;
+        const long long i = tile * PUSH_THREADS + threadIdx.x;
+        int state = 0, cell = -1, hops = 0;
+        int con[4] = {0, 0, 0, 0};
+        double lc[4] = {0, 0, 0, 0};
+        double x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 0;
+        long long id = 0;
+        if (i < n) {
+            x = a.in.px[i]; y = a.in.py[i]; z = a.in.pz[i];
+            vx = a.in.vx[i]; vy = a.in.vy[i]; vz = a.in.vz[i];
+            cell = a.in.cell[i];
+            if (a.track_ids) id = a.in.id[i];
+            const TetRec *t = a.tets + cell;
+            // v += q_over_m*ef*dt ; x += v*dt  (src/mini-pic.cpp:291-295)
+            vx = __dadd_rn(vx, __dmul_rn(__dmul_rn(a.qm, __ldg(&t->ef[0])), a.dt));
+            vy = __dadd_rn(vy, __dmul_rn(__dmul_rn(a.qm, __ldg(&t->ef[1])), a.dt));
+            vz = __dadd_rn(vz, __dmul_rn(__dmul_rn(a.qm, __ldg(&t->ef[2])), a.dt));
+            x = __dadd_rn(x, __dmul_rn(vx, a.dt));
+            y = __dadd_rn(y, __dmul_rn(vy, a.dt));
+            z = __dadd_rn(z, __dmul_rn(vz, a.dt));
+            int w = walk_fp64(a.tets, cell, x, y, z, lc, a.walk_limit, hops);
+            if (w == 1) {
+                state = 1;
+                const int4 c4 = __ldg(reinterpret_cast<const int4 *>(a.tets[cell].con));
+                con[0] = c4.x; con[1] = c4.y; con[2] = c4.z; con[3] = c4.w;
+            } else if (w == -1) {
+                state = 2;  // kept, not scattered, error raised
+                atomicOr(&a.counters[C_FLAGS], FLAG_WALK_LIMIT);
+            } else {
+                cell = -1;
+            }
+        }
+        long long o = scatter_and_rank<double>(state, cell, con, lc, a.den, a.den_fixed, a.fixed, tile, a.status,
+                                               a.counters, hops, n_tiles, s_wc, &s_base);
+        if (o >= 0) {
+            a.out.px[o] = x; a.out.py[o] = y; a.out.pz[o] = z;
+            a.out.vx[o] = vx; a.out.vy[o] = vy; a.out.vz[o] = vz;
+            a.out.cell[o] = cell;
+            if (a.track_ids) a.out.id[o] = id;
+        }
+        __syncthreads();
+    }
+}
+
+// Mixed form.  Position is an FP32 offset r from the owning tet's vertex 0 and
+// the weights are lambda_i = [i==0] + g_i . r in FP32.  When the smallest
+// weight is within 1e-5 of zero the inside test and the exit face are decided
+// in FP64 with the reference's formula on x = x0 + r.  Walking to a new tet
+// re-bases r on that tet's vertex 0 (in FP64, rounded once to FP32).
+__device__ __forceinline__ void lambdas_fp32(const TetRec32 *__restrict__ t, float rx, float ry, float rz,
+                                             float lc[4]) {
+    const float4 gx = __ldg(reinterpret_cast<const float4 *>(t->gx));
+    const float4 gy = __ldg(reinterpret_cast<const float4 *>(t->gy));
+    const float4 gz = __ldg(reinterpret_cast<const float4 *>(t->gz));
+    lc[0] = 1.0f + fmaf(gx.x, rx, fmaf(gy.x, ry, gz.x * rz));
+    lc[1] = fmaf(gx.y, rx, fmaf(gy.y, ry, gz.y * rz));
+    lc[2] = fmaf(gx.z, rx, fmaf(gy.z, ry, gz.z * rz));
+    lc[3] = fmaf(gx.w, rx, fmaf(gy.w, ry, gz.w * rz));
+}
+
+__device__ __forceinline__ void load_x0(const double *__restrict__ x0, int cell, double &x, double &y, double &z) {
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(x0 + 4ll * cell));
+    x = a.x;
+    y = a.y;
+    z = __ldg(x0 + 4ll * cell + 2);
+}
+
+__global__ void __launch_bounds__(PUSH_THREADS) k_push_mixed(PushF32Args a) {
+    __shared__ long long s_tile;
+    __shared__ int s_wc[PUSH_THREADS / 32];
+    __shared__ long long s_base;
+    const long long n = (long long)a.counters[C_N];
+    const long long n_tiles = (n + PUSH_THREADS - 1) / PUSH_THREADS;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(&a.counters[C_TILE], 1ull);
+        __syncthreads();
+        const long long tile = s_tile;
+        if (tile >= n_tiles) break;
+        const long long i = tile * PUSH_THREADS + threadIdx.x;
+        int state = 0, cell = -1, hops = 0, near = 0;
+        int con[4] = {0, 0, 0, 0};
+        float lc[4] = {0, 0, 0, 0};
+        float rx = 0, ry = 0, rz = 0, vx = 0, vy = 0, vz = 0;
+        long long id = 0;
+        if (i < n) {
+            rx = a.in.rx[i]; ry = a.in.ry[i]; rz = a.in.rz[i];
+            vx = a.in.vx[i]; vy = a.in.vy[i]; vz = a.in.vz[i];
+            cell = a.in.cell[i];
+            if (a.track_ids) id = a.in.id[i];
+            const TetRec32 *t = a.tets32 + cell;
+            vx = fmaf(a.qm_dt, __ldg(&t->ef[0]), vx);
+            vy = fmaf(a.qm_dt, __ldg(&t->ef[1]), vy);
+            vz = fmaf(a.qm_dt, __ldg(&t->ef[2]), vz);
+            rx = fmaf(vx, a.dt, rx);
+            ry = fmaf(vy, a.dt, ry);
+            rz = fmaf(vz, a.dt, rz);
+            for (;;) {
+                const TetRec32 *tc = a.tets32 + cell;
+                lambdas_fp32(tc, rx, ry, rz, lc);
+                float mn = fminf(fminf(lc[0], lc[1]), fminf(lc[2], lc[3]));
+                float mx = fmaxf(fmaxf(lc[0], lc[1]), fmaxf(lc[2], lc[3]));
+                // lambda > 1 implies another lambda < 0, so min alone picks the near-face cases
+                bool inside;
+                int min_i = 0;
+                if (fabsf(mn) < (float)NEAR_FACE) {
+                    // decide in FP64 on the reconstructed absolute position
+                    near++;
+                    double ox, oy, oz;
+                    load_x0(a.x0, cell, ox, oy, oz);
+                    double x = ox + (double)rx, y = oy + (double)ry, z = oz + (double)rz;
+                    double l64[4];
+                    lambdas_fp64(a.tets + cell, x, y, z, l64);
+                    inside = true;
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        if (l64[k] < 0 || l64[k] > 1.0) inside = false;
+                        lc[k] = (float)l64[k];
+                    }
+                    double m64 = l64[0];
+#pragma unroll
+                    for (int k = 1; k < 4; k++)
+                        if (l64[k] < m64) {
+                            m64 = l64[k];
+                            min_i = k;
+                        }
+                } else {
+                    inside = mn >= 0.0f && mx <= 1.0f;
+                    float m32 = lc[0];
+#pragma unroll
+                    for (int k = 1; k < 4; k++)
+                        if (lc[k] < m32) {
+                            m32 = lc[k];
+                            min_i = k;
+                        }
+                }
+                if (inside) {
+                    state = 1;
+                    break;
+                }
+                int nb = __ldg(&tc->cell_con[min_i]);
+                if (nb < 0) {
+                    cell = -1;
+                    break;
+                }
+                if (hops >= a.walk_limit) {
+                    state = 2;
+                    atomicOr(&a.counters[C_FLAGS], FLAG_WALK_LIMIT);
+                    break;
+                }
+                // re-base the offset on the new tet's vertex 0
+                double ax, ay, az, bx, by, bz;
+                load_x0(a.x0, cell, ax, ay, az);
+                load_x0(a.x0, nb, bx, by, bz);
+                rx = (float)((ax - bx) + (double)rx);
+                ry = (float)((ay - by) + (double)ry);
+                rz = (float)((az - bz) + (double)rz);
+                cell = nb;
+                hops++;
+            }
+            if (state == 1) {
+                const int4 c4 = __ldg(reinterpret_cast<const int4 *>(a.tets32[cell].con));
+                con[0] = c4.x; con[1] = c4.y; con[2] = c4.z; con[3] = c4.w;
+            }
+        }
+        int nsum = __reduce_add_sync(0xffffffffu, near);
+        if ((threadIdx.x & 31) == 0 && nsum) atomicAdd(&a.counters[C_NEAR], (unsigned long long)nsum);
+        long long o = scatter_and_rank<float>(state, cell, con, lc, a.den, a.den_fixed, a.fixed, tile, a.status,
+                                              a.counters, hops, n_tiles, s_wc, &s_base);
+        if (o >= 0) {
+            a.out.rx[o] = rx; a.out.ry[o] = ry; a.out.rz[o] = rz;
+            a.out.vx[o] = vx; a.out.vy[o] = vy; a.out.vz[o] = vz;
+            a.out.cell[o] = cell;
+            if (a.track_ids) a.out.id[o] = id;
+        }
+        __syncthreads();
+    }
+}
+
+// den[n] *= spwt/node_volume[n] (src/mini-pic.cpp:319); fixed-point sums are
+// converted first.  Also publishes the new particle count.
+__global__ void k_normalise(int n_nodes, double *den, const unsigned long long *den_fixed, int fixed,
+                            const double *__restrict__ vol, double spwt, unsigned long long *counters) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i == 0) counters[C_N] = counters[C_N_OUT];
+    if (i < n_nodes) {
+        double v = fixed ? (double)den_fixed[i] * (1.0 / FIXED_SCALE) : den[i];
+        den[i] = __dmul_rn(v, __ddiv_rn(spwt, vol[i]));
+    }
+}
+
+static int grid_for(mp_ctx *ctx, const void *kernel, int threads, size_t smem) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    if (per_sm < 1) per_sm = 1;
+    return per_sm * ctx->sm_count;
+}
+
+int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
+    // stats words N_OUT, TILE, HOPS, MAX_HOPS, NEAR are per push
+    MP_CUDA(ctx, cudaMemsetAsync(ctx->counters + C_N_OUT, 0, 5 * sizeof(unsigned long long), ctx->stream));
+    long long n_ub = ctx->n_host;
+    long long tiles = (n_ub + PUSH_THREADS - 1) / PUSH_THREADS;
+    if (tiles < 1) tiles = 1;
+    if (tiles > ctx->tile_status_len) {
+        if (ctx->tile_status) cudaFree(ctx->tile_status);
+        ctx->tile_status = nullptr;
+        long long len = tiles * 2;
+        MP_CUDA(ctx, cudaMalloc(&ctx->tile_status, len * sizeof(unsigned long long)));
+        ctx->tile_status_len = len;
+    }
+    MP_CUDA(ctx, cudaMemsetAsync(ctx->tile_status, 0, tiles * sizeof(unsigned long long), ctx->stream));
+    if (ctx->scatter_mode == MP_SCATTER_FIXED64)
+        MP_CUDA(ctx, cudaMemsetAsync(ctx->den_fixed, 0, ctx->n_nodes * sizeof(unsigned long long), ctx->stream));
+    else
+        MP_CUDA(ctx, cudaMemsetAsync(ctx->den, 0, ctx->n_nodes * sizeof(double), ctx->stream));
+    int nxt = ctx->cur ^ 1;
+    if (ctx->form == MP_FORM_FP64) {
+        PushF64Args a;
+        a.in = ctx->p64[ctx->cur];
+        a.out = ctx->p64[nxt];
+        a.tets = ctx->tets;
+        a.den = ctx->den;
+        a.den_fixed = ctx->den_fixed;
+        a.counters = ctx->counters;
+        a.status = ctx->tile_status;
+        a.qm = q_over_m;
+        a.dt = dt;
+        a.walk_limit = ctx->walk_limit;
+        a.fixed = ctx->scatter_mode == MP_SCATTER_FIXED64;
+        a.track_ids = ctx->track_ids;
+        if (!ctx->push_grid[0]) ctx->push_grid[0] = grid_for(ctx, (const void *)k_push_fp64, PUSH_THREADS, 0);
+        int grid = ctx->push_grid[0];
+        long long g = tiles < grid ? tiles : grid;
+        k_push_fp64<<<(unsigned)g, PUSH_THREADS, 0, ctx->stream>>>(a);
+    } else {
+        PushF32Args a;
+        a.in = ctx->p32[ctx->cur];
+        a.out = ctx->p32[nxt];
+        a.tets32 = ctx->tets32;
+        a.tets = ctx->tets;
+        a.x0 = ctx->tet_x0;
+        a.den = ctx->den;
+        a.den_fixed = ctx->den_fixed;
+        a.counters = ctx->counters;
+        a.status = ctx->tile_status;
+        a.qm_dt = (float)(q_over_m * dt);
+        a.dt = (float)dt;
+        a.walk_limit = ctx->walk_limit;
+        a.fixed = ctx->scatter_mode == MP_SCATTER_FIXED64;
+        a.track_ids = ctx->track_ids;
+        if (!ctx->push_grid[1]) ctx->push_grid[1] = grid_for(ctx, (const void *)k_push_mixed, PUSH_THREADS, 0);
+        int grid = ctx->push_grid[1];
+        long long g = tiles < grid ? tiles : grid;
+        k_push_mixed<<<(unsigned)g, PUSH_THREADS, 0, ctx->stream>>>(a);
+    }
+    MP_CUDA(ctx, cudaGetLastError());
+    ctx->cur = nxt;
+    return MP_OK;
+}
+
+int launch_normalise(mp_ctx *ctx, double spwt) {
+    int th = 256;
+    int bl = (ctx->n_nodes + th - 1) / th;
+    k_normalise<<<bl, th, 0, ctx->stream>>>(ctx->n_nodes, ctx->den, ctx->den_fixed,
+                                            ctx->scatter_mode == MP_SCATTER_FIXED64, ctx->node_volume, spwt,
+                                            ctx->counters);
+    MP_CUDA(ctx, cudaGetLastError());
+    return MP_OK;
+}
+
+// ---- append / download ----------------------------------------------------------
+
+__global__ void k_append_f64(long long n, const double *__restrict__ pos, const double *__restrict__ vel,
+                             const int *__restrict__ cell, int rewind, double qm, double half_dt,
+                             const TetRec *__restrict__ tets, PartsF64 p, int track_ids,
+                             const unsigned long long *counters) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long base = (long long)counters[C_N];
+    long long o = base + i;
+    int c = cell[i];
+    double v[3] = {vel[i], vel[n + i], vel[2 * n + i]};
+    if (rewind) {
+        // part.vel[i] -= charge/mass*ef[i]*(0.5*dt), src/mini-pic.cpp:256-257
+        for (int k = 0; k < 3; k++) v[k] = __dsub_rn(v[k], __dmul_rn(__dmul_rn(qm, __ldg(&tets[c].ef[k])), half_dt));
+    }
+    p.px[o] = pos[i]; p.py[o] = pos[n + i]; p.pz[o] = pos[2 * n + i];
+    p.vx[o] = v[0]; p.vy[o] = v[1]; p.vz[o] = v[2];
+    p.cell[o] = c;
+    if (track_ids) p.id[o] = (long long)counters[C_NEXT_ID] + i;
+}
+
+__global__ void k_append_f32(long long n, const double *__restrict__ pos, const double *__restrict__ vel,
+                             const int *__restrict__ cell, int rewind, double qm, double half_dt,
+                             const TetRec *__restrict__ tets, const double *__restrict__ x0, PartsF32 p,
+                             int track_ids, const unsigned long long *counters) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long base = (long long)counters[C_N];
+    long long o = base + i;
+    int c = cell[i];
+    double v[3] = {vel[i], vel[n + i], vel[2 * n + i]};
+    if (rewind)
+        for (int k = 0; k < 3; k++) v[k] = __dsub_rn(v[k], __dmul_rn(__dmul_rn(qm, __ldg(&tets[c].ef[k])), half_dt));
+    p.rx[o] = (float)(pos[i] - x0[4ll * c + 0]);
+    p.ry[o] = (float)(pos[n + i] - x0[4ll * c + 1]);
+    p.rz[o] = (float)(pos[2 * n + i] - x0[4ll * c + 2]);
+    p.vx[o] = (float)v[0]; p.vy[o] = (float)v[1]; p.vz[o] = (float)v[2];
+    p.cell[o] = c;
+    if (track_ids) p.id[o] = (long long)counters[C_NEXT_ID] + i;
+}
+
+__global__ void k_append_commit(long long n, unsigned long long *counters) {
+    counters[C_N] += (unsigned long long)n;
+    counters[C_NEXT_ID] += (unsigned long long)n;
+}
+
+int launch_append(mp_ctx *ctx, long long n, const double *pos_soa, const double *vel_soa, const int *cell,
+                  int rewind, double q_over_m, double half_dt) {
+    if (n <= 0) return MP_OK;
+    int th = 256;
+    long long bl = (n + th - 1) / th;
+    if (ctx->form == MP_FORM_FP64)
+        k_append_f64<<<(unsigned)bl, th, 0, ctx->stream>>>(n, pos_soa, vel_soa, cell, rewind, q_over_m, half_dt,
+                                                          ctx->tets, ctx->p64[ctx->cur], ctx->track_ids,
+                                                          ctx->counters);
+    else
+        k_append_f32<<<(unsigned)bl, th, 0, ctx->stream>>>(n, pos_soa, vel_soa, cell, rewind, q_over_m, half_dt,
+                                                          ctx->tets, ctx->tet_x0, ctx->p32[ctx->cur],
+                                                          ctx->track_ids, ctx->counters);
+    k_append_commit<<<1, 1, 0, ctx->stream>>>(n, ctx->counters);
+    MP_CUDA(ctx, cudaGetLastError());
+    return MP_OK;
+}
+
+// Packs the live particles into SoA FP64: pos[3][n], vel[3][n], lc[4][n] (the
+// walk's weights in the current tet), cell[n], id[n].
+__global__ void k_pack(long long n, int form, PartsF64 p, PartsF32 q, const TetRec *__restrict__ tets,
+                       const double *__restrict__ x0, double *out, int *cell_out, long long *id_out, int track_ids) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double x, y, z, vx, vy, vz;
+    int c;
+    long long id = i;
+    if (form == MP_FORM_FP64) {
+        x = p.px[i]; y = p.py[i]; z = p.pz[i];
+        vx = p.vx[i]; vy = p.vy[i]; vz = p.vz[i];
+        c = p.cell[i];
+        if (track_ids) id = p.id[i];
+    } else {
+        c = q.cell[i];
+        x = x0[4ll * c] + (double)q.rx[i];
+        y = x0[4ll * c + 1] + (double)q.ry[i];
+        z = x0[4ll * c + 2] + (double)q.rz[i];
+        vx = q.vx[i]; vy = q.vy[i]; vz = q.vz[i];
+        if (track_ids) id = q.id[i];
+    }
+    double lc[4];
+    lambdas_fp64(tets + c, x, y, z, lc);
+    out[i] = x; out[n + i] = y; out[2 * n + i] = z;
+    out[3 * n + i] = vx; out[4 * n + i] = vy; out[5 * n + i] = vz;
+    for (int k = 0; k < 4; k++) out[(6 + k) * n + i] = lc[k];
+    cell_out[i] = c;
+    id_out[i] = id;
+}
+
+int launch_download_pack(mp_ctx *ctx, long long n, double *out_soa, int *cell_out, long long *id_out) {
+    if (n <= 0) return MP_OK;
+    int th = 256;
+    long long bl = (n + th - 1) / th;
+    k_pack<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->form, ctx->p64[ctx->cur], ctx->p32[ctx->cur], ctx->tets,
+                                                 ctx->tet_x0, out_soa, cell_out, id_out, ctx->track_ids);
+    MP_CUDA(ctx, cudaGetLastError());
+    return MP_OK;
+}
+
+// ---- tet sort (counting sort by cell) ---------------------------------------------
+
+__global__ void k_hist(long long n, const int *__restrict__ cell, int *hist) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(&hist[cell[i]], 1);
+}
+
+// exclusive scan of hist[0..m) in place, one block
+__global__ void k_scan_single(int m, int *hist) {
+    __shared__ int s_part[1024];
+    int t = threadIdx.x;
+    int chunk = (m + blockDim.x - 1) / blockDim.x;
+    int b = t * chunk, e = min(m, b + chunk);
+    int s = 0;
+    for (int k = b; k < e; k++) s += hist[k];
+    s_part[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        int run = 0;
+        for (int k = 0; k < (int)blockDim.x; k++) {
+            int c = s_part[k];
+            s_part[k] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    int run = s_part[t];
+    for (int k = b; k < e; k++) {
+        int c = hist[k];
+        hist[k] = run;
+        run += c;
+    }
+}
+
+template <typename P>
+__global__ void k_sort_scatter(long long n, P in, P out, int *cursor, int track_ids) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = in.cell[i];
+    int o = atomicAdd(&cursor[c], 1);
+    if constexpr (sizeof(*in.vx) == 8) {
+        out.px[o] = in.px[i]; out.py[o] = in.py[i]; out.pz[o] = in.pz[i];
+    } else {
+        out.rx[o] = in.rx[i]; out.ry[o] = in.ry[i]; out.rz[o] = in.rz[i];
+    }
+    out.vx[o] = in.vx[i]; out.vy[o] = in.vy[i]; out.vz[o] = in.vz[i];
+    out.cell[o] = c;
+    if (track_ids) out.id[o] = in.id[i];
+}
+
+int launch_sort_by_tet(mp_ctx *ctx) {
+    long long n = ctx->n_host;
+    if (n <= 1) return MP_OK;
+    if (!ctx->sort_hist) MP_CUDA(ctx, cudaMalloc(&ctx->sort_hist, sizeof(int) * (ctx->n_tets + 1)));
+    MP_CUDA(ctx, cudaMemsetAsync(ctx->sort_hist, 0, sizeof(int) * ctx->n_tets, ctx->stream));
+    int th = 256;
+    long long bl = (n + th - 1) / th;
+    int nxt = ctx->cur ^ 1;
+    const int *cell = ctx->form == MP_FORM_FP64 ? ctx->p64[ctx->cur].cell : ctx->p32[ctx->cur].cell;
+    k_hist<<<(unsigned)bl, th, 0, ctx->stream>>>(n, cell, ctx->sort_hist);
+    k_scan_single<<<1, 1024, 0, ctx->stream>>>(ctx->n_tets, ctx->sort_hist);
+    if (ctx->form == MP_FORM_FP64)
+        k_sort_scatter<PartsF64><<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->p64[ctx->cur], ctx->p64[nxt],
+                                                                      ctx->sort_hist, ctx->track_ids);
+    else
+        k_sort_scatter<PartsF32><<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->p32[ctx->cur], ctx->p32[nxt],
+                                                                      ctx->sort_hist, ctx->track_ids);
+    MP_CUDA(ctx, cudaGetLastError());
+    ctx->cur = nxt;
+    return MP_OK;
+}
+
+// ---- form conversion ------------------------------------------------------------
+
+__global__ void k_f64_to_f32(long long n, PartsF64 a, PartsF32 b, const double *__restrict__ x0, int track_ids) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = a.cell[i];
+    b.rx[i] = (float)(a.px[i] - x0[4ll * c]);
+    b.ry[i] = (float)(a.py[i] - x0[4ll * c + 1]);
+    b.rz[i] = (float)(a.pz[i] - x0[4ll * c + 2]);
+    b.vx[i] = (float)a.vx[i]; b.vy[i] = (float)a.vy[i]; b.vz[i] = (float)a.vz[i];
+    b.cell[i] = c;
+    if (track_ids) b.id[i] = a.id[i];
+}
+
+__global__ void k_f32_to_f64(long long n, PartsF32 b, PartsF64 a, const double *__restrict__ x0, int track_ids) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = b.cell[i];
+    a.px[i] = x0[4ll * c] + (double)b.rx[i];
+    a.py[i] = x0[4ll * c + 1] + (double)b.ry[i];
+    a.pz[i] = x0[4ll * c + 2] + (double)b.rz[i];
+    a.vx[i] = b.vx[i]; a.vy[i] = b.vy[i]; a.vz[i] = b.vz[i];
+    a.cell[i] = c;
+    if (track_ids) a.id[i] = b.id[i];
+}
+
+int launch_convert_form(mp_ctx *ctx, int to_form) {
+    long long n = ctx->n_host;
+    int nxt = ctx->cur ^ 1;
+    if (n > 0) {
+        int th = 256;
+        long long bl = (n + th - 1) / th;
+        if (to_form == MP_FORM_MIXED)
+            k_f64_to_f32<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->p64[ctx->cur], ctx->p32[nxt], ctx->tet_x0,
+                                                              ctx->track_ids);
+        else
+            k_f32_to_f64<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->p32[ctx->cur], ctx->p64[nxt], ctx->tet_x0,
+                                                              ctx->track_ids);
+        MP_CUDA(ctx, cudaGetLastError());
+    }
+    ctx->cur = nxt;
+    ctx->form = to_form;
+    return MP_OK;
+}
+
+}  // namespace mp
