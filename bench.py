@@ -1,0 +1,443 @@
+"""Benchmark of the mini-pic hot path on B200: MoveParticles (push + tet walk +
+density scatter + removal + normalisation) and FESolver's Newton step.
+
+    python bench.py [--gpus N --steps K --warmup W] [--config 1] [--impl reference]
+
+Workload (default): the 20x20x20-hex Kuhn box (48,000 tets, 9,261 nodes,
+8,379 unknowns), O+ ions, n0 = 1e10 m^-3, 7 km/s drift + 0.1 eV Maxwellian,
+dt = 5e-8 s, spwt = 5 -> about 2M live ions, seeded synthetic population at
+steady state plus the reference injector's ~7,000 new ions per step.  A step
+is InjectIons -> MoveParticles -> computePhi (Lapack method: one Newton step,
+direct solve) -> updateEf.  FP64 form; the mixed form is measured beside it
+on the same seeded population with its errors against FP64.
+
+value      particle-steps/s of MoveParticles, device-resident inputs (injected
+           particles staged in HBM), L2 flushed between steps
+e2e        the same through the C ABI with host buffers: injected particles
+           H2D from pinned host memory, density and potential D2H each step
+newton_step_ms   computePhi + updateEf device time per step
+N > 1: weak scaling, every rank pushes its own 2M-ion shard; the node density
+is summed over ranks (NCCL all-reduce) before the replicated field solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mini-fem-pic-main_b200"))
+sys.path.insert(0, ROOT)
+
+import minipic_b200 as mp  # noqa: E402
+from minipic_b200 import kuhn, sharding  # noqa: E402
+
+METRIC = "particle-steps/sec and Newton-step ms on 1 B200: mixed vs FP64 at stated error"
+CONFIGS = {
+    0: dict(n=8, n_ions=50_000, dt=1e-7, spwt=200.0, sphere=None, label="kuhn8_50k_fp64"),
+    1: dict(n=20, n_ions=2_000_000, dt=5e-8, spwt=5.0, sphere=None, label="kuhn20_2M_fp64"),
+}
+KTI_EV = 0.1
+FLUSH_BYTES = 512 << 20
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_workload(cfg, workdir, seed):
+    kd = kuhn.build(cfg["n"], sphere=cfg["sphere"])
+    kuhn.write(kd, workdir, dt=cfg["dt"], method="lapack")
+    deck = mp.Deck.load(workdir)
+    m = deck.mesh
+    rng = np.random.default_rng(seed)
+    n = cfg["n_ions"]
+    L = kd.length_mm / 1000.0
+    pos = rng.uniform(1e-6 * L, (1 - 1e-6) * L, size=(n, 3))
+    mass = 16 * mp.AMU
+    sigma = np.sqrt(KTI_EV * mp.QE / mass)
+    vel = rng.normal(0.0, sigma, size=(n, 3))
+    vel[:, 0] += deck.params.ion_velocity
+    cell = kuhn.locate(kd, pos).astype(np.int32)
+    keep = cell >= 0
+    return kd, deck, pos[keep], vel[keep], cell[keep]
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_form(form, args, cfg, deck, pop, inj_batches, device, rank, world, torch, flush, measure_e2e):
+    """Runs warm-up + timed steps for one arithmetic form; returns a dict."""
+    pos, vel, cell = pop
+    m = deck.mesh
+    ctx = mp.Context(m, device=device)
+    fe = deck.fe_desc_arrays()
+    ctx.fe_setup(**fe)
+    ctx.set_track_ids(False)
+    ctx.reserve(int(len(cell) * 1.3) + 100_000)
+    ctx.append(pos, vel, cell)
+    if form == mp.MIXED:
+        ctx.set_form(mp.MIXED)
+    qm = mp.QE / (16 * mp.AMU)
+    dt, spwt = cfg["dt"], cfg["spwt"] / world
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
+    # device-staged injections
+    staged = []
+    for (p, v, c) in inj_batches:
+        staged.append((torch.from_numpy(np.ascontiguousarray(p.T)).to(device),
+                       torch.from_numpy(np.ascontiguousarray(v.T)).to(device),
+                       torch.from_numpy(c).to(device), len(c)))
+    torch.cuda.synchronize(device)
+
+    def step(k, host):
+        p, v, c, n = staged[k % len(staged)]
+        if host:
+            hp, hv, hc = inj_batches[k % len(inj_batches)]
+            ctx.append(hp, hv, hc, rewind=True, q_over_m=qm, half_dt=0.5 * dt)
+            st = ctx.push(qm, dt, spwt, den_out=den_host)
+        else:
+            ctx.append_device(p.data_ptr(), v.data_ptr(), c.data_ptr(), n, rewind=True, q_over_m=qm,
+                              half_dt=0.5 * dt)
+            st = ctx.push(qm, dt, spwt)
+        if world > 1:
+            sharding.allreduce_density(ctx, device)
+        nt = ctx.compute_phi(mp.LAPACK, form)
+        ctx.update_ef()
+        if host:
+            ctx._c(mp.lib().mp_field_download(ctx.h, None, mp._p(uh_host), None))
+        return st, nt
+
+    den_host = np.zeros(m.n_nodes)
+    uh_host = np.zeros(m.n_nodes)
+    for k in range(args.warmup):
+        step(k, False)
+    torch.cuda.synchronize(device)
+    res = {"push_ms": [], "push_call_ms": [], "newton_ms": [], "factor_ms": [], "step_ms": [], "n_before": [],
+           "n_after": [], "hops": [], "near": []}
+    launches0 = ctx.launches()
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st, nt = step(args.warmup + k, False)
+        e1.record(stream)
+        e1.synchronize()
+        res["push_ms"].append(st.ms_kernel)
+        res["push_call_ms"].append(st.ms_step)
+        res["newton_ms"].append(nt.ms_total)
+        res["factor_ms"].append(nt.ms_factor)
+        res["step_ms"].append(e0.elapsed_time(e1))
+        res["n_before"].append(st.n_before)
+        res["n_after"].append(st.n_after)
+        res["hops"].append(st.total_hops)
+        res["near"].append(st.near_face_fp64)
+    res["launches"] = ctx.launches() - launches0
+    if measure_e2e:
+        e2e_ms, h2d, d2h = [], [], []
+        for k in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize(device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st, nt = step(args.warmup + args.steps + k, True)
+            e1.record(stream)
+            e1.synchronize()
+            e2e_ms.append(e0.elapsed_time(e1))
+            hp, hv, hc = inj_batches[(args.warmup + args.steps + k) % len(inj_batches)]
+            h2d.append(hp.nbytes + hv.nbytes + hc.nbytes)
+            d2h.append(den_host.nbytes + uh_host.nbytes)
+            res.setdefault("e2e_push_n", []).append(st.n_before)
+        res["e2e_ms"] = e2e_ms
+        res["h2d"] = float(np.mean(h2d))
+        res["d2h"] = float(np.mean(d2h))
+    res["ctx"] = ctx
+    return res
+
+
+def error_metrics(deck, pop, inj_batches, cfg, device, steps=5):
+    """Mixed vs FP64 on the same seeded run: density L2, differing cells, phi."""
+    pos, vel, cell = pop
+    out = []
+    qm = mp.QE / (16 * mp.AMU)
+    dt, spwt = cfg["dt"], cfg["spwt"]
+    ctxs = []
+    for form in (mp.FP64, mp.MIXED):
+        c = mp.Context(deck.mesh, device=device)
+        c.fe_setup(**deck.fe_desc_arrays())
+        c.append(pos, vel, cell)
+        if form == mp.MIXED:
+            c.set_form(mp.MIXED)
+        ctxs.append(c)
+    for k in range(steps):
+        p, v, cc = inj_batches[k % len(inj_batches)]
+        dens, uhs = [], []
+        for form, c in zip((mp.FP64, mp.MIXED), ctxs):
+            c.append(p, v, cc, rewind=True, q_over_m=qm, half_dt=0.5 * dt)
+            den = np.zeros(deck.mesh.n_nodes)
+            c.push(qm, dt, spwt, den_out=den)
+            c.compute_phi(mp.LAPACK, form)
+            c.update_ef()
+            _, uh, _ = c.field()
+            dens.append(den)
+            uhs.append(uh)
+        out.append((np.linalg.norm(dens[1] - dens[0]) / np.linalg.norm(dens[0]), np.abs(uhs[1] - uhs[0]).max()))
+    ga, gb = ctxs[0].download(mp.ORDER_ID), ctxs[1].download(mp.ORDER_ID)
+    ids = np.union1d(ga["id"], gb["id"])
+    ia = np.full(ids.size, -1)
+    ib = np.full(ids.size, -1)
+    ia[np.searchsorted(ids, ga["id"])] = ga["cell"]
+    ib[np.searchsorted(ids, gb["id"])] = gb["cell"]
+    for c in ctxs:
+        c.close()
+    return {"density_l2_rel": float(max(e[0] for e in out)), "phi_max_abs_V": float(max(e[1] for e in out)),
+            "cells_differing_frac": float(np.mean(ia != ib)), "steps": steps}
+
+
+def cpu_baseline(cfg, workdir, pop, budget_s=20.0):
+    """The reference's own MoveParticles (oracle/_ref, OpenMP over all host
+    threads) on the same population; one Lapack Newton step if it fits."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    threads = os.cpu_count() or 1
+    s = ref.RefSim(workdir, spwt=cfg["spwt"])
+    pos, vel, cell = pop
+    parts = np.zeros(len(cell), dtype=ref.PARTICLE_DTYPE)
+    parts["pos"], parts["vel"], parts["cell_index"] = pos, vel, cell
+    s.set_particles(parts)
+    rate1, sec1 = s.time_move(1, threads)
+    steps = int(max(1, min(50, budget_s / max(sec1, 1e-3))))
+    s.set_particles(parts)
+    rate, sec = s.time_move(steps, threads)
+    t0 = time.perf_counter()
+    s.compute_phi(ref.LAPACK)
+    s.update_ef()
+    newton_ms = (time.perf_counter() - t0) * 1e3
+    s.close()
+    return {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+            "sample": f"{steps} MoveParticles steps on the full {len(cell)}-ion population "
+                      f"({sec:.1f} s) + 1 Lapack Newton step",
+            "newton_step_ms": newton_ms}
+
+
+def reference_arm(args):
+    """--impl reference: the reference's own CPU path (oracle/_ref) timed on the
+    host cores, same config/metric; rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = CONFIGS[args.config]
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_oracle.so was not built"}))
+        return
+    with tempfile.TemporaryDirectory() as wd:
+        kd, deck, pos, vel, cell = make_workload(cfg, wd, seed=1234)
+        threads = os.cpu_count() or 1
+        s = ref.RefSim(wd, spwt=cfg["spwt"])
+        parts = np.zeros(len(cell), dtype=ref.PARTICLE_DTYPE)
+        parts["pos"], parts["vel"], parts["cell_index"] = pos, vel, cell
+        s.set_particles(parts)
+        for _ in range(max(1, args.warmup)):
+            s.move(threads)
+        rate, sec = s.time_move(args.steps, threads)
+        t0 = time.perf_counter()
+        s.compute_phi(ref.LAPACK)
+        s.update_ef()
+        newton_ms = (time.perf_counter() - t0) * 1e3
+        line = {"metric": METRIC, "value": rate, "unit": "particle-steps/s", "impl": "reference",
+                "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": cfg["label"], "mesh_hexes": cfg["n"] ** 3,
+                                                "tets": deck.mesh.n_tets, "ions": int(len(cell)), "dt": cfg["dt"]},
+                "newton_step_ms": newton_ms,
+                "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                                 "sample": f"{args.steps} MoveParticles steps, OpenMP over {threads} threads"},
+                "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        s.close()
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", type=int, default=1, choices=sorted(CONFIGS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    cfg = CONFIGS[args.config]
+    hbm_peak, peak_kind = peaks()
+    with tempfile.TemporaryDirectory() as wd:
+        kd, deck, pos, vel, cell = make_workload(cfg, wd, seed=1234 + rank)
+        pop = (pos, vel, cell)
+        inj = mp.Injector(deck.mesh, seed=rank)
+        P = deck.params
+        n_batches = args.warmup + 2 * args.steps
+        batches = []
+        for _ in range(n_batches):
+            p, v, c = inj.sample(P.plasma_den, P.ion_velocity, cfg["dt"], cfg["spwt"])
+            batches.append((np.ascontiguousarray(p), np.ascontiguousarray(v), np.ascontiguousarray(c)))
+        flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=local)
+        clocks = Clocks(local)
+        if world > 1:
+            torch.distributed.barrier()
+        clocks.start()
+        r64 = run_form(mp.FP64, args, cfg, deck, pop, batches, local, rank, world, torch, flush, True)
+        clk = clocks.stop()
+        r32 = None
+        if not args.no_mixed:
+            r32 = run_form(mp.MIXED, args, cfg, deck, pop, batches, local, rank, world, torch, flush, False)
+        errors = None
+        if not args.no_mixed and rank == 0 and world == 1:
+            errors = error_metrics(deck, pop, batches, cfg, local)
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu:
+            cpu = cpu_baseline(cfg, wd, pop)
+
+    def agg(r):
+        push_ms = np.array(r["push_ms"])
+        nb, na = np.array(r["n_before"], float), np.array(r["n_after"], float)
+        step_ms = np.array(r["step_ms"])
+        return push_ms, nb, na, step_ms
+
+    push_ms, nb, na, step_ms = agg(r64)
+    psteps = nb.sum()
+    push_call_s = np.sum(r64["push_call_ms"]) / 1e3
+    stats = np.array([psteps, push_call_s, step_ms.sum() / 1e3, np.sum(r64["e2e_ms"]) / 1e3,
+                      np.mean(r64["newton_ms"])], dtype=np.float64)
+    if world > 1:
+        t = torch.tensor(stats, device=local)
+        tmax = t.clone()
+        torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
+        tsum = t.clone()
+        torch.distributed.all_reduce(tsum, op=torch.distributed.ReduceOp.SUM)
+        psteps_all = float(tsum[0])
+        push_s, step_s, e2e_s, newton_ms = float(tmax[1]), float(tmax[2]), float(tmax[3]), float(tmax[4])
+    else:
+        psteps_all = psteps
+        push_s, step_s, e2e_s, newton_ms = stats[1], stats[2], stats[3], stats[4]
+    if rank == 0:
+        bytes_per = 52.0  # pos 24 + vel 24 + tet 4, read and written once (FP64 SoA)
+        alg_bytes = (nb + na) * bytes_per
+        achieved = float(np.mean(alg_bytes / (push_ms * 1e-3)) / 1e9)
+        line = {
+            "metric": METRIC, "value": psteps_all / push_s, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(step_s / args.steps * 1e3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Kuhn-box ions at steady state + reference injector)",
+            "config": {"workload": cfg["label"], "mesh_hexes": cfg["n"] ** 3, "tets": deck.mesh.n_tets,
+                       "nodes": deck.mesh.n_nodes, "unknowns": int(deck.fe_desc_arrays()["neq"]),
+                       "ions_per_gpu": int(np.mean(nb)), "dt": cfg["dt"], "method": "lapack (1 Newton step)",
+                       "form": "fp64", "l2": f"flushed ({FLUSH_BYTES >> 20} MiB write) between timed steps",
+                       "parallelism": f"particles sharded x{world}, density all-reduce" if world > 1 else "1 GPU"},
+            "newton_step_ms": float(newton_ms),
+            "full_step_particle_steps_per_s": psteps_all / step_s,
+            "push_kernel_ms": float(np.mean(push_ms)),
+            "hops_per_particle_step": float(np.sum(r64["hops"]) / psteps),
+            "e2e": {"value": psteps_all / e2e_s, "unit": "particle-steps/s (full step incl. Newton, host I/O)",
+                    "h2d_bytes_per_step": int(r64["h2d"]), "d2h_bytes_per_step": int(r64["d2h"]),
+                    "ms_per_step": float(e2e_s / args.steps * 1e3)},
+            "gpu_launches": int(r64["launches"]),
+            "roofline": {"kernel": "k_push_fp64", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                         "peak_kind": peak_kind,
+                         "bytes_per_particle_step": 104},
+            "clocks": clk,
+        }
+        if r32 is not None:
+            pm, nb32, na32, sm32 = agg(r32)
+            ach32 = float(np.mean((nb32 + na32) * 28.0 / (pm * 1e-3)) / 1e9)
+            line["mixed"] = {
+                "value": float(nb32.sum() / (np.sum(r32["push_call_ms"]) / 1e3)),
+                "full_step_particle_steps_per_s": float(nb32.sum() / (sm32.sum() / 1e3)),
+                "newton_step_ms": float(np.mean(r32["newton_ms"])),
+                "push_kernel_ms": float(np.mean(pm)),
+                "roofline": {"kernel": "k_push_mixed", "bound": "hbm", "achieved": ach32, "peak": hbm_peak,
+                             "unit": "GB/s", "frac": ach32 / hbm_peak, "bytes_per_particle_step": 56},
+                "near_face_fp64_per_step": float(np.mean(r32["near"])),
+                "errors_vs_fp64": errors,
+            }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

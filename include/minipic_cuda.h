@@ -116,6 +116,8 @@ typedef struct mp_step_stats {
     int64_t total_hops;       /* tet-to-tet moves of all particles this step */
     int32_t max_hops;         /* longest walk this step */
     int32_t near_face_fp64;   /* mixed form: FP64 re-tests taken */
+    double ms_kernel;         /* device time of the push kernel alone (CUDA events) */
+    double ms_step;           /* device time of the whole push call's kernels */
 } mp_step_stats;
 
 typedef struct mp_newton_stats {
@@ -142,6 +144,17 @@ int mp_set_walk_limit(mp_ctx *ctx, int32_t max_hops);
 int mp_set_scatter_mode(mp_ctx *ctx, int mode);
 int mp_set_sort_period(mp_ctx *ctx, int32_t steps);
 int mp_set_particle_form(mp_ctx *ctx, int form);
+/* Particle IDs (16 B per particle-step of traffic) are needed only to restore
+ * injection order after tet re-sorting; without sorting the stable removal
+ * keeps the reference's order by itself.  Default on. */
+int mp_set_track_ids(mp_ctx *ctx, int on);
+/* Device address and length (elements) of a context buffer named by MP_VEC_*
+ * (FP64 vectors), for zero-copy interop on the context's stream: e.g. an
+ * all-reduce of the node density across ranks between mp_push_scatter and
+ * mp_compute_phi.  No counterpart in the reference (single process). */
+int mp_device_buffer(mp_ctx *ctx, int which, void **ptr, int64_t *len);
+/* Kernels this context has launched since creation (for launch accounting). */
+int mp_kernel_launches(mp_ctx *ctx, int64_t *n);
 
 /* ---- particles ---------------------------------------------------------------- */
 int mp_particles_reserve(mp_ctx *ctx, int64_t capacity);

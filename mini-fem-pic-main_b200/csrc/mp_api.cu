@@ -264,6 +264,8 @@ int mp_create(int device, const mp_mesh_desc *m, mp_ctx **out) {
     upload_quadrature(st);
     cudaEventCreate(&ctx->t0.a); cudaEventCreate(&ctx->t0.b);
     cudaEventCreate(&ctx->t1.a); cudaEventCreate(&ctx->t1.b);
+    cudaEventCreate(&ctx->tp.a); cudaEventCreate(&ctx->tp.b);
+    cudaEventCreate(&ctx->ts.a); cudaEventCreate(&ctx->ts.b);
     if (cudaStreamSynchronize(st) != cudaSuccess) return bail(MP_ERR_CUDA);
     std::memset(ctx->counters_host, 0, sizeof(unsigned long long) * C_COUNT);
     int rc = grow_particles(ctx, 1024);
@@ -285,7 +287,7 @@ int mp_destroy(mp_ctx *ctx) {
     if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
     if (ctx->scal_host) cudaFreeHost(ctx->scal_host);
     if (ctx->stage) cudaFreeHost(ctx->stage);
-    cudaEvent_t ev[] = {ctx->t0.a, ctx->t0.b, ctx->t1.a, ctx->t1.b};
+    cudaEvent_t ev[] = {ctx->t0.a, ctx->t0.b, ctx->t1.a, ctx->t1.b, ctx->tp.a, ctx->tp.b, ctx->ts.a, ctx->ts.b};
     for (auto e : ev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -319,6 +321,7 @@ int mp_set_scatter_mode(mp_ctx *ctx, int mode) {
 
 int mp_set_sort_period(mp_ctx *ctx, int32_t steps) {
     if (!ctx || steps < 0) return MP_ERR_ARG;
+    if (steps > 0 && !ctx->track_ids) return fail(ctx, MP_ERR_STATE, "tet re-sorting needs particle IDs");
     ctx->sort_period = steps;
     return MP_OK;
 }
@@ -331,6 +334,19 @@ int mp_set_particle_form(mp_ctx *ctx, int form) {
     int rc = launch_convert_form(ctx, form);
     if (rc) return rc;
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return MP_OK;
+}
+
+int mp_set_track_ids(mp_ctx *ctx, int on) {
+    if (!ctx) return MP_ERR_ARG;
+    if (!on && ctx->sort_period > 0) return fail(ctx, MP_ERR_STATE, "tet re-sorting needs particle IDs");
+    ctx->track_ids = on != 0;
+    return MP_OK;
+}
+
+int mp_kernel_launches(mp_ctx *ctx, int64_t *n) {
+    if (!ctx || !n) return MP_ERR_ARG;
+    *n = ctx->launches;
     return MP_OK;
 }
 
@@ -419,7 +435,7 @@ int mp_particles_download(mp_ctx *ctx, int64_t n_max, double *pos, int64_t pos_s
     const int *hc = (const int *)(h + 10 * n);
     const long long *hi = (const long long *)(hc + n + (n & 1));
     std::vector<long long> perm;
-    if (order == MP_ORDER_ID) {
+    if (order == MP_ORDER_ID && ctx->track_ids) {
         perm.resize(n);
         std::iota(perm.begin(), perm.end(), 0);
         std::sort(perm.begin(), perm.end(), [&](long long a, long long b) { return hi[a] < hi[b]; });
@@ -447,6 +463,7 @@ int mp_particles_download(mp_ctx *ctx, int64_t n_max, double *pos, int64_t pos_s
 int mp_push_scatter(mp_ctx *ctx, double q_over_m, double dt, double spwt, double *den_out, mp_step_stats *stats) {
     if (!ctx) return MP_ERR_ARG;
     long long n_before = ctx->n_host;
+    cudaEventRecord(ctx->ts.a, ctx->stream);
     if (ctx->sort_period > 0 && ++ctx->steps_since_sort >= ctx->sort_period) {
         int rc = launch_sort_by_tet(ctx);
         if (rc) return rc;
@@ -456,6 +473,7 @@ int mp_push_scatter(mp_ctx *ctx, double q_over_m, double dt, double spwt, double
     if (rc) return rc;
     rc = launch_normalise(ctx, spwt);
     if (rc) return rc;
+    cudaEventRecord(ctx->ts.b, ctx->stream);
     if (den_out)
         MP_CUDA(ctx, cudaMemcpyAsync(den_out, ctx->den, sizeof(double) * ctx->n_nodes, cudaMemcpyDeviceToHost,
                                      ctx->stream));
@@ -466,6 +484,11 @@ int mp_push_scatter(mp_ctx *ctx, double q_over_m, double dt, double spwt, double
         stats->total_hops = (int64_t)ctx->counters_host[C_HOPS];
         stats->max_hops = (int32_t)ctx->counters_host[C_MAX_HOPS];
         stats->near_face_fp64 = (int32_t)ctx->counters_host[C_NEAR];
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->tp.a, ctx->tp.b);
+        cudaEventElapsedTime(&b, ctx->ts.a, ctx->ts.b);
+        stats->ms_kernel = a;
+        stats->ms_step = b;
     }
     return rc;
 }
@@ -588,6 +611,16 @@ static double *vec_ptr(mp_ctx *ctx, int which, size_t *len) {
     }
     *len = 0;
     return nullptr;
+}
+
+int mp_device_buffer(mp_ctx *ctx, int which, void **ptr, int64_t *len) {
+    if (!ctx || !ptr || !len) return MP_ERR_ARG;
+    size_t n = 0;
+    double *p = vec_ptr(ctx, which, &n);
+    if (!p) return fail(ctx, MP_ERR_ARG, "no such device buffer");
+    *ptr = p;
+    *len = (int64_t)n;
+    return MP_OK;
 }
 
 int mp_fe_download(mp_ctx *ctx, int which, double *out) {

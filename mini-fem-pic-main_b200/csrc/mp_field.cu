@@ -81,11 +81,11 @@ int fe_build_f1(mp_ctx *ctx, const double *den_dev) {
     int th = 256;
     k_node_terms<<<(ctx->n_nodes + th - 1) / th, th, 0, ctx->stream>>>(
         ctx->n_nodes, ctx->ID, den_dev, ctx->d, qe_eps0, 0.0, ctx->n0, ctx->phi0, ctx->kTe, 1.0 / ctx->kTe,
-        ctx->fvec, nullptr);
+        ctx->fvec, nullptr), ++ctx->launches;
     // F1 is accumulated, never cleared, exactly as buildF1Vector does (it only
     // adds to F1; startAssembly is the one place that zeroes it).
     k_eq_gather<<<(ctx->neq + th - 1) / th, th, 0, ctx->stream>>>(ctx->neq, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a,
-                                                                 ctx->detJ, ctx->fvec, ctx->F1, 1);
+                                                                 ctx->detJ, ctx->fvec, ctx->F1, 1), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }
@@ -116,7 +116,7 @@ int fe_residual(mp_ctx *ctx) {
     long long ld = (ctx->neq + 31) & ~31ll;
     int th = 256;
     long long bl = ((long long)ctx->neq * 32 + th - 1) / th;
-    k_residual<<<(unsigned)bl, th, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->d, ctx->F0, ctx->F1, ctx->G);
+    k_residual<<<(unsigned)bl, th, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->d, ctx->F0, ctx->F1, ctx->G), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }
@@ -140,11 +140,11 @@ int fe_build_j(mp_ctx *ctx, int method) {
     int th = 256;
     k_node_terms<<<(ctx->n_nodes + th - 1) / th, th, 0, ctx->stream>>>(
         ctx->n_nodes, ctx->ID, nullptr, ctx->d, 0.0, -QE / EPS0, ctx->n0, ctx->phi0, ctx->kTe, 1 / ctx->kTe,
-        nullptr, ctx->work);
+        nullptr, ctx->work), ++ctx->launches;
     k_eq_gather<<<(ctx->neq + th - 1) / th, th, 0, ctx->stream>>>(ctx->neq, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a,
-                                                                 ctx->detJ, ctx->work, ctx->FP, 0);
+                                                                 ctx->detJ, ctx->work, ctx->FP, 0), ++ctx->launches;
     long long ld = (ctx->neq + 31) & ~31ll;
-    k_copy_j<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J);
+    k_copy_j<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }
@@ -170,7 +170,7 @@ __global__ void k_update_d(int neq, double *d, const double *__restrict__ y, dou
 
 int fe_update_d(mp_ctx *ctx, double *l2_out) {
     MP_CUDA(ctx, cudaMemsetAsync(ctx->scal, 0, sizeof(double), ctx->stream));
-    k_update_d<<<64, 256, 0, ctx->stream>>>(ctx->neq, ctx->d, ctx->y, ctx->scal);
+    k_update_d<<<64, 256, 0, ctx->stream>>>(ctx->neq, ctx->d, ctx->y, ctx->scal), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     if (l2_out) {
         MP_CUDA(ctx, cudaMemcpyAsync(ctx->scal_host, ctx->scal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -193,7 +193,7 @@ __global__ void k_uh(int n_nodes, const int *__restrict__ ID, const double *__re
 
 int fe_uh(mp_ctx *ctx) {
     int th = 256;
-    k_uh<<<(ctx->n_nodes + th - 1) / th, th, 0, ctx->stream>>>(ctx->n_nodes, ctx->ID, ctx->g, ctx->d, ctx->uh);
+    k_uh<<<(ctx->n_nodes + th - 1) / th, th, 0, ctx->stream>>>(ctx->n_nodes, ctx->ID, ctx->g, ctx->d, ctx->uh), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }
@@ -201,7 +201,7 @@ int fe_uh(mp_ctx *ctx) {
 int launch_update_ef(mp_ctx *ctx) {
     int th = 256;
     k_update_ef<<<(ctx->n_tets + th - 1) / th, th, 0, ctx->stream>>>(ctx->n_tets, ctx->con, ctx->nx, ctx->uh,
-                                                                     ctx->ef, ctx->tets, ctx->tets32);
+                                                                     ctx->ef, ctx->tets, ctx->tets32), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }
@@ -244,7 +244,7 @@ int fe_assemble(mp_ctx *ctx) {
     int th = 128;
     k_assemble<<<(ctx->neq + th - 1) / th, th, 0, ctx->stream>>>(ctx->neq, ld, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a,
                                                                  ctx->LM, ctx->con, ctx->nx, ctx->detJ, ctx->g,
-                                                                 ctx->K, ctx->F0);
+                                                                 ctx->K, ctx->F0), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }

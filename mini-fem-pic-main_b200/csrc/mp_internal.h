@@ -155,7 +155,8 @@ struct mp_ctx {
     unsigned char *eq_a = nullptr;
     double *gs_minv = nullptr;            // Gauss-Seidel: (D+L)^-1, [neq][neq]
 
-    mp::Timer t0, t1;
+    mp::Timer t0, t1, tp, ts;
+    long long launches = 0;
 };
 
 namespace mp {

@@ -253,13 +253,13 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         for (int k0 = 0; k0 < n; k0 += NB) {
             int kb = n - k0 < NB ? n - k0 : NB;
             int k1 = k0 + kb;
-            k_ldlt_diag<T><<<1, 256, 0, st>>>(n, ld, A, k0, kb, w.dvec, b, ctx->counters + C_FLAGS);
+            k_ldlt_diag<T><<<1, 256, 0, st>>>(n, ld, A, k0, kb, w.dvec, b, ctx->counters + C_FLAGS), ++ctx->launches;
             if (k1 < n) {
                 int rows = n - k1;
-                k_ldlt_panel<T><<<(rows + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, w.W, b);
+                k_ldlt_panel<T><<<(rows + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, w.W, b), ++ctx->launches;
                 long long tiles = (rows + 63) / 64;
                 long long nblk = tiles * (tiles + 1) / 2;
-                k_ldlt_update<T><<<(unsigned)nblk, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W, k1);
+                k_ldlt_update<T><<<(unsigned)nblk, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W, k1), ++ctx->launches;
             }
         }
     } else {
@@ -268,11 +268,11 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             int kb = n - k0 < NB ? n - k0 : NB;
             int k1 = k0 + kb;
             // z_k = L_kk^-1 b_k, then b_i -= L_ik z_k
-            k_fwd_diag<T><<<1, 64, 0, st>>>(ld, A, k0, kb, b);
-            if (k1 < n) k_fwd_rows<T><<<(n - k1 + 255) / 256, 256, 0, st>>>(n, ld, A, k0, kb, k1, b);
+            k_fwd_diag<T><<<1, 64, 0, st>>>(ld, A, k0, kb, b), ++ctx->launches;
+            if (k1 < n) k_fwd_rows<T><<<(n - k1 + 255) / 256, 256, 0, st>>>(n, ld, A, k0, kb, k1, b), ++ctx->launches;
         }
     }
-    k_diag_scale<T><<<(n + 255) / 256, 256, 0, st>>>(n, w.dvec, b);
+    k_diag_scale<T><<<(n + 255) / 256, 256, 0, st>>>(n, w.dvec, b), ++ctx->launches;
     MP_CUDA(ctx, cudaMemsetAsync(w.s, 0, sizeof(T) * NB, st));
     int last = ((n - 1) / NB) * NB;
     for (int k0 = last; k0 >= 0; k0 -= NB) {
@@ -282,9 +282,9 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             int rows = n - k1;
             int grid = (rows + 3) / 4;
             if (grid > ctx->sm_count * 4) grid = ctx->sm_count * 4;
-            k_bwd_partial<T><<<grid, 256, 0, st>>>(n, ld, A, k0, kb, k1, b, w.s);
+            k_bwd_partial<T><<<grid, 256, 0, st>>>(n, ld, A, k0, kb, k1, b, w.s), ++ctx->launches;
         }
-        k_bwd_diag<T><<<1, 64, 0, st>>>(ld, A, k0, kb, b, w.s);
+        k_bwd_diag<T><<<1, 64, 0, st>>>(ld, A, k0, kb, b, w.s), ++ctx->launches;
     }
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;

@@ -496,7 +496,9 @@ int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
         if (!ctx->push_grid[0]) ctx->push_grid[0] = grid_for(ctx, (const void *)k_push_fp64, PUSH_THREADS, 0);
         int grid = ctx->push_grid[0];
         long long g = tiles < grid ? tiles : grid;
-        k_push_fp64<<<(unsigned)g, PUSH_THREADS, 0, ctx->stream>>>(a);
+        cudaEventRecord(ctx->tp.a, ctx->stream);
+        k_push_fp64<<<(unsigned)g, PUSH_THREADS, 0, ctx->stream>>>(a), ++ctx->launches;
+        cudaEventRecord(ctx->tp.b, ctx->stream);
     } else {
         PushF32Args a;
         a.in = ctx->p32[ctx->cur];
@@ -516,7 +518,9 @@ int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
         if (!ctx->push_grid[1]) ctx->push_grid[1] = grid_for(ctx, (const void *)k_push_mixed, PUSH_THREADS, 0);
         int grid = ctx->push_grid[1];
         long long g = tiles < grid ? tiles : grid;
-        k_push_mixed<<<(unsigned)g, PUSH_THREADS, 0, ctx->stream>>>(a);
+        cudaEventRecord(ctx->tp.a, ctx->stream);
+        k_push_mixed<<<(unsigned)g, PUSH_THREADS, 0, ctx->stream>>>(a), ++ctx->launches;
+        cudaEventRecord(ctx->tp.b, ctx->stream);
     }
     MP_CUDA(ctx, cudaGetLastError());
     ctx->cur = nxt;
@@ -528,7 +532,7 @@ int launch_normalise(mp_ctx *ctx, double spwt) {
     int bl = (ctx->n_nodes + th - 1) / th;
     k_normalise<<<bl, th, 0, ctx->stream>>>(ctx->n_nodes, ctx->den, ctx->den_fixed,
                                             ctx->scatter_mode == MP_SCATTER_FIXED64, ctx->node_volume, spwt,
-                                            ctx->counters);
+                                            ctx->counters), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }
@@ -588,12 +592,12 @@ int launch_append(mp_ctx *ctx, long long n, const double *pos_soa, const double 
     if (ctx->form == MP_FORM_FP64)
         k_append_f64<<<(unsigned)bl, th, 0, ctx->stream>>>(n, pos_soa, vel_soa, cell, rewind, q_over_m, half_dt,
                                                           ctx->tets, ctx->p64[ctx->cur], ctx->track_ids,
-                                                          ctx->counters);
+                                                          ctx->counters), ++ctx->launches;
     else
         k_append_f32<<<(unsigned)bl, th, 0, ctx->stream>>>(n, pos_soa, vel_soa, cell, rewind, q_over_m, half_dt,
                                                           ctx->tets, ctx->tet_x0, ctx->p32[ctx->cur],
-                                                          ctx->track_ids, ctx->counters);
-    k_append_commit<<<1, 1, 0, ctx->stream>>>(n, ctx->counters);
+                                                          ctx->track_ids, ctx->counters), ++ctx->launches;
+    k_append_commit<<<1, 1, 0, ctx->stream>>>(n, ctx->counters), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }
@@ -634,7 +638,7 @@ int launch_download_pack(mp_ctx *ctx, long long n, double *out_soa, int *cell_ou
     int th = 256;
     long long bl = (n + th - 1) / th;
     k_pack<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->form, ctx->p64[ctx->cur], ctx->p32[ctx->cur], ctx->tets,
-                                                 ctx->tet_x0, out_soa, cell_out, id_out, ctx->track_ids);
+                                                 ctx->tet_x0, out_soa, cell_out, id_out, ctx->track_ids), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }
@@ -692,20 +696,21 @@ __global__ void k_sort_scatter(long long n, P in, P out, int *cursor, int track_
 int launch_sort_by_tet(mp_ctx *ctx) {
     long long n = ctx->n_host;
     if (n <= 1) return MP_OK;
+    if (!ctx->track_ids) return fail(ctx, MP_ERR_STATE, "tet re-sorting needs particle IDs (mp_set_track_ids)");
     if (!ctx->sort_hist) MP_CUDA(ctx, cudaMalloc(&ctx->sort_hist, sizeof(int) * (ctx->n_tets + 1)));
     MP_CUDA(ctx, cudaMemsetAsync(ctx->sort_hist, 0, sizeof(int) * ctx->n_tets, ctx->stream));
     int th = 256;
     long long bl = (n + th - 1) / th;
     int nxt = ctx->cur ^ 1;
     const int *cell = ctx->form == MP_FORM_FP64 ? ctx->p64[ctx->cur].cell : ctx->p32[ctx->cur].cell;
-    k_hist<<<(unsigned)bl, th, 0, ctx->stream>>>(n, cell, ctx->sort_hist);
-    k_scan_single<<<1, 1024, 0, ctx->stream>>>(ctx->n_tets, ctx->sort_hist);
+    k_hist<<<(unsigned)bl, th, 0, ctx->stream>>>(n, cell, ctx->sort_hist), ++ctx->launches;
+    k_scan_single<<<1, 1024, 0, ctx->stream>>>(ctx->n_tets, ctx->sort_hist), ++ctx->launches;
     if (ctx->form == MP_FORM_FP64)
         k_sort_scatter<PartsF64><<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->p64[ctx->cur], ctx->p64[nxt],
-                                                                      ctx->sort_hist, ctx->track_ids);
+                                                                      ctx->sort_hist, ctx->track_ids), ++ctx->launches;
     else
         k_sort_scatter<PartsF32><<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->p32[ctx->cur], ctx->p32[nxt],
-                                                                      ctx->sort_hist, ctx->track_ids);
+                                                                      ctx->sort_hist, ctx->track_ids), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     ctx->cur = nxt;
     return MP_OK;
@@ -745,10 +750,10 @@ int launch_convert_form(mp_ctx *ctx, int to_form) {
         long long bl = (n + th - 1) / th;
         if (to_form == MP_FORM_MIXED)
             k_f64_to_f32<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->p64[ctx->cur], ctx->p32[nxt], ctx->tet_x0,
-                                                              ctx->track_ids);
+                                                              ctx->track_ids), ++ctx->launches;
         else
             k_f32_to_f64<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->p32[ctx->cur], ctx->p64[nxt], ctx->tet_x0,
-                                                              ctx->track_ids);
+                                                              ctx->track_ids), ++ctx->launches;
         MP_CUDA(ctx, cudaGetLastError());
     }
     ctx->cur = nxt;

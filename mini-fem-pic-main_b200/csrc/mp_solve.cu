@@ -57,7 +57,7 @@ static int resid_norms(mp_ctx *ctx, const double *y, const double *b, double *r,
     MP_CUDA(ctx, cudaMemsetAsync(ctx->scal + 1, 0, 2 * sizeof(double), ctx->stream));
     int th = 256;
     long long bl = ((long long)ctx->neq * 32 + th - 1) / th;
-    k_resid_j<<<(unsigned)bl, th, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, y, b, r, r32, ctx->scal + 1);
+    k_resid_j<<<(unsigned)bl, th, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, y, b, r, r32, ctx->scal + 1), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     MP_CUDA(ctx, cudaMemcpyAsync(ctx->scal_host + 1, ctx->scal + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost,
                                  ctx->stream));
@@ -128,7 +128,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         }
     } else {
         if (!ctx->J32) MP_CUDA(ctx, cudaMalloc(&ctx->J32, sizeof(float) * (size_t)ld * n));
-        k_j_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(n, ld, ctx->J, ctx->J32);
+        k_j_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(n, ld, ctx->J, ctx->J32), ++ctx->launches;
         MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * n, ctx->stream));
         LdltWork<float> w{g_scr.dvec32, g_scr.W32, g_scr.s32};
         double rn = 0, bn = 0;
@@ -138,7 +138,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, g_scr.b32, w, true);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
-        k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, g_scr.b32, ctx->y);
+        k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, g_scr.b32, ctx->y), ++ctx->launches;
         int it = 1;
         double prev = 1e300;
         for (; it < 60; it++) {
@@ -148,7 +148,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
             prev = rn;
             rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, g_scr.b32, w, false);
             if (rc) return rc;
-            k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, g_scr.b32, ctx->y);
+            k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, g_scr.b32, ctx->y), ++ctx->launches;
         }
         if (st) {
             st->linear_iterations = it;
@@ -244,10 +244,10 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st) {
     int it;
     bool converged = false;
     for (it = 0; it < 10000; it++) {
-        k_gs_sweep<<<1, 1024, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, ctx->y);
+        k_gs_sweep<<<1, 1024, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, ctx->y), ++ctx->launches;
         if (it % 25 == 0) {
             MP_CUDA(ctx, cudaMemsetAsync(ctx->scal + 3, 0, sizeof(double), ctx->stream));
-            k_gs_resid<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, ctx->y, ctx->scal + 3);
+            k_gs_resid<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, ctx->y, ctx->scal + 3), ++ctx->launches;
             MP_CUDA(ctx, cudaMemcpyAsync(ctx->scal_host + 3, ctx->scal + 3, sizeof(double), cudaMemcpyDeviceToHost,
                                          ctx->stream));
             MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

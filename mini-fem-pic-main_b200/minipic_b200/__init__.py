@@ -56,7 +56,8 @@ EXPORTED = [
     "mp_compute_phi", "mp_fe_build_f1", "mp_fe_residual", "mp_fe_build_j", "mp_fe_solve_linear",
     "mp_update_ef", "mp_field_download", "mp_mesh_geometry", "mp_fe_geometry", "mp_inlet_faces",
     "mp_injector_create", "mp_injector_destroy", "mp_injector_sample", "mp_injector_count",
-    "mp_injector_get_rem", "mp_injector_set_rem",
+    "mp_injector_get_rem", "mp_injector_set_rem", "mp_set_track_ids", "mp_kernel_launches",
+    "mp_device_buffer",
 ]
 
 
@@ -91,7 +92,8 @@ class FeDesc(C.Structure):
 
 class StepStats(C.Structure):
     _fields_ = [("n_before", C.c_int64), ("n_after", C.c_int64), ("total_hops", C.c_int64),
-                ("max_hops", C.c_int32), ("near_face_fp64", C.c_int32)]
+                ("max_hops", C.c_int32), ("near_face_fp64", C.c_int32), ("ms_kernel", C.c_double),
+                ("ms_step", C.c_double)]
 
 
 class NewtonStats(C.Structure):
@@ -142,6 +144,9 @@ def lib():
         L.mp_set_scatter_mode.argtypes = [vp, C.c_int]
         L.mp_set_sort_period.argtypes = [vp, i32]
         L.mp_set_particle_form.argtypes = [vp, C.c_int]
+        L.mp_set_track_ids.argtypes = [vp, C.c_int]
+        L.mp_kernel_launches.argtypes = [vp, C.POINTER(i64)]
+        L.mp_device_buffer.argtypes = [vp, C.c_int, C.POINTER(vp), C.POINTER(i64)]
         L.mp_particles_reserve.argtypes = [vp, i64]
         L.mp_particles_count.argtypes = [vp, C.POINTER(i64)]
         L.mp_density_download.argtypes = [vp, vp]
@@ -418,6 +423,20 @@ class Context:
 
     def set_sort_period(self, steps):
         self._c(lib().mp_set_sort_period(self.h, steps))
+
+    def set_track_ids(self, on: bool):
+        self._c(lib().mp_set_track_ids(self.h, int(bool(on))))
+
+    def device_buffer(self, name: str):
+        """(device pointer, length) of an FP64 context vector, e.g. "den"."""
+        ptr, n = C.c_void_p(), C.c_int64()
+        self._c(lib().mp_device_buffer(self.h, VEC[name], C.byref(ptr), C.byref(n)))
+        return ptr.value, int(n.value)
+
+    def launches(self) -> int:
+        n = C.c_int64()
+        self._c(lib().mp_kernel_launches(self.h, C.byref(n)))
+        return int(n.value)
 
     def set_form(self, form):
         self._c(lib().mp_set_particle_form(self.h, form))

@@ -1,0 +1,98 @@
+"""CPU: the C ABI library loads and exports every entry point that
+include/minipic_cuda.h declares; host-only entry points validate arguments;
+without a GPU, context creation fails loudly (no CPU fallback)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+import minipic_b200 as mp
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for f in os.listdir(inc):
+        if f.endswith(".h"):
+            text = open(os.path.join(inc, f)).read()
+            names |= set(re.findall(r"^\s*(?:int|const char \*|void)\s*\*?\s*(mp_\w+)\s*\(", text, re.M))
+    return names
+
+
+def test_header_and_binding_agree():
+    assert declared_symbols() == set(mp.EXPORTED)
+
+
+def test_library_exports_every_declared_symbol():
+    L = mp.lib()
+    for name in declared_symbols():
+        assert hasattr(L, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", mp.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (mp_\w+)", out))
+    assert declared_symbols() <= exported
+
+
+def test_error_strings():
+    L = mp.lib()
+    for code in range(10):
+        assert L.mp_error_string(code)
+    assert L.mp_version() >= 10000
+
+
+def test_null_arguments_rejected():
+    L = mp.lib()
+    assert L.mp_create(0, None, None) == 1  # MP_ERR_ARG
+    assert L.mp_push_scatter(None, 1.0, 1.0, 1.0, None, None) == 1
+    assert L.mp_compute_phi(None, None, 0, 0, None) == 1
+
+
+def test_no_cpu_fallback_without_device():
+    """On a machine without an sm_100 device, mp_create must fail loudly."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    dk = mp.Deck.load(os.path.join(ROOT, "tests", "golden", "kuhn4"))
+    with pytest.raises(mp.MpError) as e:
+        mp.Context(dk.mesh)
+    assert e.value.status == 8  # MP_ERR_NO_DEVICE
+
+
+def test_mesh_geometry_rejects_bad_connectivity():
+    L = mp.lib()
+    pos = np.zeros((4, 3))
+    con = np.array([[0, 1, 2, 7]], dtype=np.int32)  # node 7 does not exist
+    out = [np.zeros(1), np.zeros(4), np.zeros(4), np.zeros(4), np.zeros(4), np.zeros(4, dtype=np.int32),
+           np.zeros(4), np.zeros(4, dtype=np.int32)]
+    rc = L.mp_mesh_geometry(4, pos.ctypes.data_as(C.c_void_p), 1, con.ctypes.data_as(C.c_void_p),
+                            *[o.ctypes.data_as(C.c_void_p) for o in out])
+    assert rc == 1
+
+
+def test_inlet_face_without_tet_rejected():
+    """The reference exits when an inlet face has no owning tet (meshes.cpp:323-326)."""
+    dk = mp.Deck.load(os.path.join(ROOT, "tests", "golden", "kuhn4"))
+    m = dk.mesh
+    bad = np.array([[0, 1, 50]], dtype=np.int32)
+    with pytest.raises(mp.MpError):
+        mp.Mesh.build(m.node_pos, m.con, [], bad, [])
+
+
+def test_injector_capacity_checked():
+    dk = mp.Deck.load(os.path.join(ROOT, "tests", "golden", "kuhn4"))
+    inj = mp.Injector(dk.mesh)
+    L = mp.lib()
+    n = C.c_int64()
+    pos, vel = np.zeros((1, 3)), np.zeros((1, 3))
+    cell = np.zeros(1, dtype=np.int32)
+    rc = L.mp_injector_sample(inj.h, 1e10, 7000.0, 2e-6, 20000.0, 1, pos.ctypes.data_as(C.c_void_p), 24,
+                              vel.ctypes.data_as(C.c_void_p), 24, cell.ctypes.data_as(C.c_void_p), 4, C.byref(n))
+    assert rc == 1
