@@ -419,7 +419,8 @@ int mp_particles_download(mp_ctx *ctx, int64_t n_max, double *pos, int64_t pos_s
     long long n = ctx->n_host;
     if (n > n_max) return fail(ctx, MP_ERR_ARG, "output capacity smaller than the particle count");
     if (n == 0) return MP_OK;
-    size_t bytes = sizeof(double) * 10 * n + sizeof(int) * n + sizeof(long long) * n;
+    // layout: 10 FP64 arrays, cell (padded to 8 B), id
+    size_t bytes = sizeof(double) * 10 * n + sizeof(int) * (n + (n & 1)) + sizeof(long long) * n;
     rc = ensure_stage(ctx, bytes);
     if (rc) return rc;
     rc = ensure_dstage(ctx, bytes);
@@ -429,7 +430,7 @@ int mp_particles_download(mp_ctx *ctx, int64_t n_max, double *pos, int64_t pos_s
     long long *di = (long long *)(dc + n + (n & 1));
     rc = launch_download_pack(ctx, n, d, dc, di);
     if (rc) return rc;
-    MP_CUDA(ctx, cudaMemcpyAsync(ctx->stage, g_dstage, bytes + 8, cudaMemcpyDeviceToHost, ctx->stream));
+    MP_CUDA(ctx, cudaMemcpyAsync(ctx->stage, g_dstage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     const double *h = (const double *)ctx->stage;
     const int *hc = (const int *)(h + 10 * n);

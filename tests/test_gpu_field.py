@@ -69,7 +69,10 @@ def test_f1_residual_j(deck6):
     assert rel_err(ctx.fe_get("F1"), s.get("F1")) < 1e-13
     ctx.fe_set("F1", s.get("F1"))  # continue from identical F1
     ctx.residual()
-    assert rel_err(ctx.fe_get("G"), s.residual()) < 1e-12
+    # G = K d - F0 - F1 cancels; bound the difference by the terms' magnitude
+    K, d = s.matrix(0), s.get("d")
+    scale = np.abs(K) @ np.abs(d) + np.abs(s.get("F0")) + np.abs(s.get("F1"))
+    assert np.all(np.abs(ctx.fe_get("G") - s.residual()) <= 1e-13 * scale.max())
     s.build_j(1)
     ctx.build_j(1)
     J_ref, J_gpu = s.matrix(1), ctx.fe_get("J")
