@@ -51,7 +51,8 @@ enum {
     MP_ERR_SINGULAR = 6,      /* factorization met a zero/non-finite pivot */
     MP_ERR_STATE = 7,         /* call out of order (e.g. no FE setup yet) */
     MP_ERR_NO_DEVICE = 8,     /* no usable sm_100 device */
-    MP_ERR_TIMEOUT = 9        /* a bounded device-side wait gave up */
+    MP_ERR_TIMEOUT = 9,       /* a bounded device-side wait gave up */
+    MP_ERR_LIMIT = 10         /* size above the fixed maximum of an allocation-free entry point */
 };
 
 /* FESolver::Method, src/FESolver.h:26 */
@@ -191,6 +192,35 @@ int mp_push_scatter(mp_ctx *ctx, double q_over_m, double dt, double spwt,
                     double *den_out, mp_step_stats *stats);
 int mp_density_download(mp_ctx *ctx, double *den);
 int mp_sort_by_tet(mp_ctx *ctx);
+
+/* Allocation-free push for callers that cannot allocate device memory: code
+ * whose GPU memory is all handed out by another allocator or runtime, and code
+ * on a latency-critical path where cudaMalloc is not allowed because it can
+ * synchronise the whole device.  No counterpart in the reference: it is the
+ * device body of MoveParticles (src/mini-pic.cpp:287-308, walk
+ * src/meshes.h:75-100) run on caller-owned device buffers in the reference's
+ * own record layouts, plus the stable removal of the particles that left the
+ * domain.
+ *   particles_in/out  n Particle records (88 B: pos[3], vel[3], lc[4], cell);
+ *                     out receives the kept particles in order with their
+ *                     weights; out may equal in
+ *   tetra             n_tets Tetra records (168 B) as LoadVolumeMesh builds them
+ *   ef, den           [n_tets][3] field; [n_nodes] density, zeroed by the call
+ *                     then summed (not yet multiplied by spwt/node volume)
+ *   stream            a cudaStream_t (NULL: the default stream); the call
+ *                     returns after the stream has finished its work
+ *   n_out             host: number of particles kept
+ * All pointers except n_out are device pointers on the current device.  The
+ * kernel's scratch (look-back words of the compaction and three counters,
+ * 262,208 B) is a fixed device array of the library, held on every GPU that
+ * loads it until exit and shared by every call: n above 8,388,608 returns
+ * MP_ERR_LIMIT; calls that overlap on the GPU race on the scratch and must be
+ * serialised; the first call on a device looks the array up with that device
+ * current and should come before any stream capture.  Walk limit 4096 hops
+ * (MP_ERR_WALK_LIMIT). */
+int mp_push_particles_noalloc(const void *particles_in, void *particles_out, int64_t n,
+                              const void *tetra, int32_t n_tets, const double *ef, double *den,
+                              int32_t n_nodes, double q_over_m, double dt, void *stream, int64_t *n_out);
 
 /* ---- field solve ------------------------------------------------------------------ */
 int mp_fe_setup(mp_ctx *ctx, const mp_fe_desc *fe);

@@ -164,6 +164,7 @@ const char *mp_error_string(int status) {
         case MP_ERR_STATE: return "call out of order";
         case MP_ERR_NO_DEVICE: return "no usable sm_100 CUDA device";
         case MP_ERR_TIMEOUT: return "bounded device wait gave up";
+        case MP_ERR_LIMIT: return "size exceeds the fixed maximum of the allocation-free entry point";
     }
     return "unknown status";
 }

@@ -33,7 +33,7 @@ LIB_PATH = os.path.join(_PKG, "lib", "libminipic_cuda.so")
 MP_OK = 0
 STATUS = {0: "MP_OK", 1: "MP_ERR_ARG", 2: "MP_ERR_OOM", 3: "MP_ERR_CUDA", 4: "MP_ERR_WALK_LIMIT",
           5: "MP_ERR_NOT_CONVERGED", 6: "MP_ERR_SINGULAR", 7: "MP_ERR_STATE", 8: "MP_ERR_NO_DEVICE",
-          9: "MP_ERR_TIMEOUT"}
+          9: "MP_ERR_TIMEOUT", 10: "MP_ERR_LIMIT"}
 NONLINEAR, GAUSS_SEIDEL, LAPACK = 0, 1, 2
 FP64, MIXED = 0, 1
 SCATTER_ATOMIC, SCATTER_FIXED = 0, 1
@@ -57,7 +57,7 @@ EXPORTED = [
     "mp_update_ef", "mp_field_download", "mp_mesh_geometry", "mp_fe_geometry", "mp_inlet_faces",
     "mp_injector_create", "mp_injector_destroy", "mp_injector_sample", "mp_injector_count",
     "mp_injector_get_rem", "mp_injector_set_rem", "mp_set_track_ids", "mp_kernel_launches",
-    "mp_device_buffer",
+    "mp_device_buffer", "mp_push_particles_noalloc",
 ]
 
 
@@ -147,6 +147,7 @@ def lib():
         L.mp_set_track_ids.argtypes = [vp, C.c_int]
         L.mp_kernel_launches.argtypes = [vp, C.POINTER(i64)]
         L.mp_device_buffer.argtypes = [vp, C.c_int, C.POINTER(vp), C.POINTER(i64)]
+        L.mp_push_particles_noalloc.argtypes = [vp, vp, i64, vp, i32, vp, vp, i32, d, d, vp, C.POINTER(i64)]
         L.mp_particles_reserve.argtypes = [vp, i64]
         L.mp_particles_count.argtypes = [vp, C.POINTER(i64)]
         L.mp_density_download.argtypes = [vp, vp]

@@ -40,7 +40,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_error_strings():
     L = mp.lib()
-    for code in range(10):
+    for code in range(11):
         assert L.mp_error_string(code)
     assert L.mp_version() >= 10000
 
