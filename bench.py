@@ -37,15 +37,14 @@ sys.path.insert(0, os.path.join(ROOT, "mini-fem-pic-main_b200"))
 sys.path.insert(0, ROOT)
 
 import minipic_b200 as mp  # noqa: E402
-from minipic_b200 import kuhn, sharding  # noqa: E402
+from minipic_b200 import kuhn, sharding, workloads  # noqa: E402
 
 METRIC = "particle-steps/sec and Newton-step ms on 1 B200: mixed vs FP64 at stated error"
-CONFIGS = {
-    0: dict(n=8, n_ions=50_000, dt=1e-7, spwt=200.0, sphere=None, label="kuhn8_50k_fp64"),
-    1: dict(n=20, n_ions=2_000_000, dt=5e-8, spwt=5.0, sphere=None, label="kuhn20_2M_fp64"),
-}
-KTI_EV = 0.1
+KTI_EV = workloads.KTI_EV
+CONFIGS = workloads.CONFIGS
+make_workload = workloads.make_workload
 FLUSH_BYTES = 512 << 20
+SORT_PERIOD = 10
 
 
 def peaks():
@@ -54,24 +53,6 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
-
-
-def make_workload(cfg, workdir, seed):
-    kd = kuhn.build(cfg["n"], sphere=cfg["sphere"])
-    kuhn.write(kd, workdir, dt=cfg["dt"], method="lapack")
-    deck = mp.Deck.load(workdir)
-    m = deck.mesh
-    rng = np.random.default_rng(seed)
-    n = cfg["n_ions"]
-    L = kd.length_mm / 1000.0
-    pos = rng.uniform(1e-6 * L, (1 - 1e-6) * L, size=(n, 3))
-    mass = 16 * mp.AMU
-    sigma = np.sqrt(KTI_EV * mp.QE / mass)
-    vel = rng.normal(0.0, sigma, size=(n, 3))
-    vel[:, 0] += deck.params.ion_velocity
-    cell = kuhn.locate(kd, pos).astype(np.int32)
-    keep = cell >= 0
-    return kd, deck, pos[keep], vel[keep], cell[keep]
 
 
 class Clocks:
@@ -130,6 +111,8 @@ def run_form(form, args, cfg, deck, pop, inj_batches, device, rank, world, torch
     ctx.set_track_ids(False)
     ctx.reserve(int(len(cell) * 1.3) + 100_000)
     ctx.append(pos, vel, cell)
+    ctx.sort_by_tet()  # a steady-state population has been sorted before
+    ctx.set_sort_period(SORT_PERIOD)
     if form == mp.MIXED:
         ctx.set_form(mp.MIXED)
     qm = mp.QE / (16 * mp.AMU)
@@ -403,6 +386,7 @@ def main():
                        "nodes": deck.mesh.n_nodes, "unknowns": int(deck.fe_desc_arrays()["neq"]),
                        "ions_per_gpu": int(np.mean(nb)), "dt": cfg["dt"], "method": "lapack (1 Newton step)",
                        "form": "fp64", "l2": f"flushed ({FLUSH_BYTES >> 20} MiB write) between timed steps",
+                       "tet_sort_every": SORT_PERIOD,
                        "parallelism": f"particles sharded x{world}, density all-reduce" if world > 1 else "1 GPU"},
             "newton_step_ms": float(newton_ms),
             "full_step_particle_steps_per_s": psteps_all / step_s,

@@ -147,7 +147,8 @@ int mp_set_sort_period(mp_ctx *ctx, int32_t steps);
 int mp_set_particle_form(mp_ctx *ctx, int form);
 /* Particle IDs (16 B per particle-step of traffic) are needed only to restore
  * injection order after tet re-sorting; without sorting the stable removal
- * keeps the reference's order by itself.  Default on. */
+ * keeps the reference's order by itself.  With IDs off and sorting on,
+ * downloads come in storage order.  Default on. */
 int mp_set_track_ids(mp_ctx *ctx, int on);
 /* Device address and length (elements) of a context buffer named by MP_VEC_*
  * (FP64 vectors), for zero-copy interop on the context's stream: e.g. an

@@ -322,7 +322,6 @@ int mp_set_scatter_mode(mp_ctx *ctx, int mode) {
 
 int mp_set_sort_period(mp_ctx *ctx, int32_t steps) {
     if (!ctx || steps < 0) return MP_ERR_ARG;
-    if (steps > 0 && !ctx->track_ids) return fail(ctx, MP_ERR_STATE, "tet re-sorting needs particle IDs");
     ctx->sort_period = steps;
     return MP_OK;
 }
@@ -340,7 +339,6 @@ int mp_set_particle_form(mp_ctx *ctx, int form) {
 
 int mp_set_track_ids(mp_ctx *ctx, int on) {
     if (!ctx) return MP_ERR_ARG;
-    if (!on && ctx->sort_period > 0) return fail(ctx, MP_ERR_STATE, "tet re-sorting needs particle IDs");
     ctx->track_ids = on != 0;
     return MP_OK;
 }

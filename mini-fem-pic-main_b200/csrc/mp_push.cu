@@ -110,32 +110,45 @@ __device__ __forceinline__ unsigned long long load_acquire(unsigned long long *p
     return a.load(cuda::memory_order_acquire);
 }
 
-// Exclusive prefix of tile `tile` given its own count (called by one thread).
-__device__ long long lookback(unsigned long long *status, long long tile, long long count,
-                              unsigned long long *counters) {
+// Exclusive prefix of tile `tile` given its own count; called by all 32 lanes
+// of one warp, which inspect 32 predecessors per poll.  The wait for a
+// predecessor that has published nothing yet is bounded (LOOKBACK_SPIN_LIMIT
+// polls); on timeout the error flag is set and the count so far is used.
+__device__ long long lookback_warp(unsigned long long *status, long long tile, long long count,
+                                   unsigned long long *counters) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     if (tile == 0) {
-        store_release(&status[0], ST_PREFIX | (unsigned long long)count);
+        if (lane == 0) store_release(&status[0], ST_PREFIX | (unsigned long long)count);
         return 0;
     }
-    store_release(&status[tile], ST_AGG | (unsigned long long)count);
+    if (lane == 0) store_release(&status[tile], ST_AGG | (unsigned long long)count);
     long long excl = 0;
-    long long p = tile - 1;
+    long long base = tile - 1;
     long long spins = 0;
-    while (p >= 0) {
-        unsigned long long s = load_acquire(&status[p]);
+    for (;;) {
+        long long p = base - lane;
+        unsigned long long s = p >= 0 ? load_acquire(&status[p]) : ST_PREFIX;
         unsigned long long flag = s & ~ST_VALUE;
-        if (flag == 0) {
+        unsigned pref = __ballot_sync(FULL, flag == ST_PREFIX);
+        unsigned notready = __ballot_sync(FULL, flag == 0);
+        int stop = pref ? __ffs(pref) - 1 : 31;
+        unsigned need = stop == 31 ? FULL : ((2u << stop) - 1u);
+        if (notready & need) {
             if (++spins > LOOKBACK_SPIN_LIMIT) {
-                atomicOr(&counters[C_FLAGS], FLAG_LOOKBACK_TIMEOUT);
+                if (lane == 0) atomicOr(&counters[C_FLAGS], FLAG_LOOKBACK_TIMEOUT);
                 break;
             }
             continue;
         }
-        excl += (long long)(s & ST_VALUE);
-        if (flag == ST_PREFIX) break;
-        p--;
+        long long v = lane <= stop ? (long long)(s & ST_VALUE) : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+        excl += v;
+        if (pref) break;
+        base -= 32;
     }
-    store_release(&status[tile], ST_PREFIX | (unsigned long long)(excl + count));
+    if (lane == 0) store_release(&status[tile], ST_PREFIX | (unsigned long long)(excl + count));
     return excl;
 }
 
@@ -237,16 +250,22 @@ __device__ __forceinline__ long long scatter_and_rank(int keep_state, int cell, 
     unsigned kb = __ballot_sync(0xffffffffu, keep);
     if (lane == 0) s_wc[warp] = __popc(kb);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        long long run = 0;
-        for (int w = 0; w < PUSH_THREADS / 32; w++) {
-            int c = s_wc[w];
-            s_wc[w] = (int)run;
-            run += c;
+    if (warp == 0) {
+        // exclusive scan of the warp counts, then the look-back, by warp 0
+        int c = lane < PUSH_THREADS / 32 ? s_wc[lane] : 0;
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
         }
-        long long excl = lookback(status, tile, run, counters);
-        *s_base = excl;
-        if (tile == n_tiles - 1) counters[C_N_OUT] = (unsigned long long)(excl + run);
+        long long run = __shfl_sync(0xffffffffu, incl, 31);
+        if (lane < PUSH_THREADS / 32) s_wc[lane] = incl - c;
+        long long excl = lookback_warp(status, tile, run, counters);
+        if (lane == 0) {
+            *s_base = excl;
+            if (tile == n_tiles - 1) counters[C_N_OUT] = (unsigned long long)(excl + run);
+        }
     }
     __syncthreads();
     long long idx = keep ? *s_base + s_wc[warp] + __popc(kb & lanemask_lt()) : -1;
@@ -696,7 +715,6 @@ __global__ void k_sort_scatter(long long n, P in, P out, int *cursor, int track_
 int launch_sort_by_tet(mp_ctx *ctx) {
     long long n = ctx->n_host;
     if (n <= 1) return MP_OK;
-    if (!ctx->track_ids) return fail(ctx, MP_ERR_STATE, "tet re-sorting needs particle IDs (mp_set_track_ids)");
     if (!ctx->sort_hist) MP_CUDA(ctx, cudaMalloc(&ctx->sort_hist, sizeof(int) * (ctx->n_tets + 1)));
     MP_CUDA(ctx, cudaMemsetAsync(ctx->sort_hist, 0, sizeof(int) * ctx->n_tets, ctx->stream));
     int th = 256;

@@ -1,0 +1,127 @@
+"""Synthetic workloads of the benchmark configurations, and single-kernel
+drivers for profiling them.
+
+Configurations (Kuhn box 0.1 m, O+ ions, n0 = 1e10 m^-3, 7 km/s drift,
+kTe = 2 eV, inlet x=0 at 0 V, wall x=0.1 at -5 V):
+  0  8^3 hexes (3,072 tets), ~50k ions, dt 1e-7, spwt 200
+  1  20^3 hexes (48,000 tets), ~2M ions, dt 5e-8, spwt 5
+  2  32^3 hexes minus a centred r=0.02 m sphere at -10 V, ~50M ions, dt 5e-8
+The ion population is seeded at steady state: uniform in the box, drift plus
+a 0.1 eV Maxwellian (sigma = sqrt(kTi*QE/m) ~ 776 m/s), each ion in the Kuhn
+tet that contains it.
+
+    python workloads.py push   --config 1 --steps 4 [--form mixed] [--sort 10]
+    python workloads.py newton --config 0 --steps 2 [--form mixed]
+
+The drivers print one JSON line per run with the device times measured by
+CUDA events inside the library (push kernel; Newton step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+if __package__ in (None, ""):
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import minipic_b200 as mp  # noqa: E402
+    from minipic_b200 import kuhn  # noqa: E402
+else:
+    from . import kuhn
+    import minipic_b200 as mp
+
+CONFIGS = {
+    0: dict(n=8, n_ions=50_000, dt=1e-7, spwt=200.0, sphere=None, label="kuhn8_50k_fp64"),
+    1: dict(n=20, n_ions=2_000_000, dt=5e-8, spwt=5.0, sphere=None, label="kuhn20_2M_fp64"),
+    2: dict(n=32, n_ions=50_000_000, dt=5e-8, spwt=0.2, sphere=(50.0, 50.0, 50.0, 20.0), label="kuhn32s_50M_mixed"),
+}
+KTI_EV = 0.1
+SPHERE_POTENTIAL = -10.0
+
+
+def make_workload(cfg: dict, workdir: str, seed: int, n_ions: int | None = None):
+    """Writes the deck into workdir, loads it as the reference would, and seeds
+    the ion population.  Returns (kuhn deck, Deck, pos, vel, cell)."""
+    kd = kuhn.build(cfg["n"], sphere=cfg["sphere"])
+    kuhn.write(kd, workdir, dt=cfg["dt"], method="lapack")
+    deck = mp.Deck.load(workdir)
+    rng = np.random.default_rng(seed)
+    n = cfg["n_ions"] if n_ions is None else n_ions
+    L = kd.length_mm / 1000.0
+    pos = rng.uniform(1e-6 * L, (1 - 1e-6) * L, size=(n, 3))
+    sigma = np.sqrt(KTI_EV * mp.QE / (16 * mp.AMU))
+    vel = rng.normal(0.0, sigma, size=(n, 3))
+    vel[:, 0] += deck.params.ion_velocity
+    cell = kuhn.locate(kd, pos).astype(np.int32)
+    keep = cell >= 0
+    return kd, deck, np.ascontiguousarray(pos[keep]), np.ascontiguousarray(vel[keep]), cell[keep]
+
+
+def fe_arrays(cfg: dict, deck):
+    return deck.fe_desc_arrays(SPHERE_POTENTIAL if cfg["sphere"] else None)
+
+
+def push_driver(args):
+    cfg = CONFIGS[args.config]
+    with tempfile.TemporaryDirectory() as wd:
+        kd, deck, pos, vel, cell = make_workload(cfg, wd, seed=1234)
+        ctx = mp.Context(deck.mesh)
+        ctx.set_track_ids(False)
+        ctx.set_sort_period(args.sort)
+        ctx.reserve(len(cell) + 1024)
+        ctx.append(pos, vel, cell)
+        if args.sort:
+            ctx.sort_by_tet()
+        if args.form == "mixed":
+            ctx.set_form(mp.MIXED)
+        rng = np.random.default_rng(5)
+        ctx.fe_set("ef", rng.normal(0.0, 20.0, size=(deck.mesh.n_tets, 3)))
+        qm = mp.QE / (16 * mp.AMU)
+        bpp = 52.0 if args.form == "fp64" else 28.0
+        out = []
+        for k in range(args.steps):
+            st = ctx.push(qm, cfg["dt"], cfg["spwt"])
+            gbs = (st.n_before + st.n_after) * bpp / (st.ms_kernel * 1e-3) / 1e9
+            out.append({"step": k, "n": st.n_before, "push_kernel_ms": st.ms_kernel, "push_call_ms": st.ms_step,
+                        "alg_GBps": gbs, "hops": st.total_hops})
+        print(json.dumps({"driver": "push", "config": cfg["label"], "form": args.form, "sort": args.sort,
+                          "steps": out}))
+        ctx.close()
+
+
+def newton_driver(args):
+    cfg = CONFIGS[args.config]
+    form = mp.MIXED if args.form == "mixed" else mp.FP64
+    with tempfile.TemporaryDirectory() as wd:
+        kd, deck, pos, vel, cell = make_workload(cfg, wd, seed=1234, n_ions=min(cfg["n_ions"], 200_000))
+        ctx = mp.Context(deck.mesh)
+        ctx.fe_setup(**fe_arrays(cfg, deck))
+        ctx.append(pos, vel, cell)
+        ctx.push(mp.QE / (16 * mp.AMU), cfg["dt"], cfg["spwt"] * cfg["n_ions"] / len(cell))
+        out = []
+        for k in range(args.steps):
+            st = ctx.compute_phi(mp.LAPACK, form)
+            out.append({"step": k, "newton_ms": st.ms_total, "factor_ms": st.ms_factor,
+                        "refinements": st.linear_iterations, "residual": st.linear_residual})
+        print(json.dumps({"driver": "newton", "config": cfg["label"], "form": args.form,
+                          "unknowns": int(fe_arrays(cfg, deck)["neq"]), "steps": out}))
+        ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("driver", choices=["push", "newton"])
+    ap.add_argument("--config", type=int, default=1, choices=sorted(CONFIGS))
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--sort", type=int, default=0)
+    args = ap.parse_args()
+    (push_driver if args.driver == "push" else newton_driver)(args)
+
+
+if __name__ == "__main__":
+    main()
