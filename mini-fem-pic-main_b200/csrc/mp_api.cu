@@ -131,6 +131,7 @@ static int sync_counters(mp_ctx *ctx) {
                                  cudaMemcpyDeviceToHost, ctx->stream));
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->n_host = (long long)ctx->counters_host[C_N];
+    ctx->dead_host = (long long)ctx->counters_host[C_DEAD];
     unsigned long long flags = ctx->counters_host[C_FLAGS];
     unsigned long long part = flags & (FLAG_WALK_LIMIT | FLAG_LOOKBACK_TIMEOUT);
     if (part) {
@@ -140,7 +141,7 @@ static int sync_counters(mp_ctx *ctx) {
                                      cudaMemcpyHostToDevice, ctx->stream));
         MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         if (part & FLAG_LOOKBACK_TIMEOUT)
-            return fail(ctx, MP_ERR_TIMEOUT, "push compaction look-back gave up waiting (bounded spin)");
+            return fail(ctx, MP_ERR_TIMEOUT, "a bounded device-side wait gave up");
         return fail(ctx, MP_ERR_WALK_LIMIT, "a particle's tet walk exceeded the hop limit");
     }
     return MP_OK;
@@ -279,7 +280,7 @@ int mp_destroy(mp_ctx *ctx) {
     if (!ctx) return MP_OK;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     void *dev[] = {ctx->tets, ctx->tets32, ctx->tet_x0, ctx->con, ctx->ef, ctx->node_volume, ctx->node_pos,
-                   ctx->den, ctx->den_fixed, ctx->counters, ctx->scal, ctx->tile_status, ctx->sort_hist,
+                   ctx->den, ctx->den_fixed, ctx->counters, ctx->scal, ctx->compact_off, ctx->sort_hist,
                    ctx->part_block[0], ctx->part_block[1], ctx->ID, ctx->LM, ctx->detJ, ctx->nx, ctx->g, ctx->uh,
                    ctx->d, ctx->F0, ctx->F1, ctx->G, ctx->y, ctx->fvec, ctx->FP, ctx->work, ctx->K, ctx->J,
                    ctx->J32, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a, ctx->gs_minv, ctx->den_in};
@@ -331,6 +332,8 @@ int mp_set_particle_form(mp_ctx *ctx, int form) {
     if (form == ctx->form) return MP_OK;
     int rc0 = sync_counters(ctx);
     if (rc0) return rc0;
+    rc0 = launch_compact(ctx);  // the conversion reads every slot's tet
+    if (rc0) return rc0;
     int rc = launch_convert_form(ctx, form);
     if (rc) return rc;
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -357,15 +360,16 @@ int mp_particles_reserve(mp_ctx *ctx, int64_t capacity) {
 int mp_particles_count(mp_ctx *ctx, int64_t *n) {
     if (!ctx || !n) return MP_ERR_ARG;
     int rc = sync_counters(ctx);
-    *n = ctx->n_host;
+    *n = ctx->n_host - ctx->dead_host;
     return rc;
 }
 
 int mp_particles_clear(mp_ctx *ctx) {
     if (!ctx) return MP_ERR_ARG;
-    MP_CUDA(ctx, cudaMemsetAsync(ctx->counters + C_N, 0, sizeof(unsigned long long), ctx->stream));
+    MP_CUDA(ctx, cudaMemsetAsync(ctx->counters + C_N, 0, 2 * sizeof(unsigned long long), ctx->stream));
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->n_host = 0;
+    ctx->dead_host = 0;
     return MP_OK;
 }
 
@@ -415,6 +419,8 @@ int mp_particles_download(mp_ctx *ctx, int64_t n_max, double *pos, int64_t pos_s
     if (!ctx) return MP_ERR_ARG;
     int rc = sync_counters(ctx);
     if (rc) return rc;
+    rc = launch_compact(ctx);
+    if (rc) return rc;
     long long n = ctx->n_host;
     if (n > n_max) return fail(ctx, MP_ERR_ARG, "output capacity smaller than the particle count");
     if (n == 0) return MP_OK;
@@ -462,14 +468,15 @@ int mp_particles_download(mp_ctx *ctx, int64_t n_max, double *pos, int64_t pos_s
 
 int mp_push_scatter(mp_ctx *ctx, double q_over_m, double dt, double spwt, double *den_out, mp_step_stats *stats) {
     if (!ctx) return MP_ERR_ARG;
-    long long n_before = ctx->n_host;
+    long long n_before = ctx->n_host - ctx->dead_host;
     cudaEventRecord(ctx->ts.a, ctx->stream);
+    int rc;
     if (ctx->sort_period > 0 && ++ctx->steps_since_sort >= ctx->sort_period) {
-        int rc = launch_sort_by_tet(ctx);
+        rc = launch_sort_by_tet(ctx);
         if (rc) return rc;
         ctx->steps_since_sort = 0;
     }
-    int rc = launch_push(ctx, q_over_m, dt);
+    rc = launch_push(ctx, q_over_m, dt);
     if (rc) return rc;
     rc = launch_normalise(ctx, spwt);
     if (rc) return rc;
@@ -480,16 +487,21 @@ int mp_push_scatter(mp_ctx *ctx, double q_over_m, double dt, double spwt, double
     rc = sync_counters(ctx);
     if (stats) {
         stats->n_before = n_before;
-        stats->n_after = ctx->n_host;
+        stats->n_after = ctx->n_host - ctx->dead_host;
         stats->total_hops = (int64_t)ctx->counters_host[C_HOPS];
         stats->max_hops = (int32_t)ctx->counters_host[C_MAX_HOPS];
         stats->near_face_fp64 = (int32_t)ctx->counters_host[C_NEAR];
-        float a = 0, b = 0;
-        cudaEventElapsedTime(&a, ctx->tp.a, ctx->tp.b);
-        cudaEventElapsedTime(&b, ctx->ts.a, ctx->ts.b);
-        stats->ms_kernel = a;
-        stats->ms_step = b;
+        float ka = 0, kb = 0;
+        cudaEventElapsedTime(&ka, ctx->tp.a, ctx->tp.b);
+        cudaEventElapsedTime(&kb, ctx->ts.a, ctx->ts.b);
+        stats->ms_kernel = ka;
+        stats->ms_step = kb;
     }
+    if (rc) return rc;
+    // holes are removed by the next re-sort; without one due soon, compact once
+    // they pass 1/16 of the slots
+    bool sort_soon = ctx->sort_period > 0 && ctx->sort_period - ctx->steps_since_sort <= 2;
+    if (!sort_soon && ctx->dead_host * 16 > ctx->n_host) rc = launch_compact(ctx);
     return rc;
 }
 
@@ -507,6 +519,7 @@ int mp_sort_by_tet(mp_ctx *ctx) {
     rc = launch_sort_by_tet(ctx);
     if (rc) return rc;
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->steps_since_sort = 0;
     return MP_OK;
 }
 

@@ -61,12 +61,12 @@ struct PartsF32 {
 
 // Device counters (one 64-bit word each).
 enum Counter {
-    C_N = 0,          // live particles (input of the next push)
-    C_N_OUT = 1,      // particles kept by the running push   } zeroed
-    C_TILE = 2,       // dynamic tile ticket of the push       } before
-    C_HOPS = 3,       // total hops this step                  } every
-    C_MAX_HOPS = 4,   // longest walk this step                } push
-    C_NEAR = 5,       // mixed form: FP64 near-face re-tests   }
+    C_N = 0,          // particle slots in use (live + holes)
+    C_DEAD = 1,       // holes: slots of particles that left the domain
+    C_EXITS = 2,      // particles that left this push          } zeroed
+    C_HOPS = 3,       // total hops this push                   } before
+    C_MAX_HOPS = 4,   // longest walk this push                 } every
+    C_NEAR = 5,       // mixed form: FP64 near-face re-tests    } push
     C_FLAGS = 6,      // error bits (FLAG_*), cleared when reported
     C_NEXT_ID = 7,    // next particle id
     C_COUNT = 16
@@ -120,15 +120,16 @@ struct mp_ctx {
     long long steps_since_sort = 0;
     bool track_ids = true;
     long long capacity = 0;
-    long long n_host = 0;                 // exact particle count as last synchronised
+    long long n_host = 0;                 // particle slots (live + holes); exact after a sync, else an upper bound
+    long long dead_host = 0;              // holes, as of the last sync
+    int *compact_off = nullptr;           // per-block offsets of the stable compaction
+    long long compact_len = 0;
     mp::PartsF64 p64[2] = {};
     mp::PartsF32 p32[2] = {};
     int cur = 0;                          // which buffer holds the live particles
     void *part_block[2] = {nullptr, nullptr};
     unsigned long long *counters = nullptr;     // device [C_COUNT]
     unsigned long long *counters_host = nullptr;  // pinned mirror
-    unsigned long long *tile_status = nullptr;  // device look-back words
-    long long tile_status_len = 0;
     // pinned staging for host appends/downloads
     void *stage = nullptr;
     size_t stage_bytes = 0;
@@ -178,6 +179,7 @@ int launch_append(mp_ctx *ctx, long long n, const double *pos_soa, const double 
 int launch_download_pack(mp_ctx *ctx, long long n, double *out_soa /*3+3+4 arrays*/, int *cell_out,
                          long long *id_out);
 int launch_sort_by_tet(mp_ctx *ctx);
+int launch_compact(mp_ctx *ctx);
 int launch_convert_form(mp_ctx *ctx, int to_form);
 int launch_update_ef(mp_ctx *ctx);
 

@@ -1,13 +1,15 @@
 // Particle push: E gather + kick + drift + barycentric tet walk + node-density
-// scatter + stable removal of exited particles, in one pass over the particle
-// arrays (MoveParticles, src/mini-pic.cpp:268-320; walk XtoLtet,
-// src/meshes.h:75-100).
+// scatter (MoveParticles, src/mini-pic.cpp:268-320; walk XtoLtet,
+// src/meshes.h:75-100), and the removal of the particles that left the domain.
 //
-// One persistent grid; each CTA takes 256-particle tiles from a ticket counter.
-// Survivors are written to the other particle buffer at their global rank,
-// found by a decoupled look-back over the tiles' running counts, so the
-// removal is stable (the reference's std::erase_if order) and particle data
-// crosses HBM once per step: read 52 B, write 52 B (FP64) or 28 B + 28 B (mixed).
+// The push updates each particle in place, one thread per particle, with no
+// block-wide synchronisation: particle data crosses HBM once per step (read
+// 52 B, write 52 B in FP64; 28 + 28 B in the mixed form).  A particle that
+// leaves the domain becomes a hole (cell = -1) that later pushes skip.  Holes
+// are removed, keeping the survivors' order (the reference's std::erase_if
+// order), by the periodic tet re-sort or by a stable compaction pass that runs
+// before any download and whenever holes exceed a fraction of the slots.
+// Observable results (particle list, density) are those of a per-step removal.
 #include <cuda/atomic>
 
 #include "mp_internal.h"
@@ -16,20 +18,15 @@ namespace mp {
 
 constexpr int PUSH_THREADS = 256;
 constexpr double ONE_SIXTH = 1.0 / 6.0;
-constexpr unsigned long long ST_AGG = 1ull << 62;
-constexpr unsigned long long ST_PREFIX = 2ull << 62;
-constexpr unsigned long long ST_VALUE = (1ull << 62) - 1;
-constexpr long long LOOKBACK_SPIN_LIMIT = 1ll << 24;
 constexpr double FIXED_SCALE = 1099511627776.0;  // 2^40
 constexpr double NEAR_FACE = 1e-5;
 
 struct PushF64Args {
-    PartsF64 in, out;
+    PartsF64 p;
     const TetRec *__restrict__ tets;
     double *den;
     unsigned long long *den_fixed;
     unsigned long long *counters;
-    unsigned long long *status;
     double qm, dt;
     int walk_limit;
     int fixed;
@@ -37,14 +34,13 @@ struct PushF64Args {
 };
 
 struct PushF32Args {
-    PartsF32 in, out;
+    PartsF32 p;
     const TetRec32 *__restrict__ tets32;
     const TetRec *__restrict__ tets;
     const double *__restrict__ x0;   // [n_tets][4]
     double *den;
     unsigned long long *den_fixed;
     unsigned long long *counters;
-    unsigned long long *status;
     float qm_dt;                     // q/m * dt
     float dt;
     int walk_limit;
@@ -101,57 +97,6 @@ __device__ __forceinline__ bool group_sum4(int key, T v[4]) {
     return r == 0;
 }
 
-__device__ __forceinline__ void store_release(unsigned long long *p, unsigned long long v) {
-    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(*p);
-    a.store(v, cuda::memory_order_release);
-}
-__device__ __forceinline__ unsigned long long load_acquire(unsigned long long *p) {
-    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(*p);
-    return a.load(cuda::memory_order_acquire);
-}
-
-// Exclusive prefix of tile `tile` given its own count; called by all 32 lanes
-// of one warp, which inspect 32 predecessors per poll.  The wait for a
-// predecessor that has published nothing yet is bounded (LOOKBACK_SPIN_LIMIT
-// polls); on timeout the error flag is set and the count so far is used.
-__device__ long long lookback_warp(unsigned long long *status, long long tile, long long count,
-                                   unsigned long long *counters) {
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    if (tile == 0) {
-        if (lane == 0) store_release(&status[0], ST_PREFIX | (unsigned long long)count);
-        return 0;
-    }
-    if (lane == 0) store_release(&status[tile], ST_AGG | (unsigned long long)count);
-    long long excl = 0;
-    long long base = tile - 1;
-    long long spins = 0;
-    for (;;) {
-        long long p = base - lane;
-        unsigned long long s = p >= 0 ? load_acquire(&status[p]) : ST_PREFIX;
-        unsigned long long flag = s & ~ST_VALUE;
-        unsigned pref = __ballot_sync(FULL, flag == ST_PREFIX);
-        unsigned notready = __ballot_sync(FULL, flag == 0);
-        int stop = pref ? __ffs(pref) - 1 : 31;
-        unsigned need = stop == 31 ? FULL : ((2u << stop) - 1u);
-        if (notready & need) {
-            if (++spins > LOOKBACK_SPIN_LIMIT) {
-                if (lane == 0) atomicOr(&counters[C_FLAGS], FLAG_LOOKBACK_TIMEOUT);
-                break;
-            }
-            continue;
-        }
-        long long v = lane <= stop ? (long long)(s & ST_VALUE) : 0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-        excl += v;
-        if (pref) break;
-        base -= 32;
-    }
-    if (lane == 0) store_release(&status[tile], ST_PREFIX | (unsigned long long)(excl + count));
-    return excl;
-}
-
 // Barycentric weight i of point (x,y,z) in tet t, the reference's expression
 // (1.0/6.0)*(alpha - x*beta + y*gamma - z*delta)/volume in its order, unfused.
 __device__ __forceinline__ void lambdas_fp64(const TetRec *__restrict__ t, double x, double y, double z,
@@ -205,95 +150,63 @@ __device__ __forceinline__ int walk_fp64(const TetRec *__restrict__ tets, int &c
     }
 }
 
-// Shared tail of both push kernels: scatter, block scan, look-back.  Returns the
-// output index of this thread's particle (or -1 if it is removed).
+// Density scatter of one warp, aggregated over the lanes that sit in one tet,
+// plus the step statistics.  All 32 lanes call it; `state` 1 = inside (scatter),
+// 2 = kept after hitting the hop limit, 3 = left the domain, 0 = nothing.
 template <typename Lc>
-__device__ __forceinline__ long long scatter_and_rank(int keep_state, int cell, const int con[4], Lc lcv[4],
-                                                      double *den, unsigned long long *den_fixed, int fixed,
-                                                      long long tile, unsigned long long *status,
-                                                      unsigned long long *counters, int hops,
-                                                      long long n_tiles, int *s_wc, long long *s_base) {
+__device__ __forceinline__ void scatter_warp(int state, int cell, const int con[4], Lc lcv[4], double *den,
+                                             unsigned long long *den_fixed, int fixed, unsigned long long *counters,
+                                             int hops) {
     const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
     __syncwarp();
-    // density scatter, aggregated over the lanes of a warp that sit in one tet
-    int key = keep_state == 1 ? cell : -2 - lane;
+    int key = state == 1 ? cell : -2 - lane;
     if (fixed) {
         unsigned long long q[4];
 #pragma unroll
         for (int i = 0; i < 4; i++)
-            q[i] = keep_state == 1 ? (unsigned long long)__double2ll_rn((double)lcv[i] * FIXED_SCALE) : 0ull;
+            q[i] = state == 1 ? (unsigned long long)__double2ll_rn((double)lcv[i] * FIXED_SCALE) : 0ull;
         bool leader = group_sum4<unsigned long long>(key, q);
-        if (leader && keep_state == 1) {
+        if (leader && state == 1) {
 #pragma unroll
             for (int i = 0; i < 4; i++) atomicAdd(&den_fixed[con[i]], q[i]);
         }
     } else {
-        double s[4];
+        double sv[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) s[i] = keep_state == 1 ? (double)lcv[i] : 0.0;
-        bool leader = group_sum4<double>(key, s);
-        if (leader && keep_state == 1) {
+        for (int i = 0; i < 4; i++) sv[i] = state == 1 ? (double)lcv[i] : 0.0;
+        bool leader = group_sum4<double>(key, sv);
+        if (leader && state == 1) {
 #pragma unroll
-            for (int i = 0; i < 4; i++) atomicAdd(&den[con[i]], s[i]);
+            for (int i = 0; i < 4; i++) atomicAdd(&den[con[i]], sv[i]);
         }
     }
-    // walk statistics
     int hsum = __reduce_add_sync(0xffffffffu, hops);
     int hmax = __reduce_max_sync(0xffffffffu, hops);
-    if (lane == 0 && hsum) {
-        atomicAdd(&counters[C_HOPS], (unsigned long long)hsum);
-        atomicMax(&counters[C_MAX_HOPS], (unsigned long long)hmax);
-    }
-    // stable rank of the kept particles
-    bool keep = keep_state != 0;
-    unsigned kb = __ballot_sync(0xffffffffu, keep);
-    if (lane == 0) s_wc[warp] = __popc(kb);
-    __syncthreads();
-    if (warp == 0) {
-        // exclusive scan of the warp counts, then the look-back, by warp 0
-        int c = lane < PUSH_THREADS / 32 ? s_wc[lane] : 0;
-        int incl = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
+    int exits = __popc(__ballot_sync(0xffffffffu, state == 3));
+    if (lane == 0) {
+        if (hsum) {
+            atomicAdd(&counters[C_HOPS], (unsigned long long)hsum);
+            atomicMax(&counters[C_MAX_HOPS], (unsigned long long)hmax);
         }
-        long long run = __shfl_sync(0xffffffffu, incl, 31);
-        if (lane < PUSH_THREADS / 32) s_wc[lane] = incl - c;
-        long long excl = lookback_warp(status, tile, run, counters);
-        if (lane == 0) {
-            *s_base = excl;
-            if (tile == n_tiles - 1) counters[C_N_OUT] = (unsigned long long)(excl + run);
+        if (exits) {
+            atomicAdd(&counters[C_EXITS], (unsigned long long)exits);
+            atomicAdd(&counters[C_DEAD], (unsigned long long)exits);
         }
     }
-    __syncthreads();
-    long long idx = keep ? *s_base + s_wc[warp] + __popc(kb & lanemask_lt()) : -1;
-    return idx;
 }
 
 __global__ void __launch_bounds__(PUSH_THREADS) k_push_fp64(PushF64Args a) {
-    __shared__ long long s_tile;
-    __shared__ int s_wc[PUSH_THREADS / 32];
-    __shared__ long long s_base;
     const long long n = (long long)a.counters[C_N];
-    const long long n_tiles = (n + PUSH_THREADS - 1) / PUSH_THREADS;
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(&a.counters[C_TILE], 1ull);
-        __syncthreads();
-        const long long tile = s_tile;
-        if (tile >= n_tiles) break;
-        const long long i = tile * PUSH_THREADS + threadIdx.x;
+    for (long long base = (long long)blockIdx.x * PUSH_THREADS; base < n; base += (long long)gridDim.x * PUSH_THREADS) {
+        const long long i = base + threadIdx.x;
         int state = 0, cell = -1, hops = 0;
         int con[4] = {0, 0, 0, 0};
         double lc[4] = {0, 0, 0, 0};
         double x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 0;
-        long long id = 0;
-        if (i < n) {
-            x = a.in.px[i]; y = a.in.py[i]; z = a.in.pz[i];
-            vx = a.in.vx[i]; vy = a.in.vy[i]; vz = a.in.vz[i];
-            cell = a.in.cell[i];
-            if (a.track_ids) id = a.in.id[i];
+        if (i < n) cell = a.p.cell[i];
+        if (cell >= 0) {
+            x = a.p.px[i]; y = a.p.py[i]; z = a.p.pz[i];
+            vx = a.p.vx[i]; vy = a.p.vy[i]; vz = a.p.vz[i];
             const TetRec *t = a.tets + cell;
             // v += q_over_m*ef*dt ; x += v*dt  (src/mini-pic.cpp:291-295)
             vx = __dadd_rn(vx, __dmul_rn(__dmul_rn(a.qm, __ldg(&t->ef[0])), a.dt));
@@ -308,21 +221,17 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_push_fp64(PushF64Args a) {
                 const int4 c4 = __ldg(reinterpret_cast<const int4 *>(a.tets[cell].con));
                 con[0] = c4.x; con[1] = c4.y; con[2] = c4.z; con[3] = c4.w;
             } else if (w == -1) {
-                state = 2;  // kept, not scattered, error raised
+                state = 2;  // kept where the walk stopped, not scattered, error raised
                 atomicOr(&a.counters[C_FLAGS], FLAG_WALK_LIMIT);
             } else {
+                state = 3;
                 cell = -1;
             }
+            a.p.px[i] = x; a.p.py[i] = y; a.p.pz[i] = z;
+            a.p.vx[i] = vx; a.p.vy[i] = vy; a.p.vz[i] = vz;
+            a.p.cell[i] = cell;
         }
-        long long o = scatter_and_rank<double>(state, cell, con, lc, a.den, a.den_fixed, a.fixed, tile, a.status,
-                                               a.counters, hops, n_tiles, s_wc, &s_base);
-        if (o >= 0) {
-            a.out.px[o] = x; a.out.py[o] = y; a.out.pz[o] = z;
-            a.out.vx[o] = vx; a.out.vy[o] = vy; a.out.vz[o] = vz;
-            a.out.cell[o] = cell;
-            if (a.track_ids) a.out.id[o] = id;
-        }
-        __syncthreads();
+        scatter_warp<double>(state, cell, con, lc, a.den, a.den_fixed, a.fixed, a.counters, hops);
     }
 }
 
@@ -350,27 +259,17 @@ __device__ __forceinline__ void load_x0(const double *__restrict__ x0, int cell,
 }
 
 __global__ void __launch_bounds__(PUSH_THREADS) k_push_mixed(PushF32Args a) {
-    __shared__ long long s_tile;
-    __shared__ int s_wc[PUSH_THREADS / 32];
-    __shared__ long long s_base;
     const long long n = (long long)a.counters[C_N];
-    const long long n_tiles = (n + PUSH_THREADS - 1) / PUSH_THREADS;
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(&a.counters[C_TILE], 1ull);
-        __syncthreads();
-        const long long tile = s_tile;
-        if (tile >= n_tiles) break;
-        const long long i = tile * PUSH_THREADS + threadIdx.x;
+    for (long long base = (long long)blockIdx.x * PUSH_THREADS; base < n; base += (long long)gridDim.x * PUSH_THREADS) {
+        const long long i = base + threadIdx.x;
         int state = 0, cell = -1, hops = 0, near = 0;
         int con[4] = {0, 0, 0, 0};
         float lc[4] = {0, 0, 0, 0};
         float rx = 0, ry = 0, rz = 0, vx = 0, vy = 0, vz = 0;
-        long long id = 0;
-        if (i < n) {
-            rx = a.in.rx[i]; ry = a.in.ry[i]; rz = a.in.rz[i];
-            vx = a.in.vx[i]; vy = a.in.vy[i]; vz = a.in.vz[i];
-            cell = a.in.cell[i];
-            if (a.track_ids) id = a.in.id[i];
+        if (i < n) cell = a.p.cell[i];
+        if (cell >= 0) {
+            rx = a.p.rx[i]; ry = a.p.ry[i]; rz = a.p.rz[i];
+            vx = a.p.vx[i]; vy = a.p.vy[i]; vz = a.p.vz[i];
             const TetRec32 *t = a.tets32 + cell;
             vx = fmaf(a.qm_dt, __ldg(&t->ef[0]), vx);
             vy = fmaf(a.qm_dt, __ldg(&t->ef[1]), vy);
@@ -423,6 +322,7 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_push_mixed(PushF32Args a) {
                 }
                 int nb = __ldg(&tc->cell_con[min_i]);
                 if (nb < 0) {
+                    state = 3;
                     cell = -1;
                     break;
                 }
@@ -445,27 +345,21 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_push_mixed(PushF32Args a) {
                 const int4 c4 = __ldg(reinterpret_cast<const int4 *>(a.tets32[cell].con));
                 con[0] = c4.x; con[1] = c4.y; con[2] = c4.z; con[3] = c4.w;
             }
+            a.p.rx[i] = rx; a.p.ry[i] = ry; a.p.rz[i] = rz;
+            a.p.vx[i] = vx; a.p.vy[i] = vy; a.p.vz[i] = vz;
+            a.p.cell[i] = cell;
         }
         int nsum = __reduce_add_sync(0xffffffffu, near);
         if ((threadIdx.x & 31) == 0 && nsum) atomicAdd(&a.counters[C_NEAR], (unsigned long long)nsum);
-        long long o = scatter_and_rank<float>(state, cell, con, lc, a.den, a.den_fixed, a.fixed, tile, a.status,
-                                              a.counters, hops, n_tiles, s_wc, &s_base);
-        if (o >= 0) {
-            a.out.rx[o] = rx; a.out.ry[o] = ry; a.out.rz[o] = rz;
-            a.out.vx[o] = vx; a.out.vy[o] = vy; a.out.vz[o] = vz;
-            a.out.cell[o] = cell;
-            if (a.track_ids) a.out.id[o] = id;
-        }
-        __syncthreads();
+        scatter_warp<float>(state, cell, con, lc, a.den, a.den_fixed, a.fixed, a.counters, hops);
     }
 }
 
 // den[n] *= spwt/node_volume[n] (src/mini-pic.cpp:319); fixed-point sums are
-// converted first.  Also publishes the new particle count.
+// converted first.
 __global__ void k_normalise(int n_nodes, double *den, const unsigned long long *den_fixed, int fixed,
                             const double *__restrict__ vol, double spwt, unsigned long long *counters) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i == 0) counters[C_N] = counters[C_N_OUT];
     if (i < n_nodes) {
         double v = fixed ? (double)den_fixed[i] * (1.0 / FIXED_SCALE) : den[i];
         den[i] = __dmul_rn(v, __ddiv_rn(spwt, vol[i]));
@@ -480,69 +374,150 @@ static int grid_for(mp_ctx *ctx, const void *kernel, int threads, size_t smem) {
 }
 
 int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
-    // stats words N_OUT, TILE, HOPS, MAX_HOPS, NEAR are per push
-    MP_CUDA(ctx, cudaMemsetAsync(ctx->counters + C_N_OUT, 0, 5 * sizeof(unsigned long long), ctx->stream));
-    long long n_ub = ctx->n_host;
-    long long tiles = (n_ub + PUSH_THREADS - 1) / PUSH_THREADS;
-    if (tiles < 1) tiles = 1;
-    if (tiles > ctx->tile_status_len) {
-        if (ctx->tile_status) cudaFree(ctx->tile_status);
-        ctx->tile_status = nullptr;
-        long long len = tiles * 2;
-        MP_CUDA(ctx, cudaMalloc(&ctx->tile_status, len * sizeof(unsigned long long)));
-        ctx->tile_status_len = len;
-    }
-    MP_CUDA(ctx, cudaMemsetAsync(ctx->tile_status, 0, tiles * sizeof(unsigned long long), ctx->stream));
+    // per-push statistics words
+    MP_CUDA(ctx, cudaMemsetAsync(ctx->counters + C_EXITS, 0, 4 * sizeof(unsigned long long), ctx->stream));
     if (ctx->scatter_mode == MP_SCATTER_FIXED64)
         MP_CUDA(ctx, cudaMemsetAsync(ctx->den_fixed, 0, ctx->n_nodes * sizeof(unsigned long long), ctx->stream));
     else
         MP_CUDA(ctx, cudaMemsetAsync(ctx->den, 0, ctx->n_nodes * sizeof(double), ctx->stream));
-    int nxt = ctx->cur ^ 1;
+    long long blocks = (ctx->n_host + PUSH_THREADS - 1) / PUSH_THREADS;
+    if (blocks < 1) blocks = 1;
     if (ctx->form == MP_FORM_FP64) {
         PushF64Args a;
-        a.in = ctx->p64[ctx->cur];
-        a.out = ctx->p64[nxt];
+        a.p = ctx->p64[ctx->cur];
         a.tets = ctx->tets;
         a.den = ctx->den;
         a.den_fixed = ctx->den_fixed;
         a.counters = ctx->counters;
-        a.status = ctx->tile_status;
         a.qm = q_over_m;
         a.dt = dt;
         a.walk_limit = ctx->walk_limit;
         a.fixed = ctx->scatter_mode == MP_SCATTER_FIXED64;
         a.track_ids = ctx->track_ids;
-        if (!ctx->push_grid[0]) ctx->push_grid[0] = grid_for(ctx, (const void *)k_push_fp64, PUSH_THREADS, 0);
-        int grid = ctx->push_grid[0];
-        long long g = tiles < grid ? tiles : grid;
+        if (!ctx->push_grid[0]) ctx->push_grid[0] = grid_for(ctx, (const void *)k_push_fp64, PUSH_THREADS, 0) * 8;
+        long long g = blocks < ctx->push_grid[0] ? blocks : ctx->push_grid[0];
         cudaEventRecord(ctx->tp.a, ctx->stream);
         k_push_fp64<<<(unsigned)g, PUSH_THREADS, 0, ctx->stream>>>(a), ++ctx->launches;
         cudaEventRecord(ctx->tp.b, ctx->stream);
     } else {
         PushF32Args a;
-        a.in = ctx->p32[ctx->cur];
-        a.out = ctx->p32[nxt];
+        a.p = ctx->p32[ctx->cur];
         a.tets32 = ctx->tets32;
         a.tets = ctx->tets;
         a.x0 = ctx->tet_x0;
         a.den = ctx->den;
         a.den_fixed = ctx->den_fixed;
         a.counters = ctx->counters;
-        a.status = ctx->tile_status;
         a.qm_dt = (float)(q_over_m * dt);
         a.dt = (float)dt;
         a.walk_limit = ctx->walk_limit;
         a.fixed = ctx->scatter_mode == MP_SCATTER_FIXED64;
         a.track_ids = ctx->track_ids;
-        if (!ctx->push_grid[1]) ctx->push_grid[1] = grid_for(ctx, (const void *)k_push_mixed, PUSH_THREADS, 0);
-        int grid = ctx->push_grid[1];
-        long long g = tiles < grid ? tiles : grid;
+        if (!ctx->push_grid[1]) ctx->push_grid[1] = grid_for(ctx, (const void *)k_push_mixed, PUSH_THREADS, 0) * 8;
+        long long g = blocks < ctx->push_grid[1] ? blocks : ctx->push_grid[1];
         cudaEventRecord(ctx->tp.a, ctx->stream);
         k_push_mixed<<<(unsigned)g, PUSH_THREADS, 0, ctx->stream>>>(a), ++ctx->launches;
         cudaEventRecord(ctx->tp.b, ctx->stream);
     }
     MP_CUDA(ctx, cudaGetLastError());
+    return MP_OK;
+}
+
+// ---- stable removal of holes -----------------------------------------------------------
+constexpr int COMPACT_THREADS = 256;
+constexpr int COMPACT_ITEMS = 4;  // particles per thread per block
+constexpr int COMPACT_TILE = COMPACT_THREADS * COMPACT_ITEMS;
+
+__global__ void k_compact_count(long long n, const int *__restrict__ cell, int *block_count) {
+    __shared__ int s_w[COMPACT_THREADS / 32];
+    long long base = (long long)blockIdx.x * COMPACT_TILE;
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < COMPACT_ITEMS; k++) {
+        long long i = base + k * COMPACT_THREADS + threadIdx.x;
+        c += (i < n && cell[i] >= 0) ? 1 : 0;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < COMPACT_THREADS / 32; w++) t += s_w[w];
+        block_count[blockIdx.x] = t;
+    }
+}
+
+// Writes the live particles of each block, in order, at the block's offset.
+template <typename P>
+__global__ void k_compact_scatter(long long n, P in, P out, const int *__restrict__ block_off, int track_ids) {
+    __shared__ int s_w[COMPACT_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long base = (long long)blockIdx.x * COMPACT_TILE;
+    int run = block_off[blockIdx.x];
+#pragma unroll 1
+    for (int k = 0; k < COMPACT_ITEMS; k++) {
+        long long i = base + k * COMPACT_THREADS + threadIdx.x;
+        bool live = i < n && in.cell[i] >= 0;
+        unsigned b = __ballot_sync(0xffffffffu, live);
+        if (lane == 0) s_w[warp] = __popc(b);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < COMPACT_THREADS / 32; w++) {
+            int c = s_w[w];
+            if (w < warp) before += c;
+            total += c;
+        }
+        if (live) {
+            long long o = run + before + __popc(b & lanemask_lt());
+            if constexpr (sizeof(*in.vx) == 8) {
+                out.px[o] = in.px[i]; out.py[o] = in.py[i]; out.pz[o] = in.pz[i];
+            } else {
+                out.rx[o] = in.rx[i]; out.ry[o] = in.ry[i]; out.rz[o] = in.rz[i];
+            }
+            out.vx[o] = in.vx[i]; out.vy[o] = in.vy[i]; out.vz[o] = in.vz[i];
+            out.cell[o] = in.cell[i];
+            if (track_ids) out.id[o] = in.id[i];
+        }
+        run += total;
+        __syncthreads();
+    }
+}
+
+__global__ void k_set_counts(unsigned long long *counters, long long live) {
+    counters[C_N] = (unsigned long long)live;
+    counters[C_DEAD] = 0;
+}
+
+// Exclusive scan of hist[0..m) in place, one block (defined below).
+__global__ void k_scan_single(int m, int *hist);
+
+// Requires ctx->n_host and ctx->dead_host to be exact (after a counter sync).
+int launch_compact(mp_ctx *ctx) {
+    long long n = ctx->n_host;
+    long long live = n - ctx->dead_host;
+    if (ctx->dead_host == 0) return MP_OK;
+    long long blocks = (n + COMPACT_TILE - 1) / COMPACT_TILE;
+    if (!ctx->compact_off || ctx->compact_len < blocks + 1) {
+        if (ctx->compact_off) cudaFree(ctx->compact_off);
+        ctx->compact_off = nullptr;
+        MP_CUDA(ctx, cudaMalloc(&ctx->compact_off, sizeof(int) * (blocks + 1) * 2));
+        ctx->compact_len = (blocks + 1) * 2;
+    }
+    int nxt = ctx->cur ^ 1;
+    const int *cell = ctx->form == MP_FORM_FP64 ? ctx->p64[ctx->cur].cell : ctx->p32[ctx->cur].cell;
+    k_compact_count<<<(unsigned)blocks, COMPACT_THREADS, 0, ctx->stream>>>(n, cell, ctx->compact_off), ++ctx->launches;
+    k_scan_single<<<1, 1024, 0, ctx->stream>>>((int)blocks, ctx->compact_off), ++ctx->launches;
+    if (ctx->form == MP_FORM_FP64)
+        k_compact_scatter<PartsF64><<<(unsigned)blocks, COMPACT_THREADS, 0, ctx->stream>>>(
+            n, ctx->p64[ctx->cur], ctx->p64[nxt], ctx->compact_off, ctx->track_ids), ++ctx->launches;
+    else
+        k_compact_scatter<PartsF32><<<(unsigned)blocks, COMPACT_THREADS, 0, ctx->stream>>>(
+            n, ctx->p32[ctx->cur], ctx->p32[nxt], ctx->compact_off, ctx->track_ids), ++ctx->launches;
+    k_set_counts<<<1, 1, 0, ctx->stream>>>(ctx->counters, live), ++ctx->launches;
+    MP_CUDA(ctx, cudaGetLastError());
     ctx->cur = nxt;
+    ctx->n_host = live;
+    ctx->dead_host = 0;
     return MP_OK;
 }
 
@@ -666,7 +641,7 @@ int launch_download_pack(mp_ctx *ctx, long long n, double *out_soa, int *cell_ou
 
 __global__ void k_hist(long long n, const int *__restrict__ cell, int *hist) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n) atomicAdd(&hist[cell[i]], 1);
+    if (i < n && cell[i] >= 0) atomicAdd(&hist[cell[i]], 1);
 }
 
 // exclusive scan of hist[0..m) in place, one block
@@ -701,6 +676,7 @@ __global__ void k_sort_scatter(long long n, P in, P out, int *cursor, int track_
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= n) return;
     int c = in.cell[i];
+    if (c < 0) return;
     int o = atomicAdd(&cursor[c], 1);
     if constexpr (sizeof(*in.vx) == 8) {
         out.px[o] = in.px[i]; out.py[o] = in.py[i]; out.pz[o] = in.pz[i];
@@ -729,8 +705,12 @@ int launch_sort_by_tet(mp_ctx *ctx) {
     else
         k_sort_scatter<PartsF32><<<(unsigned)bl, th, 0, ctx->stream>>>(n, ctx->p32[ctx->cur], ctx->p32[nxt],
                                                                       ctx->sort_hist, ctx->track_ids), ++ctx->launches;
+    long long live = n - ctx->dead_host;
+    k_set_counts<<<1, 1, 0, ctx->stream>>>(ctx->counters, live), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     ctx->cur = nxt;
+    ctx->n_host = live;
+    ctx->dead_host = 0;
     return MP_OK;
 }
 
