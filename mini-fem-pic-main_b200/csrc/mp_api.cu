@@ -54,6 +54,7 @@ static int grow_particles(mp_ctx *ctx, long long need) {
     if (need <= ctx->capacity) return MP_OK;
     long long cap = std::max<long long>(need, 2 * ctx->capacity);
     cap = std::max<long long>(cap, 1024);
+    cap = (cap + 255) & ~255ll;  // whole 256-particle tiles: the push's bulk copies may round up to 16 B
     void *nb[2] = {nullptr, nullptr};
     for (int k = 0; k < 2; k++) {
         cudaError_t e = cudaMalloc(&nb[k], block_bytes(cap));
