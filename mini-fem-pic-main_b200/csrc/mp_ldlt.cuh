@@ -20,6 +20,7 @@
 #include <cmath>
 
 #include "mp_internal.h"
+#include "mp_tc.cuh"
 
 namespace mp {
 
@@ -30,104 +31,146 @@ __device__ __forceinline__ bool bad_pivot(T d) {
     return !(fabs((double)d) > 0.0) || !isfinite((double)d);
 }
 
-// Factor the kb x kb diagonal block at (k0,k0); write L (strict lower) back,
-// D into dvec, and z_k = L_kk^-1 b_k into b (b may be null).
+// Factor the kb x kb diagonal block at (k0,k0) in shared memory with one warp:
+// L (strict lower) and D written back, and Linv = L_kk^-1 (unit lower, row-major
+// kb x NB) for the panel.  If b is non-null, z_k = L_kk^-1 b_k (forward
+// substitution riding on the factorization).  Dynamic smem: 2 (NB x NB+1) tiles.
 template <typename T>
-__global__ void k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *b,
-                            unsigned long long *flags) {
-    __shared__ T s[NB][NB + 1];
-    __shared__ T s_w[NB];
+__global__ void __launch_bounds__(128) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
+                                                   T *b, unsigned long long *flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T(*s)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
+    T(*si)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw + sizeof(T) * NB * (NB + 1));
+    T *sl = reinterpret_cast<T *>(smem_raw + sizeof(T) * 2 * NB * (NB + 1));
+    T *sb = sl + NB;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
         int r = idx / kb, c = idx % kb;
         s[r][c] = c <= r ? A[(long long)(k0 + r) * ld + k0 + c] : T(0);
     }
+    if (b && threadIdx.x < kb) sb[threadIdx.x] = b[k0 + threadIdx.x];
     __syncthreads();
-    for (int j = 0; j < kb; j++) {
-        T d = s[j][j];
-        bool bad = bad_pivot(d);
-        for (int i = j + 1 + threadIdx.x; i < kb; i += blockDim.x) s_w[i] = s[i][j];
-        __syncthreads();
-        if (bad) {
-            if (threadIdx.x == 0) atomicOr(flags, FLAG_SINGULAR);
-            d = T(1);
+    if (warp == 0) {
+        for (int j = 0; j < kb; j++) {
+            T d = s[j][j];
+            if (bad_pivot(d)) {
+                if (lane == 0) atomicOr(flags, FLAG_SINGULAR);
+                d = T(1);
+            }
+            for (int i = j + 1 + lane; i < kb; i += 32) sl[i] = s[i][j] / d;
+            __syncwarp();
+            for (int i = j + 1 + lane; i < kb; i += 32) {
+                const T li = sl[i];
+                for (int l = j + 1; l <= i; l++) s[i][l] -= li * s[l][j];
+            }
+            __syncwarp();
+            for (int i = j + 1 + lane; i < kb; i += 32) s[i][j] = sl[i];
+            __syncwarp();
         }
-        // rank-1 update of the remaining lower triangle
-        int m = kb - j - 1;
-        for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
-            int i = j + 1 + idx / m, l = j + 1 + idx % m;
-            if (l <= i) s[i][l] -= (s_w[i] / d) * s_w[l];
-        }
-        __syncthreads();
-        for (int i = j + 1 + threadIdx.x; i < kb; i += blockDim.x) s[i][j] = s_w[i] / d;
-        __syncthreads();
     }
+    __syncthreads();
+    // Linv column q by forward substitution on e_q
+    if (threadIdx.x < kb) {
+        const int q = threadIdx.x;
+        for (int i = 0; i < q; i++) si[i][q] = T(0);
+        si[q][q] = T(1);
+        for (int i = q + 1; i < kb; i++) {
+            T acc = 0;
+            for (int pp = q; pp < i; pp++) acc += s[i][pp] * si[pp][q];
+            si[i][q] = -acc;
+        }
+    }
+    __syncthreads();
     for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
         int r = idx / kb, c = idx % kb;
-        if (c < r) A[(long long)(k0 + r) * ld + k0 + c] = s[r][c];
-        else if (c == r) A[(long long)(k0 + r) * ld + k0 + c] = s[r][r];
+        if (c <= r) A[(long long)(k0 + r) * ld + k0 + c] = s[r][c];
+        Linv[r * NB + c] = si[r][c];
     }
-    if (threadIdx.x < kb) dvec[k0 + threadIdx.x] = s[threadIdx.x][threadIdx.x];
-    if (b && threadIdx.x == 0) {
-        for (int c = 0; c < kb; c++) {
-            T x = b[k0 + c];
-            for (int p = 0; p < c; p++) x -= s[c][p] * b[k0 + p];
-            b[k0 + c] = x;
+    if (threadIdx.x < kb) {
+        dvec[k0 + threadIdx.x] = s[threadIdx.x][threadIdx.x];
+        if (b) {
+            const int i = threadIdx.x;
+            T z = 0;
+            for (int pp = 0; pp <= i; pp++) z += si[i][pp] * sb[pp];
+            b[k0 + i] = z;
         }
     }
 }
 
-// Panel: rows [r0, r0+64) below the diagonal block.  Dynamic smem: L_kk [NB][NB]
-// plus the CTA's rows [64][NB+1].
+// Panel: rows [r0, r0+64) below the diagonal block.  W = A_ik L_kk^-T (a small
+// product with Linv), L_ik = W D^-1, and b_i -= L_ik z_k.  Dynamic smem: the
+// rows' panel [64][NB+1] and Linv [NB][NB+1].
 template <typename T>
-__global__ void k_ldlt_panel(int n, long long ld, T *A, int k0, int kb, const T *dvec, T *W, T *b) {
-    extern __shared__ unsigned char smem_raw[];
-    T *sL = reinterpret_cast<T *>(smem_raw);           // [NB][NB]
-    T *sR = sL + NB * NB;                               // [64][NB+1]
+__global__ void __launch_bounds__(256) k_ldlt_panel(int n, long long ld, T *A, int k0, int kb, const T *dvec,
+                                                    const T *Linv, T *W, int ldw, T *b) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T(*sA)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
+    T(*sI)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw + sizeof(T) * 64 * (NB + 1));
+    T *sd = reinterpret_cast<T *>(smem_raw + sizeof(T) * 2 * 64 * (NB + 1));
+    T *sz = sd + NB;
     const int r0 = k0 + kb + blockIdx.x * 64;
+    for (int idx = threadIdx.x; idx < 64 * kb; idx += blockDim.x) {
+        int r = idx / kb, c = idx % kb;
+        int row = r0 + r;
+        sA[r][c] = row < n ? A[(long long)row * ld + k0 + c] : T(0);
+    }
     for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
         int r = idx / kb, c = idx % kb;
-        sL[r * NB + c] = c < r ? A[(long long)(k0 + r) * ld + k0 + c] : T(0);
+        sI[r][c] = Linv[r * NB + c];
     }
-    for (int idx = threadIdx.x; idx < 64 * kb; idx += blockDim.x) {
-        int r = idx / kb, c = idx % kb;
-        int row = r0 + r;
-        sR[r * (NB + 1) + c] = row < n ? A[(long long)row * ld + k0 + c] : T(0);
-    }
-    __syncthreads();
-    if (threadIdx.x < 64) {
-        int r = threadIdx.x;
-        T *x = sR + r * (NB + 1);
-        for (int c = 0; c < kb; c++) {
-            T v = x[c];
-            for (int p = 0; p < c; p++) v -= x[p] * sL[c * NB + p];
-            x[c] = v;
-        }
+    if (threadIdx.x < kb) {
+        sd[threadIdx.x] = dvec[k0 + threadIdx.x];
+        if (b) sz[threadIdx.x] = b[k0 + threadIdx.x];
     }
     __syncthreads();
-    // write W (= L D) and L, and the forward-substitution update of b
-    for (int idx = threadIdx.x; idx < 64 * kb; idx += blockDim.x) {
-        int r = idx / kb, c = idx % kb;
-        int row = r0 + r;
-        if (row < n) {
-            T w = sR[r * (NB + 1) + c];
-            W[(long long)row * NB + c] = w;
-            A[(long long)row * ld + k0 + c] = w / dvec[k0 + c];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 4 rows x 4 cols each
+    T acc[4][4] = {};
+    for (int pp = 0; pp < kb; pp++) {
+        T a[4], w[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) a[u] = sA[ty * 4 + u][pp];
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            int c = tx * 4 + v;
+            w[v] = (c < kb && pp <= c) ? sI[c][pp] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], w[v], acc[u][v]);
+    }
+    T bsum[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const int row = r0 + ty * 4 + u;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const int c = tx * 4 + v;
+            if (row < n && c < kb) {
+                const T wv = acc[u][v];
+                const T lv = wv / sd[c];
+                W[(long long)row * ldw + c] = wv;
+                A[(long long)row * ld + k0 + c] = lv;
+                if (b) bsum[u] += lv * sz[c];
+            }
         }
     }
-    if (b && threadIdx.x < 64) {
-        int r = threadIdx.x, row = r0 + r;
-        if (row < n) {
-            T acc = 0;
-            for (int c = 0; c < kb; c++) acc += (sR[r * (NB + 1) + c] / dvec[k0 + c]) * b[k0 + c];
-            b[row] -= acc;
+    if (b) {
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            T v = bsum[u];
+            for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            const int row = r0 + ty * 4 + u;
+            if (tx == 0 && row < n) b[row] -= v;
         }
     }
 }
 
 // Trailing update of the lower 64x64 tiles: A_ij -= L_i W_j^T over p < kb.
 template <typename T>
-__global__ void __launch_bounds__(256) k_ldlt_update(int n, long long ld, T *A, int k0, int kb, const T *W, int k1) {
-    extern __shared__ unsigned char smem_raw[];
+__global__ void __launch_bounds__(256) k_ldlt_update(int n, long long ld, T *A, int k0, int kb, const T *W, int ldw,
+                                                     int k1) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     T *sLt = reinterpret_cast<T *>(smem_raw);   // [NB][64+pad] transposed: sLt[p][r]
     T *sWt = sLt + NB * 68;                      // [NB][68]
     long long bidx = blockIdx.x;
@@ -140,7 +183,7 @@ __global__ void __launch_bounds__(256) k_ldlt_update(int n, long long ld, T *A, 
         int r = idx / NB, p = idx % NB;
         int ri = i0 + r, rj = j0 + r;
         sLt[p * 68 + r] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : T(0);
-        sWt[p * 68 + r] = (p < kb && rj < n) ? W[(long long)rj * NB + p] : T(0);
+        sWt[p * 68 + r] = (p < kb && rj < n) ? W[(long long)rj * ldw + p] : T(0);
     }
     __syncthreads();
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -168,124 +211,259 @@ __global__ void __launch_bounds__(256) k_ldlt_update(int n, long long ld, T *A, 
     }
 }
 
-// z <- D^-1 z
+// Update restricted to the columns [k1, jend) of the current outer panel:
+// A_ij -= L_i W_j^T for rows i in [k1, n), 64x64 tiles, grid (col tile, row tile).
 template <typename T>
-__global__ void k_diag_scale(int n, const T *dvec, T *z) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) z[i] /= dvec[i];
-}
-
-// Backward substitution step for block column k: s[c] = sum_{i>=k1} L[i][k0+c] y[i]
-template <typename T>
-__global__ void k_bwd_partial(int n, long long ld, const T *A, int k0, int kb, int k1, const T *y, T *s) {
-    __shared__ T red[8][NB];
-    int c = threadIdx.x & 63;
-    int g = threadIdx.x >> 6;  // 4 row groups of 64 threads
-    T acc = 0;
-    if (c < kb)
-        for (int i = k1 + blockIdx.x * 4 + g; i < n; i += gridDim.x * 4) acc += A[(long long)i * ld + k0 + c] * y[i];
-    red[g][c] = acc;
-    __syncthreads();
-    if (g == 0 && c < kb) {
-        T t = red[0][c] + red[1][c] + red[2][c] + red[3][c];
-        atomicAdd(&s[c], t);
-    }
-}
-
-template <typename T>
-__global__ void k_bwd_diag(long long ld, const T *A, int k0, int kb, T *y, T *s) {
-    __shared__ T sL[NB][NB + 1];
-    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
-        int r = idx / kb, c = idx % kb;
-        sL[r][c] = c < r ? A[(long long)(k0 + r) * ld + k0 + c] : T(0);
+__global__ void __launch_bounds__(256) k_ldlt_update_cols(int n, long long ld, T *A, int k0, int kb, const T *W,
+                                                          int ldw, int k1, int jend) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *sLt = reinterpret_cast<T *>(smem_raw);
+    T *sWt = sLt + NB * 68;
+    const int i0 = k1 + blockIdx.y * 64, j0 = k1 + blockIdx.x * 64;
+    if (j0 > i0 + 63 || j0 >= jend) return;  // tile entirely above the diagonal or outside the panel
+    for (int idx = threadIdx.x; idx < 64 * NB; idx += blockDim.x) {
+        int r = idx / NB, p = idx % NB;
+        int ri = i0 + r, rj = j0 + r;
+        sLt[p * 68 + r] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : T(0);
+        sWt[p * 68 + r] = (p < kb && rj < jend) ? W[(long long)rj * ldw + p] : T(0);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int c = kb - 1; c >= 0; c--) {
-            T v = y[k0 + c] - s[c];
-            for (int r = c + 1; r < kb; r++) v -= sL[r][c] * y[k0 + r];
-            y[k0 + c] = v;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    T acc[4][4] = {};
+    for (int p = 0; p < kb; p++) {
+        T a[4], w[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) a[u] = sLt[p * 68 + ty * 4 + u];
+#pragma unroll
+        for (int v = 0; v < 4; v++) w[v] = sWt[p * 68 + tx * 4 + v];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], w[v], acc[u][v]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        int i = i0 + ty * 4 + u;
+        if (i >= n) continue;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            int j = j0 + tx * 4 + v;
+            if (j < jend && j <= i) A[(long long)i * ld + j] -= acc[u][v];
         }
     }
-    __syncthreads();
-    if (threadIdx.x < NB) s[threadIdx.x] = 0;
 }
 
-// Forward substitution with an existing factor (refinement solves).
+// ---- triangular solves with an existing factor --------------------------------------
+// One persistent launch per direction.  CTA g takes row blocks g, g+G, ... (in
+// solve order); a block first subtracts the contributions of the blocks already
+// solved (each published by a per-block ready word holding the solve's epoch),
+// then solves its unit-triangular diagonal block with one warp.  The grid never
+// exceeds the resident capacity, so the lowest unsolved block always runs.
+// Waits are bounded (TRSV_SPIN_LIMIT polls); a timeout sets the error flag.
+constexpr long long TRSV_SPIN_LIMIT = 1ll << 20;
+
+__device__ __forceinline__ bool wait_ready(const int *ready, int blk, int epoch, unsigned long long *flags) {
+    long long spins = 0;
+    while (*(volatile const int *)&ready[blk] != epoch) {
+        if (++spins > TRSV_SPIN_LIMIT) {
+            atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    __threadfence();
+    return true;
+}
+
+// L z = b (unit lower, in place on x)
 template <typename T>
-__global__ void k_fwd_diag(long long ld, const T *A, int k0, int kb, T *b) {
-    if (threadIdx.x != 0) return;
-    for (int c = 0; c < kb; c++) {
-        T x = b[k0 + c];
-        for (int p = 0; p < c; p++) x -= A[(long long)(k0 + c) * ld + k0 + p] * b[k0 + p];
-        b[k0 + c] = x;
+__global__ void __launch_bounds__(256) k_trsv_fwd(int n, long long ld, const T *A, T *x, int *ready, int epoch,
+                                                  unsigned long long *flags) {
+    __shared__ T sL[NB][NB + 1];
+    __shared__ T sx[NB], srhs[NB];
+    __shared__ T spart[4][NB];
+    const int nblk = (n + NB - 1) / NB;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
+        const int r = t >> 2, q = t & 3;  // row, quarter of the 64 columns
+        T acc = 0;
+        for (int c = 0; c < blk; c++) {
+            if (t == 0) wait_ready(ready, c, epoch, flags);
+            __syncthreads();
+            if (t < NB) sx[t] = __ldcg(&x[c * NB + t]);  // written by another CTA: bypass L1
+            __syncthreads();
+            if (r < kb) {
+                const T *row = A + (long long)(r0 + r) * ld + c * NB + q * 16;
+#pragma unroll
+                for (int k = 0; k < 16; k++) acc += row[k] * sx[q * 16 + k];
+            }
+        }
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        if (q == 0 && r < kb) srhs[r] = x[r0 + r] - acc;
+        for (int idx = t; idx < kb * kb; idx += blockDim.x) {
+            int i = idx / kb, j = idx % kb;
+            sL[i][j] = j < i ? A[(long long)(r0 + i) * ld + r0 + j] : T(0);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            T v0 = lane < kb ? srhs[lane] : T(0), v1 = lane + 32 < kb ? srhs[lane + 32] : T(0);
+            for (int j = 0; j < kb; j++) {
+                T xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
+                if (lane > j && lane < kb) v0 -= sL[lane][j] * xj;
+                if (lane + 32 > j && lane + 32 < kb) v1 -= sL[lane + 32][j] * xj;
+            }
+            if (lane < kb) x[r0 + lane] = v0;
+            if (lane + 32 < kb) x[r0 + lane + 32] = v1;
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) *(volatile int *)&ready[blk] = epoch;
+        }
+        __syncthreads();
     }
 }
 
+// L^T y = D^-1 z (unit upper after scaling, in place on x), blocks from the last
 template <typename T>
-__global__ void k_fwd_rows(int n, long long ld, const T *A, int k0, int kb, int k1, T *b) {
-    int i = k1 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    T acc = 0;
-    for (int c = 0; c < kb; c++) acc += A[(long long)i * ld + k0 + c] * b[k0 + c];
-    b[i] -= acc;
+__global__ void __launch_bounds__(256) k_trsv_bwd(int n, long long ld, const T *A, const T *dvec, T *x, int *ready,
+                                                  int epoch, unsigned long long *flags) {
+    __shared__ T sL[NB][NB + 1];
+    __shared__ T sy[NB], srhs[NB];
+    __shared__ T spart[4][NB];
+    const int nblk = (n + NB - 1) / NB;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    for (int g = blockIdx.x; g < nblk; g += gridDim.x) {
+        const int blk = nblk - 1 - g;
+        const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
+        const int col = t & 63, part = t >> 6;  // column of this block, quarter of the other block's rows
+        T acc = 0;
+        for (int c = nblk - 1; c > blk; c--) {
+            if (t == 0) wait_ready(ready, c, epoch, flags);
+            __syncthreads();
+            const int c0 = c * NB, cb = n - c0 < NB ? n - c0 : NB;
+            if (t < cb) sy[t] = __ldcg(&x[c0 + t]);
+            __syncthreads();
+            if (col < kb)
+                for (int i = part * 16; i < part * 16 + 16 && i < cb; i++)
+                    acc += A[(long long)(c0 + i) * ld + r0 + col] * sy[i];
+        }
+        spart[part][col] = acc;
+        for (int idx = t; idx < kb * kb; idx += blockDim.x) {
+            int i = idx / kb, j = idx % kb;
+            sL[i][j] = j < i ? A[(long long)(r0 + i) * ld + r0 + j] : T(0);
+        }
+        __syncthreads();
+        if (t < kb) srhs[t] = x[r0 + t] / dvec[r0 + t] - (spart[0][t] + spart[1][t] + spart[2][t] + spart[3][t]);
+        __syncthreads();
+        if (warp == 0) {
+            T v0 = lane < kb ? srhs[lane] : T(0), v1 = lane + 32 < kb ? srhs[lane + 32] : T(0);
+            for (int j = kb - 1; j >= 0; j--) {
+                T yj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
+                if (lane < j) v0 -= sL[j][lane] * yj;
+                if (lane + 32 < j) v1 -= sL[j][lane + 32] * yj;
+            }
+            if (lane < kb) x[r0 + lane] = v0;
+            if (lane + 32 < kb) x[r0 + lane + 32] = v1;
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) *(volatile int *)&ready[blk] = epoch;
+        }
+        __syncthreads();
+    }
 }
 
 template <typename T>
 struct LdltWork {
     T *dvec, *W, *s;
+    T *Linv;       // [NB][NB] inverse of the current diagonal block's L
+    int *ready;    // [2][blocks] per-block ready words of the two solves
 };
 
+static int g_solve_epoch = 0;
+
 template <typename T>
-int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> w, bool factor) {
+int trsv_grid(mp_ctx *ctx, const void *kernel, int nblk) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+    if (per_sm < 1) per_sm = 1;
+    int cap = per_sm * ctx->sm_count;  // every CTA resident: the wavefront cannot stall
+    return nblk < cap ? nblk : cap;
+}
+
+template <typename T>
+int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> w, bool factor,
+                      bool tensor_cores = false) {
     cudaStream_t st = ctx->stream;
-    size_t panel_smem = sizeof(T) * (NB * NB + 64 * (NB + 1));
-    size_t upd_smem = sizeof(T) * 2 * NB * 68;
+    const size_t diag_smem = sizeof(T) * (2 * NB * (NB + 1) + 2 * NB);
+    const size_t panel_smem = sizeof(T) * (64 * (NB + 1) + NB * (NB + 1) + 2 * NB);
+    const size_t upd_smem = sizeof(T) * 2 * NB * 68;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_ldlt_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024);
-        cudaFuncSetAttribute(k_ldlt_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024);
-        cudaFuncSetAttribute(k_ldlt_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024);
-        cudaFuncSetAttribute(k_ldlt_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024);
+        const int big = 96 * 1024;
+        cudaFuncSetAttribute(k_ldlt_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(k_ldlt_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(k_ldlt_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(k_ldlt_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(k_ldlt_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(k_ldlt_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(k_ldlt_update_cols<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(k_ldlt_update_cols<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(tc::k_update_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM_BYTES);
         attr = true;
     }
-    if (factor) {
-        for (int k0 = 0; k0 < n; k0 += NB) {
-            int kb = n - k0 < NB ? n - k0 : NB;
-            int k1 = k0 + kb;
-            k_ldlt_diag<T><<<1, 256, 0, st>>>(n, ld, A, k0, kb, w.dvec, b, ctx->counters + C_FLAGS), ++ctx->launches;
-            if (k1 < n) {
-                int rows = n - k1;
-                k_ldlt_panel<T><<<(rows + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, w.W, b), ++ctx->launches;
-                long long tiles = (rows + 63) / 64;
+    unsigned long long *flags = ctx->counters + C_FLAGS;
+    auto diag_and_panel = [&](int k0, int kb, T *W, int ldw) {
+        k_ldlt_diag<T><<<1, 128, diag_smem, st>>>(n, ld, A, k0, kb, w.dvec, w.Linv, b, flags), ++ctx->launches;
+        int k1 = k0 + kb;
+        if (k1 < n)
+            k_ldlt_panel<T><<<(n - k1 + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, w.Linv, W, ldw, b),
+                ++ctx->launches;
+    };
+    if (factor && tensor_cores) {
+        // two-level LDL^T: 256-wide outer panels factored with the 64-wide kernels,
+        // trailing update of each outer panel on the tensor cores
+        const int PW = 256;
+        for (int P0 = 0; P0 < n; P0 += PW) {
+            const int P1 = P0 + PW < n ? P0 + PW : n;
+            for (int k0 = P0; k0 < P1; k0 += NB) {
+                int kb = P1 - k0 < NB ? P1 - k0 : NB;
+                int k1 = k0 + kb;
+                diag_and_panel(k0, kb, w.W + (k0 - P0), PW);
+                if (k1 < n && k1 < P1) {
+                    dim3 g((P1 - k1 + 63) / 64, (n - k1 + 63) / 64);
+                    k_ldlt_update_cols<T><<<g, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W + (k0 - P0), PW, k1, P1),
+                        ++ctx->launches;
+                }
+            }
+            if (P1 < n) {
+                long long tiles = (n - P1 + tc::TILE - 1) / tc::TILE;
                 long long nblk = tiles * (tiles + 1) / 2;
-                k_ldlt_update<T><<<(unsigned)nblk, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W, k1), ++ctx->launches;
+                tc::k_update_tf32<<<(unsigned)nblk, tc::THREADS, tc::SMEM_BYTES, st>>>(
+                    n, ld, reinterpret_cast<float *>(A), P0, P1 - P0, P1, reinterpret_cast<const float *>(w.W), PW,
+                    flags), ++ctx->launches;
             }
         }
-    } else {
-        // forward substitution with an existing factor
+    } else if (factor) {
         for (int k0 = 0; k0 < n; k0 += NB) {
             int kb = n - k0 < NB ? n - k0 : NB;
             int k1 = k0 + kb;
-            // z_k = L_kk^-1 b_k, then b_i -= L_ik z_k
-            k_fwd_diag<T><<<1, 64, 0, st>>>(ld, A, k0, kb, b), ++ctx->launches;
-            if (k1 < n) k_fwd_rows<T><<<(n - k1 + 255) / 256, 256, 0, st>>>(n, ld, A, k0, kb, k1, b), ++ctx->launches;
+            diag_and_panel(k0, kb, w.W, NB);
+            if (k1 < n) {
+                long long tiles = (n - k1 + 63) / 64;
+                long long nblk = tiles * (tiles + 1) / 2;
+                k_ldlt_update<T><<<(unsigned)nblk, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W, NB, k1), ++ctx->launches;
+            }
         }
     }
-    k_diag_scale<T><<<(n + 255) / 256, 256, 0, st>>>(n, w.dvec, b), ++ctx->launches;
-    MP_CUDA(ctx, cudaMemsetAsync(w.s, 0, sizeof(T) * NB, st));
-    int last = ((n - 1) / NB) * NB;
-    for (int k0 = last; k0 >= 0; k0 -= NB) {
-        int kb = n - k0 < NB ? n - k0 : NB;
-        int k1 = k0 + kb;
-        if (k1 < n) {
-            int rows = n - k1;
-            int grid = (rows + 3) / 4;
-            if (grid > ctx->sm_count * 4) grid = ctx->sm_count * 4;
-            k_bwd_partial<T><<<grid, 256, 0, st>>>(n, ld, A, k0, kb, k1, b, w.s), ++ctx->launches;
-        }
-        k_bwd_diag<T><<<1, 64, 0, st>>>(ld, A, k0, kb, b, w.s), ++ctx->launches;
+    const int nblk = (n + NB - 1) / NB;
+    const int epoch = ++g_solve_epoch;
+    if (!factor) {
+        int g = trsv_grid<T>(ctx, (const void *)k_trsv_fwd<T>, nblk);
+        k_trsv_fwd<T><<<g, 256, 0, st>>>(n, ld, A, b, w.ready, epoch, flags), ++ctx->launches;
     }
+    int g = trsv_grid<T>(ctx, (const void *)k_trsv_bwd<T>, nblk);
+    k_trsv_bwd<T><<<g, 256, 0, st>>>(n, ld, A, w.dvec, b, w.ready + nblk, epoch, flags), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }

@@ -83,8 +83,9 @@ static int check_flags(mp_ctx *ctx, unsigned long long mask, unsigned long long 
 
 // Scratch of the solvers, allocated on first use.
 struct SolveScratch {
-    double *dvec64 = nullptr, *W64 = nullptr, *s64 = nullptr, *r = nullptr;
-    float *dvec32 = nullptr, *W32 = nullptr, *s32 = nullptr, *b32 = nullptr;
+    double *dvec64 = nullptr, *W64 = nullptr, *s64 = nullptr, *r = nullptr, *Linv64 = nullptr;
+    float *dvec32 = nullptr, *W32 = nullptr, *s32 = nullptr, *b32 = nullptr, *Linv32 = nullptr;
+    int *ready = nullptr;
     int neq = 0;
 };
 static SolveScratch g_scr;
@@ -94,15 +95,20 @@ static int ensure_scratch(mp_ctx *ctx) {
     int n = ctx->neq;
     cudaFree(g_scr.dvec64); cudaFree(g_scr.W64); cudaFree(g_scr.s64); cudaFree(g_scr.r);
     cudaFree(g_scr.dvec32); cudaFree(g_scr.W32); cudaFree(g_scr.s32); cudaFree(g_scr.b32);
+    cudaFree(g_scr.Linv64); cudaFree(g_scr.Linv32); cudaFree(g_scr.ready);
     g_scr = SolveScratch();
     MP_CUDA(ctx, cudaMalloc(&g_scr.dvec64, sizeof(double) * (n + 64)));
     MP_CUDA(ctx, cudaMalloc(&g_scr.W64, sizeof(double) * (size_t)(n + 64) * NB));
     MP_CUDA(ctx, cudaMalloc(&g_scr.s64, sizeof(double) * NB));
     MP_CUDA(ctx, cudaMalloc(&g_scr.r, sizeof(double) * (n + 64)));
     MP_CUDA(ctx, cudaMalloc(&g_scr.dvec32, sizeof(float) * (n + 64)));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.W32, sizeof(float) * (size_t)(n + 64) * NB));
+    MP_CUDA(ctx, cudaMalloc(&g_scr.W32, sizeof(float) * (size_t)(n + 256) * 256));
     MP_CUDA(ctx, cudaMalloc(&g_scr.s32, sizeof(float) * NB));
     MP_CUDA(ctx, cudaMalloc(&g_scr.b32, sizeof(float) * (n + 64)));
+    MP_CUDA(ctx, cudaMalloc(&g_scr.Linv64, sizeof(double) * NB * NB));
+    MP_CUDA(ctx, cudaMalloc(&g_scr.Linv32, sizeof(float) * NB * NB));
+    MP_CUDA(ctx, cudaMalloc(&g_scr.ready, sizeof(int) * 2 * ((n + NB - 1) / NB + 1)));
+    MP_CUDA(ctx, cudaMemset(g_scr.ready, 0, sizeof(int) * 2 * ((n + NB - 1) / NB + 1)));
     g_scr.neq = n;
     return MP_OK;
 }
@@ -115,7 +121,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
     cudaEventRecord(ctx->t1.a, ctx->stream);
     if (form == MP_FORM_FP64) {
         MP_CUDA(ctx, cudaMemcpyAsync(ctx->y, ctx->G, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
-        LdltWork<double> w{g_scr.dvec64, g_scr.W64, g_scr.s64};
+        LdltWork<double> w{g_scr.dvec64, g_scr.W64, g_scr.s64, g_scr.Linv64, g_scr.ready};
         rc = ldlt_factor_solve<double>(ctx, ctx->J, ld, n, ctx->y, w, true);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
@@ -130,12 +136,12 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         if (!ctx->J32) MP_CUDA(ctx, cudaMalloc(&ctx->J32, sizeof(float) * (size_t)ld * n));
         k_j_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(n, ld, ctx->J, ctx->J32), ++ctx->launches;
         MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * n, ctx->stream));
-        LdltWork<float> w{g_scr.dvec32, g_scr.W32, g_scr.s32};
+        LdltWork<float> w{g_scr.dvec32, g_scr.W32, g_scr.s32, g_scr.Linv32, g_scr.ready};
         double rn = 0, bn = 0;
         // r = G (y = 0), in FP32 for the first solve, which also factors J32
         rc = resid_norms(ctx, ctx->y, ctx->G, g_scr.r, g_scr.b32, &rn, &bn);
         if (rc) return rc;
-        rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, g_scr.b32, w, true);
+        rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, g_scr.b32, w, true, true);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
         k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, g_scr.b32, ctx->y), ++ctx->launches;

@@ -94,7 +94,9 @@ def push_driver(args):
 
 
 def newton_driver(args):
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.n:
+        cfg["n"] = args.n
     form = mp.MIXED if args.form == "mixed" else mp.FP64
     with tempfile.TemporaryDirectory() as wd:
         kd, deck, pos, vel, cell = make_workload(cfg, wd, seed=1234, n_ions=min(cfg["n_ions"], 200_000))
@@ -119,6 +121,7 @@ def main():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--sort", type=int, default=0)
+    ap.add_argument("--n", type=int, default=0, help="override the mesh's hexes per side (newton driver)")
     args = ap.parse_args()
     (push_driver if args.driver == "push" else newton_driver)(args)
 
