@@ -31,68 +31,86 @@ __device__ __forceinline__ bool bad_pivot(T d) {
     return !(fabs((double)d) > 0.0) || !isfinite((double)d);
 }
 
-// Factor the kb x kb diagonal block at (k0,k0) in shared memory with one warp:
-// L (strict lower) and D written back, and Linv = L_kk^-1 (unit lower, row-major
-// kb x NB) for the panel.  If b is non-null, z_k = L_kk^-1 b_k (forward
-// substitution riding on the factorization).  Dynamic smem: 2 (NB x NB+1) tiles.
+// Factor the kb x kb diagonal block at (k0,k0) in shared memory: L (strict
+// lower) and D written back, and Linv = L_kk^-1 (unit lower, row-major, leading
+// dimension NB) for the panel, built during the elimination by applying each
+// step's row operations to an identity.  If b is non-null, z_k = L_kk^-1 b_k
+// (the forward substitution riding on the factorization).  256 threads; the
+// only serial dimension is the kb elimination steps, two barriers each.
+// Dynamic smem: s, si [NB][NB+1], sl [2][NB], sb [NB].
 template <typename T>
-__global__ void __launch_bounds__(128) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
+__global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
                                                    T *b, unsigned long long *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T(*s)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
     T(*si)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw + sizeof(T) * NB * (NB + 1));
-    T *sl = reinterpret_cast<T *>(smem_raw + sizeof(T) * 2 * NB * (NB + 1));
-    T *sb = sl + NB;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
-        int r = idx / kb, c = idx % kb;
-        s[r][c] = c <= r ? A[(long long)(k0 + r) * ld + k0 + c] : T(0);
-    }
-    if (b && threadIdx.x < kb) sb[threadIdx.x] = b[k0 + threadIdx.x];
-    __syncthreads();
-    if (warp == 0) {
-        for (int j = 0; j < kb; j++) {
-            T d = s[j][j];
-            if (bad_pivot(d)) {
-                if (lane == 0) atomicOr(flags, FLAG_SINGULAR);
-                d = T(1);
-            }
-            for (int i = j + 1 + lane; i < kb; i += 32) sl[i] = s[i][j] / d;
-            __syncwarp();
-            for (int i = j + 1 + lane; i < kb; i += 32) {
-                const T li = sl[i];
-                for (int l = j + 1; l <= i; l++) s[i][l] -= li * s[l][j];
-            }
-            __syncwarp();
-            for (int i = j + 1 + lane; i < kb; i += 32) s[i][j] = sl[i];
-            __syncwarp();
+    T *slbuf = reinterpret_cast<T *>(smem_raw + sizeof(T) * 2 * NB * (NB + 1));  // [2][NB]
+    T *sb = slbuf + 2 * NB;
+    const int t = threadIdx.x;
+    {
+        T v[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            int idx = q * 256 + t;
+            int r = idx >> 6, c = idx & 63;
+            v[q] = (r < kb && c <= r) ? A[(long long)(k0 + r) * ld + k0 + c] : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            int idx = q * 256 + t;
+            int r = idx >> 6, c = idx & 63;
+            s[r][c] = v[q];
+            si[r][c] = r == c ? T(1) : T(0);
         }
     }
+    if (b && t < kb) sb[t] = b[k0 + t];
     __syncthreads();
-    // Linv column q by forward substitution on e_q
-    if (threadIdx.x < kb) {
-        const int q = threadIdx.x;
-        for (int i = 0; i < q; i++) si[i][q] = T(0);
-        si[q][q] = T(1);
-        for (int i = q + 1; i < kb; i++) {
-            T acc = 0;
-            for (int pp = q; pp < i; pp++) acc += s[i][pp] * si[pp][q];
-            si[i][q] = -acc;
+    for (int j = 0; j < kb; j++) {
+        T *sl = slbuf + (j & 1) * NB;
+        T d = s[j][j];
+        if (bad_pivot(d)) {
+            if (t == 0) atomicOr(flags, FLAG_SINGULAR);
+            d = T(1);
+        }
+        const int m = kb - j - 1;
+        if (t < m) sl[j + 1 + t] = s[j + 1 + t][j] / d;
+        __syncthreads();
+        // trailing rank-1 update with the unscaled column w_l = s[l][j]: thread
+        // (column l, row phase) walks rows i >= l of its phase
+        {
+            const int l = j + 1 + (t & 63), ph = t >> 6;
+            if (l < kb) {
+                const T wl = s[l][j];
+                for (int i = l + ((j + 1 + ph - l) & 3); i < kb; i += 4) s[i][l] -= sl[i] * wl;
+            }
+            // the same row operation on the identity: row_i -= l_ij row_j (columns <= j)
+            const int c = t & 63;
+            if (c <= j) {
+                const T rj = si[j][c];
+                for (int i = j + 1 + ph; i < kb; i += 4) si[i][c] -= sl[i] * rj;
+            }
+        }
+        __syncthreads();
+        if (t < m) s[j + 1 + t][j] = sl[j + 1 + t];
+    }
+    __syncthreads();
+    {
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            int idx = q * 256 + t;
+            int r = idx >> 6, c = idx & 63;
+            if (r < kb && c < kb) {
+                if (c <= r) A[(long long)(k0 + r) * ld + k0 + c] = s[r][c];
+                Linv[r * NB + c] = si[r][c];
+            }
         }
     }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
-        int r = idx / kb, c = idx % kb;
-        if (c <= r) A[(long long)(k0 + r) * ld + k0 + c] = s[r][c];
-        Linv[r * NB + c] = si[r][c];
-    }
-    if (threadIdx.x < kb) {
-        dvec[k0 + threadIdx.x] = s[threadIdx.x][threadIdx.x];
+    if (t < kb) {
+        dvec[k0 + t] = s[t][t];
         if (b) {
-            const int i = threadIdx.x;
             T z = 0;
-            for (int pp = 0; pp <= i; pp++) z += si[i][pp] * sb[pp];
-            b[k0 + i] = z;
+            for (int pp = 0; pp <= t; pp++) z += si[t][pp] * sb[pp];
+            b[k0 + t] = z;
         }
     }
 }
@@ -109,14 +127,22 @@ __global__ void __launch_bounds__(256) k_ldlt_panel(int n, long long ld, T *A, i
     T *sd = reinterpret_cast<T *>(smem_raw + sizeof(T) * 2 * 64 * (NB + 1));
     T *sz = sd + NB;
     const int r0 = k0 + kb + blockIdx.x * 64;
-    for (int idx = threadIdx.x; idx < 64 * kb; idx += blockDim.x) {
-        int r = idx / kb, c = idx % kb;
-        int row = r0 + r;
-        sA[r][c] = row < n ? A[(long long)row * ld + k0 + c] : T(0);
-    }
-    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
-        int r = idx / kb, c = idx % kb;
-        sI[r][c] = Linv[r * NB + c];
+    {
+        T va[16], vi[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            int idx = q * 256 + threadIdx.x;
+            int r = idx >> 6, c = idx & 63;
+            int row = r0 + r;
+            va[q] = (row < n && c < kb) ? A[(long long)row * ld + k0 + c] : T(0);
+            vi[q] = (r < kb && c < kb) ? __ldg(&Linv[r * NB + c]) : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            int idx = q * 256 + threadIdx.x;
+            sA[idx >> 6][idx & 63] = va[q];
+            sI[idx >> 6][idx & 63] = vi[q];
+        }
     }
     if (threadIdx.x < kb) {
         sd[threadIdx.x] = dvec[k0 + threadIdx.x];
@@ -179,11 +205,24 @@ __global__ void __launch_bounds__(256) k_ldlt_update(int n, long long ld, T *A, 
     while ((long long)bi * (bi + 1) / 2 > bidx) bi--;
     int bj = (int)(bidx - (long long)bi * (bi + 1) / 2);
     const int i0 = k1 + bi * 64, j0 = k1 + bj * 64;
-    for (int idx = threadIdx.x; idx < 64 * NB; idx += blockDim.x) {
-        int r = idx / NB, p = idx % NB;
-        int ri = i0 + r, rj = j0 + r;
-        sLt[p * 68 + r] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : T(0);
-        sWt[p * 68 + r] = (p < kb && rj < n) ? W[(long long)rj * ldw + p] : T(0);
+    {
+        // 64 x NB elements of each operand, 16 per thread: issue all loads first
+        T la[16], wa[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            int idx = q * 256 + threadIdx.x;
+            int r = idx / NB, p = idx % NB;
+            int ri = i0 + r, rj = j0 + r;
+            la[q] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : T(0);
+            wa[q] = (p < kb && rj < n) ? __ldg(&W[(long long)rj * ldw + p]) : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            int idx = q * 256 + threadIdx.x;
+            int r = idx / NB, p = idx % NB;
+            sLt[p * 68 + r] = la[q];
+            sWt[p * 68 + r] = wa[q];
+        }
     }
     __syncthreads();
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -221,11 +260,23 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols(int n, long long ld, T
     T *sWt = sLt + NB * 68;
     const int i0 = k1 + blockIdx.y * 64, j0 = k1 + blockIdx.x * 64;
     if (j0 > i0 + 63 || j0 >= jend) return;  // tile entirely above the diagonal or outside the panel
-    for (int idx = threadIdx.x; idx < 64 * NB; idx += blockDim.x) {
-        int r = idx / NB, p = idx % NB;
-        int ri = i0 + r, rj = j0 + r;
-        sLt[p * 68 + r] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : T(0);
-        sWt[p * 68 + r] = (p < kb && rj < jend) ? W[(long long)rj * ldw + p] : T(0);
+    {
+        T la[16], wa[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            int idx = q * 256 + threadIdx.x;
+            int r = idx / NB, p = idx % NB;
+            int ri = i0 + r, rj = j0 + r;
+            la[q] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : T(0);
+            wa[q] = (p < kb && rj < jend) ? __ldg(&W[(long long)rj * ldw + p]) : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            int idx = q * 256 + threadIdx.x;
+            int r = idx / NB, p = idx % NB;
+            sLt[p * 68 + r] = la[q];
+            sWt[p * 68 + r] = wa[q];
+        }
     }
     __syncthreads();
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -257,22 +308,33 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols(int n, long long ld, T
 // One persistent launch per direction.  CTA g takes row blocks g, g+G, ... (in
 // solve order); a block first subtracts the contributions of the blocks already
 // solved (each published by a per-block ready word holding the solve's epoch),
-// then solves its unit-triangular diagonal block with one warp.  The grid never
-// exceeds the resident capacity, so the lowest unsolved block always runs.
-// Waits are bounded (TRSV_SPIN_LIMIT polls); a timeout sets the error flag.
+// then solves its unit-triangular diagonal block with one warp.  Each poll takes
+// every block already published (up to 256) at once, so a block's wait ends one
+// block behind the wavefront.  The grid never exceeds the resident capacity, so
+// the lowest unsolved block always runs.  Waits are bounded (TRSV_SPIN_LIMIT
+// empty polls); a timeout sets the error flag.
 constexpr long long TRSV_SPIN_LIMIT = 1ll << 20;
 
-__device__ __forceinline__ bool wait_ready(const int *ready, int blk, int epoch, unsigned long long *flags) {
-    long long spins = 0;
-    while (*(volatile const int *)&ready[blk] != epoch) {
-        if (++spins > TRSV_SPIN_LIMIT) {
-            atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
-            return false;
-        }
-        __nanosleep(64);
+// Number of leading blocks (from `from`) known solved, up to `to`: a block is
+// published only after all blocks before it (it waited for them), so the ready
+// words form a prefix.  All threads call it; one round trip per call.
+__device__ __forceinline__ int ready_prefix(const int *ready, int from, int to, int step, int epoch, int *s_cnt) {
+    const int t = threadIdx.x;
+    const int span = (to - from) * step;  // number of candidate blocks (step = +1 or -1)
+    int k = from + step * t;
+    bool ok = t < span && *(volatile const int *)&ready[k] == epoch;
+    unsigned bal = __ballot_sync(0xffffffffu, ok);
+    if (ok) __threadfence();  // acquire: the block's x values are read after this
+    if ((t & 31) == 0) s_cnt[t >> 5] = bal == 0xffffffffu ? 32 : __ffs(~bal) - 1;
+    __syncthreads();
+    int cnt = 0;
+    for (int w = 0; w < 8; w++) {
+        int c = s_cnt[w];
+        cnt += c;
+        if (c < 32) break;
     }
-    __threadfence();
-    return true;
+    __syncthreads();
+    return cnt < span ? cnt : span;
 }
 
 // L z = b (unit lower, in place on x)
@@ -280,32 +342,44 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_trsv_fwd(int n, long long ld, const T *A, T *x, int *ready, int epoch,
                                                   unsigned long long *flags) {
     __shared__ T sL[NB][NB + 1];
-    __shared__ T sx[NB], srhs[NB];
-    __shared__ T spart[4][NB];
+    __shared__ T srhs[NB];
+    __shared__ int s_cnt[8];
     const int nblk = (n + NB - 1) / NB;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
-        const int r = t >> 2, q = t & 3;  // row, quarter of the 64 columns
-        T acc = 0;
-        for (int c = 0; c < blk; c++) {
-            if (t == 0) wait_ready(ready, c, epoch, flags);
-            __syncthreads();
-            if (t < NB) sx[t] = __ldcg(&x[c * NB + t]);  // written by another CTA: bypass L1
-            __syncthreads();
-            if (r < kb) {
-                const T *row = A + (long long)(r0 + r) * ld + c * NB + q * 16;
-#pragma unroll
-                for (int k = 0; k < 16; k++) acc += row[k] * sx[q * 16 + k];
-            }
-        }
-        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        if (q == 0 && r < kb) srhs[r] = x[r0 + r] - acc;
+        const int r = t >> 2, q = t & 3;  // row, quarter of each 64-column block
         for (int idx = t; idx < kb * kb; idx += blockDim.x) {
             int i = idx / kb, j = idx % kb;
             sL[i][j] = j < i ? A[(long long)(r0 + i) * ld + r0 + j] : T(0);
         }
+        T acc = 0;
+        int done = 0;  // columns blocks [0, done) accumulated
+        long long spins = 0;
+        while (done < blk) {
+            int avail = done + ready_prefix(ready, done, blk < done + 256 ? blk : done + 256, 1, epoch, s_cnt);
+            if (avail == done) {
+                if (++spins > TRSV_SPIN_LIMIT) {
+                    if (t == 0) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
+                    break;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            __threadfence();
+            if (r < kb) {
+                const T *row = A + (long long)(r0 + r) * ld;
+                for (int c = done; c < avail; c++) {
+                    const int cb = c * NB + q * 16;
+#pragma unroll
+                    for (int k = 0; k < 16; k++) acc += __ldg(&row[cb + k]) * __ldcg(&x[cb + k]);
+                }
+            }
+            done = avail;
+        }
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        if (q == 0 && r < kb) srhs[r] = x[r0 + r] - acc;
         __syncthreads();
         if (warp == 0) {
             T v0 = lane < kb ? srhs[lane] : T(0), v1 = lane + 32 < kb ? srhs[lane + 32] : T(0);
@@ -329,30 +403,44 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_trsv_bwd(int n, long long ld, const T *A, const T *dvec, T *x, int *ready,
                                                   int epoch, unsigned long long *flags) {
     __shared__ T sL[NB][NB + 1];
-    __shared__ T sy[NB], srhs[NB];
+    __shared__ T srhs[NB];
     __shared__ T spart[4][NB];
+    __shared__ int s_cnt[8];
     const int nblk = (n + NB - 1) / NB;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     for (int g = blockIdx.x; g < nblk; g += gridDim.x) {
         const int blk = nblk - 1 - g;
         const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
-        const int col = t & 63, part = t >> 6;  // column of this block, quarter of the other block's rows
-        T acc = 0;
-        for (int c = nblk - 1; c > blk; c--) {
-            if (t == 0) wait_ready(ready, c, epoch, flags);
-            __syncthreads();
-            const int c0 = c * NB, cb = n - c0 < NB ? n - c0 : NB;
-            if (t < cb) sy[t] = __ldcg(&x[c0 + t]);
-            __syncthreads();
-            if (col < kb)
-                for (int i = part * 16; i < part * 16 + 16 && i < cb; i++)
-                    acc += A[(long long)(c0 + i) * ld + r0 + col] * sy[i];
-        }
-        spart[part][col] = acc;
+        const int col = t & 63, part = t >> 6;  // column of this block, quarter of each later block's rows
         for (int idx = t; idx < kb * kb; idx += blockDim.x) {
             int i = idx / kb, j = idx % kb;
             sL[i][j] = j < i ? A[(long long)(r0 + i) * ld + r0 + j] : T(0);
         }
+        T acc = 0;
+        int done = nblk - 1;  // blocks (done, nblk) accumulated
+        long long spins = 0;
+        while (done > blk) {
+            int lim = done - blk < 256 ? blk : done - 256;
+            int avail = done - ready_prefix(ready, done, lim, -1, epoch, s_cnt);
+            if (avail == done) {
+                if (++spins > TRSV_SPIN_LIMIT) {
+                    if (t == 0) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
+                    break;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            __threadfence();
+            if (col < kb) {
+                for (int c = done; c > avail; c--) {
+                    const int c0 = c * NB, cb = n - c0 < NB ? n - c0 : NB;
+                    for (int i = part * 16; i < part * 16 + 16 && i < cb; i++)
+                        acc += __ldg(&A[(long long)(c0 + i) * ld + r0 + col]) * __ldcg(&x[c0 + i]);
+                }
+            }
+            done = avail;
+        }
+        spart[part][col] = acc;
         __syncthreads();
         if (t < kb) srhs[t] = x[r0 + t] / dvec[r0 + t] - (spart[0][t] + spart[1][t] + spart[2][t] + spart[3][t]);
         __syncthreads();
@@ -395,7 +483,7 @@ template <typename T>
 int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> w, bool factor,
                       bool tensor_cores = false) {
     cudaStream_t st = ctx->stream;
-    const size_t diag_smem = sizeof(T) * (2 * NB * (NB + 1) + 2 * NB);
+    const size_t diag_smem = sizeof(T) * (2 * NB * (NB + 1) + 3 * NB);
     const size_t panel_smem = sizeof(T) * (64 * (NB + 1) + NB * (NB + 1) + 2 * NB);
     const size_t upd_smem = sizeof(T) * 2 * NB * 68;
     static bool attr = false;
@@ -414,7 +502,7 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     }
     unsigned long long *flags = ctx->counters + C_FLAGS;
     auto diag_and_panel = [&](int k0, int kb, T *W, int ldw) {
-        k_ldlt_diag<T><<<1, 128, diag_smem, st>>>(n, ld, A, k0, kb, w.dvec, w.Linv, b, flags), ++ctx->launches;
+        k_ldlt_diag<T><<<1, 256, diag_smem, st>>>(n, ld, A, k0, kb, w.dvec, w.Linv, b, flags), ++ctx->launches;
         int k1 = k0 + kb;
         if (k1 < n)
             k_ldlt_panel<T><<<(n - k1 + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, w.Linv, W, ldw, b),

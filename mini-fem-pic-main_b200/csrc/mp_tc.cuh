@@ -70,25 +70,32 @@ __device__ __forceinline__ void mma_commit(unsigned long long *bar) {
 // one swizzled chunk; rows >= nrows and cols >= kmax are zero.
 __device__ __forceinline__ void load_chunk(unsigned char *dst, const float *src, long long ld, long long r0,
                                            long long nrows, int k0, int kmax) {
-    // 128 rows x 8 sixteen-byte pieces = 1024 pieces, 8 per thread
+    // 128 rows x 8 sixteen-byte pieces = 1024 pieces, 8 per thread; all eight
+    // loads are issued before any store so they are in flight together
+    float4 v[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
         int piece = q * THREADS + threadIdx.x;
         int r = piece >> 3, c = piece & 7;
         long long row = r0 + r;
         int col = k0 + c * 4;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        v[q] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (row < nrows) {
             const float *p = src + row * ld + col;
             if (col + 3 < kmax) {
-                v = *reinterpret_cast<const float4 *>(p);
+                v[q] = __ldg(reinterpret_cast<const float4 *>(p));
             } else {
-                if (col < kmax) v.x = p[0];
-                if (col + 1 < kmax) v.y = p[1];
-                if (col + 2 < kmax) v.z = p[2];
+                if (col < kmax) v[q].x = __ldg(p);
+                if (col + 1 < kmax) v[q].y = __ldg(p + 1);
+                if (col + 2 < kmax) v[q].z = __ldg(p + 2);
             }
         }
-        *reinterpret_cast<float4 *>(dst + r * 128 + ((c ^ (r & 7)) << 4)) = v;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        int piece = q * THREADS + threadIdx.x;
+        int r = piece >> 3, c = piece & 7;
+        *reinterpret_cast<float4 *>(dst + r * 128 + ((c ^ (r & 7)) << 4)) = v[q];
     }
 }
 
@@ -163,26 +170,52 @@ __global__ void __launch_bounds__(THREADS, 1) k_update_tf32(int n, long long ld,
     if (!mbar_wait(&bars[2], 0)) ok = false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (!ok) s_bad = 1;
-    // epilogue: this thread's row of D, 16 columns at a time
-    const long long row = i0 + warp * 32 + lane;
+    // epilogue, in two halves of 64 columns: TMEM -> registers -> shared
+    // (row-major, padded), then each warp subtracts whole rows from the tile
+    // with coalesced loads and stores (the operand stages are free now)
+    float(*sD)[65] = reinterpret_cast<float(*)[65]>(base);
     const unsigned taddr = tmem + ((unsigned)(warp * 32) << 16);
 #pragma unroll 1
-    for (int cb = 0; cb < TILE / 16; cb++) {
-        unsigned v[16];
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(taddr + cb * 16));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (row < n) {
-            float *dst = A + row * ld;
+    for (int half = 0; half < 2; half++) {
+#pragma unroll 1
+        for (int cb = 0; cb < 4; cb++) {
+            unsigned v[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(taddr + half * 64 + cb * 16));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int q = 0; q < 16; q++) {
-                long long col = j0 + cb * 16 + q;
-                if (col < n && col <= row) dst[col] -= __uint_as_float(v[q]);
+            for (int q = 0; q < 16; q++) sD[warp * 32 + lane][cb * 16 + q] = __uint_as_float(v[q]);
+        }
+        __syncthreads();
+        const long long c0 = j0 + half * 64 + lane;
+#pragma unroll 1
+        for (int rr = 0; rr < 32; rr += 4) {
+            float old[4][2];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const long long row = i0 + warp * 32 + rr + u;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const long long col = c0 + h * 32;
+                    old[u][h] = (row < n && col < n) ? A[row * ld + col] : 0.f;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const long long row = i0 + warp * 32 + rr + u;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const long long col = c0 + h * 32;
+                    // the strict upper part of the diagonal tiles is never read again; skip it anyway
+                    if (row < n && col < n && col <= row)
+                        A[row * ld + col] = old[u][h] - sD[warp * 32 + rr + u][lane + h * 32];
+                }
             }
         }
+        __syncthreads();
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
