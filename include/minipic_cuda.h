@@ -64,6 +64,11 @@ enum { MP_METHOD_NONLINEAR = 0, MP_METHOD_GAUSS_SEIDEL = 1, MP_METHOD_LAPACK = 2
  * Jacobian in TF32 on the tensor cores with FP64 iterative refinement. */
 enum { MP_FORM_FP64 = 0, MP_FORM_MIXED = 1 };
 
+/* Tensor-core arithmetic of the mixed form's FP32 factorization: one TF32
+ * product per term, or the 3xTF32 split (hi*hi + hi*lo + lo*hi, about FP32
+ * accuracy; fewer FP64 refinement iterations). */
+enum { MP_MIXED_TF32 = 1, MP_MIXED_TF32X3 = 3 };
+
 /* Density accumulation: FP64 atomics (order-dependent rounding, like the
  * reference's atomic_ref) or 64-bit fixed point (run-to-run deterministic). */
 enum { MP_SCATTER_FP64_ATOMIC = 0, MP_SCATTER_FIXED64 = 1 };
@@ -145,6 +150,10 @@ int mp_set_walk_limit(mp_ctx *ctx, int32_t max_hops);
 int mp_set_scatter_mode(mp_ctx *ctx, int mode);
 int mp_set_sort_period(mp_ctx *ctx, int32_t steps);
 int mp_set_particle_form(mp_ctx *ctx, int form);
+/* Arithmetic of the mixed-form Newton factorization (MP_MIXED_TF32 or
+ * MP_MIXED_TF32X3, the default).  No reference counterpart: the reference's
+ * dsysv_ call (src/FESolver.cpp:528-558) is FP64 throughout. */
+int mp_set_mixed_factor(mp_ctx *ctx, int mode);
 /* Particle IDs (16 B per particle-step of traffic) are needed only to restore
  * injection order after tet re-sorting; without sorting the stable removal
  * keeps the reference's order by itself.  With IDs off and sorting on,

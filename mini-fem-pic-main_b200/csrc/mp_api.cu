@@ -328,6 +328,12 @@ int mp_set_sort_period(mp_ctx *ctx, int32_t steps) {
     return MP_OK;
 }
 
+int mp_set_mixed_factor(mp_ctx *ctx, int mode) {
+    if (!ctx || (mode != MP_MIXED_TF32 && mode != MP_MIXED_TF32X3)) return MP_ERR_ARG;
+    ctx->mixed_factor = mode;
+    return MP_OK;
+}
+
 int mp_set_particle_form(mp_ctx *ctx, int form) {
     if (!ctx || (form != MP_FORM_FP64 && form != MP_FORM_MIXED)) return MP_ERR_ARG;
     if (form == ctx->form) return MP_OK;

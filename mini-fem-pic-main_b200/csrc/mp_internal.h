@@ -117,6 +117,7 @@ struct mp_ctx {
     int scatter_mode = MP_SCATTER_FP64_ATOMIC;
     int walk_limit = 4096;
     int sort_period = 0;
+    int mixed_factor = MP_MIXED_TF32X3;  // tensor-core terms of the mixed factorization
     long long steps_since_sort = 0;
     bool track_ids = true;
     long long capacity = 0;

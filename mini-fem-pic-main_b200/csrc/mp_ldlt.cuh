@@ -31,85 +31,90 @@ __device__ __forceinline__ bool bad_pivot(T d) {
     return !(fabs((double)d) > 0.0) || !isfinite((double)d);
 }
 
-// Factor the kb x kb diagonal block at (k0,k0) in shared memory: L (strict
-// lower) and D written back, and Linv = L_kk^-1 (unit lower, row-major, leading
-// dimension NB) for the panel, built during the elimination by applying each
-// step's row operations to an identity.  If b is non-null, z_k = L_kk^-1 b_k
-// (the forward substitution riding on the factorization).  256 threads; the
-// only serial dimension is the kb elimination steps, two barriers each.
-// Dynamic smem: s, si [NB][NB+1], sl [2][NB], sb [NB].
+// Factor the kb x kb diagonal block at (k0,k0): L (strict lower) and D written
+// back, and Linv = L_kk^-1 (unit lower, row-major NB x NB, zero outside kb x kb)
+// for the panel and the triangular solves, built during the elimination by
+// applying each step's row operations to an identity.  If b is non-null,
+// z_k = L_kk^-1 b_k (the forward substitution riding on the factorization).
+// 256 threads; thread (column l = t & 63, phase ph = t >> 6) keeps rows
+// i = ph + 4k (k < 16) of column l of the block and of the inverse in
+// registers.  Step j publishes column j of the block and row j of the inverse
+// through shared memory (double-buffered), one barrier per step.
+// Dynamic smem: the inverse [NB][NB+1] (for z) and b.
 template <typename T>
 __global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
                                                    T *b, unsigned long long *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T(*s)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
-    T(*si)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw + sizeof(T) * NB * (NB + 1));
-    T *slbuf = reinterpret_cast<T *>(smem_raw + sizeof(T) * 2 * NB * (NB + 1));  // [2][NB]
-    T *sb = slbuf + 2 * NB;
-    const int t = threadIdx.x;
-    {
-        T v[16];
+    T(*sinv)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
+    T *sb = reinterpret_cast<T *>(smem_raw + sizeof(T) * NB * (NB + 1));
+    __shared__ T sw[2][NB];    // column j of the block, unscaled (rows >= j)
+    __shared__ T srow[2][NB];  // row j of the inverse (columns <= j)
+    const int t = threadIdx.x, l = t & 63, ph = t >> 6;
+    T a[16], v[16];
 #pragma unroll
-        for (int q = 0; q < 16; q++) {
-            int idx = q * 256 + t;
-            int r = idx >> 6, c = idx & 63;
-            v[q] = (r < kb && c <= r) ? A[(long long)(k0 + r) * ld + k0 + c] : T(0);
-        }
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            int idx = q * 256 + t;
-            int r = idx >> 6, c = idx & 63;
-            s[r][c] = v[q];
-            si[r][c] = r == c ? T(1) : T(0);
-        }
+    for (int k = 0; k < 16; k++) {
+        const int i = ph + 4 * k;
+        a[k] = (i < kb && l <= i) ? A[(long long)(k0 + i) * ld + k0 + l] : T(0);
+        v[k] = (i == l && i < kb) ? T(1) : T(0);
     }
     if (b && t < kb) sb[t] = b[k0 + t];
+    // publish column 0 and row 0 of the inverse (e_0)
+    if (l == 0) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) sw[0][ph + 4 * k] = a[k];
+    }
+    if (ph == 0) srow[0][l] = l == 0 ? T(1) : T(0);
     __syncthreads();
+    bool singular = false;
     for (int j = 0; j < kb; j++) {
-        T *sl = slbuf + (j & 1) * NB;
-        T d = s[j][j];
+        const int buf = j & 1;
+        T d = sw[buf][j];
         if (bad_pivot(d)) {
-            if (t == 0) atomicOr(flags, FLAG_SINGULAR);
+            singular = true;
             d = T(1);
         }
-        const int m = kb - j - 1;
-        if (t < m) sl[j + 1 + t] = s[j + 1 + t][j] / d;
-        __syncthreads();
-        // trailing rank-1 update with the unscaled column w_l = s[l][j]: thread
-        // (column l, row phase) walks rows i >= l of its phase
-        {
-            const int l = j + 1 + (t & 63), ph = t >> 6;
-            if (l < kb) {
-                const T wl = s[l][j];
-                for (int i = l + ((j + 1 + ph - l) & 3); i < kb; i += 4) s[i][l] -= sl[i] * wl;
-            }
-            // the same row operation on the identity: row_i -= l_ij row_j (columns <= j)
-            const int c = t & 63;
-            if (c <= j) {
-                const T rj = si[j][c];
-                for (int i = j + 1 + ph; i < kb; i += 4) si[i][c] -= sl[i] * rj;
-            }
-        }
-        __syncthreads();
-        if (t < m) s[j + 1 + t][j] = sl[j + 1 + t];
-    }
-    __syncthreads();
-    {
+        const T rd = T(1) / d;
+        const T wl = sw[buf][l] * rd;    // l_lj, used by columns l > j
+        const T rc = srow[buf][l] * rd;  // Linv[j][l] / d, used by columns l <= j
+        const bool upd = l > j, inv = l <= j;
+        // column j+1 of the block (by its owner) and row j+1 of the inverse are
+        // final once this step's update has run: publish them into the other buffer
+        const int jn = j + 1, nb = jn & 1;
+        const bool pub = jn < kb;
 #pragma unroll
-        for (int q = 0; q < 16; q++) {
-            int idx = q * 256 + t;
-            int r = idx >> 6, c = idx & 63;
-            if (r < kb && c < kb) {
-                if (c <= r) A[(long long)(k0 + r) * ld + k0 + c] = s[r][c];
-                Linv[r * NB + c] = si[r][c];
+        for (int k = 0; k < 16; k++) {
+            const int i = ph + 4 * k;
+            const T wi = sw[buf][i];
+            if (i > j && i < kb) {
+                if (upd && l <= i) a[k] -= wi * wl;
+                if (inv) v[k] -= wi * rc;
             }
+            if (pub && l == jn) sw[nb][i] = a[k];
+            if (pub && i == jn) srow[nb][l] = v[k];
         }
+        if (l == j) {
+#pragma unroll
+            for (int k = 0; k < 16; k++)
+                if (ph + 4 * k > j) a[k] *= rd;  // column j becomes L's column
+        }
+        __syncthreads();
     }
-    if (t < kb) {
-        dvec[k0 + t] = s[t][t];
-        if (b) {
+    if (singular && t == 0) atomicOr(flags, FLAG_SINGULAR);
+    T *Lb = Linv;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        const int i = ph + 4 * k;
+        const bool in = i < kb && l < kb;
+        if (in && l <= i) A[(long long)(k0 + i) * ld + k0 + l] = a[k];
+        if (in && l == i) dvec[k0 + i] = a[k];
+        Lb[i * NB + l] = in ? v[k] : T(0);
+        sinv[i][l] = in ? v[k] : T(0);
+    }
+    if (b) {
+        __syncthreads();
+        if (t < kb) {
             T z = 0;
-            for (int pp = 0; pp <= t; pp++) z += si[t][pp] * sb[pp];
+            for (int pp = 0; pp <= t; pp++) z += sinv[t][pp] * sb[pp];
             b[k0 + t] = z;
         }
     }
@@ -306,30 +311,38 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols(int n, long long ld, T
 
 // ---- triangular solves with an existing factor --------------------------------------
 // One persistent launch per direction.  CTA g takes row blocks g, g+G, ... (in
-// solve order); a block first subtracts the contributions of the blocks already
-// solved (each published by a per-block ready word holding the solve's epoch),
-// then solves its unit-triangular diagonal block with one warp.  Each poll takes
-// every block already published (up to 256) at once, so a block's wait ends one
-// block behind the wavefront.  The grid never exceeds the resident capacity, so
-// the lowest unsolved block always runs.  Waits are bounded (TRSV_SPIN_LIMIT
-// empty polls); a timeout sets the error flag.
+// solve order); a block subtracts the contributions of the blocks already
+// solved (each published by a per-block ready word holding the solve's epoch,
+// stored with release semantics and polled with acquire loads), then applies
+// its diagonal block's stored inverse: the block's own solve is a 64 x 64
+// product, not a serial substitution.  Each poll takes every block already
+// published (up to 256) at once, and the operand chunk of the next awaited block
+// is loaded before the poll, so a block's wait ends one chunk behind the
+// wavefront.  The grid never exceeds the resident capacity, so the lowest
+// unsolved block always runs.  Waits are bounded (TRSV_SPIN_LIMIT empty polls);
+// a timeout sets the error flag.
 constexpr long long TRSV_SPIN_LIMIT = 1ll << 20;
 
-// Number of leading blocks (from `from`) known solved, up to `to`: a block is
-// published only after all blocks before it (it waited for them), so the ready
-// words form a prefix.  All threads call it; one round trip per call.
-__device__ __forceinline__ int ready_prefix(const int *ready, int from, int to, int step, int epoch, int *s_cnt) {
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Number of consecutive published blocks from `from` in direction `step`
+// (+1 or -1), at most `span`.  All threads call it; one round trip per call.
+__device__ __forceinline__ int ready_prefix(const int *ready, int from, int span, int step, int epoch, int *s_cnt) {
     const int t = threadIdx.x;
-    const int span = (to - from) * step;  // number of candidate blocks (step = +1 or -1)
-    int k = from + step * t;
-    bool ok = t < span && *(volatile const int *)&ready[k] == epoch;
-    unsigned bal = __ballot_sync(0xffffffffu, ok);
-    if (ok) __threadfence();  // acquire: the block's x values are read after this
+    const bool ok = t < span && ld_acquire(ready + from + step * t) == epoch;
+    const unsigned bal = __ballot_sync(0xffffffffu, ok);
     if ((t & 31) == 0) s_cnt[t >> 5] = bal == 0xffffffffu ? 32 : __ffs(~bal) - 1;
     __syncthreads();
     int cnt = 0;
     for (int w = 0; w < 8; w++) {
-        int c = s_cnt[w];
+        const int c = s_cnt[w];
         cnt += c;
         if (c < 32) break;
     }
@@ -337,28 +350,50 @@ __device__ __forceinline__ int ready_prefix(const int *ready, int from, int to, 
     return cnt < span ? cnt : span;
 }
 
+// 16 consecutive values (64-byte aligned for float, 128 for double) as vector loads
+template <typename T, bool CG>
+__device__ __forceinline__ void load16(const T *p, T (&v)[16]) {
+    if constexpr (sizeof(T) == 8) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            double2 d = CG ? __ldcg(reinterpret_cast<const double2 *>(p) + k) : __ldg(reinterpret_cast<const double2 *>(p) + k);
+            v[2 * k] = d.x;
+            v[2 * k + 1] = d.y;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            float4 f = CG ? __ldcg(reinterpret_cast<const float4 *>(p) + k) : __ldg(reinterpret_cast<const float4 *>(p) + k);
+            v[4 * k] = f.x;
+            v[4 * k + 1] = f.y;
+            v[4 * k + 2] = f.z;
+            v[4 * k + 3] = f.w;
+        }
+    }
+}
+
 // L z = b (unit lower, in place on x)
 template <typename T>
-__global__ void __launch_bounds__(256) k_trsv_fwd(int n, long long ld, const T *A, T *x, int *ready, int epoch,
-                                                  unsigned long long *flags) {
-    __shared__ T sL[NB][NB + 1];
+__global__ void __launch_bounds__(256) k_trsv_fwd(int n, long long ld, const T *A, const T *Linv, T *x, int *ready,
+                                                  int epoch, unsigned long long *flags) {
+    __shared__ T sI[NB][NB + 1];
     __shared__ T srhs[NB];
     __shared__ int s_cnt[8];
     const int nblk = (n + NB - 1) / NB;
-    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int t = threadIdx.x;
+    const int r = t >> 2, q = t & 3;  // row of the block, quarter of each 64-column chunk
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
-        const int r = t >> 2, q = t & 3;  // row, quarter of each 64-column block
-        for (int idx = t; idx < kb * kb; idx += blockDim.x) {
-            int i = idx / kb, j = idx % kb;
-            sL[i][j] = j < i ? A[(long long)(r0 + i) * ld + r0 + j] : T(0);
-        }
-        T acc = 0;
-        int done = 0;  // columns blocks [0, done) accumulated
+        for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = __ldg(&Linv[(size_t)blk * NB * NB + idx]);
+        const T *row = A + (long long)(r0 + (r < kb ? r : 0)) * ld + q * 16;
+        T acc = 0, ap[16], xv[16];
+        int done = 0;  // column chunks [0, done) accumulated
+        if (done < blk) load16<T, false>(row, ap);
         long long spins = 0;
         while (done < blk) {
-            int avail = done + ready_prefix(ready, done, blk < done + 256 ? blk : done + 256, 1, epoch, s_cnt);
-            if (avail == done) {
+            const int span = blk - done < 256 ? blk - done : 256;
+            const int cnt = ready_prefix(ready, done, span, 1, epoch, s_cnt);
+            if (cnt == 0) {
                 if (++spins > TRSV_SPIN_LIMIT) {
                     if (t == 0) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
                     break;
@@ -366,63 +401,66 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(int n, long long ld, const T *
                 __nanosleep(32);
                 continue;
             }
-            __threadfence();
-            if (r < kb) {
-                const T *row = A + (long long)(r0 + r) * ld;
-                for (int c = done; c < avail; c++) {
-                    const int cb = c * NB + q * 16;
+            const int avail = done + cnt;
+            load16<T, true>(x + done * NB + q * 16, xv);
 #pragma unroll
-                    for (int k = 0; k < 16; k++) acc += __ldg(&row[cb + k]) * __ldcg(&x[cb + k]);
-                }
+            for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
+            for (int c = done + 1; c < avail; c++) {
+                load16<T, false>(row + c * NB, ap);
+                load16<T, true>(x + c * NB + q * 16, xv);
+#pragma unroll
+                for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
             }
             done = avail;
+            if (done < blk) load16<T, false>(row + done * NB, ap);
         }
         acc += __shfl_xor_sync(0xffffffffu, acc, 1);
         acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        if (q == 0 && r < kb) srhs[r] = x[r0 + r] - acc;
+        if (q == 0) srhs[r] = r < kb ? __ldcg(&x[r0 + r]) - acc : T(0);
         __syncthreads();
-        if (warp == 0) {
-            T v0 = lane < kb ? srhs[lane] : T(0), v1 = lane + 32 < kb ? srhs[lane + 32] : T(0);
-            for (int j = 0; j < kb; j++) {
-                T xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-                if (lane > j && lane < kb) v0 -= sL[lane][j] * xj;
-                if (lane + 32 > j && lane + 32 < kb) v1 -= sL[lane + 32][j] * xj;
-            }
-            if (lane < kb) x[r0 + lane] = v0;
-            if (lane + 32 < kb) x[r0 + lane + 32] = v1;
-            __threadfence();
-            __syncwarp();
-            if (lane == 0) *(volatile int *)&ready[blk] = epoch;
-        }
+        T v = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) v = fma(sI[r][q * 16 + k], srhs[q * 16 + k], v);
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+        v += __shfl_xor_sync(0xffffffffu, v, 2);
+        if (q == 0 && r < kb) x[r0 + r] = v;
         __syncthreads();
+        if (t == 0) st_release(ready + blk, epoch);
     }
 }
 
 // L^T y = D^-1 z (unit upper after scaling, in place on x), blocks from the last
 template <typename T>
-__global__ void __launch_bounds__(256) k_trsv_bwd(int n, long long ld, const T *A, const T *dvec, T *x, int *ready,
-                                                  int epoch, unsigned long long *flags) {
-    __shared__ T sL[NB][NB + 1];
+__global__ void __launch_bounds__(256) k_trsv_bwd(int n, long long ld, const T *A, const T *Linv, const T *dvec, T *x,
+                                                  int *ready, int epoch, unsigned long long *flags) {
+    __shared__ T sI[NB][NB + 1];
     __shared__ T srhs[NB];
     __shared__ T spart[4][NB];
     __shared__ int s_cnt[8];
     const int nblk = (n + NB - 1) / NB;
-    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int t = threadIdx.x;
+    const int col = t & 63, part = t >> 6;  // column of this block, quarter of each later chunk's rows
     for (int g = blockIdx.x; g < nblk; g += gridDim.x) {
         const int blk = nblk - 1 - g;
         const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
-        const int col = t & 63, part = t >> 6;  // column of this block, quarter of each later block's rows
-        for (int idx = t; idx < kb * kb; idx += blockDim.x) {
-            int i = idx / kb, j = idx % kb;
-            sL[i][j] = j < i ? A[(long long)(r0 + i) * ld + r0 + j] : T(0);
-        }
-        T acc = 0;
-        int done = nblk - 1;  // blocks (done, nblk) accumulated
+        for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = __ldg(&Linv[(size_t)blk * NB * NB + idx]);
+        const int cc = col < kb ? col : 0;
+        T acc = 0, ap[16];
+        // rows c*NB + part*16 + k of column r0 + col (zero past n)
+        auto fetch = [&](int c) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int i = c * NB + part * 16 + k;
+                ap[k] = i < n ? __ldg(&A[(long long)i * ld + r0 + cc]) : T(0);
+            }
+        };
+        int done = nblk - 1;  // chunks (done, nblk) accumulated
+        if (done > blk) fetch(done);
         long long spins = 0;
         while (done > blk) {
-            int lim = done - blk < 256 ? blk : done - 256;
-            int avail = done - ready_prefix(ready, done, lim, -1, epoch, s_cnt);
-            if (avail == done) {
+            const int span = done - blk < 256 ? done - blk : 256;
+            const int cnt = ready_prefix(ready, done, span, -1, epoch, s_cnt);
+            if (cnt == 0) {
                 if (++spins > TRSV_SPIN_LIMIT) {
                     if (t == 0) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
                     break;
@@ -430,41 +468,36 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(int n, long long ld, const T *
                 __nanosleep(32);
                 continue;
             }
-            __threadfence();
-            if (col < kb) {
-                for (int c = done; c > avail; c--) {
-                    const int c0 = c * NB, cb = n - c0 < NB ? n - c0 : NB;
-                    for (int i = part * 16; i < part * 16 + 16 && i < cb; i++)
-                        acc += __ldg(&A[(long long)(c0 + i) * ld + r0 + col]) * __ldcg(&x[c0 + i]);
-                }
+            const int avail = done - cnt;
+            for (int c = done; c > avail; c--) {
+                if (c != done) fetch(c);
+                const int i0 = c * NB + part * 16;
+#pragma unroll
+                for (int k = 0; k < 16; k++)
+                    if (i0 + k < n) acc = fma(ap[k], __ldcg(&x[i0 + k]), acc);
             }
             done = avail;
+            if (done > blk) fetch(done);
         }
-        spart[part][col] = acc;
+        spart[part][col] = col < kb ? acc : T(0);
         __syncthreads();
-        if (t < kb) srhs[t] = x[r0 + t] / dvec[r0 + t] - (spart[0][t] + spart[1][t] + spart[2][t] + spart[3][t]);
+        if (t < NB) srhs[t] = t < kb ? __ldcg(&x[r0 + t]) / dvec[r0 + t] - (spart[0][t] + spart[1][t] + spart[2][t] + spart[3][t]) : T(0);
         __syncthreads();
-        if (warp == 0) {
-            T v0 = lane < kb ? srhs[lane] : T(0), v1 = lane + 32 < kb ? srhs[lane + 32] : T(0);
-            for (int j = kb - 1; j >= 0; j--) {
-                T yj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-                if (lane < j) v0 -= sL[j][lane] * yj;
-                if (lane + 32 < j) v1 -= sL[j][lane + 32] * yj;
-            }
-            if (lane < kb) x[r0 + lane] = v0;
-            if (lane + 32 < kb) x[r0 + lane + 32] = v1;
-            __threadfence();
-            __syncwarp();
-            if (lane == 0) *(volatile int *)&ready[blk] = epoch;
-        }
+        T v = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) v = fma(sI[part * 16 + k][col], srhs[part * 16 + k], v);
+        spart[part][col] = v;
         __syncthreads();
+        if (t < kb) x[r0 + t] = spart[0][t] + spart[1][t] + spart[2][t] + spart[3][t];
+        __syncthreads();
+        if (t == 0) st_release(ready + blk, epoch);
     }
 }
 
 template <typename T>
 struct LdltWork {
     T *dvec, *W, *s;
-    T *Linv;       // [NB][NB] inverse of the current diagonal block's L
+    T *Linv;       // [blocks][NB][NB] inverses of the diagonal blocks' L (the solves use them)
     int *ready;    // [2][blocks] per-block ready words of the two solves
 };
 
@@ -481,9 +514,9 @@ int trsv_grid(mp_ctx *ctx, const void *kernel, int nblk) {
 
 template <typename T>
 int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> w, bool factor,
-                      bool tensor_cores = false) {
+                      int tc_terms = 0) {
     cudaStream_t st = ctx->stream;
-    const size_t diag_smem = sizeof(T) * (2 * NB * (NB + 1) + 3 * NB);
+    const size_t diag_smem = sizeof(T) * (NB * (NB + 1) + NB);
     const size_t panel_smem = sizeof(T) * (64 * (NB + 1) + NB * (NB + 1) + 2 * NB);
     const size_t upd_smem = sizeof(T) * 2 * NB * 68;
     static bool attr = false;
@@ -497,20 +530,25 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         cudaFuncSetAttribute(k_ldlt_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_update_cols<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_update_cols<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(tc::k_update_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM_BYTES);
+        cudaFuncSetAttribute(tc::k_update_tf32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tc::smem_bytes(false));
+        cudaFuncSetAttribute(tc::k_update_tf32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tc::smem_bytes(true));
         attr = true;
     }
     unsigned long long *flags = ctx->counters + C_FLAGS;
     auto diag_and_panel = [&](int k0, int kb, T *W, int ldw) {
-        k_ldlt_diag<T><<<1, 256, diag_smem, st>>>(n, ld, A, k0, kb, w.dvec, w.Linv, b, flags), ++ctx->launches;
+        T *Li = w.Linv + (size_t)(k0 / NB) * NB * NB;
+        k_ldlt_diag<T><<<1, 256, diag_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, b, flags), ++ctx->launches;
         int k1 = k0 + kb;
         if (k1 < n)
-            k_ldlt_panel<T><<<(n - k1 + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, w.Linv, W, ldw, b),
+            k_ldlt_panel<T><<<(n - k1 + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b),
                 ++ctx->launches;
     };
-    if (factor && tensor_cores) {
+    if (factor && tc_terms) {
         // two-level LDL^T: 256-wide outer panels factored with the 64-wide kernels,
-        // trailing update of each outer panel on the tensor cores
+        // trailing update of each outer panel on the tensor cores (TF32, or
+        // 3xTF32 when tc_terms == 3)
         const int PW = 256;
         for (int P0 = 0; P0 < n; P0 += PW) {
             const int P1 = P0 + PW < n ? P0 + PW : n;
@@ -527,7 +565,8 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             if (P1 < n) {
                 long long tiles = (n - P1 + tc::TILE - 1) / tc::TILE;
                 long long nblk = tiles * (tiles + 1) / 2;
-                tc::k_update_tf32<<<(unsigned)nblk, tc::THREADS, tc::SMEM_BYTES, st>>>(
+                auto kern = tc_terms == 3 ? tc::k_update_tf32<true> : tc::k_update_tf32<false>;
+                kern<<<(unsigned)nblk, tc::THREADS, tc::smem_bytes(tc_terms == 3), st>>>(
                     n, ld, reinterpret_cast<float *>(A), P0, P1 - P0, P1, reinterpret_cast<const float *>(w.W), PW,
                     flags), ++ctx->launches;
             }
@@ -548,10 +587,10 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     const int epoch = ++g_solve_epoch;
     if (!factor) {
         int g = trsv_grid<T>(ctx, (const void *)k_trsv_fwd<T>, nblk);
-        k_trsv_fwd<T><<<g, 256, 0, st>>>(n, ld, A, b, w.ready, epoch, flags), ++ctx->launches;
+        k_trsv_fwd<T><<<g, 256, 0, st>>>(n, ld, A, w.Linv, b, w.ready, epoch, flags), ++ctx->launches;
     }
     int g = trsv_grid<T>(ctx, (const void *)k_trsv_bwd<T>, nblk);
-    k_trsv_bwd<T><<<g, 256, 0, st>>>(n, ld, A, w.dvec, b, w.ready + nblk, epoch, flags), ++ctx->launches;
+    k_trsv_bwd<T><<<g, 256, 0, st>>>(n, ld, A, w.Linv, w.dvec, b, w.ready + nblk, epoch, flags), ++ctx->launches;
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }

@@ -105,8 +105,9 @@ static int ensure_scratch(mp_ctx *ctx) {
     MP_CUDA(ctx, cudaMalloc(&g_scr.W32, sizeof(float) * (size_t)(n + 256) * 256));
     MP_CUDA(ctx, cudaMalloc(&g_scr.s32, sizeof(float) * NB));
     MP_CUDA(ctx, cudaMalloc(&g_scr.b32, sizeof(float) * (n + 64)));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.Linv64, sizeof(double) * NB * NB));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.Linv32, sizeof(float) * NB * NB));
+    const size_t nblk = (n + NB - 1) / NB;
+    MP_CUDA(ctx, cudaMalloc(&g_scr.Linv64, sizeof(double) * nblk * NB * NB));
+    MP_CUDA(ctx, cudaMalloc(&g_scr.Linv32, sizeof(float) * nblk * NB * NB));
     MP_CUDA(ctx, cudaMalloc(&g_scr.ready, sizeof(int) * 2 * ((n + NB - 1) / NB + 1)));
     MP_CUDA(ctx, cudaMemset(g_scr.ready, 0, sizeof(int) * 2 * ((n + NB - 1) / NB + 1)));
     g_scr.neq = n;
@@ -141,7 +142,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         // r = G (y = 0), in FP32 for the first solve, which also factors J32
         rc = resid_norms(ctx, ctx->y, ctx->G, g_scr.r, g_scr.b32, &rn, &bn);
         if (rc) return rc;
-        rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, g_scr.b32, w, true, true);
+        rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, g_scr.b32, w, true, ctx->mixed_factor);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
         k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, g_scr.b32, ctx->y), ++ctx->launches;

@@ -10,8 +10,15 @@
 // stage's mbarrier, which tells the loaders when the stage may be refilled.
 // The epilogue reads the accumulator with tcgen05.ld and subtracts it from the
 // tile in global memory.  No multicast and no cluster: each CTA loads its own
-// operands.  Every mbarrier wait is bounded; a timeout sets FLAG_NONFINITE-free
-// error bit FLAG_LOOKBACK_TIMEOUT, reported as MP_ERR_TIMEOUT by the caller.
+// operands.  Every mbarrier wait is bounded; a timeout sets the error bit
+// FLAG_LOOKBACK_TIMEOUT, reported as MP_ERR_TIMEOUT by the caller.
+//
+// SPLIT (3xTF32): each FP32 operand x is split on the way into shared memory
+// into hi = x rounded to TF32 (11 significant bits) and lo = x - hi (exact in
+// FP32), and the product is accumulated as hi*hi + hi*lo + lo*hi, three MMAs on
+// the same TMEM accumulator.  The dropped lo*lo term is ~2^-22 relative, so the
+// update carries about FP32 accuracy instead of TF32's 2^-11, which is what the
+// FP64 refinement of the mixed solve converges against.
 #pragma once
 
 #include "mp_internal.h"
@@ -66,10 +73,17 @@ __device__ __forceinline__ void mma_commit(unsigned long long *bar) {
                  : "memory");
 }
 
+// x rounded to the nearest TF32 value (low 13 mantissa bits cleared)
+__device__ __forceinline__ float tf32_hi(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
 // Copies rows [r0, r0+128) x cols [k0, k0+32) of a row-major FP32 matrix into
-// one swizzled chunk; rows >= nrows and cols >= kmax are zero.
-__device__ __forceinline__ void load_chunk(unsigned char *dst, const float *src, long long ld, long long r0,
-                                           long long nrows, int k0, int kmax) {
+// one swizzled chunk (and, for SPLIT, its hi part into dst and lo part into
+// dst_lo); rows >= nrows and cols >= kmax are zero.
+template <bool SPLIT>
+__device__ __forceinline__ void load_chunk(unsigned char *dst, unsigned char *dst_lo, const float *src, long long ld,
+                                           long long r0, long long nrows, int k0, int kmax) {
     // 128 rows x 8 sixteen-byte pieces = 1024 pieces, 8 per thread; all eight
     // loads are issued before any store so they are in flight together
     float4 v[8];
@@ -95,20 +109,29 @@ __device__ __forceinline__ void load_chunk(unsigned char *dst, const float *src,
     for (int q = 0; q < 8; q++) {
         int piece = q * THREADS + threadIdx.x;
         int r = piece >> 3, c = piece & 7;
-        *reinterpret_cast<float4 *>(dst + r * 128 + ((c ^ (r & 7)) << 4)) = v[q];
+        const int off = r * 128 + ((c ^ (r & 7)) << 4);
+        if constexpr (SPLIT) {
+            const float4 h = make_float4(tf32_hi(v[q].x), tf32_hi(v[q].y), tf32_hi(v[q].z), tf32_hi(v[q].w));
+            *reinterpret_cast<float4 *>(dst + off) = h;
+            *reinterpret_cast<float4 *>(dst_lo + off) =
+                make_float4(v[q].x - h.x, v[q].y - h.y, v[q].z - h.z, v[q].w - h.w);
+        } else {
+            *reinterpret_cast<float4 *>(dst + off) = v[q];
+        }
     }
 }
 
 // A[i][j] -= sum_{k<K} L[i][k] * W[j][k] for the lower tiles of rows/cols
 // [k1, n).  L = Abase + k0 (row-major, ld), W row-major with leading dim ldw.
 // Each CTA takes lower tile number blockIdx.x.
+template <bool SPLIT>
 __global__ void __launch_bounds__(THREADS, 1) k_update_tf32(int n, long long ld, float *A, int k0, int K, int k1,
                                                            const float *W, int ldw, unsigned long long *flags) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // align the operand stages to 1024 B (swizzle atoms)
     unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<size_t>(smem_raw) + 1023) & ~size_t(1023));
-    unsigned char *sa[2] = {base, base + 2 * CHUNK_BYTES};
-    unsigned char *sb[2] = {base + CHUNK_BYTES, base + 3 * CHUNK_BYTES};
+    // stage s: L hi, W hi (and for SPLIT: L lo, W lo), CHUNK_BYTES each
+    constexpr int PER_STAGE = SPLIT ? 4 : 2;
     __shared__ unsigned long long bars[3];
     __shared__ unsigned tmem_slot;
     __shared__ int s_bad;
@@ -143,25 +166,34 @@ __global__ void __launch_bounds__(THREADS, 1) k_update_tf32(int n, long long ld,
 
     const float *Lrows = A + k0;  // L[i][k] = A[i*ld + k0 + k]
     const int nchunks = (K + KC - 1) / KC;
-    unsigned use[2] = {0, 0};  // completed uses of each stage (mbarrier phases)
     bool ok = true;
     for (int c = 0; c < nchunks; c++) {
         const int s = c & 1;
         if (c >= 2) {
             // the MMAs of chunk c-2 read this stage: wait for their commit
-            if (!mbar_wait(&bars[s], use[s] & 1)) ok = false;
-            use[s]++;
+            // chunk c-2 was use number (c-2)/2 of this stage: its commit completes that phase
+            if (!mbar_wait(&bars[s], (unsigned)((c >> 1) - 1) & 1u)) ok = false;
         }
-        load_chunk(sa[s], Lrows, ld, i0, n, c * KC, K);
-        load_chunk(sb[s], W, ldw, j0, n, c * KC, K);
+        unsigned char *sa = base + s * PER_STAGE * CHUNK_BYTES, *sb = sa + CHUNK_BYTES;
+        unsigned char *sal = sa + 2 * CHUNK_BYTES, *sbl = sa + 3 * CHUNK_BYTES;  // SPLIT only
+        load_chunk<SPLIT>(sa, sal, Lrows, ld, i0, n, c * KC, K);
+        load_chunk<SPLIT>(sb, sbl, W, ldw, j0, n, c * KC, K);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (threadIdx.x == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const unsigned long long da = smem_desc(saddr(sa[s])), db = smem_desc(saddr(sb[s]));
+            const unsigned long long da = smem_desc(saddr(sa)), db = smem_desc(saddr(sb));
+            const unsigned long long dal = smem_desc(saddr(sal)), dbl = smem_desc(saddr(sbl));
 #pragma unroll
-            for (int kk = 0; kk < KC / 8; kk++)  // 8 TF32 = 32 B per MMA step: +2 in the descriptor
-                mma_tf32(tmem, da + 2 * kk, db + 2 * kk, (c > 0 || kk > 0) ? 1u : 0u);
+            for (int kk = 0; kk < KC / 8; kk++) {  // 8 TF32 = 32 B per MMA step: +2 in the descriptor
+                if constexpr (SPLIT) {
+                    mma_tf32(tmem, dal + 2 * kk, db + 2 * kk, (c > 0 || kk > 0) ? 1u : 0u);
+                    mma_tf32(tmem, da + 2 * kk, dbl + 2 * kk, 1u);
+                    mma_tf32(tmem, da + 2 * kk, db + 2 * kk, 1u);
+                } else {
+                    mma_tf32(tmem, da + 2 * kk, db + 2 * kk, (c > 0 || kk > 0) ? 1u : 0u);
+                }
+            }
             mma_commit(&bars[s]);
         }
     }
@@ -223,7 +255,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_update_tf32(int n, long long ld,
     if (threadIdx.x == 0 && s_bad) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
 }
 
-constexpr size_t SMEM_BYTES = 4 * CHUNK_BYTES + 1024;  // two stages of L and W + alignment slack
+// two stages of the operand chunks + alignment slack
+constexpr size_t smem_bytes(bool split) { return (split ? 8 : 4) * (size_t)CHUNK_BYTES + 1024; }
 
 }  // namespace tc
 }  // namespace mp

@@ -36,6 +36,7 @@ STATUS = {0: "MP_OK", 1: "MP_ERR_ARG", 2: "MP_ERR_OOM", 3: "MP_ERR_CUDA", 4: "MP
           9: "MP_ERR_TIMEOUT", 10: "MP_ERR_LIMIT"}
 NONLINEAR, GAUSS_SEIDEL, LAPACK = 0, 1, 2
 FP64, MIXED = 0, 1
+MIXED_TF32, MIXED_TF32X3 = 1, 3
 SCATTER_ATOMIC, SCATTER_FIXED = 0, 1
 ORDER_STORAGE, ORDER_ID = 0, 1
 VEC = {"F0": 0, "F1": 1, "d": 2, "g": 3, "uh": 4, "den": 5, "ef": 6, "G": 7, "y": 8, "K": 16, "J": 17}
@@ -57,7 +58,7 @@ EXPORTED = [
     "mp_update_ef", "mp_field_download", "mp_mesh_geometry", "mp_fe_geometry", "mp_inlet_faces",
     "mp_injector_create", "mp_injector_destroy", "mp_injector_sample", "mp_injector_count",
     "mp_injector_get_rem", "mp_injector_set_rem", "mp_set_track_ids", "mp_kernel_launches",
-    "mp_device_buffer", "mp_push_particles_noalloc",
+    "mp_device_buffer", "mp_push_particles_noalloc", "mp_set_mixed_factor",
 ]
 
 
@@ -143,6 +144,7 @@ def lib():
         L.mp_set_walk_limit.argtypes = [vp, i32]
         L.mp_set_scatter_mode.argtypes = [vp, C.c_int]
         L.mp_set_sort_period.argtypes = [vp, i32]
+        L.mp_set_mixed_factor.argtypes = [vp, C.c_int]
         L.mp_set_particle_form.argtypes = [vp, C.c_int]
         L.mp_set_track_ids.argtypes = [vp, C.c_int]
         L.mp_kernel_launches.argtypes = [vp, C.POINTER(i64)]
@@ -421,6 +423,10 @@ class Context:
 
     def set_scatter_mode(self, mode):
         self._c(lib().mp_set_scatter_mode(self.h, mode))
+
+    def set_mixed_factor(self, mode):
+        """MIXED_TF32 or MIXED_TF32X3: tensor-core arithmetic of the mixed-form factorization."""
+        self._c(lib().mp_set_mixed_factor(self.h, mode))
 
     def set_sort_period(self, steps):
         self._c(lib().mp_set_sort_period(self.h, steps))

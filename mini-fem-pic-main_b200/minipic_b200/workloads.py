@@ -11,7 +11,7 @@ a 0.1 eV Maxwellian (sigma = sqrt(kTi*QE/m) ~ 776 m/s), each ion in the Kuhn
 tet that contains it.
 
     python workloads.py push   --config 1 --steps 4 [--form mixed] [--sort 10]
-    python workloads.py newton --config 0 --steps 2 [--form mixed]
+    python workloads.py newton --config 0 --steps 2 [--form mixed] [--mixed-factor tf32]
 
 The drivers print one JSON line per run with the device times measured by
 CUDA events inside the library (push kernel; Newton step).
@@ -101,6 +101,7 @@ def newton_driver(args):
     with tempfile.TemporaryDirectory() as wd:
         kd, deck, pos, vel, cell = make_workload(cfg, wd, seed=1234, n_ions=min(cfg["n_ions"], 200_000))
         ctx = mp.Context(deck.mesh)
+        ctx.set_mixed_factor(mp.MIXED_TF32 if getattr(args, "mixed_factor", "tf32x3") == "tf32" else mp.MIXED_TF32X3)
         ctx.fe_setup(**fe_arrays(cfg, deck))
         ctx.append(pos, vel, cell)
         ctx.push(mp.QE / (16 * mp.AMU), cfg["dt"], cfg["spwt"] * cfg["n_ions"] / len(cell))
@@ -110,6 +111,7 @@ def newton_driver(args):
             out.append({"step": k, "newton_ms": st.ms_total, "factor_ms": st.ms_factor,
                         "refinements": st.linear_iterations, "residual": st.linear_residual})
         print(json.dumps({"driver": "newton", "config": cfg["label"], "form": args.form,
+                          "mixed_factor": getattr(args, "mixed_factor", "tf32x3"),
                           "unknowns": int(fe_arrays(cfg, deck)["neq"]), "steps": out}))
         ctx.close()
 
@@ -122,6 +124,8 @@ def main():
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--sort", type=int, default=0)
     ap.add_argument("--n", type=int, default=0, help="override the mesh's hexes per side (newton driver)")
+    ap.add_argument("--mixed-factor", default="tf32x3", choices=["tf32", "tf32x3"],
+                    help="tensor-core arithmetic of the mixed-form factorization (newton driver)")
     args = ap.parse_args()
     (push_driver if args.driver == "push" else newton_driver)(args)
 
