@@ -29,6 +29,9 @@
  *   mp_mesh_geometry              LoadVolumeMesh geometry precompute, src/meshes.cpp:87-251
  *   mp_fe_geometry                FESolver::computeNX + ID/LM, src/FESolver.cpp:108-118, 207-287
  *   mp_injector_*                 InjectIons, src/mini-pic.cpp:208-265
+ *   mp_adjoint_*                  no reference counterpart: derivatives of K steps of
+ *                                 MoveParticles + InjectIons (src/mini-pic.cpp:208-320)
+ *                                 with respect to the node potential and the drift
  */
 #ifndef MINIPIC_CUDA_H
 #define MINIPIC_CUDA_H
@@ -284,6 +287,56 @@ int mp_injector_count(mp_injector *inj, double plasma_den, double ion_velocity, 
                       int64_t *n_next);
 int mp_injector_get_rem(mp_injector *inj, double *rem);
 int mp_injector_set_rem(mp_injector *inj, double rem);
+
+/* ---- adjoint of K push + scatter steps ---------------------------------------
+ * phi (node potential, uh's layout) is held for K steps, so ef = updateEf(phi)
+ * (src/FESolver.cpp:622-636) is fixed and each particle moves on its own:
+ *   injected at step k0: v = inlet_dir*v_drift + v_th - (q_over_m*ef[c])*(0.5*dt)
+ *                        (src/mini-pic.cpp:239-257; v_th = 0 is the reference's cold beam)
+ *   each step:           the MoveParticles kernel body and XtoLtet walk
+ *                        (src/mini-pic.cpp:287-308, src/meshes.h:75-100)
+ * Outputs: den, the last step's node density normalised by spwt/Vnode
+ * (src/mini-pic.cpp:319), and flux, the wall energy flux
+ *   F = sum over particles leaving through a wall face of spwt*(0.5*mass)*|v|^2
+ * (v after the exit step's kick; a wall face is a boundary face whose three
+ * nodes have wall_nodes[n] != 0).  Derivatives treat the walk as piecewise
+ * fixed (cells and exits held).  Particles keep their slots for the K steps;
+ * the forward stores each slot's state every checkpoint_every steps and the
+ * reverse recomputes each segment from its checkpoint.
+ * Vector arguments (phi, den, bars, tangents, particle arrays) may be host or
+ * device memory. */
+enum { MP_ADJ_WALK = 0,    /* walk with XtoLtet (records the path if asked) */
+       MP_ADJ_PINNED = 1   /* replay the recorded path: the piecewise-fixed model itself */ };
+typedef struct {
+    int64_t slots;        /* particles carried: initial population + injections */
+    int64_t alive;        /* inside the domain after the last step */
+    int64_t wall_exits;   /* left through a wall face */
+    int64_t other_exits;  /* left through another boundary face */
+    double flux;          /* wall energy flux F [J] */
+    float ms;             /* device time of the forward */
+} mp_adjoint_stats;
+/* steps K >= 1; checkpoint_every in [1, 32]; inlet_dir[3] is the inlet face
+ * normal of InjectIons; nx [n_tets][4][3] (FESolver::NX) or NULL for the FE
+ * setup's; record_path keeps the walked cells for MP_ADJ_PINNED replays. */
+int mp_adjoint_setup(mp_ctx *ctx, int32_t steps, int32_t checkpoint_every, double q_over_m, double mass,
+                     double dt, double spwt, const double *inlet_dir, const uint8_t *wall_nodes, const double *nx,
+                     int record_path);
+/* Adds n particles entering at first_step (0 = the initial population).
+ * pos/vel packed [n][3]; injected != 0: vel is the thermal part v_th and the
+ * drift and rewind are applied as above; injected == 0: vel is the velocity. */
+int mp_adjoint_add_particles(mp_ctx *ctx, int32_t first_step, int injected, int64_t n, const double *pos,
+                             const double *vel, const int32_t *cell);
+/* Runs the K steps: den_out [n_nodes] (nullable), stats (nullable).  Keeps the
+ * tape (checkpoints, outcomes) for mp_adjoint_backward / mp_adjoint_tangent. */
+int mp_adjoint_forward(mp_ctx *ctx, const double *phi, double v_drift, int mode, double *den_out,
+                       mp_adjoint_stats *st);
+int mp_adjoint_flux(mp_ctx *ctx, double *flux);
+/* Vector-Jacobian product at the last forward: phi_bar = (dden/dphi)^T den_bar
+ * + (dF/dphi)^T flux_bar, *v_drift_bar likewise.  den_bar NULL means zero. */
+int mp_adjoint_backward(mp_ctx *ctx, const double *den_bar, double flux_bar, double *phi_bar, double *v_drift_bar);
+/* Jacobian-vector product at the last forward: dden = dden/dphi dphi + dden/dvd dv_drift,
+ * *dflux likewise (the tangents a coupled ion-phi Newton-Krylov solve uses). */
+int mp_adjoint_tangent(mp_ctx *ctx, const double *dphi, double dv_drift, double *dden, double *dflux);
 
 #ifdef __cplusplus
 }

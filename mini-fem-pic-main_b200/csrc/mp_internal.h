@@ -159,6 +159,8 @@ struct mp_ctx {
 
     mp::Timer t0, t1, tp, ts;
     long long launches = 0;
+
+    void *adjoint = nullptr;              // adjoint state (mp_adjoint.cu), created by mp_adjoint_setup
 };
 
 namespace mp {
@@ -192,5 +194,6 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st);
 int fe_update_d(mp_ctx *ctx, double *l2_out);
 int fe_uh(mp_ctx *ctx);
 int fe_assemble(mp_ctx *ctx);
+void adjoint_free(mp_ctx *ctx);
 
 }  // namespace mp

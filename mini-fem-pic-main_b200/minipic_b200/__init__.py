@@ -59,6 +59,8 @@ EXPORTED = [
     "mp_injector_create", "mp_injector_destroy", "mp_injector_sample", "mp_injector_count",
     "mp_injector_get_rem", "mp_injector_set_rem", "mp_set_track_ids", "mp_kernel_launches",
     "mp_device_buffer", "mp_push_particles_noalloc", "mp_set_mixed_factor",
+    "mp_adjoint_setup", "mp_adjoint_add_particles", "mp_adjoint_forward", "mp_adjoint_flux",
+    "mp_adjoint_backward", "mp_adjoint_tangent",
 ]
 
 
@@ -100,6 +102,11 @@ class StepStats(C.Structure):
 class NewtonStats(C.Structure):
     _fields_ = [("newton_iterations", C.c_int32), ("linear_iterations", C.c_int32), ("l2", C.c_double),
                 ("linear_residual", C.c_double), ("ms_total", C.c_double), ("ms_factor", C.c_double)]
+
+
+class AdjointStats(C.Structure):
+    _fields_ = [("slots", C.c_int64), ("alive", C.c_int64), ("wall_exits", C.c_int64),
+                ("other_exits", C.c_int64), ("flux", C.c_double), ("ms", C.c_float)]
 
 
 _lib = None
@@ -145,6 +152,12 @@ def lib():
         L.mp_set_scatter_mode.argtypes = [vp, C.c_int]
         L.mp_set_sort_period.argtypes = [vp, i32]
         L.mp_set_mixed_factor.argtypes = [vp, C.c_int]
+        L.mp_adjoint_setup.argtypes = [vp, i32, i32, d, d, d, d, vp, vp, vp, C.c_int]
+        L.mp_adjoint_add_particles.argtypes = [vp, i32, C.c_int, i64, vp, vp, vp]
+        L.mp_adjoint_forward.argtypes = [vp, vp, d, C.c_int, vp, C.POINTER(AdjointStats)]
+        L.mp_adjoint_flux.argtypes = [vp, C.POINTER(d)]
+        L.mp_adjoint_backward.argtypes = [vp, vp, d, vp, C.POINTER(d)]
+        L.mp_adjoint_tangent.argtypes = [vp, vp, d, vp, C.POINTER(d)]
         L.mp_set_particle_form.argtypes = [vp, C.c_int]
         L.mp_set_track_ids.argtypes = [vp, C.c_int]
         L.mp_kernel_launches.argtypes = [vp, C.POINTER(i64)]

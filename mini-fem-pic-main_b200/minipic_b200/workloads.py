@@ -6,6 +6,7 @@ kTe = 2 eV, inlet x=0 at 0 V, wall x=0.1 at -5 V):
   0  8^3 hexes (3,072 tets), ~50k ions, dt 1e-7, spwt 200
   1  20^3 hexes (48,000 tets), ~2M ions, dt 5e-8, spwt 5
   2  32^3 hexes minus a centred r=0.02 m sphere at -10 V, ~50M ions, dt 5e-8
+  3  16^3 hexes (24,576 tets), ~1M ions, adjoint over K=20 steps, checkpoints every 5
 The ion population is seeded at steady state: uniform in the box, drift plus
 a 0.1 eV Maxwellian (sigma = sqrt(kTi*QE/m) ~ 776 m/s), each ion in the Kuhn
 tet that contains it.
@@ -38,6 +39,8 @@ CONFIGS = {
     0: dict(n=8, n_ions=50_000, dt=1e-7, spwt=200.0, sphere=None, label="kuhn8_50k_fp64"),
     1: dict(n=20, n_ions=2_000_000, dt=5e-8, spwt=5.0, sphere=None, label="kuhn20_2M_fp64"),
     2: dict(n=32, n_ions=50_000_000, dt=5e-8, spwt=0.2, sphere=(50.0, 50.0, 50.0, 20.0), label="kuhn32s_50M_mixed"),
+    3: dict(n=16, n_ions=1_000_000, dt=1e-7, spwt=5.0, sphere=None, label="kuhn16_1M_adjoint_K20",
+            adjoint_steps=20, checkpoint_every=5),
 }
 KTI_EV = 0.1
 SPHERE_POTENTIAL = -10.0
@@ -63,6 +66,47 @@ def make_workload(cfg: dict, workdir: str, seed: int, n_ions: int | None = None)
 
 def fe_arrays(cfg: dict, deck):
     return deck.fe_desc_arrays(SPHERE_POTENTIAL if cfg["sphere"] else None)
+
+
+def adjoint_phi(mesh, wall_potential: float = -5.0) -> np.ndarray:
+    """A smooth node potential for the adjoint workloads: the inlet-to-wall ramp
+    (0 V at x=0, wall_potential at x=L) plus a transverse bump of 0.5 V."""
+    L = float(mesh.node_pos[:, 0].max())
+    x, y, z = (mesh.node_pos[:, d] / L for d in range(3))
+    return wall_potential * x + 0.5 * np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z)
+
+
+def make_adjoint_case(cfg: dict, workdir: str, seed: int, n_ions: int | None = None, steps: int | None = None):
+    """The adjoint workload: the deck, the initial population (first step 0)
+    and K steps of the reference injector's inlet samples with a 0.1 eV
+    Maxwellian thermal part (injected = 1, first step k).  Returns (deck,
+    slots dict of first/inj/pos/vel/cell, K)."""
+    kd, deck, pos, vel, cell = make_workload(cfg, workdir, seed, n_ions=n_ions)
+    K = steps or cfg.get("adjoint_steps", 20)
+    m = deck.mesh
+    rng = np.random.default_rng(seed + 1)
+    sigma = np.sqrt(KTI_EV * mp.QE / (16 * mp.AMU))
+    inj = mp.Injector(m, seed=0)
+    P = deck.params
+    firsts, injs, ps, vs, cs = [np.zeros(len(cell), np.int32)], [np.zeros(len(cell), np.uint8)], [pos], [vel], [cell]
+    for k in range(K):
+        p, _, c = inj.sample(P.plasma_den, P.ion_velocity, cfg["dt"], cfg["spwt"])
+        firsts.append(np.full(len(c), k, np.int32))
+        injs.append(np.ones(len(c), np.uint8))
+        ps.append(p)
+        vs.append(rng.normal(0.0, sigma, size=(len(c), 3)))
+        cs.append(c.astype(np.int32))
+    slots = {"first": np.concatenate(firsts), "inj": np.concatenate(injs), "pos": np.concatenate(ps),
+             "vel": np.concatenate(vs), "cell": np.concatenate(cs)}
+    return deck, slots, K
+
+
+def load_adjoint(adj, slots):
+    """Adds the slots to an Adjoint, grouped by (first step, injected)."""
+    keys = slots["first"].astype(np.int64) * 2 + slots["inj"]
+    for key in np.unique(keys):
+        sel = keys == key
+        adj.add_particles(int(key // 2), bool(key % 2), slots["pos"][sel], slots["vel"][sel], slots["cell"][sel])
 
 
 def push_driver(args):

@@ -205,3 +205,52 @@ class FE:
 
     def update_ef(self):
         return update_ef(self.mesh, self.nx, self.uh)
+
+
+# ---------------------------------------------------------------------------
+# dual-number (forward-mode) build of the push: oracle/dual.cpp -> libdual.so
+
+DUAL_PATH = os.path.join(HERE, "libdual.so")
+_dual = None
+
+
+def dual_available() -> bool:
+    return os.path.exists(DUAL_PATH)
+
+
+def _dual_lib():
+    global _dual
+    if _dual is None:
+        L = C.CDLL(DUAL_PATH)
+        vp, i, d, l = C.c_void_p, C.c_int, C.c_double, C.c_long
+        L.or_dual_ksteps.restype = i
+        L.or_dual_ksteps.argtypes = ([i] + [vp] * 8 + [i, vp, vp, l] + [vp] * 5 + [i, d, d, d, d, vp, vp, vp, d, d]
+                                     + [vp] * 10)
+        _dual = L
+    return _dual
+
+
+def dual_ksteps(mesh, nx, wall_nodes, slots, K, qm, mass, dt, spwt, inlet_dir, phi, vd, dphi=None, dvd=0.0):
+    """K push + scatter steps with phi held (the adjoint's model) in dual
+    numbers.  slots: dict of first [n] int32, inj [n] uint8, pos/vel [n][3],
+    cell [n] int32.  Returns dict den, dden, flux, dflux, kind, exit, pos,
+    vel, cell."""
+    n = int(slots["cell"].size)
+    f = lambda a, t: np.ascontiguousarray(a, dtype=t)  # noqa: E731
+    first, inj = f(slots["first"], np.int32), f(slots["inj"], np.uint8)
+    pos, vel, cell = f(slots["pos"], np.float64), f(slots["vel"], np.float64), f(slots["cell"], np.int32)
+    out = {"den": np.zeros(mesh.n_nodes), "dden": np.zeros(mesh.n_nodes), "kind": np.zeros(n, np.int32),
+           "exit": np.zeros(n, np.int32), "pos": np.zeros((n, 3)), "vel": np.zeros((n, 3)),
+           "cell": np.zeros(n, np.int32), "path": np.zeros(n, np.uint64)}
+    flux, dflux = C.c_double(0), C.c_double(0)
+    dphi = None if dphi is None else f(dphi, np.float64)
+    rc = _dual_lib().or_dual_ksteps(
+        mesh.n_tets, _p(mesh.con), _p(mesh.volume), _p(mesh.alpha), _p(mesh.beta), _p(mesh.gamma), _p(mesh.delta),
+        _p(mesh.cell_con), _p(f(nx, np.float64)), mesh.n_nodes, _p(mesh.node_volume), _p(f(wall_nodes, np.uint8)),
+        n, _p(first), _p(inj), _p(pos), _p(vel), _p(cell), K, qm, mass, dt, spwt, _p(f(inlet_dir, np.float64)),
+        _p(f(phi, np.float64)), _p(dphi), vd, dvd, _p(out["den"]), _p(out["dden"]), C.byref(flux), C.byref(dflux),
+        _p(out["kind"]), _p(out["exit"]), _p(out["pos"]), _p(out["vel"]), _p(out["cell"]), _p(out["path"]))
+    if rc != 0:
+        raise RuntimeError("dual push: a tet walk did not end")
+    out["flux"], out["dflux"] = flux.value, dflux.value
+    return out
