@@ -207,6 +207,7 @@ int mp_create(int device, const mp_mesh_desc *m, mp_ctx **out) {
         if (m->node_pos)
             for (int d = 0; d < 3; d++) npos[3 * n + d] = strided<double>(m->node_pos, m->node_pos_stride, n)[d];
     }
+    bool small = true;  // 0 < V < 1 for every tet: the push's exact division-free inside test holds
     for (int t = 0; t < nt; t++) {
         TetRec &r = rec[t];
         std::memset(&r, 0, sizeof(r));
@@ -217,6 +218,7 @@ int mp_create(int device, const mp_mesh_desc *m, mp_ctx **out) {
         const double *ga = strided<double>(m->gamma, m->gamma_stride, t);
         const double *de = strided<double>(m->delta, m->delta_stride, t);
         r.volume = *strided<double>(m->volume, m->volume_stride, t);
+        if (!(r.volume > 0.0 && r.volume < 1.0)) small = false;
         for (int i = 0; i < 4; i++) {
             if (c[i] < 0 || c[i] >= nn || cc[i] < -1 || cc[i] >= nt) {
                 delete ctx;
@@ -238,6 +240,7 @@ int mp_create(int device, const mp_mesh_desc *m, mp_ctx **out) {
         }
         for (int d = 0; d < 3; d++) x0[4 * (size_t)t + d] = npos[3 * (size_t)c[0] + d];
     }
+    ctx->small_tets = small;
 #define ALLOC(ptr, bytes) if (cudaMalloc(&(ptr), (bytes)) != cudaSuccess) return bail(MP_ERR_OOM)
     ALLOC(ctx->tets, sizeof(TetRec) * nt);
     ALLOC(ctx->tets32, sizeof(TetRec32) * nt);

@@ -101,6 +101,7 @@ struct mp_ctx {
 
     // mesh
     int n_nodes = 0, n_tets = 0;
+    bool small_tets = false;              // every tet volume < 1: exact division-free inside test
     mp::TetRec *tets = nullptr;           // [n_tets]
     mp::TetRec32 *tets32 = nullptr;       // [n_tets] (mixed form)
     double *tet_x0 = nullptr;             // [n_tets][4] vertex 0 position (x,y,z,pad)

@@ -127,8 +127,7 @@ __device__ __forceinline__ bool group_sum4(int key, T v[4]) {
     unsigned peers = __match_any_sync(FULL, key);
     int r = __popc(peers & lanemask_lt());
     int gsize = __popc(peers);
-    int maxg = __reduce_max_sync(FULL, gsize);
-    for (int s = 1; s < maxg; s <<= 1) {
+    for (int s = 1; __any_sync(FULL, s < gsize); s <<= 1) {
         int pr = r + s;
         int src = pr < gsize ? nth_set_bit(peers, pr) : lane;
         T t[4];
@@ -142,13 +141,42 @@ __device__ __forceinline__ bool group_sum4(int key, T v[4]) {
     return r == 0;
 }
 
-// Density scatter of one warp, aggregated over the lanes that sit in one tet,
-// plus the step statistics.  All 32 lanes call it; `state` 1 = inside (scatter),
-// 2 = kept after hitting the hop limit, 3 = left the domain, 0 = nothing.
+// Step statistics of one thread, accumulated over all the tiles a persistent
+// CTA pushes and reduced once per warp when the kernel ends: a warp reduction
+// per tile costs more than the scatter itself.
+struct PushStats {
+    unsigned hops = 0, hmax = 0, exits = 0, near = 0;
+    __device__ __forceinline__ void add(int state, int h, int nr) {
+        hops += (unsigned)h;
+        hmax = hmax > (unsigned)h ? hmax : (unsigned)h;
+        exits += state == 3;
+        near += (unsigned)nr;
+    }
+    // all 32 lanes call it
+    __device__ __forceinline__ void flush(unsigned long long *counters) {
+        const unsigned FULL = 0xffffffffu;
+        const unsigned hs = __reduce_add_sync(FULL, hops), hm = __reduce_max_sync(FULL, hmax);
+        const unsigned ex = __reduce_add_sync(FULL, exits), nr = __reduce_add_sync(FULL, near);
+        if ((threadIdx.x & 31) == 0) {
+            if (hs) {
+                atomicAdd(&counters[C_HOPS], (unsigned long long)hs);
+                atomicMax(&counters[C_MAX_HOPS], (unsigned long long)hm);
+            }
+            if (ex) {
+                atomicAdd(&counters[C_EXITS], (unsigned long long)ex);
+                atomicAdd(&counters[C_DEAD], (unsigned long long)ex);
+            }
+            if (nr) atomicAdd(&counters[C_NEAR], (unsigned long long)nr);
+        }
+    }
+};
+
+// Density scatter of one warp, aggregated over the lanes that sit in one tet.
+// All 32 lanes call it; `state` 1 = inside (scatter), 2 = kept after hitting
+// the hop limit, 3 = left the domain, 0 = nothing.
 template <typename Lc>
 __device__ __forceinline__ void scatter_warp(int state, int cell, const int con[4], Lc lcv[4], double *den,
-                                             unsigned long long *den_fixed, int fixed, unsigned long long *counters,
-                                             int hops) {
+                                             unsigned long long *den_fixed, int fixed) {
     const int lane = threadIdx.x & 31;
     __syncwarp();
     int key = state == 1 ? cell : -2 - lane;
@@ -170,19 +198,6 @@ __device__ __forceinline__ void scatter_warp(int state, int cell, const int con[
         if (leader && state == 1) {
 #pragma unroll
             for (int i = 0; i < 4; i++) atomicAdd(&den[con[i]], sv[i]);
-        }
-    }
-    int hsum = __reduce_add_sync(0xffffffffu, hops);
-    int hmax = __reduce_max_sync(0xffffffffu, hops);
-    int exits = __popc(__ballot_sync(0xffffffffu, state == 3));
-    if (lane == 0) {
-        if (hsum) {
-            atomicAdd(&counters[C_HOPS], (unsigned long long)hsum);
-            atomicMax(&counters[C_MAX_HOPS], (unsigned long long)hmax);
-        }
-        if (exits) {
-            atomicAdd(&counters[C_EXITS], (unsigned long long)exits);
-            atomicAdd(&counters[C_DEAD], (unsigned long long)exits);
         }
     }
 }
@@ -234,6 +249,7 @@ __device__ __forceinline__ void issue_tile_f32(StageF32 *st, const PartsF32 &p, 
     bulk_load(st->cell, p.cell + base, b4, bar);
 }
 
+template <bool EXACT_CMP>
 __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_fp64(PushF64Args a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     StageF64 *stage = reinterpret_cast<StageF64 *>(smem_raw);
@@ -248,6 +264,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_fp64(PushF64Args a) {
     if (threadIdx.x == 0)
         for (long long k = 0; k < STAGES && k < mine; k++)
             issue_tile_f64(&stage[k], a.p, (blockIdx.x + k * gridDim.x) * (long long)PUSH_THREADS, n, &bars[k]);
+    PushStats stats;
     for (long long k = 0; k < mine; k++) {
         const int sidx = (int)(k % STAGES);
         mbar_wait(&bars[sidx], (unsigned)((k / STAGES) & 1), a.counters);
@@ -277,7 +294,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_fp64(PushF64Args a) {
             x = __dadd_rn(x, __dmul_rn(vx, a.dt));
             y = __dadd_rn(y, __dmul_rn(vy, a.dt));
             z = __dadd_rn(z, __dmul_rn(vz, a.dt));
-            int w = walk_fp64(a.tets, cell, x, y, z, lc, a.walk_limit, hops);
+            int w = walk_fp64<EXACT_CMP>(a.tets, cell, x, y, z, lc, a.walk_limit, hops);
             if (w == 1) {
                 state = 1;
                 const int4 c4 = __ldg(reinterpret_cast<const int4 *>(a.tets[cell].con));
@@ -293,8 +310,10 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_fp64(PushF64Args a) {
             a.p.vx[i] = vx; a.p.vy[i] = vy; a.p.vz[i] = vz;
             a.p.cell[i] = cell;
         }
-        scatter_warp<double>(state, cell, con, lc, a.den, a.den_fixed, a.fixed, a.counters, hops);
+        scatter_warp<double>(state, cell, con, lc, a.den, a.den_fixed, a.fixed);
+        stats.add(state, hops, 0);
     }
+    stats.flush(a.counters);
 }
 
 // Mixed form.  Position is an FP32 offset r from the owning tet's vertex 0 and
@@ -334,6 +353,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_mixed(PushF32Args a) {
     if (threadIdx.x == 0)
         for (long long k = 0; k < STAGES && k < mine; k++)
             issue_tile_f32(&stage[k], a.p, (blockIdx.x + k * gridDim.x) * (long long)PUSH_THREADS, n, &bars[k]);
+    PushStats stats;
     for (long long k = 0; k < mine; k++) {
         const int sidx = (int)(k % STAGES);
         mbar_wait(&bars[sidx], (unsigned)((k / STAGES) & 1), a.counters);
@@ -434,10 +454,10 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_mixed(PushF32Args a) {
             a.p.vx[i] = vx; a.p.vy[i] = vy; a.p.vz[i] = vz;
             a.p.cell[i] = cell;
         }
-        int nsum = __reduce_add_sync(0xffffffffu, near);
-        if ((threadIdx.x & 31) == 0 && nsum) atomicAdd(&a.counters[C_NEAR], (unsigned long long)nsum);
-        scatter_warp<float>(state, cell, con, lc, a.den, a.den_fixed, a.fixed, a.counters, hops);
+        scatter_warp<float>(state, cell, con, lc, a.den, a.den_fixed, a.fixed);
+        stats.add(state, hops, near);
     }
+    stats.flush(a.counters);
 }
 
 // den[n] *= spwt/node_volume[n] (src/mini-pic.cpp:319); fixed-point sums are
@@ -480,13 +500,16 @@ int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
         a.fixed = ctx->scatter_mode == MP_SCATTER_FIXED64;
         a.track_ids = ctx->track_ids;
         const size_t smem = sizeof(StageF64) * STAGES;
+        // division-free inside test when every tet volume is below 1 (see walk_fp64)
+        auto kern = ctx->small_tets ? k_push_fp64<true> : k_push_fp64<false>;
         if (!ctx->push_grid[0]) {
-            MP_CUDA(ctx, cudaFuncSetAttribute(k_push_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            ctx->push_grid[0] = grid_for(ctx, (const void *)k_push_fp64, PUSH_THREADS, smem);
+            MP_CUDA(ctx, cudaFuncSetAttribute(k_push_fp64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            MP_CUDA(ctx, cudaFuncSetAttribute(k_push_fp64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            ctx->push_grid[0] = grid_for(ctx, (const void *)kern, PUSH_THREADS, smem);
         }
         long long g = blocks < ctx->push_grid[0] ? blocks : ctx->push_grid[0];
         cudaEventRecord(ctx->tp.a, ctx->stream);
-        k_push_fp64<<<(unsigned)g, PUSH_THREADS, smem, ctx->stream>>>(a), ++ctx->launches;
+        kern<<<(unsigned)g, PUSH_THREADS, smem, ctx->stream>>>(a), ++ctx->launches;
         cudaEventRecord(ctx->tp.b, ctx->stream);
     } else {
         PushF32Args a;
