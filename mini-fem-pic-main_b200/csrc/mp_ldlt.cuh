@@ -17,7 +17,10 @@
 //
 // The FP32 instantiation is the factorization of the mixed form; its solve is
 // wrapped in FP64 iterative refinement (residual from the FP64 K and FP).
+#include <algorithm>
 #include <cmath>
+
+#include <cudaTypedefs.h>
 
 #include "mp_internal.h"
 #include "mp_tc.cuh"
@@ -33,88 +36,153 @@ __device__ __forceinline__ bool bad_pivot(T d) {
 
 // Factor the kb x kb diagonal block at (k0,k0): L (strict lower) and D written
 // back, and Linv = L_kk^-1 (unit lower, row-major NB x NB, zero outside kb x kb)
-// for the panel and the triangular solves, built during the elimination by
-// applying each step's row operations to an identity.  If b is non-null,
+// for the panel and the triangular solves.  If b is non-null,
 // z_k = L_kk^-1 b_k (the forward substitution riding on the factorization).
-// 256 threads; thread (column l = t & 63, phase ph = t >> 6) keeps rows
-// i = ph + 4k (k < 16) of column l of the block and of the inverse in
-// registers.  Step j publishes column j of the block and row j of the inverse
-// through shared memory (double-buffered), one barrier per step.
-// Dynamic smem: the inverse [NB][NB+1] (for z) and b.
+//
+// 256 threads, the block in shared memory (padded to 64 x 64 with an identity).
+// Four sub-panels of SUB = 16 columns:
+//   factor the sub-panel (64 x 16): 16 elimination steps, one barrier each;
+//     thread (row i, column quad g) updates its 4 columns from the step's
+//     published column (double-buffered), and the rows of the sub-panel's
+//     16 x 16 diagonal block apply the same row operation to an identity,
+//     which leaves that block's inverse;
+//   rank-16 update of the trailing block, 4 x 4 register tiles per thread.
+// The off-diagonal blocks of Linv follow by block substitution:
+//   X_qp = -X_qq sum_{r=p}^{q-1} L_qr X_rp.
+// Dynamic smem: A [64][65], Linv [64][65], W [64][17], T [16][17], w [2][64], b [64].
+constexpr int SUB = 16;
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
                                                    T *b, unsigned long long *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T(*sinv)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
-    T *sb = reinterpret_cast<T *>(smem_raw + sizeof(T) * NB * (NB + 1));
-    __shared__ T sw[2][NB];    // column j of the block, unscaled (rows >= j)
-    __shared__ T srow[2][NB];  // row j of the inverse (columns <= j)
-    const int t = threadIdx.x, l = t & 63, ph = t >> 6;
-    T a[16], v[16];
+    T(*sA)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
+    T(*sI)[NB + 1] = sA + NB;
+    T(*sW)[SUB + 1] = reinterpret_cast<T(*)[SUB + 1]>(sI + NB);
+    T(*sT)[SUB + 1] = sW + NB;
+    T *sw = reinterpret_cast<T *>(sT + SUB);  // [2][NB]
+    T *sb = sw + 2 * NB;
+    const int t = threadIdx.x;
+    // load the lower triangle, pad with an identity past kb; Linv starts as the identity
+    {
+        T v[16];
 #pragma unroll
-    for (int k = 0; k < 16; k++) {
-        const int i = ph + 4 * k;
-        a[k] = (i < kb && l <= i) ? A[(long long)(k0 + i) * ld + k0 + l] : T(0);
-        v[k] = (i == l && i < kb) ? T(1) : T(0);
-    }
-    if (b && t < kb) sb[t] = b[k0 + t];
-    // publish column 0 and row 0 of the inverse (e_0)
-    if (l == 0) {
+        for (int q = 0; q < 16; q++) {
+            const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
+            v[q] = (r < kb && c < kb && c <= r) ? A[(long long)(k0 + r) * ld + k0 + c] : T(0);
+        }
 #pragma unroll
-        for (int k = 0; k < 16; k++) sw[0][ph + 4 * k] = a[k];
+        for (int q = 0; q < 16; q++) {
+            const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
+            sA[r][c] = (r >= kb && r == c) ? T(1) : v[q];
+            sI[r][c] = r == c ? T(1) : T(0);
+        }
     }
-    if (ph == 0) srow[0][l] = l == 0 ? T(1) : T(0);
+    if (b && t < NB) sb[t] = t < kb ? b[k0 + t] : T(0);
     __syncthreads();
+    if (t < NB) sw[t] = sA[t][0];  // publish column 0
+    __syncthreads();
+    const int i = t >> 2, g = t & 3;  // this thread's row and column quad in the sub-panel
     bool singular = false;
-    for (int j = 0; j < kb; j++) {
-        const int buf = j & 1;
-        T d = sw[buf][j];
-        if (bad_pivot(d)) {
-            singular = true;
-            d = T(1);
-        }
-        const T rd = T(1) / d;
-        const T wl = sw[buf][l] * rd;    // l_lj, used by columns l > j
-        const T rc = srow[buf][l] * rd;  // Linv[j][l] / d, used by columns l <= j
-        const bool upd = l > j, inv = l <= j;
-        // column j+1 of the block (by its owner) and row j+1 of the inverse are
-        // final once this step's update has run: publish them into the other buffer
-        const int jn = j + 1, nb = jn & 1;
-        const bool pub = jn < kb;
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-            const int i = ph + 4 * k;
-            const T wi = sw[buf][i];
-            if (i > j && i < kb) {
-                if (upd && l <= i) a[k] -= wi * wl;
-                if (inv) v[k] -= wi * rc;
+    for (int p = 0; p < NB / SUB; p++) {
+        const int c0 = p * SUB;
+        // ---- factor the sub-panel: columns [c0, c0+16), rows [c0, 64) ----
+        for (int j = c0; j < c0 + SUB; j++) {
+            const T *w = sw + (j & 1) * NB;
+            T d = w[j];
+            if (bad_pivot(d)) {
+                singular = true;
+                d = T(1);
             }
-            if (pub && l == jn) sw[nb][i] = a[k];
-            if (pub && i == jn) srow[nb][l] = v[k];
-        }
-        if (l == j) {
+            const T rd = T(1) / d;
+            const T wi = w[i];
+            const T li = wi * rd;  // L[i][j] for i > j
+            if (i > j) {
 #pragma unroll
-            for (int k = 0; k < 16; k++)
-                if (ph + 4 * k > j) a[k] *= rd;  // column j becomes L's column
+                for (int cc = 0; cc < 4; cc++) {
+                    const int col = c0 + 4 * g + cc;
+                    if (col > j && col <= i) sA[i][col] -= li * w[col];
+                    if (col == j) sA[i][j] = li;
+                    // the sub-panel's diagonal block: the same row operation on the identity
+                    if (i < c0 + SUB && col <= j) sI[i][col] -= li * sI[j][col];
+                }
+            }
+            // publish column j+1 (final for this step once its own update above has run)
+            if (j + 1 < c0 + SUB && 4 * g <= j + 1 - c0 && j + 1 - c0 < 4 * g + 4) sw[((j + 1) & 1) * NB + i] = sA[i][j + 1];
+            __syncthreads();
         }
+        if (p == NB / SUB - 1) break;
+        // ---- rank-16 update of the trailing block [c0+16, 64)^2 ----
+        const int e0 = c0 + SUB;
+        if (t < NB) {
+#pragma unroll
+            for (int jl = 0; jl < SUB; jl++) sW[t][jl] = sA[t][c0 + jl] * sA[c0 + jl][c0 + jl];
+        }
+        __syncthreads();
+        {
+            const int ti = t >> 4, tk = t & 15;
+            const int r0 = 4 * ti, q0 = 4 * tk;
+            if (r0 + 3 >= e0 && q0 + 3 >= e0 && q0 <= r0 + 3) {
+                T acc[4][4] = {};
+#pragma unroll
+                for (int jl = 0; jl < SUB; jl++) {
+                    T av[4], wv[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) av[u] = sA[r0 + u][c0 + jl];
+#pragma unroll
+                    for (int v = 0; v < 4; v++) wv[v] = sW[q0 + v][jl];
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+#pragma unroll
+                        for (int v = 0; v < 4; v++) acc[u][v] += av[u] * wv[v];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+#pragma unroll
+                    for (int v = 0; v < 4; v++) {
+                        const int r = r0 + u, q = q0 + v;
+                        if (r >= e0 && q >= e0 && q <= r) sA[r][q] -= acc[u][v];
+                    }
+            }
+        }
+        __syncthreads();
+        if (t < NB) sw[(e0 & 1) * NB + t] = sA[t][e0];  // publish the next sub-panel's first column
         __syncthreads();
     }
     if (singular && t == 0) atomicOr(flags, FLAG_SINGULAR);
-    T *Lb = Linv;
+    // ---- off-diagonal blocks of Linv, by block distance ----
+    for (int dist = 1; dist < NB / SUB; dist++) {
+        for (int p = 0; p + dist < NB / SUB; p++) {
+            const int q = p + dist;
+            const int a = t >> 4, c = t & 15;  // element (a, c) of the 16 x 16 block
+            // T = sum_{r=p}^{q-1} L_qr X_rp
+            T acc = 0;
+            for (int r = p; r < q; r++)
 #pragma unroll
-    for (int k = 0; k < 16; k++) {
-        const int i = ph + 4 * k;
-        const bool in = i < kb && l < kb;
-        if (in && l <= i) A[(long long)(k0 + i) * ld + k0 + l] = a[k];
-        if (in && l == i) dvec[k0 + i] = a[k];
-        Lb[i * NB + l] = in ? v[k] : T(0);
-        sinv[i][l] = in ? v[k] : T(0);
+                for (int m = 0; m < SUB; m++) acc += sA[q * SUB + a][r * SUB + m] * sI[r * SUB + m][p * SUB + c];
+            sT[a][c] = acc;
+            __syncthreads();
+            // X_qp = -X_qq T (X_qq unit lower)
+            T x = 0;
+#pragma unroll
+            for (int m = 0; m < SUB; m++) x += sI[q * SUB + a][q * SUB + m] * sT[m][c];
+            sI[q * SUB + a][p * SUB + c] = -x;
+            __syncthreads();
+        }
     }
-    if (b) {
-        __syncthreads();
-        if (t < kb) {
+    // ---- write back L, D, Linv; z = Linv b ----
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
+        const bool in = r < kb && c < kb;
+        if (in && c <= r) A[(long long)(k0 + r) * ld + k0 + c] = sA[r][c];
+        Linv[r * NB + c] = in ? sI[r][c] : T(0);
+    }
+    if (t < kb) {
+        dvec[k0 + t] = sA[t][t];
+        if (b) {
             T z = 0;
-            for (int pp = 0; pp <= t; pp++) z += sinv[t][pp] * sb[pp];
+            for (int pp = 0; pp <= t; pp++) z += sI[t][pp] * sb[pp];
             b[k0 + t] = z;
         }
     }
@@ -499,7 +567,36 @@ struct LdltWork {
     T *dvec, *W, *s;
     T *Linv;       // [blocks][NB][NB] inverses of the diagonal blocks' L (the solves use them)
     int *ready;    // [2][blocks] per-block ready words of the two solves
+    float *split;  // tensor-core path: [4][n][256] hi/lo copies of one outer panel's L and W rows
 };
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// Map of a [rows][256] FP32 operand with row pitch `pitch` elements, loaded as
+// boxes of 32 (K) x 128 rows with the 128-byte swizzle the UMMA descriptors use.
+// base must be 16-byte aligned and pitch*4 a multiple of 16.
+static bool operand_map(CUtensorMap *m, const float *base, long long rows, long long pitch) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
+    if (!fn || rows < 1 || (reinterpret_cast<size_t>(base) & 15) || ((pitch * 4) & 15)) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)tc::PANEL, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
+    cuuint32_t box[2] = {(cuuint32_t)tc::KC, (cuuint32_t)tc::TILE};
+    cuuint32_t estr[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 static int g_solve_epoch = 0;
 
@@ -516,7 +613,7 @@ template <typename T>
 int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> w, bool factor,
                       int tc_terms = 0) {
     cudaStream_t st = ctx->stream;
-    const size_t diag_smem = sizeof(T) * (NB * (NB + 1) + NB);
+    const size_t diag_smem = sizeof(T) * (2 * NB * (NB + 1) + NB * (SUB + 1) + SUB * (SUB + 1) + 3 * NB);
     const size_t panel_smem = sizeof(T) * (64 * (NB + 1) + NB * (NB + 1) + 2 * NB);
     const size_t upd_smem = sizeof(T) * 2 * NB * 68;
     static bool attr = false;
@@ -530,9 +627,9 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         cudaFuncSetAttribute(k_ldlt_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_update_cols<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_update_cols<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(tc::k_update_tf32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(tc::k_update_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)tc::smem_bytes(false));
-        cudaFuncSetAttribute(tc::k_update_tf32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(tc::k_update_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)tc::smem_bytes(true));
         attr = true;
     }
@@ -563,12 +660,33 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                 }
             }
             if (P1 < n) {
-                long long tiles = (n - P1 + tc::TILE - 1) / tc::TILE;
-                long long nblk = tiles * (tiles + 1) / 2;
-                auto kern = tc_terms == 3 ? tc::k_update_tf32<true> : tc::k_update_tf32<false>;
-                kern<<<(unsigned)nblk, tc::THREADS, tc::smem_bytes(tc_terms == 3), st>>>(
-                    n, ld, reinterpret_cast<float *>(A), P0, P1 - P0, P1, reinterpret_cast<const float *>(w.W), PW,
-                    flags), ++ctx->launches;
+                // P1 < n: this outer panel is a full PW = 256 columns wide
+                const long long tiles = (n - P1 + tc::TILE - 1) / tc::TILE;
+                const long long ntiles = tiles * (tiles + 1) / 2;
+                const bool split = tc_terms == 3;
+                float *Af = reinterpret_cast<float *>(A);
+                const float *Wf = reinterpret_cast<const float *>(w.W);
+                CUtensorMap mLh, mWh, mLl, mWl;
+                bool ok;
+                if (split) {
+                    const size_t plane = (size_t)n * tc::PANEL;
+                    float *Lh = w.split, *Ll = w.split + plane, *Wh = w.split + 2 * plane, *Wl = w.split + 3 * plane;
+                    const long long q = (long long)(n - P1) * (tc::PANEL / 4);
+                    const int g = (int)std::min<long long>((q + 255) / 256, (long long)ctx->sm_count * 8);
+                    tc::k_split_panel<<<g, 256, 0, st>>>(n, ld, Af, P0, P1, Wf, PW, Lh, Ll, Wh, Wl), ++ctx->launches;
+                    ok = operand_map(&mLh, Lh, n - P1, tc::PANEL) && operand_map(&mWh, Wh, n - P1, tc::PANEL) &&
+                         operand_map(&mLl, Ll, n - P1, tc::PANEL) && operand_map(&mWl, Wl, n - P1, tc::PANEL);
+                } else {
+                    ok = operand_map(&mLh, Af + (long long)P1 * ld + P0, n - P1, ld) &&
+                         operand_map(&mWh, Wf + (long long)P1 * PW, n - P1, PW);
+                    mLl = mLh;
+                    mWl = mWh;
+                }
+                if (!ok) return fail(ctx, MP_ERR_CUDA, "cuTensorMapEncodeTiled failed for the tensor-core update");
+                const int grid = (int)std::min<long long>(ntiles, (long long)ctx->sm_count);
+                auto kern = split ? tc::k_update_tc<true> : tc::k_update_tc<false>;
+                kern<<<grid, tc::THREADS, tc::smem_bytes(split), st>>>(mLh, mWh, mLl, mWl, n, ld, Af, P1, ntiles, flags),
+                    ++ctx->launches;
             }
         }
     } else if (factor) {

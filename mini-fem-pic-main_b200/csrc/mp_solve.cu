@@ -84,7 +84,7 @@ static int check_flags(mp_ctx *ctx, unsigned long long mask, unsigned long long 
 // Scratch of the solvers, allocated on first use.
 struct SolveScratch {
     double *dvec64 = nullptr, *W64 = nullptr, *s64 = nullptr, *r = nullptr, *Linv64 = nullptr;
-    float *dvec32 = nullptr, *W32 = nullptr, *s32 = nullptr, *b32 = nullptr, *Linv32 = nullptr;
+    float *dvec32 = nullptr, *W32 = nullptr, *s32 = nullptr, *b32 = nullptr, *Linv32 = nullptr, *split32 = nullptr;
     int *ready = nullptr;
     int neq = 0;
 };
@@ -95,7 +95,7 @@ static int ensure_scratch(mp_ctx *ctx) {
     int n = ctx->neq;
     cudaFree(g_scr.dvec64); cudaFree(g_scr.W64); cudaFree(g_scr.s64); cudaFree(g_scr.r);
     cudaFree(g_scr.dvec32); cudaFree(g_scr.W32); cudaFree(g_scr.s32); cudaFree(g_scr.b32);
-    cudaFree(g_scr.Linv64); cudaFree(g_scr.Linv32); cudaFree(g_scr.ready);
+    cudaFree(g_scr.Linv64); cudaFree(g_scr.Linv32); cudaFree(g_scr.ready); cudaFree(g_scr.split32);
     g_scr = SolveScratch();
     MP_CUDA(ctx, cudaMalloc(&g_scr.dvec64, sizeof(double) * (n + 64)));
     MP_CUDA(ctx, cudaMalloc(&g_scr.W64, sizeof(double) * (size_t)(n + 64) * NB));
@@ -108,6 +108,7 @@ static int ensure_scratch(mp_ctx *ctx) {
     const size_t nblk = (n + NB - 1) / NB;
     MP_CUDA(ctx, cudaMalloc(&g_scr.Linv64, sizeof(double) * nblk * NB * NB));
     MP_CUDA(ctx, cudaMalloc(&g_scr.Linv32, sizeof(float) * nblk * NB * NB));
+    MP_CUDA(ctx, cudaMalloc(&g_scr.split32, sizeof(float) * 4 * (size_t)n * tc::PANEL));
     MP_CUDA(ctx, cudaMalloc(&g_scr.ready, sizeof(int) * 2 * ((n + NB - 1) / NB + 1)));
     MP_CUDA(ctx, cudaMemset(g_scr.ready, 0, sizeof(int) * 2 * ((n + NB - 1) / NB + 1)));
     g_scr.neq = n;
@@ -122,7 +123,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
     cudaEventRecord(ctx->t1.a, ctx->stream);
     if (form == MP_FORM_FP64) {
         MP_CUDA(ctx, cudaMemcpyAsync(ctx->y, ctx->G, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
-        LdltWork<double> w{g_scr.dvec64, g_scr.W64, g_scr.s64, g_scr.Linv64, g_scr.ready};
+        LdltWork<double> w{g_scr.dvec64, g_scr.W64, g_scr.s64, g_scr.Linv64, g_scr.ready, nullptr};
         rc = ldlt_factor_solve<double>(ctx, ctx->J, ld, n, ctx->y, w, true);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
@@ -137,7 +138,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         if (!ctx->J32) MP_CUDA(ctx, cudaMalloc(&ctx->J32, sizeof(float) * (size_t)ld * n));
         k_j_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(n, ld, ctx->J, ctx->J32), ++ctx->launches;
         MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * n, ctx->stream));
-        LdltWork<float> w{g_scr.dvec32, g_scr.W32, g_scr.s32, g_scr.Linv32, g_scr.ready};
+        LdltWork<float> w{g_scr.dvec32, g_scr.W32, g_scr.s32, g_scr.Linv32, g_scr.ready, g_scr.split32};
         double rn = 0, bn = 0;
         // r = G (y = 0), in FP32 for the first solve, which also factors J32
         rc = resid_norms(ctx, ctx->y, ctx->G, g_scr.r, g_scr.b32, &rn, &bn);
@@ -163,13 +164,15 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         }
     }
     unsigned long long bad = 0;
-    rc = check_flags(ctx, FLAG_SINGULAR, &bad);
+    rc = check_flags(ctx, FLAG_SINGULAR | FLAG_LOOKBACK_TIMEOUT, &bad);
     if (rc) return rc;
     if (st) {
         float ms = 0;
         cudaEventElapsedTime(&ms, ctx->t1.a, ctx->t1.b);
         st->ms_factor = ms;
     }
+    if (bad & FLAG_LOOKBACK_TIMEOUT)
+        return fail(ctx, MP_ERR_TIMEOUT, "a bounded wait in the factorization or the triangular solves gave up");
     if (bad) return fail(ctx, MP_ERR_SINGULAR, "LDL^T met a zero or non-finite pivot");
     return MP_OK;
 }

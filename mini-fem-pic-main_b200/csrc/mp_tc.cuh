@@ -1,35 +1,51 @@
 // Tensor-core (tcgen05, TF32 inputs, FP32 accumulators in TMEM) trailing update
 // of the mixed-form LDL^T:  A[i][j] -= sum_k L[i][k] W[j][k]  on the lower
-// 128x128 tiles of the trailing matrix.
+// 128x128 tiles of the trailing matrix, K = one 256-wide outer panel.
 //
-// One CTA per output tile, 128 threads (4 warps, one per 32 TMEM lanes).  The
-// K dimension streams through shared memory in 32-element chunks, two stages:
-// all threads copy a chunk of L (128 rows) and of W (128 rows) into the
-// K-major 128-byte-swizzled layout the UMMA descriptors describe, then one
-// thread issues four 128x128x8 tcgen05.mma (kind::tf32) and commits them to the
-// stage's mbarrier, which tells the loaders when the stage may be refilled.
-// The epilogue reads the accumulator with tcgen05.ld and subtracts it from the
-// tile in global memory.  No multicast and no cluster: each CTA loads its own
-// operands.  Every mbarrier wait is bounded; a timeout sets the error bit
-// FLAG_LOOKBACK_TIMEOUT, reported as MP_ERR_TIMEOUT by the caller.
+// Persistent, warp-specialised.  One CTA per SM walks the lower tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...:
+//   warp 0 (one lane)  producer: 2-D TMA tile loads (cp.async.bulk.tensor, no
+//                      multicast, 128-byte swizzle) of 32-wide K chunks of the
+//                      tile's L rows and W rows into STAGES shared-memory
+//                      stages, each completing on its stage's "full" mbarrier;
+//   warp 1 (one lane)  MMA issuer: tcgen05.mma.cta_group::1.kind::tf32 from the
+//                      stage into one of two 128-column TMEM accumulators, then
+//                      tcgen05.commit to the stage's "empty" mbarrier (frees it
+//                      for the producer) and, after a tile's last chunk, to the
+//                      accumulator's "full" mbarrier;
+//   warps 2-5          epilogue: tcgen05.ld of their 32 TMEM lanes (= tile rows),
+//                      A[row][col] -= acc for col <= row, then arrive on the
+//                      accumulator's "empty" mbarrier.
+// Two accumulators let the epilogue of one tile overlap the MMAs of the next.
 //
-// SPLIT (3xTF32): each FP32 operand x is split on the way into shared memory
-// into hi = x rounded to TF32 (11 significant bits) and lo = x - hi (exact in
-// FP32), and the product is accumulated as hi*hi + hi*lo + lo*hi, three MMAs on
-// the same TMEM accumulator.  The dropped lo*lo term is ~2^-22 relative, so the
-// update carries about FP32 accuracy instead of TF32's 2^-11, which is what the
-// FP64 refinement of the mixed solve converges against.
+// SPLIT (3xTF32): the operands arrive pre-split by k_split_panel into
+// hi = x rounded to TF32 (11 significant bits) and lo = x - hi (exact in FP32);
+// each tile accumulates hi*hi + hi*lo + lo*hi on the same TMEM accumulator.
+// The dropped lo*lo term is ~2^-22 relative, so the update carries about FP32
+// accuracy instead of TF32's 2^-11, which is what the FP64 refinement of the
+// mixed solve converges against.  Without SPLIT the TMA reads L straight from
+// the factor and W from the panel scratch.
+//
+// Every mbarrier wait is bounded.  A wait that gives up raises a CTA-wide abort
+// flag; every role leaves its loop, the producer and the MMA issuer wait
+// (bounded) for their copies and MMAs in flight, TMEM is freed, and the kernel
+// sets FLAG_LOOKBACK_TIMEOUT (reported as MP_ERR_TIMEOUT by the caller).
 #pragma once
+
+#include <cuda.h>
 
 #include "mp_internal.h"
 
 namespace mp {
 namespace tc {
 
-constexpr int TILE = 128;         // M = N = 128
-constexpr int KC = 32;            // K elements per chunk (one 128-byte swizzle atom row)
-constexpr int CHUNK_BYTES = TILE * KC * 4;  // 16 KB per operand per stage
-constexpr int THREADS = 128;
+constexpr int TILE = 128;                   // M = N = 128
+constexpr int KC = 32;                      // K elements per chunk (one 128-byte swizzle row)
+constexpr int PANEL = 256;                  // K of one launch: the outer panel width
+constexpr int NCHUNK = PANEL / KC;          // chunks per tile
+constexpr int CHUNK_BYTES = TILE * KC * 4;  // 16 KB per operand chunk
+constexpr int STAGES = 3;
+constexpr int THREADS = 192;                // producer warp, MMA warp, 4 epilogue warps
 constexpr long long SPIN_LIMIT = 1ll << 22;
 
 __device__ __forceinline__ unsigned saddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -42,8 +58,8 @@ __device__ __forceinline__ unsigned long long smem_desc(unsigned addr) {
 // Instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = 128.
 constexpr unsigned IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 
-__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(bar)) : "memory");
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
 }
 __device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
     unsigned ok;
@@ -54,11 +70,31 @@ __device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parit
         : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
-    long long spins = 0;
-    while (!mbar_try(bar, parity))
-        if (++spins > SPIN_LIMIT) return false;
-    return true;
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
+}
+// Bounded wait; false when it gave up (then the abort flag is set) or another
+// role already aborted.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, volatile int *abort) {
+    for (long long i = 0;; i++) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 255) == 255 && *abort) return false;
+        if (i > SPIN_LIMIT) {
+            *abort = 1;
+            return false;
+        }
+    }
+}
+
+// 2-D tiled TMA load of the box (KC, TILE) at element coordinates (x, y).
+__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, int x, int y, unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(saddr(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(saddr(bar))
+        : "memory");
 }
 
 __device__ __forceinline__ void mma_tf32(unsigned tmem_d, unsigned long long a, unsigned long long b, unsigned acc) {
@@ -73,190 +109,221 @@ __device__ __forceinline__ void mma_commit(unsigned long long *bar) {
                  : "memory");
 }
 
+// lower tile number -> (bi, bj), bj <= bi
+__device__ __forceinline__ void tile_coords(long long t, int &bi, int &bj) {
+    int b = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((long long)(b + 1) * (b + 2) / 2 <= t) b++;
+    while ((long long)b * (b + 1) / 2 > t) b--;
+    bi = b;
+    bj = (int)(t - (long long)b * (b + 1) / 2);
+}
+
 // x rounded to the nearest TF32 value (low 13 mantissa bits cleared)
 __device__ __forceinline__ float tf32_hi(float x) {
     return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
-// Copies rows [r0, r0+128) x cols [k0, k0+32) of a row-major FP32 matrix into
-// one swizzled chunk (and, for SPLIT, its hi part into dst and lo part into
-// dst_lo); rows >= nrows and cols >= kmax are zero.
-template <bool SPLIT>
-__device__ __forceinline__ void load_chunk(unsigned char *dst, unsigned char *dst_lo, const float *src, long long ld,
-                                           long long r0, long long nrows, int k0, int kmax) {
-    // 128 rows x 8 sixteen-byte pieces = 1024 pieces, 8 per thread; all eight
-    // loads are issued before any store so they are in flight together
-    float4 v[8];
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-        int piece = q * THREADS + threadIdx.x;
-        int r = piece >> 3, c = piece & 7;
-        long long row = r0 + r;
-        int col = k0 + c * 4;
-        v[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (row < nrows) {
-            const float *p = src + row * ld + col;
-            if (col + 3 < kmax) {
-                v[q] = __ldg(reinterpret_cast<const float4 *>(p));
-            } else {
-                if (col < kmax) v[q].x = __ldg(p);
-                if (col + 1 < kmax) v[q].y = __ldg(p + 1);
-                if (col + 2 < kmax) v[q].z = __ldg(p + 2);
-            }
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-        int piece = q * THREADS + threadIdx.x;
-        int r = piece >> 3, c = piece & 7;
-        const int off = r * 128 + ((c ^ (r & 7)) << 4);
-        if constexpr (SPLIT) {
-            const float4 h = make_float4(tf32_hi(v[q].x), tf32_hi(v[q].y), tf32_hi(v[q].z), tf32_hi(v[q].w));
-            *reinterpret_cast<float4 *>(dst + off) = h;
-            *reinterpret_cast<float4 *>(dst_lo + off) =
-                make_float4(v[q].x - h.x, v[q].y - h.y, v[q].z - h.z, v[q].w - h.w);
-        } else {
-            *reinterpret_cast<float4 *>(dst + off) = v[q];
-        }
+// Splits the outer panel's L rows (A[r][P0, P0+256)) and W rows (W[r][0, 256))
+// of rows r in [P1, n) into hi/lo arrays [n - P1][256] for the TMA.
+__global__ void k_split_panel(int n, long long ld, const float *__restrict__ A, int P0, int P1,
+                              const float *__restrict__ W, int ldw, float *Lh, float *Ll, float *Wh, float *Wl) {
+    const long long total = (long long)(n - P1) * (PANEL / 4);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long r = q / (PANEL / 4);
+        const int c = (int)(q % (PANEL / 4)) * 4;
+        const float4 x = __ldg(reinterpret_cast<const float4 *>(A + (P1 + r) * ld + P0 + c));
+        const float4 w = __ldg(reinterpret_cast<const float4 *>(W + (P1 + r) * (long long)ldw + c));
+        const float4 xh = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
+        const float4 wh = make_float4(tf32_hi(w.x), tf32_hi(w.y), tf32_hi(w.z), tf32_hi(w.w));
+        const long long o = r * PANEL + c;
+        *reinterpret_cast<float4 *>(Lh + o) = xh;
+        *reinterpret_cast<float4 *>(Ll + o) = make_float4(x.x - xh.x, x.y - xh.y, x.z - xh.z, x.w - xh.w);
+        *reinterpret_cast<float4 *>(Wh + o) = wh;
+        *reinterpret_cast<float4 *>(Wl + o) = make_float4(w.x - wh.x, w.y - wh.y, w.z - wh.z, w.w - wh.w);
     }
 }
 
-// A[i][j] -= sum_{k<K} L[i][k] * W[j][k] for the lower tiles of rows/cols
-// [k1, n).  L = Abase + k0 (row-major, ld), W row-major with leading dim ldw.
-// Each CTA takes lower tile number blockIdx.x.
+// A[i][j] -= sum_{k<256} L[i][k] W[j][k] on the lower 128x128 tiles of rows and
+// columns [P1, n).  The maps cover rows [P1, n) of the operands (rows past the
+// end read as zero).
 template <bool SPLIT>
-__global__ void __launch_bounds__(THREADS, 1) k_update_tf32(int n, long long ld, float *A, int k0, int K, int k1,
-                                                           const float *W, int ldw, unsigned long long *flags) {
+__global__ void __launch_bounds__(THREADS, 1)
+    k_update_tc(const __grid_constant__ CUtensorMap mLh, const __grid_constant__ CUtensorMap mWh,
+                const __grid_constant__ CUtensorMap mLl, const __grid_constant__ CUtensorMap mWl, int n, long long ld,
+                float *A, int P1, long long ntiles, unsigned long long *flags) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // align the operand stages to 1024 B (swizzle atoms)
     unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<size_t>(smem_raw) + 1023) & ~size_t(1023));
-    // stage s: L hi, W hi (and for SPLIT: L lo, W lo), CHUNK_BYTES each
-    constexpr int PER_STAGE = SPLIT ? 4 : 2;
-    __shared__ unsigned long long bars[3];
-    __shared__ unsigned tmem_slot;
-    __shared__ int s_bad;
-
-    long long bidx = blockIdx.x;
-    int bi = (int)((sqrt(8.0 * (double)bidx + 1.0) - 1.0) * 0.5);
-    while ((long long)(bi + 1) * (bi + 2) / 2 <= bidx) bi++;
-    while ((long long)bi * (bi + 1) / 2 > bidx) bi--;
-    const int bj = (int)(bidx - (long long)bi * (bi + 1) / 2);
-    const long long i0 = k1 + (long long)bi * TILE, j0 = k1 + (long long)bj * TILE;
+    constexpr int OPS = SPLIT ? 4 : 2;  // operand chunks per stage: L hi, W hi (, L lo, W lo)
+    constexpr unsigned STAGE_BYTES = OPS * CHUNK_BYTES;
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(base + STAGES * STAGE_BYTES);
+    unsigned long long *full = bars, *empty = bars + STAGES, *acc_full = bars + 2 * STAGES,
+                       *acc_empty = bars + 2 * STAGES + 2, *drain = bars + 2 * STAGES + 4;
+    unsigned *tmem_slot = reinterpret_cast<unsigned *>(bars + 2 * STAGES + 5);
+    volatile int *abort = reinterpret_cast<volatile int *>(tmem_slot + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
-        mbar_init(&bars[0]);
-        mbar_init(&bars[1]);
-        mbar_init(&bars[2]);
-        // an earlier tile of this factorization timed out: do nothing more
-        s_bad = (*(volatile unsigned long long *)flags & FLAG_LOOKBACK_TIMEOUT) ? 2 : 0;
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 4 * 32);
+        }
+        mbar_init(drain, 1);
+        // an earlier launch of this factorization timed out: do nothing more
+        *abort = (*(volatile unsigned long long *)flags & FLAG_LOOKBACK_TIMEOUT) ? 2 : 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();
-    if (s_bad) return;
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(saddr(&tmem_slot))
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(saddr(tmem_slot))
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const unsigned tmem = tmem_slot;
+    const unsigned tmem = *tmem_slot;
 
-    const float *Lrows = A + k0;  // L[i][k] = A[i*ld + k0 + k]
-    const int nchunks = (K + KC - 1) / KC;
-    bool ok = true;
-    for (int c = 0; c < nchunks; c++) {
-        const int s = c & 1;
-        if (c >= 2) {
-            // the MMAs of chunk c-2 read this stage: wait for their commit
-            // chunk c-2 was use number (c-2)/2 of this stage: its commit completes that phase
-            if (!mbar_wait(&bars[s], (unsigned)((c >> 1) - 1) & 1u)) ok = false;
-        }
-        unsigned char *sa = base + s * PER_STAGE * CHUNK_BYTES, *sb = sa + CHUNK_BYTES;
-        unsigned char *sal = sa + 2 * CHUNK_BYTES, *sbl = sa + 3 * CHUNK_BYTES;  // SPLIT only
-        load_chunk<SPLIT>(sa, sal, Lrows, ld, i0, n, c * KC, K);
-        load_chunk<SPLIT>(sb, sbl, W, ldw, j0, n, c * KC, K);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const unsigned long long da = smem_desc(saddr(sa)), db = smem_desc(saddr(sb));
-            const unsigned long long dal = smem_desc(saddr(sal)), dbl = smem_desc(saddr(sbl));
-#pragma unroll
-            for (int kk = 0; kk < KC / 8; kk++) {  // 8 TF32 = 32 B per MMA step: +2 in the descriptor
-                if constexpr (SPLIT) {
-                    mma_tf32(tmem, dal + 2 * kk, db + 2 * kk, (c > 0 || kk > 0) ? 1u : 0u);
-                    mma_tf32(tmem, da + 2 * kk, dbl + 2 * kk, 1u);
-                    mma_tf32(tmem, da + 2 * kk, db + 2 * kk, 1u);
-                } else {
-                    mma_tf32(tmem, da + 2 * kk, db + 2 * kk, (c > 0 || kk > 0) ? 1u : 0u);
+    if (*abort == 0) {
+        if (warp == 0 && lane == 0) {
+            // ---- producer ----
+            long long it = 0;
+            bool ok = true;
+            for (long long t = blockIdx.x; ok && t < ntiles; t += gridDim.x) {
+                int bi, bj;
+                tile_coords(t, bi, bj);
+                for (int kc = 0; kc < NCHUNK; kc++, it++) {
+                    const int s = (int)(it % STAGES);
+                    const long long u = it / STAGES;
+                    if (u > 0 && !mbar_wait(&empty[s], (unsigned)((u - 1) & 1), abort)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char *st = base + s * STAGE_BYTES;
+                    mbar_expect_tx(&full[s], STAGE_BYTES);
+                    tma_load(st, &mLh, kc * KC, bi * TILE, &full[s]);
+                    tma_load(st + CHUNK_BYTES, &mWh, kc * KC, bj * TILE, &full[s]);
+                    if (SPLIT) {
+                        tma_load(st + 2 * CHUNK_BYTES, &mLl, kc * KC, bi * TILE, &full[s]);
+                        tma_load(st + 3 * CHUNK_BYTES, &mWl, kc * KC, bj * TILE, &full[s]);
+                    }
                 }
             }
-            mma_commit(&bars[s]);
-        }
-    }
-    // all MMAs done: the last commit covers every earlier MMA of this thread
-    if (threadIdx.x == 0) mma_commit(&bars[2]);
-    if (!mbar_wait(&bars[2], 0)) ok = false;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!ok) s_bad = 1;
-    // epilogue, in two halves of 64 columns: TMEM -> registers -> shared
-    // (row-major, padded), then each warp subtracts whole rows from the tile
-    // with coalesced loads and stores (the operand stages are free now)
-    float(*sD)[65] = reinterpret_cast<float(*)[65]>(base);
-    const unsigned taddr = tmem + ((unsigned)(warp * 32) << 16);
-#pragma unroll 1
-    for (int half = 0; half < 2; half++) {
-#pragma unroll 1
-        for (int cb = 0; cb < 4; cb++) {
-            unsigned v[16];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                : "r"(taddr + half * 64 + cb * 16));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-            for (int q = 0; q < 16; q++) sD[warp * 32 + lane][cb * 16 + q] = __uint_as_float(v[q]);
-        }
-        __syncthreads();
-        const long long c0 = j0 + half * 64 + lane;
-#pragma unroll 1
-        for (int rr = 0; rr < 32; rr += 4) {
-            float old[4][2];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const long long row = i0 + warp * 32 + rr + u;
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const long long col = c0 + h * 32;
-                    old[u][h] = (row < n && col < n) ? A[row * ld + col] : 0.f;
+            // the last loads of each stage have landed before the CTA may exit
+            for (long long k = it - STAGES; k < it; k++) {
+                if (k < 0) continue;
+                const int s = (int)(k % STAGES);
+                long long spins = 0;
+                while (!mbar_try(&full[s], (unsigned)((k / STAGES) & 1)) && ++spins < SPIN_LIMIT) {
                 }
             }
+        } else if (warp == 1 && lane == 0) {
+            // ---- MMA issuer ----
+            long long it = 0, lt = 0;
+            bool ok = true;
+            for (long long t = blockIdx.x; ok && t < ntiles; t += gridDim.x, lt++) {
+                const int a = (int)(lt & 1);
+                const long long v = lt >> 1;
+                if (v > 0 && !mbar_wait(&acc_empty[a], (unsigned)((v - 1) & 1), abort)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const unsigned d = tmem + (unsigned)(a * TILE);
+                for (int kc = 0; kc < NCHUNK; kc++, it++) {
+                    const int s = (int)(it % STAGES);
+                    if (!mbar_wait(&full[s], (unsigned)((it / STAGES) & 1), abort)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const unsigned char *st = base + s * STAGE_BYTES;
+                    const unsigned long long dl = smem_desc(saddr(st)), dw = smem_desc(saddr(st + CHUNK_BYTES));
+                    const unsigned long long dll = smem_desc(saddr(st + 2 * CHUNK_BYTES));
+                    const unsigned long long dwl = smem_desc(saddr(st + 3 * CHUNK_BYTES));
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const long long row = i0 + warp * 32 + rr + u;
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const long long col = c0 + h * 32;
-                    // the strict upper part of the diagonal tiles is never read again; skip it anyway
-                    if (row < n && col < n && col <= row)
-                        A[row * ld + col] = old[u][h] - sD[warp * 32 + rr + u][lane + h * 32];
+                    for (int kk = 0; kk < KC / 8; kk++) {  // 8 TF32 = 32 B per MMA step: +2 in the descriptor
+                        const unsigned accum = (kc > 0 || kk > 0) ? 1u : 0u;
+                        if (SPLIT) {
+                            mma_tf32(d, dll + 2 * kk, dw + 2 * kk, accum);
+                            mma_tf32(d, dl + 2 * kk, dwl + 2 * kk, 1u);
+                            mma_tf32(d, dl + 2 * kk, dw + 2 * kk, 1u);
+                        } else {
+                            mma_tf32(d, dl + 2 * kk, dw + 2 * kk, accum);
+                        }
+                    }
+                    mma_commit(&empty[s]);  // the stage is free once these MMAs have read it
                 }
+                if (!ok) break;
+                mma_commit(&acc_full[a]);  // the accumulator is complete
+            }
+            // every MMA this thread issued has completed once this commit arrives
+            mma_commit(drain);
+            long long spins = 0;
+            while (!mbar_try(drain, 0) && ++spins < SPIN_LIMIT) {
+            }
+        } else if (warp >= 2) {
+            // ---- epilogue: TMEM lanes 32*(warp%4) .. +31 are this warp's tile rows ----
+            const int q = warp & 3;
+            const int r = q * 32 + lane;
+            long long lt = 0;
+            for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
+                const int a = (int)(lt & 1);
+                int ok = 1;
+                if (lane == 0) ok = mbar_wait(&acc_full[a], (unsigned)((lt >> 1) & 1), abort);
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                int bi, bj;
+                tile_coords(t, bi, bj);
+                const long long row = P1 + (long long)bi * TILE + r;
+                const long long c0 = P1 + (long long)bj * TILE;
+                const unsigned taddr = tmem + (unsigned)(a * TILE) + ((unsigned)(q * 32) << 16);
+#pragma unroll 1
+                for (int cb = 0; cb < TILE / 16; cb++) {
+                    unsigned v[16];
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                        "[%16];"
+                        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                          "=r"(v[14]), "=r"(v[15])
+                        : "r"(taddr + cb * 16));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    const long long col = c0 + cb * 16;
+                    if (row < n && col <= row) {
+                        float *p = A + row * ld + col;
+                        if (col + 15 <= row && col + 15 < n) {
+#pragma unroll
+                            for (int g = 0; g < 4; g++) {
+                                float4 o = *reinterpret_cast<float4 *>(p + 4 * g);
+                                o.x -= __uint_as_float(v[4 * g]);
+                                o.y -= __uint_as_float(v[4 * g + 1]);
+                                o.z -= __uint_as_float(v[4 * g + 2]);
+                                o.w -= __uint_as_float(v[4 * g + 3]);
+                                *reinterpret_cast<float4 *>(p + 4 * g) = o;
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 16; j++)
+                                if (col + j <= row && col + j < n) p[j] -= __uint_as_float(v[j]);
+                        }
+                    }
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                mbar_arrive(&acc_empty[a]);
             }
         }
-        __syncthreads();
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tmem) : "memory");
-    if (threadIdx.x == 0 && s_bad) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem) : "memory");
+    if (threadIdx.x == 0 && *abort == 1) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
 }
 
-// two stages of the operand chunks + alignment slack
-constexpr size_t smem_bytes(bool split) { return (split ? 8 : 4) * (size_t)CHUNK_BYTES + 1024; }
+// operand stages + barriers, TMEM slot, abort flag + 1024-byte alignment slack
+constexpr size_t smem_bytes(bool split) { return (size_t)STAGES * (split ? 4 : 2) * CHUNK_BYTES + 256 + 1024; }
 
 }  // namespace tc
 }  // namespace mp
