@@ -250,6 +250,106 @@ def error_metrics(deck, pop, inj_batches, cfg, device, steps=5):
             "cells_differing_frac": float(np.mean(ia != ib)), "steps": steps}
 
 
+def mixed_vs_fp64_at_scale(args, device, torch, flush, steps=3, warmup=2):
+    """The mixed-form workload (32^3 Kuhn box minus the r = 0.02 m sphere at
+    -10 V, ~50M ions): the FP64 and mixed forms run in lockstep on the same
+    seeded population and injections.  Per form: full-step particle-steps/s
+    (inject + push + scatter + computePhi + updateEf, device time), Newton-step
+    ms, push-kernel ms; the mixed form's errors against the FP64 form: node
+    density L2, max |phi| difference per step, and the fraction of particles
+    whose cell differs at the end."""
+    cfg = CONFIGS[2]
+    qm = mp.QE / (16 * mp.AMU)
+    with tempfile.TemporaryDirectory() as wd:
+        kd, deck, pos, vel, cell = make_workload(cfg, wd, seed=4321)
+        fe = workloads.fe_arrays(cfg, deck)
+        inj = mp.Injector(deck.mesh, seed=0)
+        P = deck.params
+        batches = [inj.sample(P.plasma_den, P.ion_velocity, cfg["dt"], cfg["spwt"]) for _ in range(warmup + steps)]
+        ctxs = {}
+        for name, form in (("fp64", mp.FP64), ("mixed", mp.MIXED)):
+            c = mp.Context(deck.mesh, device=device)
+            c.fe_setup(**fe)
+            c.set_track_ids(True)  # for the cell comparison at the end
+            # an ion stepping into the sphere lies in no tet; the reference's greedy walk can
+            # cycle around the cavity without end: absorb such walks (counted) instead
+            c.set_walk_limit(256)
+            c.set_walk_policy(mp.WALK_LIMIT_ABSORB)
+            c.reserve(int(len(cell) * 1.05) + 100_000)
+            c.append(pos, vel, cell)
+            c.sort_by_tet()
+            c.set_sort_period(SORT_PERIOD)
+            if form == mp.MIXED:
+                c.set_form(mp.MIXED)
+            ctxs[name] = (c, form, torch.cuda.ExternalStream(c.stream(), device=device))
+        del pos, vel, cell
+        res = {k: {"step_ms": [], "newton_ms": [], "push_ms": [], "n": [], "refinements": [], "lost": []} for k in ctxs}
+        den_err, phi_err = [], []
+        for k in range(warmup + steps):
+            hp, hv, hc = batches[k]
+            dens, uhs = {}, {}
+            for name, (c, form, stream) in ctxs.items():
+                flush.zero_()
+                torch.cuda.synchronize(device)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                c.append(hp, hv, hc, rewind=True, q_over_m=qm, half_dt=0.5 * cfg["dt"])
+                st = c.push(qm, cfg["dt"], cfg["spwt"])
+                nt = c.compute_phi(mp.LAPACK, form)
+                c.update_ef()
+                e1.record(stream)
+                e1.synchronize()
+                if k >= warmup:
+                    r = res[name]
+                    r["step_ms"].append(e0.elapsed_time(e1))
+                    r["newton_ms"].append(nt.ms_total)
+                    r["push_ms"].append(st.ms_kernel)
+                    r["n"].append(st.n_before)
+                    r["refinements"].append(nt.linear_iterations)
+                    r["lost"].append(st.lost)
+                den = np.zeros(deck.mesh.n_nodes)
+                c._c(mp.lib().mp_density_download(c.h, mp._p(den)))
+                _, uh, _ = c.field()
+                dens[name], uhs[name] = den, uh
+            den_err.append(float(np.linalg.norm(dens["mixed"] - dens["fp64"]) / np.linalg.norm(dens["fp64"])))
+            phi_err.append(float(np.abs(uhs["mixed"] - uhs["fp64"]).max()))
+        # the solver's own precision: one Newton step of each form from the same state
+        # (d, the accumulated F1) and the same density, the FP64 context's
+        c64, cm = ctxs["fp64"][0], ctxs["mixed"][0]
+        for name in ("d", "F1"):
+            cm.fe_set(name, c64.fe_get(name))
+        c64.compute_phi(mp.LAPACK, mp.FP64, ion_den=dens["fp64"])
+        cm.compute_phi(mp.LAPACK, mp.MIXED, ion_den=dens["fp64"])
+        phi_solve_err = float(np.abs(cm.field()[1] - c64.field()[1]).max())
+        ga, gb = ctxs["fp64"][0].download(mp.ORDER_ID), ctxs["mixed"][0].download(mp.ORDER_ID)
+        ids = np.union1d(ga["id"], gb["id"])
+        ia = np.full(ids.size, -1)
+        ib = np.full(ids.size, -1)
+        ia[np.searchsorted(ids, ga["id"])] = ga["cell"]
+        ib[np.searchsorted(ids, gb["id"])] = gb["cell"]
+        for c, _, _ in ctxs.values():
+            c.close()
+    out = {"workload": cfg["label"], "mesh_hexes": cfg["n"] ** 3, "tets": deck.mesh.n_tets,
+           "unknowns": int(fe["neq"]), "ions": int(np.mean(res["fp64"]["n"])), "steps": steps, "warmup": warmup,
+           "l2": f"flushed ({FLUSH_BYTES >> 20} MiB write) before each timed step"}
+    for name, r in res.items():
+        out[name] = {"full_step_particle_steps_per_s": float(np.sum(r["n"]) / (np.sum(r["step_ms"]) / 1e3)),
+                     "newton_step_ms": float(np.mean(r["newton_ms"])), "push_kernel_ms": float(np.mean(r["push_ms"])),
+                     "refinement_solves": int(max(r["refinements"])),
+                     "absorbed_at_walk_limit_per_step": float(np.mean(r["lost"]))}
+    out["mixed_over_fp64_full_step"] = (out["mixed"]["full_step_particle_steps_per_s"] /
+                                        out["fp64"]["full_step_particle_steps_per_s"])
+    out["errors_vs_fp64"] = {"density_l2_rel": max(den_err),
+                             "phi_solve_max_abs_V": phi_solve_err,
+                             "phi_closed_loop_max_abs_V": max(phi_err),
+                             "cells_differing_frac": float(np.mean(ia != ib)), "steps": warmup + steps,
+                             "what": "density and cells: the mixed form's particles against the FP64 form's on "
+                                     "the same seeded run; phi_solve: the mixed Newton step against the FP64 one "
+                                     "from the same state and density; phi_closed_loop: the two runs' potentials, "
+                                     "which also carry their density difference"}
+    return out
+
+
 def cpu_baseline(cfg, workdir, pop, budget_s=20.0):
     """The reference's own MoveParticles (oracle/_ref, OpenMP over all host
     threads) on the same population; one Lapack Newton step if it fits."""
@@ -328,6 +428,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-scale", action="store_true", help="skip the mixed-vs-FP64 run on the 32^3 sphere workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -372,6 +473,9 @@ def main():
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu:
             cpu = cpu_baseline(cfg, wd, pop)
+    scale = None
+    if rank == 0 and world == 1 and not args.no_scale and args.config == 1:
+        scale = mixed_vs_fp64_at_scale(args, local, torch, flush)
 
     def agg(r):
         push_ms = np.array(r["push_ms"])
@@ -450,6 +554,8 @@ def main():
             }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if scale is not None:
+            line["mixed_vs_fp64_kuhn32s_50M"] = scale
         print(json.dumps(line))
     if world > 1:
         torch.distributed.barrier()

@@ -72,6 +72,14 @@ enum { MP_FORM_FP64 = 0, MP_FORM_MIXED = 1 };
  * accuracy; fewer FP64 refinement iterations). */
 enum { MP_MIXED_TF32 = 1, MP_MIXED_TF32X3 = 3 };
 
+/* What a walk that reaches the hop limit does.  In a mesh with a cavity (the
+ * sphere workload) a particle that steps into the cavity lies in no tet, and
+ * the reference's greedy XtoLtet walk (src/meshes.h:75-100) can then cycle
+ * among the tets around it without end.  ERROR keeps the particle where the
+ * walk stopped and returns MP_ERR_WALK_LIMIT; ABSORB removes it as absorbed by
+ * the boundary and counts it in mp_step_stats.lost. */
+enum { MP_WALK_LIMIT_ERROR = 0, MP_WALK_LIMIT_ABSORB = 1 };
+
 /* Density accumulation: FP64 atomics (order-dependent rounding, like the
  * reference's atomic_ref) or 64-bit fixed point (run-to-run deterministic). */
 enum { MP_SCATTER_FP64_ATOMIC = 0, MP_SCATTER_FIXED64 = 1 };
@@ -127,6 +135,7 @@ typedef struct mp_step_stats {
     int32_t near_face_fp64;   /* mixed form: FP64 re-tests taken */
     double ms_kernel;         /* device time of the push kernel alone (CUDA events) */
     double ms_step;           /* device time of the whole push call's kernels */
+    int64_t lost;             /* walks that hit the hop limit and were absorbed (MP_WALK_LIMIT_ABSORB) */
 } mp_step_stats;
 
 typedef struct mp_newton_stats {
@@ -151,6 +160,7 @@ int mp_get_stream(mp_ctx *ctx, void **cuda_stream);
  * particle-ID tracking (default on), tet re-sort period in steps (0 = never). */
 int mp_set_walk_limit(mp_ctx *ctx, int32_t max_hops);
 int mp_set_scatter_mode(mp_ctx *ctx, int mode);
+int mp_set_walk_policy(mp_ctx *ctx, int policy);
 int mp_set_sort_period(mp_ctx *ctx, int32_t steps);
 int mp_set_particle_form(mp_ctx *ctx, int form);
 /* Arithmetic of the mixed-form Newton factorization (MP_MIXED_TF32 or

@@ -320,6 +320,12 @@ int mp_set_walk_limit(mp_ctx *ctx, int32_t max_hops) {
     return MP_OK;
 }
 
+int mp_set_walk_policy(mp_ctx *ctx, int policy) {
+    if (!ctx || (policy != MP_WALK_LIMIT_ERROR && policy != MP_WALK_LIMIT_ABSORB)) return MP_ERR_ARG;
+    ctx->walk_absorb = policy == MP_WALK_LIMIT_ABSORB;
+    return MP_OK;
+}
+
 int mp_set_scatter_mode(mp_ctx *ctx, int mode) {
     if (!ctx || (mode != MP_SCATTER_FP64_ATOMIC && mode != MP_SCATTER_FIXED64)) return MP_ERR_ARG;
     ctx->scatter_mode = mode;
@@ -502,6 +508,7 @@ int mp_push_scatter(mp_ctx *ctx, double q_over_m, double dt, double spwt, double
         stats->total_hops = (int64_t)ctx->counters_host[C_HOPS];
         stats->max_hops = (int32_t)ctx->counters_host[C_MAX_HOPS];
         stats->near_face_fp64 = (int32_t)ctx->counters_host[C_NEAR];
+        stats->lost = (int64_t)ctx->counters_host[C_LOST];
         float ka = 0, kb = 0;
         cudaEventElapsedTime(&ka, ctx->tp.a, ctx->tp.b);
         cudaEventElapsedTime(&kb, ctx->ts.a, ctx->ts.b);

@@ -69,6 +69,7 @@ enum Counter {
     C_NEAR = 5,       // mixed form: FP64 near-face re-tests    } push
     C_FLAGS = 6,      // error bits (FLAG_*), cleared when reported
     C_NEXT_ID = 7,    // next particle id
+    C_LOST = 8,       // walks that hit the hop limit and were absorbed (zeroed before every push)
     C_COUNT = 16
 };
 enum Flag : unsigned long long {
@@ -117,6 +118,7 @@ struct mp_ctx {
     int form = MP_FORM_FP64;
     int scatter_mode = MP_SCATTER_FP64_ATOMIC;
     int walk_limit = 4096;
+    bool walk_absorb = false;             // hop limit: absorb the particle instead of raising MP_ERR_WALK_LIMIT
     int sort_period = 0;
     int mixed_factor = MP_MIXED_TF32X3;  // tensor-core terms of the mixed factorization
     long long steps_since_sort = 0;

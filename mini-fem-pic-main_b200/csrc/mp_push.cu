@@ -29,6 +29,7 @@ struct PushF64Args {
     unsigned long long *counters;
     double qm, dt;
     int walk_limit;
+    int absorb;  // hop limit reached: remove the particle (counted in C_LOST) instead of raising the error
     int fixed;
     int track_ids;
 };
@@ -44,6 +45,7 @@ struct PushF32Args {
     float qm_dt;                     // q/m * dt
     float dt;
     int walk_limit;
+    int absorb;
     int fixed;
     int track_ids;
 };
@@ -145,18 +147,20 @@ __device__ __forceinline__ bool group_sum4(int key, T v[4]) {
 // CTA pushes and reduced once per warp when the kernel ends: a warp reduction
 // per tile costs more than the scatter itself.
 struct PushStats {
-    unsigned hops = 0, hmax = 0, exits = 0, near = 0;
-    __device__ __forceinline__ void add(int state, int h, int nr) {
+    unsigned hops = 0, hmax = 0, exits = 0, near = 0, lost = 0;
+    __device__ __forceinline__ void add(int state, int h, int nr, int lst) {
         hops += (unsigned)h;
         hmax = hmax > (unsigned)h ? hmax : (unsigned)h;
         exits += state == 3;
         near += (unsigned)nr;
+        lost += (unsigned)lst;
     }
     // all 32 lanes call it
     __device__ __forceinline__ void flush(unsigned long long *counters) {
         const unsigned FULL = 0xffffffffu;
         const unsigned hs = __reduce_add_sync(FULL, hops), hm = __reduce_max_sync(FULL, hmax);
         const unsigned ex = __reduce_add_sync(FULL, exits), nr = __reduce_add_sync(FULL, near);
+        const unsigned ls = __reduce_add_sync(FULL, lost);
         if ((threadIdx.x & 31) == 0) {
             if (hs) {
                 atomicAdd(&counters[C_HOPS], (unsigned long long)hs);
@@ -167,6 +171,7 @@ struct PushStats {
                 atomicAdd(&counters[C_DEAD], (unsigned long long)ex);
             }
             if (nr) atomicAdd(&counters[C_NEAR], (unsigned long long)nr);
+            if (ls) atomicAdd(&counters[C_LOST], (unsigned long long)ls);
         }
     }
 };
@@ -270,7 +275,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_fp64(PushF64Args a) {
         mbar_wait(&bars[sidx], (unsigned)((k / STAGES) & 1), a.counters);
         const StageF64 &st = stage[sidx];
         const long long i = (blockIdx.x + k * gridDim.x) * (long long)PUSH_THREADS + threadIdx.x;
-        int state = 0, cell = -1, hops = 0;
+        int state = 0, cell = -1, hops = 0, lost = 0;
         int con[4] = {0, 0, 0, 0};
         double lc[4] = {0, 0, 0, 0};
         double x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 0;
@@ -299,6 +304,10 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_fp64(PushF64Args a) {
                 state = 1;
                 const int4 c4 = __ldg(reinterpret_cast<const int4 *>(a.tets[cell].con));
                 con[0] = c4.x; con[1] = c4.y; con[2] = c4.z; con[3] = c4.w;
+            } else if (w == -1 && a.absorb) {
+                state = 3;  // the point lies outside the mesh where the walk cannot end: absorbed
+                cell = -1;
+                lost = 1;
             } else if (w == -1) {
                 state = 2;  // kept where the walk stopped, not scattered, error raised
                 atomicOr(&a.counters[C_FLAGS], FLAG_WALK_LIMIT);
@@ -311,7 +320,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_fp64(PushF64Args a) {
             a.p.cell[i] = cell;
         }
         scatter_warp<double>(state, cell, con, lc, a.den, a.den_fixed, a.fixed);
-        stats.add(state, hops, 0);
+        stats.add(state, hops, 0, lost);
     }
     stats.flush(a.counters);
 }
@@ -359,7 +368,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_mixed(PushF32Args a) {
         mbar_wait(&bars[sidx], (unsigned)((k / STAGES) & 1), a.counters);
         const StageF32 &st = stage[sidx];
         const long long i = (blockIdx.x + k * gridDim.x) * (long long)PUSH_THREADS + threadIdx.x;
-        int state = 0, cell = -1, hops = 0, near = 0;
+        int state = 0, cell = -1, hops = 0, near = 0, lost = 0;
         int con[4] = {0, 0, 0, 0};
         float lc[4] = {0, 0, 0, 0};
         float rx = 0, ry = 0, rz = 0, vx = 0, vy = 0, vz = 0;
@@ -432,8 +441,14 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_mixed(PushF32Args a) {
                     break;
                 }
                 if (hops >= a.walk_limit) {
-                    state = 2;
-                    atomicOr(&a.counters[C_FLAGS], FLAG_WALK_LIMIT);
+                    if (a.absorb) {
+                        state = 3;
+                        cell = -1;
+                        lost = 1;
+                    } else {
+                        state = 2;
+                        atomicOr(&a.counters[C_FLAGS], FLAG_WALK_LIMIT);
+                    }
                     break;
                 }
                 // re-base the offset on the new tet's vertex 0
@@ -455,7 +470,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_mixed(PushF32Args a) {
             a.p.cell[i] = cell;
         }
         scatter_warp<float>(state, cell, con, lc, a.den, a.den_fixed, a.fixed);
-        stats.add(state, hops, near);
+        stats.add(state, hops, near, lost);
     }
     stats.flush(a.counters);
 }
@@ -481,6 +496,7 @@ static int grid_for(mp_ctx *ctx, const void *kernel, int threads, size_t smem) {
 int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
     // per-push statistics words
     MP_CUDA(ctx, cudaMemsetAsync(ctx->counters + C_EXITS, 0, 4 * sizeof(unsigned long long), ctx->stream));
+    MP_CUDA(ctx, cudaMemsetAsync(ctx->counters + C_LOST, 0, sizeof(unsigned long long), ctx->stream));
     if (ctx->scatter_mode == MP_SCATTER_FIXED64)
         MP_CUDA(ctx, cudaMemsetAsync(ctx->den_fixed, 0, ctx->n_nodes * sizeof(unsigned long long), ctx->stream));
     else
@@ -497,6 +513,7 @@ int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
         a.qm = q_over_m;
         a.dt = dt;
         a.walk_limit = ctx->walk_limit;
+        a.absorb = ctx->walk_absorb;
         a.fixed = ctx->scatter_mode == MP_SCATTER_FIXED64;
         a.track_ids = ctx->track_ids;
         const size_t smem = sizeof(StageF64) * STAGES;
@@ -523,6 +540,7 @@ int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
         a.qm_dt = (float)(q_over_m * dt);
         a.dt = (float)dt;
         a.walk_limit = ctx->walk_limit;
+        a.absorb = ctx->walk_absorb;
         a.fixed = ctx->scatter_mode == MP_SCATTER_FIXED64;
         a.track_ids = ctx->track_ids;
         const size_t smem = sizeof(StageF32) * STAGES;

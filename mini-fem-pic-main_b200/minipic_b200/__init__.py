@@ -37,6 +37,7 @@ STATUS = {0: "MP_OK", 1: "MP_ERR_ARG", 2: "MP_ERR_OOM", 3: "MP_ERR_CUDA", 4: "MP
 NONLINEAR, GAUSS_SEIDEL, LAPACK = 0, 1, 2
 FP64, MIXED = 0, 1
 MIXED_TF32, MIXED_TF32X3 = 1, 3
+WALK_LIMIT_ERROR, WALK_LIMIT_ABSORB = 0, 1
 SCATTER_ATOMIC, SCATTER_FIXED = 0, 1
 ORDER_STORAGE, ORDER_ID = 0, 1
 VEC = {"F0": 0, "F1": 1, "d": 2, "g": 3, "uh": 4, "den": 5, "ef": 6, "G": 7, "y": 8, "K": 16, "J": 17}
@@ -60,7 +61,7 @@ EXPORTED = [
     "mp_injector_get_rem", "mp_injector_set_rem", "mp_set_track_ids", "mp_kernel_launches",
     "mp_device_buffer", "mp_push_particles_noalloc", "mp_set_mixed_factor",
     "mp_adjoint_setup", "mp_adjoint_add_particles", "mp_adjoint_forward", "mp_adjoint_flux",
-    "mp_adjoint_backward", "mp_adjoint_tangent",
+    "mp_adjoint_backward", "mp_adjoint_tangent", "mp_set_walk_policy",
 ]
 
 
@@ -96,7 +97,7 @@ class FeDesc(C.Structure):
 class StepStats(C.Structure):
     _fields_ = [("n_before", C.c_int64), ("n_after", C.c_int64), ("total_hops", C.c_int64),
                 ("max_hops", C.c_int32), ("near_face_fp64", C.c_int32), ("ms_kernel", C.c_double),
-                ("ms_step", C.c_double)]
+                ("ms_step", C.c_double), ("lost", C.c_int64)]
 
 
 class NewtonStats(C.Structure):
@@ -152,6 +153,7 @@ def lib():
         L.mp_set_scatter_mode.argtypes = [vp, C.c_int]
         L.mp_set_sort_period.argtypes = [vp, i32]
         L.mp_set_mixed_factor.argtypes = [vp, C.c_int]
+        L.mp_set_walk_policy.argtypes = [vp, C.c_int]
         L.mp_adjoint_setup.argtypes = [vp, i32, i32, d, d, d, d, vp, vp, vp, C.c_int]
         L.mp_adjoint_add_particles.argtypes = [vp, i32, C.c_int, i64, vp, vp, vp]
         L.mp_adjoint_forward.argtypes = [vp, vp, d, C.c_int, vp, C.POINTER(AdjointStats)]
@@ -433,6 +435,10 @@ class Context:
     # options
     def set_walk_limit(self, n):
         self._c(lib().mp_set_walk_limit(self.h, n))
+
+    def set_walk_policy(self, policy):
+        """WALK_LIMIT_ERROR (default) or WALK_LIMIT_ABSORB: what a walk that reaches the hop limit does."""
+        self._c(lib().mp_set_walk_policy(self.h, policy))
 
     def set_scatter_mode(self, mode):
         self._c(lib().mp_set_scatter_mode(self.h, mode))

@@ -196,6 +196,27 @@ def test_walk_limit_reports_error(deck6):
     ctx.push(0.0, 1e-7, 1.0)  # the context stays usable
 
 
+@pytest.mark.parametrize("form", [mp.FP64, mp.MIXED])
+def test_walk_limit_absorb_policy(deck6, form):
+    """WALK_LIMIT_ABSORB: a walk that reaches the hop limit removes the particle
+    (counted in StepStats.lost, not an error); the others are pushed as usual."""
+    kd, path = deck6
+    dk = mp.Deck.load(path)
+    ctx = gpu_context(dk, fe=False)
+    if form == mp.MIXED:
+        ctx.set_form(mp.MIXED)
+    ctx.set_walk_limit(1)
+    ctx.set_walk_policy(mp.WALK_LIMIT_ABSORB)
+    pos = np.array([[0.001, 0.05, 0.05], [0.05, 0.05, 0.05]])
+    cell = kuhn_locate(kd, pos)
+    vel = np.array([[3e5, 0.0, 0.0], [0.0, 0.0, 0.0]])  # the first must cross many tets, the second stays
+    ctx.append(pos, vel, cell)
+    st = ctx.push(0.0, 1e-7, 1.0)
+    assert st.lost == 1 and st.n_after == 1
+    out = ctx.download(mp.ORDER_ID)
+    assert out["cell"].size == 1 and out["cell"][0] == cell[1]
+
+
 def test_append_rejects_bad_cell(deck4):
     kd, path = deck4
     dk = mp.Deck.load(path)
