@@ -264,22 +264,35 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         } else if (warp >= 2) {
             // ---- epilogue: TMEM lanes 32*(warp%4) .. +31 are this warp's tile rows ----
+            // Each thread owns one tile row: it loads the row's 128 old values of
+            // A first (they do not depend on the MMAs, so the loads overlap the
+            // wait), then subtracts the accumulator chunk by chunk.
             const int q = warp & 3;
             const int r = q * 32 + lane;
             long long lt = 0;
             for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
+                int bi, bj;
+                tile_coords(t, bi, bj);
+                const long long row = P1 + (long long)bi * TILE + r;
+                const long long c0 = P1 + (long long)bj * TILE;
+                // full 16-column chunks of this row inside the lower triangle and the matrix
+                const bool row_ok = row < n;
+                float4 old[TILE / 4];
+#pragma unroll
+                for (int g = 0; g < TILE / 4; g++) {
+                    const long long col = c0 + 4 * g;
+                    old[g] = (row_ok && col + 3 <= row && col + 3 < n)
+                                 ? *reinterpret_cast<const float4 *>(A + row * ld + col)
+                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
                 const int a = (int)(lt & 1);
                 int ok = 1;
                 if (lane == 0) ok = mbar_wait(&acc_full[a], (unsigned)((lt >> 1) & 1), abort);
                 ok = __shfl_sync(0xffffffffu, ok, 0);
                 if (!ok) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                int bi, bj;
-                tile_coords(t, bi, bj);
-                const long long row = P1 + (long long)bi * TILE + r;
-                const long long c0 = P1 + (long long)bj * TILE;
                 const unsigned taddr = tmem + (unsigned)(a * TILE) + ((unsigned)(q * 32) << 16);
-#pragma unroll 1
+#pragma unroll
                 for (int cb = 0; cb < TILE / 16; cb++) {
                     unsigned v[16];
                     asm volatile(
@@ -291,22 +304,23 @@ __global__ void __launch_bounds__(THREADS, 1)
                         : "r"(taddr + cb * 16));
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                     const long long col = c0 + cb * 16;
-                    if (row < n && col <= row) {
+                    if (row_ok && col <= row) {
                         float *p = A + row * ld + col;
-                        if (col + 15 <= row && col + 15 < n) {
 #pragma unroll
-                            for (int g = 0; g < 4; g++) {
-                                float4 o = *reinterpret_cast<float4 *>(p + 4 * g);
+                        for (int g = 0; g < 4; g++) {
+                            const long long cg = col + 4 * g;
+                            if (cg + 3 <= row && cg + 3 < n) {
+                                float4 o = old[cb * 4 + g];
                                 o.x -= __uint_as_float(v[4 * g]);
                                 o.y -= __uint_as_float(v[4 * g + 1]);
                                 o.z -= __uint_as_float(v[4 * g + 2]);
                                 o.w -= __uint_as_float(v[4 * g + 3]);
                                 *reinterpret_cast<float4 *>(p + 4 * g) = o;
-                            }
-                        } else {
+                            } else {
 #pragma unroll
-                            for (int j = 0; j < 16; j++)
-                                if (col + j <= row && col + j < n) p[j] -= __uint_as_float(v[j]);
+                                for (int j = 0; j < 4; j++)
+                                    if (cg + j <= row && cg + j < n) p[4 * g + j] -= __uint_as_float(v[4 * g + j]);
+                            }
                         }
                     }
                 }

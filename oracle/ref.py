@@ -15,6 +15,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libref_oracle.so")
+# the same harness linked with the C++ drop-in shim (mini-fem-pic-main_b200/shim)
+# and libminipic_cuda.so: the reference's own types driven through the device path
+SHIM_PATH = os.path.join(HERE, "_ref", "libref_shim.so")
 
 TETRA_DTYPE = np.dtype({
     "names": ["con", "volume", "alpha", "beta", "gamma", "delta", "cell_con"],
@@ -32,17 +35,20 @@ PARTICLE_DTYPE = np.dtype({
 # FESolver::Method (src/FESolver.h:26)
 NONLINEAR, GAUSS_SEIDEL, LAPACK = 0, 1, 2
 
-_lib = None
+_libs = {}
 
 
 def available() -> bool:
     return os.path.exists(LIB_PATH)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        L = C.CDLL(LIB_PATH)
+def shim_available() -> bool:
+    return os.path.exists(SHIM_PATH)
+
+
+def lib(shim: bool = False):
+    if shim not in _libs:
+        L = C.CDLL(SHIM_PATH if shim else LIB_PATH)
         vp, i, d, l = C.c_void_p, C.c_int, C.c_double, C.c_long
         sig = {
             "ref_sizeof_tetra": (i, []), "ref_sizeof_particle": (i, []),
@@ -70,10 +76,17 @@ def lib():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
+        if shim:
+            for name, (res, args) in {"ref_shim_device": (vp, [vp]), "ref_shim_free": (None, [vp]),
+                                      "ref_shim_move": (None, [vp, vp]), "ref_shim_compute_phi": (None, [vp, vp, i]),
+                                      "ref_shim_update_ef": (None, [vp, vp])}.items():
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
         assert L.ref_sizeof_tetra() == TETRA_DTYPE.itemsize
         assert L.ref_sizeof_particle() == PARTICLE_DTYPE.itemsize
-        _lib = L
-    return _lib
+        _libs[shim] = L
+    return _libs[shim]
 
 
 def _p(a: np.ndarray):
@@ -86,8 +99,9 @@ class RefSim:
     the way ``main`` does (src/mini-pic.cpp:75-116)."""
 
     def __init__(self, deck_dir: str, *, spwt: float = 200.0, mass_amu: float = 16.0,
-                 extra_fixed: dict | None = None):
-        L = lib()
+                 extra_fixed: dict | None = None, shim: bool = False):
+        self.L = L = lib(shim)
+        self.device = None
         L.ref_reseed(0)  # each simulation starts the reference's RNG stream afresh
         self.h = L.ref_open(deck_dir.encode())
         if not self.h:
@@ -108,9 +122,27 @@ class RefSim:
         self.neq = L.ref_neq(self.h)
 
     def close(self):
+        if getattr(self, "device", None):
+            self.L.ref_shim_free(self.device)
+            self.device = None
         if self.h:
-            lib().ref_close(self.h)
+            self.L.ref_close(self.h)
             self.h = None
+
+    # ---- the device path through the C++ drop-in (shim libraries only) ----
+    def shim_device(self) -> None:
+        """DeviceData device(volume), as main() creates it."""
+        self.device = self.L.ref_shim_device(self.h)
+
+    def shim_move(self) -> None:
+        """MoveParticles(ions, volume, solver, params, device) of the drop-in."""
+        self.L.ref_shim_move(self.h, self.device)
+
+    def shim_compute_phi(self, method: int) -> None:
+        self.L.ref_shim_compute_phi(self.h, self.device, method)
+
+    def shim_update_ef(self) -> None:
+        self.L.ref_shim_update_ef(self.h, self.device)
 
     def __del__(self):
         try:
@@ -119,7 +151,7 @@ class RefSim:
             pass
 
     def param(self, which: int) -> float:
-        return lib().ref_param(self.h, which)
+        return self.L.ref_param(self.h, which)
 
     @property
     def dt(self):
@@ -135,14 +167,14 @@ class RefSim:
 
     def tetra(self) -> np.ndarray:
         out = np.zeros(self.n_tets, dtype=TETRA_DTYPE)
-        lib().ref_get_tetra_raw(self.h, _p(out))
+        self.L.ref_get_tetra_raw(self.h, _p(out))
         return out
 
     def nodes(self):
         pos = np.zeros((self.n_nodes, 3))
         typ = np.zeros(self.n_nodes, dtype=np.int32)
         vol = np.zeros(self.n_nodes)
-        lib().ref_get_nodes(self.h, _p(pos), _p(typ), _p(vol))
+        self.L.ref_get_nodes(self.h, _p(pos), _p(typ), _p(vol))
         return pos, typ, vol
 
     def inlet(self) -> dict:
@@ -153,7 +185,7 @@ class RefSim:
         v = np.zeros((n, 3))
         cell = np.zeros(n, dtype=np.int32)
         normal = np.zeros((n, 3))
-        lib().ref_get_inlet(self.h, _p(con), _p(area), _p(u), _p(v), _p(cell), _p(normal))
+        self.L.ref_get_inlet(self.h, _p(con), _p(area), _p(u), _p(v), _p(cell), _p(normal))
         return dict(con=con, area=area, u=u, v=v, cell_con=cell, normal=normal)
 
     def fe(self) -> dict:
@@ -161,12 +193,12 @@ class RefSim:
         LM = np.zeros((self.n_tets, 4), dtype=np.int32)
         NX = np.zeros((self.n_tets, 4, 3))
         detJ = np.zeros(self.n_tets)
-        lib().ref_get_fe(self.h, _p(ID), _p(LM), _p(NX), _p(detJ))
+        self.L.ref_get_fe(self.h, _p(ID), _p(LM), _p(NX), _p(detJ))
         return dict(ID=ID, LM=LM, NX=NX, detJ=detJ)
 
     def matrix(self, which: int = 0) -> np.ndarray:
         out = np.zeros((self.neq, self.neq))
-        lib().ref_get_matrix(self.h, which, _p(out))
+        self.L.ref_get_matrix(self.h, which, _p(out))
         return out
 
     _VEC = {"F0": 0, "F1": 1, "d": 2, "g": 3, "uh": 4, "den": 5, "ef": 6}
@@ -180,73 +212,73 @@ class RefSim:
 
     def get(self, name: str) -> np.ndarray:
         out = np.zeros(self._veclen(name))
-        lib().ref_get_vec(self.h, self._VEC[name], _p(out))
+        self.L.ref_get_vec(self.h, self._VEC[name], _p(out))
         return out.reshape(-1, 3) if name == "ef" else out
 
     def set(self, name: str, values) -> None:
         a = np.ascontiguousarray(values, dtype=np.float64).ravel()
         assert a.size == self._veclen(name)
-        lib().ref_set_vec(self.h, self._VEC[name], _p(a))
+        self.L.ref_set_vec(self.h, self._VEC[name], _p(a))
 
     def particles(self) -> np.ndarray:
-        out = np.zeros(lib().ref_n_particles(self.h), dtype=PARTICLE_DTYPE)
+        out = np.zeros(self.L.ref_n_particles(self.h), dtype=PARTICLE_DTYPE)
         if out.size:
-            lib().ref_get_particles(self.h, _p(out))
+            self.L.ref_get_particles(self.h, _p(out))
         return out
 
     def set_particles(self, parts: np.ndarray) -> None:
         parts = np.ascontiguousarray(parts, dtype=PARTICLE_DTYPE)
-        lib().ref_set_particles(self.h, _p(parts) if parts.size else None, parts.size)
+        self.L.ref_set_particles(self.h, _p(parts) if parts.size else None, parts.size)
 
     @property
     def rem(self):
-        return lib().ref_rem(self.h)
+        return self.L.ref_rem(self.h)
 
     def inject(self) -> int:
-        return lib().ref_inject(self.h)
+        return self.L.ref_inject(self.h)
 
     def push_only(self, nthreads: int = 1) -> None:
-        lib().ref_push_only(self.h, nthreads)
+        self.L.ref_push_only(self.h, nthreads)
 
     def compact_normalise(self) -> int:
-        return lib().ref_compact_normalise(self.h)
+        return self.L.ref_compact_normalise(self.h)
 
     def move(self, nthreads: int = 1) -> int:
-        return lib().ref_move(self.h, nthreads)
+        return self.L.ref_move(self.h, nthreads)
 
     def compute_phi(self, method: int) -> None:
-        lib().ref_compute_phi(self.h, method)
+        self.L.ref_compute_phi(self.h, method)
 
     def update_ef(self) -> None:
-        lib().ref_update_ef(self.h)
+        self.L.ref_update_ef(self.h)
 
     def build_f1(self, den: np.ndarray) -> None:
         den = np.ascontiguousarray(den, dtype=np.float64)
-        lib().ref_build_f1(self.h, _p(den))
+        self.L.ref_build_f1(self.h, _p(den))
 
     def build_j(self, method: int) -> None:
-        lib().ref_build_j(self.h, method)
+        self.L.ref_build_j(self.h, method)
 
     def residual(self) -> np.ndarray:
         G = np.zeros(self.neq)
-        lib().ref_residual(self.h, _p(G))
+        self.L.ref_residual(self.h, _p(G))
         return G
 
     def solve_gs(self, b: np.ndarray, x0: np.ndarray | None = None) -> np.ndarray:
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros(self.neq) if x0 is None else np.array(x0, dtype=np.float64)
-        lib().ref_solve_gs(self.h, _p(b), _p(x))
+        self.L.ref_solve_gs(self.h, _p(b), _p(x))
         return x
 
     def solve_lapack(self, b: np.ndarray) -> np.ndarray:
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros(self.neq)
-        lib().ref_solve_lapack(self.h, _p(b), _p(x))
+        self.L.ref_solve_lapack(self.h, _p(b), _p(x))
         return x
 
     def time_move(self, steps: int, nthreads: int):
         sec = C.c_double(0)
-        rate = lib().ref_time_move(self.h, steps, nthreads, C.byref(sec))
+        rate = self.L.ref_time_move(self.h, steps, nthreads, C.byref(sec))
         return rate, sec.value
 
 

@@ -30,6 +30,9 @@
 #include "parameters.h"
 #include "particles.h"
 #include "trace.h"
+#ifdef REF_WITH_SHIM
+#include "mini_pic_cuda.h"
+#endif
 
 /* The reference's RNG state, a global of src/maths.cpp:17 with external linkage. */
 extern std::mt19937 mt_gen;
@@ -385,5 +388,23 @@ int ref_max_threads() { return omp_get_max_threads(); }
 /* Restarts the reference's RNG stream (the process-wide mt19937 of maths.cpp),
  * so every simulation opened in one process injects like a fresh `mini-pic`. */
 void ref_reseed(unsigned seed) { mt_gen.seed(seed); }
+
+
+#ifdef REF_WITH_SHIM
+/* The device path through the C++ drop-in (mini-fem-pic-main_b200/shim): the
+ * same Species, Volume, FESolver and Parameters objects, handed to the
+ * reference's own signatures as main() would hand them. */
+void *ref_shim_device(void *h) { return new DeviceData(((RefSim *)h)->volume); }
+void ref_shim_free(void *d) { delete (DeviceData *)d; }
+void ref_shim_move(void *h, void *d) {
+    RefSim *s = (RefSim *)h;
+    MoveParticles(*s->ions, s->volume, *s->solver, s->params, *(DeviceData *)d);
+}
+void ref_shim_compute_phi(void *h, void *d, int method) {
+    RefSim *s = (RefSim *)h;
+    computePhiDevice(*s->solver, s->ions->den, (FESolver::Method)method, *(DeviceData *)d);
+}
+void ref_shim_update_ef(void *h, void *d) { updateEfDevice(*((RefSim *)h)->solver, *(DeviceData *)d); }
+#endif
 
 }  /* extern "C" */

@@ -96,3 +96,14 @@ def test_injector_capacity_checked():
     rc = L.mp_injector_sample(inj.h, 1e10, 7000.0, 2e-6, 20000.0, 1, pos.ctypes.data_as(C.c_void_p), 24,
                               vel.ctypes.data_as(C.c_void_p), 24, cell.ctypes.data_as(C.c_void_p), 4, C.byref(n))
     assert rc == 1
+
+
+def test_drop_in_harness_links():
+    """The C++ drop-in compiled against the reference's headers links with the
+    library and exports its entry points (no device needed to load it)."""
+    from oracle import ref
+    if not ref.shim_available():
+        pytest.skip("oracle/_ref/libref_shim.so not built (needs the reference sources)")
+    L = ref.lib(shim=True)
+    for name in ("ref_shim_device", "ref_shim_move", "ref_shim_compute_phi", "ref_shim_update_ef"):
+        assert getattr(L, name)
