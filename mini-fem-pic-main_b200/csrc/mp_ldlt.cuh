@@ -6,9 +6,11 @@
 // storage, leading dimension padded to 32).  Per block column k of width NB:
 //   diag   : L_kk D_k L_kk^T = A_kk in shared memory (one CTA); z_k = L_kk^-1 b_k
 //   panel  : W_ik = A_ik L_kk^-T,  L_ik = W_ik D_k^-1, b_i -= L_ik z_k  (rows below)
-//   update : A_ij -= L_ik W_jk^T on the lower tiles of the trailing matrix
+//   update : A_ij -= L_ik W_jk^T on the lower tiles of the trailing matrix,
+//            two-level: within each 256-wide outer panel only the panel's own
+//            columns, and the rest of the trailing matrix once per outer panel
 // The forward substitution rides on the panel pass; the backward substitution
-// L^T y = D^-1 z runs block column by block column afterwards.
+// L^T y = D^-1 z runs afterwards.
 //
 // J is symmetric (K is assembled symmetric, FP only touches the diagonal) and
 // in these problems sign-definite, the case where LDL^T needs no pivoting.  A
@@ -19,6 +21,7 @@
 // wrapped in FP64 iterative refinement (residual from the FP64 K and FP).
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include <cudaTypedefs.h>
 
@@ -265,64 +268,6 @@ __global__ void __launch_bounds__(256) k_ldlt_panel(int n, long long ld, T *A, i
     }
 }
 
-// Trailing update of the lower 64x64 tiles: A_ij -= L_i W_j^T over p < kb.
-template <typename T>
-__global__ void __launch_bounds__(256) k_ldlt_update(int n, long long ld, T *A, int k0, int kb, const T *W, int ldw,
-                                                     int k1) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *sLt = reinterpret_cast<T *>(smem_raw);   // [NB][64+pad] transposed: sLt[p][r]
-    T *sWt = sLt + NB * 68;                      // [NB][68]
-    long long bidx = blockIdx.x;
-    int bi = (int)((sqrt(8.0 * (double)bidx + 1.0) - 1.0) * 0.5);
-    while ((long long)(bi + 1) * (bi + 2) / 2 <= bidx) bi++;
-    while ((long long)bi * (bi + 1) / 2 > bidx) bi--;
-    int bj = (int)(bidx - (long long)bi * (bi + 1) / 2);
-    const int i0 = k1 + bi * 64, j0 = k1 + bj * 64;
-    {
-        // 64 x NB elements of each operand, 16 per thread: issue all loads first
-        T la[16], wa[16];
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            int idx = q * 256 + threadIdx.x;
-            int r = idx / NB, p = idx % NB;
-            int ri = i0 + r, rj = j0 + r;
-            la[q] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : T(0);
-            wa[q] = (p < kb && rj < n) ? __ldg(&W[(long long)rj * ldw + p]) : T(0);
-        }
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            int idx = q * 256 + threadIdx.x;
-            int r = idx / NB, p = idx % NB;
-            sLt[p * 68 + r] = la[q];
-            sWt[p * 68 + r] = wa[q];
-        }
-    }
-    __syncthreads();
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    T acc[4][4] = {};
-    for (int p = 0; p < kb; p++) {
-        T a[4], w[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) a[u] = sLt[p * 68 + ty * 4 + u];
-#pragma unroll
-        for (int v = 0; v < 4; v++) w[v] = sWt[p * 68 + tx * 4 + v];
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-#pragma unroll
-            for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], w[v], acc[u][v]);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-        int i = i0 + ty * 4 + u;
-        if (i >= n) continue;
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-            int j = j0 + tx * 4 + v;
-            if (j < n && j <= i) A[(long long)i * ld + j] -= acc[u][v];
-        }
-    }
-}
-
 // Update restricted to the columns [k1, jend) of the current outer panel:
 // A_ij -= L_i W_j^T for rows i in [k1, n), 64x64 tiles, grid (col tile, row tile).
 template <typename T>
@@ -373,6 +318,87 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols(int n, long long ld, T
         for (int v = 0; v < 4; v++) {
             int j = j0 + tx * 4 + v;
             if (j < jend && j <= i) A[(long long)i * ld + j] -= acc[u][v];
+        }
+    }
+}
+
+// FP64 form: trailing update of one 256-wide outer panel, A[i][j] -= sum_k
+// L[i][k] W[j][k] (k < 256) on the lower 128x128 tiles of rows/cols [P1, n).
+// 256 threads, 8x8 accumulators per thread (rows ty + 16u, columns tx + 16v),
+// K streamed in 16-wide chunks through two shared-memory buffers stored
+// k-major (the next chunk is loaded into registers while this one computes).
+constexpr int WTILE = 128, WKC = 16;
+
+__global__ void __launch_bounds__(256, 1) k_update_f64(int n, long long ld, double *A, int P0, int P1,
+                                                       const double *__restrict__ W, int ldw) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double(*sL)[WKC][WTILE] = reinterpret_cast<double(*)[WKC][WTILE]>(smem_raw);
+    double(*sW)[WKC][WTILE] = sL + 2;
+    long long bidx = blockIdx.x;
+    int bi = (int)((sqrt(8.0 * (double)bidx + 1.0) - 1.0) * 0.5);
+    while ((long long)(bi + 1) * (bi + 2) / 2 <= bidx) bi++;
+    while ((long long)bi * (bi + 1) / 2 > bidx) bi--;
+    const int bj = (int)(bidx - (long long)bi * (bi + 1) / 2);
+    const long long i0 = P1 + (long long)bi * WTILE, j0 = P1 + (long long)bj * WTILE;
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    // loader: row lr of the tile, k half lh (8 values)
+    const int lr = t >> 1, lh = t & 1;
+    const bool lrow = i0 + lr < n, wrow = j0 + lr < n;
+    const double *lsrc = A + (i0 + (lrow ? lr : 0)) * ld + P0 + lh * 8;
+    const double *wsrc = W + (j0 + (wrow ? lr : 0)) * (long long)ldw + lh * 8;
+    double2 pl[4], pw[4];
+    auto fetch = [&](int kc) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            pl[e] = lrow ? __ldg(reinterpret_cast<const double2 *>(lsrc + kc * WKC) + e) : make_double2(0.0, 0.0);
+            pw[e] = wrow ? __ldg(reinterpret_cast<const double2 *>(wsrc + kc * WKC) + e) : make_double2(0.0, 0.0);
+        }
+    };
+    auto stash = [&](int buf) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            sL[buf][lh * 8 + 2 * e][lr] = pl[e].x;
+            sL[buf][lh * 8 + 2 * e + 1][lr] = pl[e].y;
+            sW[buf][lh * 8 + 2 * e][lr] = pw[e].x;
+            sW[buf][lh * 8 + 2 * e + 1][lr] = pw[e].y;
+        }
+    };
+    double acc[8][8];
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+#pragma unroll
+        for (int v = 0; v < 8; v++) acc[u][v] = 0.0;
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    constexpr int NKC = 256 / WKC;
+#pragma unroll 1
+    for (int kc = 0; kc < NKC; kc++) {
+        const int buf = kc & 1;
+        if (kc + 1 < NKC) fetch(kc + 1);
+#pragma unroll
+        for (int k = 0; k < WKC; k++) {
+            double a[8], b[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) a[u] = sL[buf][k][ty + 16 * u];
+#pragma unroll
+            for (int v = 0; v < 8; v++) b[v] = sW[buf][k][tx + 16 * v];
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+#pragma unroll
+                for (int v = 0; v < 8; v++) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+        }
+        if (kc + 1 < NKC) stash(buf ^ 1);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        const long long row = i0 + ty + 16 * u;
+        if (row >= n) continue;
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+            const long long col = j0 + tx + 16 * v;
+            if (col < n && col <= row) A[row * ld + col] -= acc[u][v];
         }
     }
 }
@@ -616,6 +642,7 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     const size_t diag_smem = sizeof(T) * (2 * NB * (NB + 1) + NB * (SUB + 1) + SUB * (SUB + 1) + 3 * NB);
     const size_t panel_smem = sizeof(T) * (64 * (NB + 1) + NB * (NB + 1) + 2 * NB);
     const size_t upd_smem = sizeof(T) * 2 * NB * 68;
+    const size_t f64_smem = sizeof(double) * 4 * WKC * WTILE;
     static bool attr = false;
     if (!attr) {
         const int big = 96 * 1024;
@@ -623,8 +650,7 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         cudaFuncSetAttribute(k_ldlt_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(k_ldlt_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(k_ldlt_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(k_update_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_update_cols<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_update_cols<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(tc::k_update_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -642,10 +668,11 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             k_ldlt_panel<T><<<(n - k1 + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b),
                 ++ctx->launches;
     };
-    if (factor && tc_terms) {
+    if (factor) {
         // two-level LDL^T: 256-wide outer panels factored with the 64-wide kernels,
-        // trailing update of each outer panel on the tensor cores (TF32, or
-        // 3xTF32 when tc_terms == 3)
+        // then one trailing update per outer panel: on the tensor cores for the
+        // FP32 factor (TF32, or 3xTF32 when tc_terms == 3), register-tiled FP64
+        // for the FP64 factor
         const int PW = 256;
         for (int P0 = 0; P0 < n; P0 += PW) {
             const int P1 = P0 + PW < n ? P0 + PW : n;
@@ -659,7 +686,12 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                         ++ctx->launches;
                 }
             }
-            if (P1 < n) {
+            if (P1 < n && std::is_same<T, double>::value) {
+                const long long tiles = (n - P1 + WTILE - 1) / WTILE;
+                k_update_f64<<<(unsigned)(tiles * (tiles + 1) / 2), 256, f64_smem, st>>>(
+                    n, ld, reinterpret_cast<double *>(A), P0, P1, reinterpret_cast<const double *>(w.W), PW),
+                    ++ctx->launches;
+            } else if (P1 < n) {
                 // P1 < n: this outer panel is a full PW = 256 columns wide
                 const long long tiles = (n - P1 + tc::TILE - 1) / tc::TILE;
                 const long long ntiles = tiles * (tiles + 1) / 2;
@@ -687,17 +719,6 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                 auto kern = split ? tc::k_update_tc<true> : tc::k_update_tc<false>;
                 kern<<<grid, tc::THREADS, tc::smem_bytes(split), st>>>(mLh, mWh, mLl, mWl, n, ld, Af, P1, ntiles, flags),
                     ++ctx->launches;
-            }
-        }
-    } else if (factor) {
-        for (int k0 = 0; k0 < n; k0 += NB) {
-            int kb = n - k0 < NB ? n - k0 : NB;
-            int k1 = k0 + kb;
-            diag_and_panel(k0, kb, w.W, NB);
-            if (k1 < n) {
-                long long tiles = (n - k1 + 63) / 64;
-                long long nblk = tiles * (tiles + 1) / 2;
-                k_ldlt_update<T><<<(unsigned)nblk, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W, NB, k1), ++ctx->launches;
             }
         }
     }

@@ -98,7 +98,7 @@ static int ensure_scratch(mp_ctx *ctx) {
     cudaFree(g_scr.Linv64); cudaFree(g_scr.Linv32); cudaFree(g_scr.ready); cudaFree(g_scr.split32);
     g_scr = SolveScratch();
     MP_CUDA(ctx, cudaMalloc(&g_scr.dvec64, sizeof(double) * (n + 64)));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.W64, sizeof(double) * (size_t)(n + 64) * NB));
+    MP_CUDA(ctx, cudaMalloc(&g_scr.W64, sizeof(double) * (size_t)(n + 256) * 256));
     MP_CUDA(ctx, cudaMalloc(&g_scr.s64, sizeof(double) * NB));
     MP_CUDA(ctx, cudaMalloc(&g_scr.r, sizeof(double) * (n + 64)));
     MP_CUDA(ctx, cudaMalloc(&g_scr.dvec32, sizeof(float) * (n + 64)));
