@@ -782,7 +782,7 @@ int mp_compute_phi(mp_ctx *ctx, const double *ion_den, int method, int form, mp_
         for (it = 0; it < 10; it++) {
             if ((rc = fe_build_f1(ctx, den))) return rc;
             if ((rc = fe_residual(ctx))) return rc;
-            if ((rc = fe_build_j(ctx, MP_METHOD_NONLINEAR))) return rc;
+            if ((rc = fe_build_j(ctx, MP_METHOD_NONLINEAR, form))) return rc;
             rc = form == MP_FORM_FP64 ? fe_solve_gs(ctx, st) : fe_solve_ldlt(ctx, form, st);
             if (rc) return rc;
             ms_factor += st->ms_factor;
@@ -803,7 +803,7 @@ int mp_compute_phi(mp_ctx *ctx, const double *ion_den, int method, int form, mp_
         // one Newton step, src/FESolver.cpp:301-317
         if ((rc = fe_build_f1(ctx, den))) return rc;
         if ((rc = fe_residual(ctx))) return rc;
-        if ((rc = fe_build_j(ctx, method))) return rc;
+        if ((rc = fe_build_j(ctx, method, method == MP_METHOD_GAUSS_SEIDEL ? MP_FORM_FP64 : form))) return rc;
         rc = method == MP_METHOD_GAUSS_SEIDEL ? fe_solve_gs(ctx, st) : fe_solve_ldlt(ctx, form, st);
         if (rc) return rc;
         ms_factor = st->ms_factor;

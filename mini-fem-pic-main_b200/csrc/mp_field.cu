@@ -135,7 +135,25 @@ __global__ void k_copy_j(int neq, long long ld, const double *__restrict__ K, co
     }
 }
 
-int fe_build_j(mp_ctx *ctx, int method) {
+// Mixed form: the FP32 Jacobian for the factorization, straight from K and FP:
+// the lower triangle (all the LDL^T reads) of J = K - diag(FP), rounded to
+// FP32.  One CTA per row.
+__global__ void k_copy_j32(int neq, long long ld, const double *__restrict__ K, const double *__restrict__ FP,
+                           float *J32) {
+    for (long long r = blockIdx.x; r < neq; r += gridDim.x) {
+        const double *kr = K + r * ld;
+        float *jr = J32 + r * ld;
+        for (long long c = 4 * threadIdx.x; c <= r; c += 4 * blockDim.x) {
+            const double2 a = *reinterpret_cast<const double2 *>(kr + c);
+            const double2 b = *reinterpret_cast<const double2 *>(kr + c + 2);
+            double v[4] = {a.x, a.y, b.x, b.y};
+            if (r >= c && r < c + 4) v[r - c] = __dsub_rn(v[r - c], FP[r]);
+            *reinterpret_cast<float4 *>(jr + c) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+        }
+    }
+}
+
+int fe_build_j(mp_ctx *ctx, int method, int form) {
     (void)method;  // the full symmetric J serves both solvers (Lapack reads only one triangle)
     int th = 256;
     k_node_terms<<<(ctx->n_nodes + th - 1) / th, th, 0, ctx->stream>>>(
@@ -144,7 +162,15 @@ int fe_build_j(mp_ctx *ctx, int method) {
     k_eq_gather<<<(ctx->neq + th - 1) / th, th, 0, ctx->stream>>>(ctx->neq, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a,
                                                                  ctx->detJ, ctx->work, ctx->FP, 0), ++ctx->launches;
     long long ld = (ctx->neq + 31) & ~31ll;
-    k_copy_j<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J), ++ctx->launches;
+    if (form == MP_FORM_MIXED) {
+        if (!ctx->J32) MP_CUDA(ctx, cudaMalloc(&ctx->J32, sizeof(float) * (size_t)ld * ctx->neq));
+        k_copy_j32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J32),
+            ++ctx->launches;
+        ctx->j32_current = true;
+    } else {
+        k_copy_j<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J), ++ctx->launches;
+        ctx->j32_current = false;
+    }
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }

@@ -154,6 +154,7 @@ struct mp_ctx {
     double *fvec = nullptr, *FP = nullptr, *work = nullptr;  // [neq]
     double *K = nullptr, *J = nullptr;    // [neq][neq] row-major
     float *J32 = nullptr;                 // [neq][neq] mixed-form factor
+    bool j32_current = false;             // J32 holds the lower triangle of the current J
     double *scal = nullptr;               // device scalars for reductions
     double *scal_host = nullptr;          // pinned
     int *eq_ptr = nullptr, *eq_tet = nullptr;   // CSR equation -> (tet, a) sorted by tet
@@ -191,7 +192,7 @@ int launch_update_ef(mp_ctx *ctx);
 
 int fe_build_f1(mp_ctx *ctx, const double *den_dev);
 int fe_residual(mp_ctx *ctx);
-int fe_build_j(mp_ctx *ctx, int method);
+int fe_build_j(mp_ctx *ctx, int method, int form = MP_FORM_FP64);
 int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st);
 int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st);
 int fe_update_d(mp_ctx *ctx, double *l2_out);

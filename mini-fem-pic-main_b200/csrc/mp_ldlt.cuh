@@ -523,29 +523,50 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(int n, long long ld, const T *
     }
 }
 
-// L^T y = D^-1 z (unit upper after scaling, in place on x), blocks from the last
+// 4 consecutive values (16-byte aligned for float, 32 for double) as vector loads
+template <typename T, bool CG>
+__device__ __forceinline__ void load4(const T *p, T (&v)[4]) {
+    if constexpr (sizeof(T) == 8) {
+        const double2 a = CG ? __ldcg(reinterpret_cast<const double2 *>(p)) : __ldg(reinterpret_cast<const double2 *>(p));
+        const double2 b = CG ? __ldcg(reinterpret_cast<const double2 *>(p) + 1)
+                             : __ldg(reinterpret_cast<const double2 *>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else {
+        const float4 a = CG ? __ldcg(reinterpret_cast<const float4 *>(p)) : __ldg(reinterpret_cast<const float4 *>(p));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    }
+}
+
+// L^T y = D^-1 z (unit upper after scaling, in place on x), blocks from the last.
+// Thread (column quad c4, row quad part) takes a 4 x 4 piece of every later
+// 64 x 64 chunk with vector loads; the 16 partial sums of each column meet in
+// shared memory.
 template <typename T>
 __global__ void __launch_bounds__(256) k_trsv_bwd(int n, long long ld, const T *A, const T *Linv, const T *dvec, T *x,
                                                   int *ready, int epoch, unsigned long long *flags) {
     __shared__ T sI[NB][NB + 1];
     __shared__ T srhs[NB];
-    __shared__ T spart[4][NB];
+    __shared__ T spart[16][NB + 1];
     __shared__ int s_cnt[8];
     const int nblk = (n + NB - 1) / NB;
     const int t = threadIdx.x;
-    const int col = t & 63, part = t >> 6;  // column of this block, quarter of each later chunk's rows
+    const int c4 = t & 15, part = t >> 4;  // columns 4*c4 .. +3 of this block, rows 4*part .. +3 of each chunk
     for (int g = blockIdx.x; g < nblk; g += gridDim.x) {
         const int blk = nblk - 1 - g;
         const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
         for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = __ldg(&Linv[(size_t)blk * NB * NB + idx]);
-        const int cc = col < kb ? col : 0;
-        T acc = 0, ap[16];
-        // rows c*NB + part*16 + k of column r0 + col (zero past n)
+        T acc[4] = {0, 0, 0, 0}, ap[4][4];
+        // rows c*NB + 4*part + e, columns r0 + 4*c4 .. +3 (zero past n; every block before the last is full)
         auto fetch = [&](int c) {
 #pragma unroll
-            for (int k = 0; k < 16; k++) {
-                const int i = c * NB + part * 16 + k;
-                ap[k] = i < n ? __ldg(&A[(long long)i * ld + r0 + cc]) : T(0);
+            for (int e = 0; e < 4; e++) {
+                const int i = c * NB + 4 * part + e;
+                if (i < n) {
+                    load4<T, false>(A + (long long)i * ld + r0 + 4 * c4, ap[e]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; j++) ap[e][j] = T(0);
+                }
             }
         };
         int done = nblk - 1;  // chunks (done, nblk) accumulated
@@ -565,24 +586,49 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(int n, long long ld, const T *
             const int avail = done - cnt;
             for (int c = done; c > avail; c--) {
                 if (c != done) fetch(c);
-                const int i0 = c * NB + part * 16;
+                const int i0 = c * NB + 4 * part;
+                T xv[4];
+                if (i0 + 3 < n) {
+                    load4<T, true>(x + i0, xv);
+                } else {
 #pragma unroll
-                for (int k = 0; k < 16; k++)
-                    if (i0 + k < n) acc = fma(ap[k], __ldcg(&x[i0 + k]), acc);
+                    for (int e = 0; e < 4; e++) xv[e] = i0 + e < n ? __ldcg(&x[i0 + e]) : T(0);
+                }
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) acc[j] = fma(ap[e][j], xv[e], acc[j]);
             }
             done = avail;
             if (done > blk) fetch(done);
         }
-        spart[part][col] = col < kb ? acc : T(0);
-        __syncthreads();
-        if (t < NB) srhs[t] = t < kb ? __ldcg(&x[r0 + t]) / dvec[r0 + t] - (spart[0][t] + spart[1][t] + spart[2][t] + spart[3][t]) : T(0);
-        __syncthreads();
-        T v = 0;
 #pragma unroll
-        for (int k = 0; k < 16; k++) v = fma(sI[part * 16 + k][col], srhs[part * 16 + k], v);
-        spart[part][col] = v;
+        for (int j = 0; j < 4; j++) spart[part][4 * c4 + j] = acc[j];
         __syncthreads();
-        if (t < kb) x[r0 + t] = spart[0][t] + spart[1][t] + spart[2][t] + spart[3][t];
+        if (t < NB) {
+            T sum = 0;
+#pragma unroll
+            for (int pp = 0; pp < 16; pp++) sum += spart[pp][t];
+            srhs[t] = t < kb ? __ldcg(&x[r0 + t]) / dvec[r0 + t] - sum : T(0);
+        }
+        __syncthreads();
+        // y = Linv^T srhs
+        T v[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const T rr = srhs[4 * part + e];
+#pragma unroll
+            for (int j = 0; j < 4; j++) v[j] = fma(sI[4 * part + e][4 * c4 + j], rr, v[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) spart[part][4 * c4 + j] = v[j];
+        __syncthreads();
+        if (t < kb) {
+            T sum = 0;
+#pragma unroll
+            for (int pp = 0; pp < 16; pp++) sum += spart[pp][t];
+            x[r0 + t] = sum;
+        }
         __syncthreads();
         if (t == 0) st_release(ready + blk, epoch);
     }
@@ -610,14 +656,14 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // Map of a [rows][256] FP32 operand with row pitch `pitch` elements, loaded as
-// boxes of 32 (K) x 128 rows with the 128-byte swizzle the UMMA descriptors use.
-// base must be 16-byte aligned and pitch*4 a multiple of 16.
-static bool operand_map(CUtensorMap *m, const float *base, long long rows, long long pitch) {
+// boxes of 32 (K) x box_rows rows with the 128-byte swizzle the UMMA
+// descriptors use.  base must be 16-byte aligned and pitch*4 a multiple of 16.
+static bool operand_map(CUtensorMap *m, const float *base, long long rows, long long pitch, int box_rows) {
     PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
     if (!fn || rows < 1 || (reinterpret_cast<size_t>(base) & 15) || ((pitch * 4) & 15)) return false;
     cuuint64_t dims[2] = {(cuuint64_t)tc::PANEL, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
-    cuuint32_t box[2] = {(cuuint32_t)tc::KC, (cuuint32_t)tc::TILE};
+    cuuint32_t box[2] = {(cuuint32_t)tc::KC, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box, estr,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -693,8 +739,7 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                     ++ctx->launches;
             } else if (P1 < n) {
                 // P1 < n: this outer panel is a full PW = 256 columns wide
-                const long long tiles = (n - P1 + tc::TILE - 1) / tc::TILE;
-                const long long ntiles = tiles * (tiles + 1) / 2;
+                const long long ntiles = tc::tile_count((n - P1 + tc::TILE - 1) / tc::TILE);
                 const bool split = tc_terms == 3;
                 float *Af = reinterpret_cast<float *>(A);
                 const float *Wf = reinterpret_cast<const float *>(w.W);
@@ -706,11 +751,13 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                     const long long q = (long long)(n - P1) * (tc::PANEL / 4);
                     const int g = (int)std::min<long long>((q + 255) / 256, (long long)ctx->sm_count * 8);
                     tc::k_split_panel<<<g, 256, 0, st>>>(n, ld, Af, P0, P1, Wf, PW, Lh, Ll, Wh, Wl), ++ctx->launches;
-                    ok = operand_map(&mLh, Lh, n - P1, tc::PANEL) && operand_map(&mWh, Wh, n - P1, tc::PANEL) &&
-                         operand_map(&mLl, Ll, n - P1, tc::PANEL) && operand_map(&mWl, Wl, n - P1, tc::PANEL);
+                    ok = operand_map(&mLh, Lh, n - P1, tc::PANEL, tc::TILE) &&
+                         operand_map(&mWh, Wh, n - P1, tc::PANEL, tc::TILE_N) &&
+                         operand_map(&mLl, Ll, n - P1, tc::PANEL, tc::TILE) &&
+                         operand_map(&mWl, Wl, n - P1, tc::PANEL, tc::TILE_N);
                 } else {
-                    ok = operand_map(&mLh, Af + (long long)P1 * ld + P0, n - P1, ld) &&
-                         operand_map(&mWh, Wf + (long long)P1 * PW, n - P1, PW);
+                    ok = operand_map(&mLh, Af + (long long)P1 * ld + P0, n - P1, ld, tc::TILE) &&
+                         operand_map(&mWh, Wf + (long long)P1 * PW, n - P1, PW, tc::TILE_N);
                     mLl = mLh;
                     mWl = mWh;
                 }

@@ -136,7 +136,10 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         }
     } else {
         if (!ctx->J32) MP_CUDA(ctx, cudaMalloc(&ctx->J32, sizeof(float) * (size_t)ld * n));
-        k_j_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(n, ld, ctx->J, ctx->J32), ++ctx->launches;
+        // the factorization overwrites J32: it is current once per build of J
+        if (!ctx->j32_current)
+            k_j_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(n, ld, ctx->J, ctx->J32), ++ctx->launches;
+        ctx->j32_current = false;
         MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * n, ctx->stream));
         LdltWork<float> w{g_scr.dvec32, g_scr.W32, g_scr.s32, g_scr.Linv32, g_scr.ready, g_scr.split32};
         double rn = 0, bn = 0;

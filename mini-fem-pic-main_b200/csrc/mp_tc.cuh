@@ -1,6 +1,9 @@
 // Tensor-core (tcgen05, TF32 inputs, FP32 accumulators in TMEM) trailing update
-// of the mixed-form LDL^T:  A[i][j] -= sum_k L[i][k] W[j][k]  on the lower
-// 128x128 tiles of the trailing matrix, K = one 256-wide outer panel.
+// of the mixed-form LDL^T:  A[i][j] -= sum_k L[i][k] W[j][k]  on the tiles of
+// 128 rows x 256 columns that meet the lower triangle of the trailing matrix,
+// K = one 256-wide outer panel.  The 256-wide tiles halve the operand bytes
+// per FLOP against square 128 x 128 tiles (the operand stream from L2 is what
+// bounds this kernel).
 //
 // Persistent, warp-specialised.  One CTA per SM walks the lower tiles
 // blockIdx.x, blockIdx.x + gridDim.x, ...:
@@ -8,8 +11,9 @@
 //                      multicast, 128-byte swizzle) of 32-wide K chunks of the
 //                      tile's L rows and W rows into STAGES shared-memory
 //                      stages, each completing on its stage's "full" mbarrier;
-//   warp 1 (one lane)  MMA issuer: tcgen05.mma.cta_group::1.kind::tf32 from the
-//                      stage into one of two 128-column TMEM accumulators, then
+//   warp 1 (one lane)  MMA issuer: tcgen05.mma.cta_group::1.kind::tf32 (M = 128,
+//                      N = 256) from the stage into one of two 256-column TMEM
+//                      accumulators (all 512 columns), then
 //                      tcgen05.commit to the stage's "empty" mbarrier (frees it
 //                      for the producer) and, after a tile's last chunk, to the
 //                      accumulator's "full" mbarrier;
@@ -39,12 +43,14 @@
 namespace mp {
 namespace tc {
 
-constexpr int TILE = 128;                   // M = N = 128
+constexpr int TILE = 128;                   // M: tile rows
+constexpr int TILE_N = 256;                 // N: tile columns
 constexpr int KC = 32;                      // K elements per chunk (one 128-byte swizzle row)
 constexpr int PANEL = 256;                  // K of one launch: the outer panel width
 constexpr int NCHUNK = PANEL / KC;          // chunks per tile
-constexpr int CHUNK_BYTES = TILE * KC * 4;  // 16 KB per operand chunk
-constexpr int STAGES = 3;
+constexpr int CHUNK_L = TILE * KC * 4;      // 16 KB: one L operand chunk
+constexpr int CHUNK_W = TILE_N * KC * 4;    // 32 KB: one W operand chunk
+__host__ __device__ constexpr int stages(bool split) { return split ? 2 : 4; }  // 192 KB of stages either way
 constexpr int THREADS = 192;                // producer warp, MMA warp, 4 epilogue warps
 constexpr long long SPIN_LIMIT = 1ll << 22;
 
@@ -55,8 +61,8 @@ __device__ __forceinline__ unsigned long long smem_desc(unsigned addr) {
     return (unsigned long long)((addr >> 4) & 0x3FFF) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
 
-// Instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = 128.
-constexpr unsigned IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+// Instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = 256.
+constexpr unsigned IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
 
 __device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
@@ -89,7 +95,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
     }
 }
 
-// 2-D tiled TMA load of the box (KC, TILE) at element coordinates (x, y).
+// 2-D tiled TMA load of the map's box at element coordinates (x, y).
 __device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, int x, int y, unsigned long long *bar) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
@@ -109,13 +115,26 @@ __device__ __forceinline__ void mma_commit(unsigned long long *bar) {
                  : "memory");
 }
 
-// lower tile number -> (bi, bj), bj <= bi
+// Tile number -> (bi, bj): 128-row block bi, 256-column block bj, over the
+// tiles that meet the lower triangle (bj <= bi/2).  Row blocks 2M and 2M+1
+// both hold M+1 tiles, so tiles before row block 2M number M(M+1) and before
+// 2M+1 number (M+1)^2.
 __device__ __forceinline__ void tile_coords(long long t, int &bi, int &bj) {
-    int b = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while ((long long)(b + 1) * (b + 2) / 2 <= t) b++;
-    while ((long long)b * (b + 1) / 2 > t) b--;
-    bi = b;
-    bj = (int)(t - (long long)b * (b + 1) / 2);
+    long long M = (long long)((sqrt(4.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((M + 1) * (M + 2) <= t) M++;
+    while (M * (M + 1) > t) M--;
+    if (t < (M + 1) * (M + 1)) {
+        bi = (int)(2 * M);
+        bj = (int)(t - M * (M + 1));
+    } else {
+        bi = (int)(2 * M + 1);
+        bj = (int)(t - (M + 1) * (M + 1));
+    }
+}
+// number of tiles over `rb` row blocks
+__host__ __device__ inline long long tile_count(long long rb) {
+    const long long M = rb / 2;
+    return (rb & 1) ? (M + 1) * (M + 1) : M * (M + 1);
 }
 
 // x rounded to the nearest TF32 value (low 13 mantissa bits cleared)
@@ -144,9 +163,10 @@ __global__ void k_split_panel(int n, long long ld, const float *__restrict__ A, 
     }
 }
 
-// A[i][j] -= sum_{k<256} L[i][k] W[j][k] on the lower 128x128 tiles of rows and
-// columns [P1, n).  The maps cover rows [P1, n) of the operands (rows past the
-// end read as zero).
+// A[i][j] -= sum_{k<256} L[i][k] W[j][k] on the 128 x 256 tiles that meet the
+// lower triangle of rows and columns [P1, n).  The maps cover rows [P1, n) of
+// the operands (rows past the end read as zero); the L maps load boxes of 128
+// rows, the W maps boxes of 256 rows.
 template <bool SPLIT>
 __global__ void __launch_bounds__(THREADS, 1)
     k_update_tc(const __grid_constant__ CUtensorMap mLh, const __grid_constant__ CUtensorMap mWh,
@@ -154,8 +174,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                 float *A, int P1, long long ntiles, unsigned long long *flags) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<size_t>(smem_raw) + 1023) & ~size_t(1023));
-    constexpr int OPS = SPLIT ? 4 : 2;  // operand chunks per stage: L hi, W hi (, L lo, W lo)
-    constexpr unsigned STAGE_BYTES = OPS * CHUNK_BYTES;
+    constexpr int STAGES = stages(SPLIT);
+    // stage: L hi, W hi (, L lo, W lo)
+    constexpr unsigned STAGE_BYTES = SPLIT ? 2 * (CHUNK_L + CHUNK_W) : CHUNK_L + CHUNK_W;
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(base + STAGES * STAGE_BYTES);
     unsigned long long *full = bars, *empty = bars + STAGES, *acc_full = bars + 2 * STAGES,
                        *acc_empty = bars + 2 * STAGES + 2, *drain = bars + 2 * STAGES + 4;
@@ -178,7 +199,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(saddr(tmem_slot))
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(saddr(tmem_slot))
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -205,10 +226,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                     unsigned char *st = base + s * STAGE_BYTES;
                     mbar_expect_tx(&full[s], STAGE_BYTES);
                     tma_load(st, &mLh, kc * KC, bi * TILE, &full[s]);
-                    tma_load(st + CHUNK_BYTES, &mWh, kc * KC, bj * TILE, &full[s]);
+                    tma_load(st + CHUNK_L, &mWh, kc * KC, bj * TILE_N, &full[s]);
                     if (SPLIT) {
-                        tma_load(st + 2 * CHUNK_BYTES, &mLl, kc * KC, bi * TILE, &full[s]);
-                        tma_load(st + 3 * CHUNK_BYTES, &mWl, kc * KC, bj * TILE, &full[s]);
+                        tma_load(st + CHUNK_L + CHUNK_W, &mLl, kc * KC, bi * TILE, &full[s]);
+                        tma_load(st + 2 * CHUNK_L + CHUNK_W, &mWl, kc * KC, bj * TILE_N, &full[s]);
                     }
                 }
             }
@@ -229,7 +250,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const long long v = lt >> 1;
                 if (v > 0 && !mbar_wait(&acc_empty[a], (unsigned)((v - 1) & 1), abort)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const unsigned d = tmem + (unsigned)(a * TILE);
+                const unsigned d = tmem + (unsigned)(a * TILE_N);
                 for (int kc = 0; kc < NCHUNK; kc++, it++) {
                     const int s = (int)(it % STAGES);
                     if (!mbar_wait(&full[s], (unsigned)((it / STAGES) & 1), abort)) {
@@ -238,9 +259,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const unsigned char *st = base + s * STAGE_BYTES;
-                    const unsigned long long dl = smem_desc(saddr(st)), dw = smem_desc(saddr(st + CHUNK_BYTES));
-                    const unsigned long long dll = smem_desc(saddr(st + 2 * CHUNK_BYTES));
-                    const unsigned long long dwl = smem_desc(saddr(st + 3 * CHUNK_BYTES));
+                    const unsigned long long dl = smem_desc(saddr(st)), dw = smem_desc(saddr(st + CHUNK_L));
+                    const unsigned long long dll = smem_desc(saddr(st + CHUNK_L + CHUNK_W));
+                    const unsigned long long dwl = smem_desc(saddr(st + 2 * CHUNK_L + CHUNK_W));
 #pragma unroll
                     for (int kk = 0; kk < KC / 8; kk++) {  // 8 TF32 = 32 B per MMA step: +2 in the descriptor
                         const unsigned accum = (kc > 0 || kk > 0) ? 1u : 0u;
@@ -264,9 +285,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         } else if (warp >= 2) {
             // ---- epilogue: TMEM lanes 32*(warp%4) .. +31 are this warp's tile rows ----
-            // Each thread owns one tile row: it loads the row's 128 old values of
-            // A first (they do not depend on the MMAs, so the loads overlap the
-            // wait), then subtracts the accumulator chunk by chunk.
+            // Each thread owns one tile row and walks its 256 columns in four
+            // quarters of 64: the old values of A for a quarter are loaded one
+            // quarter ahead (the first before the accumulator wait), since they do
+            // not depend on the MMAs.
             const int q = warp & 3;
             const int r = q * 32 + lane;
             long long lt = 0;
@@ -274,54 +296,64 @@ __global__ void __launch_bounds__(THREADS, 1)
                 int bi, bj;
                 tile_coords(t, bi, bj);
                 const long long row = P1 + (long long)bi * TILE + r;
-                const long long c0 = P1 + (long long)bj * TILE;
-                // full 16-column chunks of this row inside the lower triangle and the matrix
+                const long long c0 = P1 + (long long)bj * TILE_N;
                 const bool row_ok = row < n;
-                float4 old[TILE / 4];
+                auto load_quarter = [&](int qq, float4 (&dst)[16]) {
 #pragma unroll
-                for (int g = 0; g < TILE / 4; g++) {
-                    const long long col = c0 + 4 * g;
-                    old[g] = (row_ok && col + 3 <= row && col + 3 < n)
-                                 ? *reinterpret_cast<const float4 *>(A + row * ld + col)
-                                 : make_float4(0.f, 0.f, 0.f, 0.f);
-                }
+                    for (int g = 0; g < 16; g++) {
+                        const long long col = c0 + 64 * qq + 4 * g;
+                        dst[g] = (row_ok && col + 3 <= row && col + 3 < n)
+                                     ? *reinterpret_cast<const float4 *>(A + row * ld + col)
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                };
+                float4 cur[16], nxt[16];
+                load_quarter(0, cur);
                 const int a = (int)(lt & 1);
                 int ok = 1;
                 if (lane == 0) ok = mbar_wait(&acc_full[a], (unsigned)((lt >> 1) & 1), abort);
                 ok = __shfl_sync(0xffffffffu, ok, 0);
                 if (!ok) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const unsigned taddr = tmem + (unsigned)(a * TILE) + ((unsigned)(q * 32) << 16);
+                const unsigned taddr = tmem + (unsigned)(a * TILE_N) + ((unsigned)(q * 32) << 16);
 #pragma unroll
-                for (int cb = 0; cb < TILE / 16; cb++) {
-                    unsigned v[16];
-                    asm volatile(
-                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                        "[%16];"
-                        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                          "=r"(v[14]), "=r"(v[15])
-                        : "r"(taddr + cb * 16));
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                    const long long col = c0 + cb * 16;
-                    if (row_ok && col <= row) {
-                        float *p = A + row * ld + col;
+                for (int qq = 0; qq < 4; qq++) {
+                    if (qq + 1 < 4) load_quarter(qq + 1, nxt);
 #pragma unroll
-                        for (int g = 0; g < 4; g++) {
-                            const long long cg = col + 4 * g;
-                            if (cg + 3 <= row && cg + 3 < n) {
-                                float4 o = old[cb * 4 + g];
-                                o.x -= __uint_as_float(v[4 * g]);
-                                o.y -= __uint_as_float(v[4 * g + 1]);
-                                o.z -= __uint_as_float(v[4 * g + 2]);
-                                o.w -= __uint_as_float(v[4 * g + 3]);
-                                *reinterpret_cast<float4 *>(p + 4 * g) = o;
-                            } else {
+                    for (int cb = 0; cb < 4; cb++) {
+                        unsigned v[16];
+                        asm volatile(
+                            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+                            "%15}, [%16];"
+                            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                              "=r"(v[14]), "=r"(v[15])
+                            : "r"(taddr + qq * 64 + cb * 16));
+                        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                        const long long col = c0 + 64 * qq + 16 * cb;
+                        if (row_ok && col <= row) {
+                            float *p = A + row * ld + col;
 #pragma unroll
-                                for (int j = 0; j < 4; j++)
-                                    if (cg + j <= row && cg + j < n) p[4 * g + j] -= __uint_as_float(v[4 * g + j]);
+                            for (int g = 0; g < 4; g++) {
+                                const long long cg = col + 4 * g;
+                                if (cg + 3 <= row && cg + 3 < n) {
+                                    float4 o = cur[cb * 4 + g];
+                                    o.x -= __uint_as_float(v[4 * g]);
+                                    o.y -= __uint_as_float(v[4 * g + 1]);
+                                    o.z -= __uint_as_float(v[4 * g + 2]);
+                                    o.w -= __uint_as_float(v[4 * g + 3]);
+                                    *reinterpret_cast<float4 *>(p + 4 * g) = o;
+                                } else {
+#pragma unroll
+                                    for (int j = 0; j < 4; j++)
+                                        if (cg + j <= row && cg + j < n) p[4 * g + j] -= __uint_as_float(v[4 * g + j]);
+                                }
                             }
                         }
+                    }
+                    if (qq + 1 < 4) {
+#pragma unroll
+                        for (int g = 0; g < 16; g++) cur[g] = nxt[g];
                     }
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -332,12 +364,14 @@ __global__ void __launch_bounds__(THREADS, 1)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem) : "memory");
+    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
     if (threadIdx.x == 0 && *abort == 1) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
 }
 
 // operand stages + barriers, TMEM slot, abort flag + 1024-byte alignment slack
-constexpr size_t smem_bytes(bool split) { return (size_t)STAGES * (split ? 4 : 2) * CHUNK_BYTES + 256 + 1024; }
+constexpr size_t smem_bytes(bool split) {
+    return (size_t)stages(split) * (split ? 2 * (CHUNK_L + CHUNK_W) : CHUNK_L + CHUNK_W) + 256 + 1024;
+}
 
 }  // namespace tc
 }  // namespace mp
