@@ -322,29 +322,39 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols(int n, long long ld, T
     }
 }
 
-// FP64 form: trailing update of one 256-wide outer panel, A[i][j] -= sum_k
-// L[i][k] W[j][k] (k < 256) on the lower 128x128 tiles of rows/cols [P1, n).
-// 256 threads, 8x8 accumulators per thread (rows ty + 16u, columns tx + 16v),
-// K streamed in 16-wide chunks through two shared-memory buffers stored
-// k-major (the next chunk is loaded into registers while this one computes).
+// FP64 form: A[i][j] -= sum_{k<K} L[i][k] W[j][k] for rows/cols from R0, with
+// L = A[i][K0 ...] and W rows of pitch ldw (K a multiple of 16).  colblocks = 0:
+// the lower 128x128 tiles of [R0, n)^2 (the trailing update of a super-panel);
+// colblocks > 0: every tile of rows [R0, n) x columns [R0, R0 + 128*colblocks)
+// (a strip inside a super-panel), lower parts only.  256 threads, 8x8
+// accumulators per thread (rows ty + 16u, columns tx + 16v), K streamed in
+// 16-wide chunks through two shared-memory buffers stored k-major (the next
+// chunk is loaded into registers while this one computes).
 constexpr int WTILE = 128, WKC = 16;
 
-__global__ void __launch_bounds__(256, 1) k_update_f64(int n, long long ld, double *A, int P0, int P1,
-                                                       const double *__restrict__ W, int ldw) {
+__global__ void __launch_bounds__(256, 1) k_update_f64(int n, long long ld, double *A, int K0, int K, int R0,
+                                                       const double *__restrict__ W, int ldw, int colblocks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double(*sL)[WKC][WTILE] = reinterpret_cast<double(*)[WKC][WTILE]>(smem_raw);
     double(*sW)[WKC][WTILE] = sL + 2;
     long long bidx = blockIdx.x;
-    int bi = (int)((sqrt(8.0 * (double)bidx + 1.0) - 1.0) * 0.5);
-    while ((long long)(bi + 1) * (bi + 2) / 2 <= bidx) bi++;
-    while ((long long)bi * (bi + 1) / 2 > bidx) bi--;
-    const int bj = (int)(bidx - (long long)bi * (bi + 1) / 2);
-    const long long i0 = P1 + (long long)bi * WTILE, j0 = P1 + (long long)bj * WTILE;
+    int bi, bj;
+    if (colblocks > 0) {
+        bi = (int)(bidx / colblocks);
+        bj = (int)(bidx % colblocks);
+    } else {
+        bi = (int)((sqrt(8.0 * (double)bidx + 1.0) - 1.0) * 0.5);
+        while ((long long)(bi + 1) * (bi + 2) / 2 <= bidx) bi++;
+        while ((long long)bi * (bi + 1) / 2 > bidx) bi--;
+        bj = (int)(bidx - (long long)bi * (bi + 1) / 2);
+    }
+    const long long i0 = R0 + (long long)bi * WTILE, j0 = R0 + (long long)bj * WTILE;
+    if (j0 > i0 + WTILE - 1) return;  // strip tile entirely above the diagonal
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
     // loader: row lr of the tile, k half lh (8 values)
     const int lr = t >> 1, lh = t & 1;
     const bool lrow = i0 + lr < n, wrow = j0 + lr < n;
-    const double *lsrc = A + (i0 + (lrow ? lr : 0)) * ld + P0 + lh * 8;
+    const double *lsrc = A + (i0 + (lrow ? lr : 0)) * ld + K0 + lh * 8;
     const double *wsrc = W + (j0 + (wrow ? lr : 0)) * (long long)ldw + lh * 8;
     double2 pl[4], pw[4];
     auto fetch = [&](int kc) {
@@ -371,7 +381,7 @@ __global__ void __launch_bounds__(256, 1) k_update_f64(int n, long long ld, doub
     fetch(0);
     stash(0);
     __syncthreads();
-    constexpr int NKC = 256 / WKC;
+    const int NKC = K / WKC;
 #pragma unroll 1
     for (int kc = 0; kc < NKC; kc++) {
         const int buf = kc & 1;
@@ -639,7 +649,7 @@ struct LdltWork {
     T *dvec, *W, *s;
     T *Linv;       // [blocks][NB][NB] inverses of the diagonal blocks' L (the solves use them)
     int *ready;    // [2][blocks] per-block ready words of the two solves
-    float *split;  // tensor-core path: [4][n][256] hi/lo copies of one outer panel's L and W rows
+    float *split;  // tensor-core path: [4][n][SUPER_W] hi/lo copies of the update's L and W rows
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
@@ -655,13 +665,13 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// Map of a [rows][256] FP32 operand with row pitch `pitch` elements, loaded as
+// Map of a [rows][K] FP32 operand with row pitch `pitch` elements, loaded as
 // boxes of 32 (K) x box_rows rows with the 128-byte swizzle the UMMA
 // descriptors use.  base must be 16-byte aligned and pitch*4 a multiple of 16.
-static bool operand_map(CUtensorMap *m, const float *base, long long rows, long long pitch, int box_rows) {
+static bool operand_map(CUtensorMap *m, const float *base, long long rows, long long pitch, int box_rows, int K) {
     PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
     if (!fn || rows < 1 || (reinterpret_cast<size_t>(base) & 15) || ((pitch * 4) & 15)) return false;
-    cuuint64_t dims[2] = {(cuuint64_t)tc::PANEL, (cuuint64_t)rows};
+    cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
     cuuint32_t box[2] = {(cuuint32_t)tc::KC, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
@@ -671,6 +681,11 @@ static bool operand_map(CUtensorMap *m, const float *base, long long rows, long 
 }
 
 static int g_solve_epoch = 0;
+
+// Super-panel width of the two-level LDL^T: the trailing matrix is read and
+// written once per SUPER_W columns (the HBM traffic that bounds the trailing
+// update), the panels inside a super-panel update only its remaining columns.
+constexpr int PANEL_W = 256, SUPER_W = 4 * PANEL_W;
 
 template <typename T>
 int trsv_grid(mp_ctx *ctx, const void *kernel, int nblk) {
@@ -714,58 +729,85 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             k_ldlt_panel<T><<<(n - k1 + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b),
                 ++ctx->launches;
     };
+    // A[i][j] -= sum_{k<K} L[i][K0+k] W[j][kofs+k] for rows [R0, n) and columns
+    // [R0, C1): a strip inside a super-panel when C1 < n, else the lower
+    // triangle of the trailing matrix.  W rows are global rows, pitch SUPER_W.
+    auto update = [&](int R0, int C1, int K0, int K, int kofs) -> int {
+        const bool strip = C1 < n;
+        if (std::is_same<T, double>::value) {
+            const long long rb = (n - R0 + WTILE - 1) / WTILE;
+            const int cb = strip ? (C1 - R0) / WTILE : 0;
+            const long long ntiles = strip ? rb * cb : rb * (rb + 1) / 2;
+            k_update_f64<<<(unsigned)ntiles, 256, f64_smem, st>>>(n, ld, reinterpret_cast<double *>(A), K0, K, R0,
+                                                                 reinterpret_cast<const double *>(w.W) + kofs,
+                                                                 SUPER_W, cb),
+                ++ctx->launches;
+            return MP_OK;
+        }
+        const long long rb = (n - R0 + tc::TILE - 1) / tc::TILE;
+        const int cb = strip ? (C1 - R0) / tc::TILE_N : 0;
+        const long long ntiles = strip ? rb * cb : tc::tile_count(rb);
+        const long long wrows = (strip ? C1 : n) - R0;
+        const bool split = tc_terms == 3;
+        float *Af = reinterpret_cast<float *>(A);
+        const float *Wf = reinterpret_cast<const float *>(w.W);
+        const float *Lsrc = Af + (long long)R0 * ld + K0, *Wsrc = Wf + (long long)R0 * SUPER_W + kofs;
+        CUtensorMap mLh, mWh, mLl, mWl;
+        bool ok;
+        if (split) {
+            const size_t plane = (size_t)n * SUPER_W;
+            float *Lh = w.split, *Ll = w.split + plane, *Wh = w.split + 2 * plane, *Wl = w.split + 3 * plane;
+            const int gl = (int)std::min<long long>(((n - R0) * (K / 4) + 255) / 256, (long long)ctx->sm_count * 8);
+            const int gw = (int)std::min<long long>((wrows * (K / 4) + 255) / 256, (long long)ctx->sm_count * 8);
+            tc::k_split_rows<<<gl, 256, 0, st>>>(Lsrc, ld, n - R0, K, Lh, Ll), ++ctx->launches;
+            tc::k_split_rows<<<gw, 256, 0, st>>>(Wsrc, SUPER_W, wrows, K, Wh, Wl), ++ctx->launches;
+            ok = operand_map(&mLh, Lh, n - R0, K, tc::TILE, K) && operand_map(&mWh, Wh, wrows, K, tc::TILE_N, K) &&
+                 operand_map(&mLl, Ll, n - R0, K, tc::TILE, K) && operand_map(&mWl, Wl, wrows, K, tc::TILE_N, K);
+        } else {
+            ok = operand_map(&mLh, Lsrc, n - R0, ld, tc::TILE, K) &&
+                 operand_map(&mWh, Wsrc, wrows, SUPER_W, tc::TILE_N, K);
+            mLl = mLh;
+            mWl = mWh;
+        }
+        if (!ok) return fail(ctx, MP_ERR_CUDA, "cuTensorMapEncodeTiled failed for the tensor-core update");
+        const int grid = (int)std::min<long long>(ntiles, (long long)ctx->sm_count);
+        auto kern = split ? tc::k_update_tc<true> : tc::k_update_tc<false>;
+        kern<<<grid, tc::THREADS, tc::smem_bytes(split), st>>>(mLh, mWh, mLl, mWl, n, ld, Af, R0, ntiles, K / tc::KC,
+                                                               cb, flags),
+            ++ctx->launches;
+        return MP_OK;
+    };
     if (factor) {
-        // two-level LDL^T: 256-wide outer panels factored with the 64-wide kernels,
-        // then one trailing update per outer panel: on the tensor cores for the
-        // FP32 factor (TF32, or 3xTF32 when tc_terms == 3), register-tiled FP64
-        // for the FP64 factor
-        const int PW = 256;
-        for (int P0 = 0; P0 < n; P0 += PW) {
-            const int P1 = P0 + PW < n ? P0 + PW : n;
-            for (int k0 = P0; k0 < P1; k0 += NB) {
-                int kb = P1 - k0 < NB ? P1 - k0 : NB;
-                int k1 = k0 + kb;
-                diag_and_panel(k0, kb, w.W + (k0 - P0), PW);
-                if (k1 < n && k1 < P1) {
-                    dim3 g((P1 - k1 + 63) / 64, (n - k1 + 63) / 64);
-                    k_ldlt_update_cols<T><<<g, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W + (k0 - P0), PW, k1, P1),
-                        ++ctx->launches;
+        // Two-level LDL^T over super-panels of SUPER_W columns, each made of
+        // PANEL_W-wide panels.  A panel is factored with the 64-wide kernels
+        // (diagonal block, panel, updates restricted to the panel's columns),
+        // then updates the rest of its super-panel (a strip); the trailing
+        // matrix gets one update per super-panel with K = SUPER_W: on the tensor
+        // cores for the FP32 factor (TF32, or 3xTF32 when tc_terms == 3),
+        // register-tiled FP64 for the FP64 factor.
+        for (int S0 = 0; S0 < n; S0 += SUPER_W) {
+            const int S1 = S0 + SUPER_W < n ? S0 + SUPER_W : n;
+            for (int P0 = S0; P0 < S1; P0 += PANEL_W) {
+                const int P1 = P0 + PANEL_W < S1 ? P0 + PANEL_W : S1;
+                for (int k0 = P0; k0 < P1; k0 += NB) {
+                    const int kb = P1 - k0 < NB ? P1 - k0 : NB;
+                    const int k1 = k0 + kb;
+                    diag_and_panel(k0, kb, w.W + (k0 - S0), SUPER_W);
+                    if (k1 < n && k1 < P1) {
+                        dim3 g((P1 - k1 + 63) / 64, (n - k1 + 63) / 64);
+                        k_ldlt_update_cols<T><<<g, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W + (k0 - S0), SUPER_W,
+                                                                        k1, P1),
+                            ++ctx->launches;
+                    }
+                }
+                if (P1 < S1) {  // a full panel with more of its super-panel to the right
+                    int rc = update(P1, S1, P0, PANEL_W, P0 - S0);
+                    if (rc) return rc;
                 }
             }
-            if (P1 < n && std::is_same<T, double>::value) {
-                const long long tiles = (n - P1 + WTILE - 1) / WTILE;
-                k_update_f64<<<(unsigned)(tiles * (tiles + 1) / 2), 256, f64_smem, st>>>(
-                    n, ld, reinterpret_cast<double *>(A), P0, P1, reinterpret_cast<const double *>(w.W), PW),
-                    ++ctx->launches;
-            } else if (P1 < n) {
-                // P1 < n: this outer panel is a full PW = 256 columns wide
-                const long long ntiles = tc::tile_count((n - P1 + tc::TILE - 1) / tc::TILE);
-                const bool split = tc_terms == 3;
-                float *Af = reinterpret_cast<float *>(A);
-                const float *Wf = reinterpret_cast<const float *>(w.W);
-                CUtensorMap mLh, mWh, mLl, mWl;
-                bool ok;
-                if (split) {
-                    const size_t plane = (size_t)n * tc::PANEL;
-                    float *Lh = w.split, *Ll = w.split + plane, *Wh = w.split + 2 * plane, *Wl = w.split + 3 * plane;
-                    const long long q = (long long)(n - P1) * (tc::PANEL / 4);
-                    const int g = (int)std::min<long long>((q + 255) / 256, (long long)ctx->sm_count * 8);
-                    tc::k_split_panel<<<g, 256, 0, st>>>(n, ld, Af, P0, P1, Wf, PW, Lh, Ll, Wh, Wl), ++ctx->launches;
-                    ok = operand_map(&mLh, Lh, n - P1, tc::PANEL, tc::TILE) &&
-                         operand_map(&mWh, Wh, n - P1, tc::PANEL, tc::TILE_N) &&
-                         operand_map(&mLl, Ll, n - P1, tc::PANEL, tc::TILE) &&
-                         operand_map(&mWl, Wl, n - P1, tc::PANEL, tc::TILE_N);
-                } else {
-                    ok = operand_map(&mLh, Af + (long long)P1 * ld + P0, n - P1, ld, tc::TILE) &&
-                         operand_map(&mWh, Wf + (long long)P1 * PW, n - P1, PW, tc::TILE_N);
-                    mLl = mLh;
-                    mWl = mWh;
-                }
-                if (!ok) return fail(ctx, MP_ERR_CUDA, "cuTensorMapEncodeTiled failed for the tensor-core update");
-                const int grid = (int)std::min<long long>(ntiles, (long long)ctx->sm_count);
-                auto kern = split ? tc::k_update_tc<true> : tc::k_update_tc<false>;
-                kern<<<grid, tc::THREADS, tc::smem_bytes(split), st>>>(mLh, mWh, mLl, mWl, n, ld, Af, P1, ntiles, flags),
-                    ++ctx->launches;
+            if (S1 < n) {  // a full super-panel
+                int rc = update(S1, n, S0, SUPER_W, 0);
+                if (rc) return rc;
             }
         }
     }

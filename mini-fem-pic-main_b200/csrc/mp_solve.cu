@@ -98,17 +98,17 @@ static int ensure_scratch(mp_ctx *ctx) {
     cudaFree(g_scr.Linv64); cudaFree(g_scr.Linv32); cudaFree(g_scr.ready); cudaFree(g_scr.split32);
     g_scr = SolveScratch();
     MP_CUDA(ctx, cudaMalloc(&g_scr.dvec64, sizeof(double) * (n + 64)));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.W64, sizeof(double) * (size_t)(n + 256) * 256));
+    MP_CUDA(ctx, cudaMalloc(&g_scr.W64, sizeof(double) * (size_t)(n + NB) * SUPER_W));
     MP_CUDA(ctx, cudaMalloc(&g_scr.s64, sizeof(double) * NB));
     MP_CUDA(ctx, cudaMalloc(&g_scr.r, sizeof(double) * (n + 64)));
     MP_CUDA(ctx, cudaMalloc(&g_scr.dvec32, sizeof(float) * (n + 64)));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.W32, sizeof(float) * (size_t)(n + 256) * 256));
+    MP_CUDA(ctx, cudaMalloc(&g_scr.W32, sizeof(float) * (size_t)(n + NB) * SUPER_W));
     MP_CUDA(ctx, cudaMalloc(&g_scr.s32, sizeof(float) * NB));
     MP_CUDA(ctx, cudaMalloc(&g_scr.b32, sizeof(float) * (n + 64)));
     const size_t nblk = (n + NB - 1) / NB;
     MP_CUDA(ctx, cudaMalloc(&g_scr.Linv64, sizeof(double) * nblk * NB * NB));
     MP_CUDA(ctx, cudaMalloc(&g_scr.Linv32, sizeof(float) * nblk * NB * NB));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.split32, sizeof(float) * 4 * (size_t)n * tc::PANEL));
+    MP_CUDA(ctx, cudaMalloc(&g_scr.split32, sizeof(float) * 4 * (size_t)n * SUPER_W));
     MP_CUDA(ctx, cudaMalloc(&g_scr.ready, sizeof(int) * 2 * ((n + NB - 1) / NB + 1)));
     MP_CUDA(ctx, cudaMemset(g_scr.ready, 0, sizeof(int) * 2 * ((n + NB - 1) / NB + 1)));
     g_scr.neq = n;

@@ -46,8 +46,7 @@ namespace tc {
 constexpr int TILE = 128;                   // M: tile rows
 constexpr int TILE_N = 256;                 // N: tile columns
 constexpr int KC = 32;                      // K elements per chunk (one 128-byte swizzle row)
-constexpr int PANEL = 256;                  // K of one launch: the outer panel width
-constexpr int NCHUNK = PANEL / KC;          // chunks per tile
+constexpr int PANEL = 256;                  // panel width: K of a strip update
 constexpr int CHUNK_L = TILE * KC * 4;      // 16 KB: one L operand chunk
 constexpr int CHUNK_W = TILE_N * KC * 4;    // 32 KB: one W operand chunk
 __host__ __device__ constexpr int stages(bool split) { return split ? 2 : 4; }  // 192 KB of stages either way
@@ -131,6 +130,14 @@ __device__ __forceinline__ void tile_coords(long long t, int &bi, int &bj) {
         bj = (int)(t - (M + 1) * (M + 1));
     }
 }
+__device__ __forceinline__ void tile_of(long long t, int colblocks, int &bi, int &bj) {
+    if (colblocks > 0) {
+        bi = (int)(t / colblocks);
+        bj = (int)(t % colblocks);
+    } else {
+        tile_coords(t, bi, bj);
+    }
+}
 // number of tiles over `rb` row blocks
 __host__ __device__ inline long long tile_count(long long rb) {
     const long long M = rb / 2;
@@ -142,36 +149,35 @@ __device__ __forceinline__ float tf32_hi(float x) {
     return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
-// Splits the outer panel's L rows (A[r][P0, P0+256)) and W rows (W[r][0, 256))
-// of rows r in [P1, n) into hi/lo arrays [n - P1][256] for the TMA.
-__global__ void k_split_panel(int n, long long ld, const float *__restrict__ A, int P0, int P1,
-                              const float *__restrict__ W, int ldw, float *Lh, float *Ll, float *Wh, float *Wl) {
-    const long long total = (long long)(n - P1) * (PANEL / 4);
+// Splits rows [0, nrows) x columns [0, K) of a row-major FP32 operand (pitch
+// ld) into hi/lo arrays [nrows][K] for the TMA (K a multiple of 4).
+__global__ void k_split_rows(const float *__restrict__ src, long long ld, long long nrows, int K, float *hi,
+                             float *lo) {
+    const long long total = nrows * (K / 4);
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
          q += (long long)gridDim.x * blockDim.x) {
-        const long long r = q / (PANEL / 4);
-        const int c = (int)(q % (PANEL / 4)) * 4;
-        const float4 x = __ldg(reinterpret_cast<const float4 *>(A + (P1 + r) * ld + P0 + c));
-        const float4 w = __ldg(reinterpret_cast<const float4 *>(W + (P1 + r) * (long long)ldw + c));
-        const float4 xh = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
-        const float4 wh = make_float4(tf32_hi(w.x), tf32_hi(w.y), tf32_hi(w.z), tf32_hi(w.w));
-        const long long o = r * PANEL + c;
-        *reinterpret_cast<float4 *>(Lh + o) = xh;
-        *reinterpret_cast<float4 *>(Ll + o) = make_float4(x.x - xh.x, x.y - xh.y, x.z - xh.z, x.w - xh.w);
-        *reinterpret_cast<float4 *>(Wh + o) = wh;
-        *reinterpret_cast<float4 *>(Wl + o) = make_float4(w.x - wh.x, w.y - wh.y, w.z - wh.z, w.w - wh.w);
+        const long long r = q / (K / 4);
+        const int c = (int)(q % (K / 4)) * 4;
+        const float4 x = __ldg(reinterpret_cast<const float4 *>(src + r * ld + c));
+        const float4 h = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
+        const long long o = r * K + c;
+        *reinterpret_cast<float4 *>(hi + o) = h;
+        *reinterpret_cast<float4 *>(lo + o) = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
     }
 }
 
-// A[i][j] -= sum_{k<256} L[i][k] W[j][k] on the 128 x 256 tiles that meet the
-// lower triangle of rows and columns [P1, n).  The maps cover rows [P1, n) of
-// the operands (rows past the end read as zero); the L maps load boxes of 128
-// rows, the W maps boxes of 256 rows.
+// A[i][j] -= sum_{k<K} L[i][k] W[j][k] (K = 32*nchunk) for rows from P1 and
+// columns from P1.  colblocks = 0: the 128 x 256 tiles that meet the lower
+// triangle of [P1, n)^2 (the trailing update of a super-panel); colblocks > 0:
+// every tile of rows [P1, n) x columns [P1, P1 + 256*colblocks) (a strip inside
+// a super-panel), lower parts only.  The L maps cover the rows from P1 (rows
+// past the end read as zero) and load boxes of 128 rows; the W maps cover the
+// output columns' rows and load boxes of 256 rows.
 template <bool SPLIT>
 __global__ void __launch_bounds__(THREADS, 1)
     k_update_tc(const __grid_constant__ CUtensorMap mLh, const __grid_constant__ CUtensorMap mWh,
                 const __grid_constant__ CUtensorMap mLl, const __grid_constant__ CUtensorMap mWl, int n, long long ld,
-                float *A, int P1, long long ntiles, unsigned long long *flags) {
+                float *A, int P1, long long ntiles, int nchunk, int colblocks, unsigned long long *flags) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<size_t>(smem_raw) + 1023) & ~size_t(1023));
     constexpr int STAGES = stages(SPLIT);
@@ -215,8 +221,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             bool ok = true;
             for (long long t = blockIdx.x; ok && t < ntiles; t += gridDim.x) {
                 int bi, bj;
-                tile_coords(t, bi, bj);
-                for (int kc = 0; kc < NCHUNK; kc++, it++) {
+                tile_of(t, colblocks, bi, bj);
+                for (int kc = 0; kc < nchunk; kc++, it++) {
                     const int s = (int)(it % STAGES);
                     const long long u = it / STAGES;
                     if (u > 0 && !mbar_wait(&empty[s], (unsigned)((u - 1) & 1), abort)) {
@@ -251,7 +257,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 if (v > 0 && !mbar_wait(&acc_empty[a], (unsigned)((v - 1) & 1), abort)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const unsigned d = tmem + (unsigned)(a * TILE_N);
-                for (int kc = 0; kc < NCHUNK; kc++, it++) {
+                for (int kc = 0; kc < nchunk; kc++, it++) {
                     const int s = (int)(it % STAGES);
                     if (!mbar_wait(&full[s], (unsigned)((it / STAGES) & 1), abort)) {
                         ok = false;
@@ -294,7 +300,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             long long lt = 0;
             for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
                 int bi, bj;
-                tile_coords(t, bi, bj);
+                tile_of(t, colblocks, bi, bj);
                 const long long row = P1 + (long long)bi * TILE + r;
                 const long long c0 = P1 + (long long)bj * TILE_N;
                 const bool row_ok = row < n;
