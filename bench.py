@@ -11,8 +11,8 @@ is InjectIons -> MoveParticles -> computePhi (Lapack method: one Newton step,
 direct solve) -> updateEf.  FP64 form; the mixed form is measured beside it
 on the same seeded population with its errors against FP64.
 
-value      particle-steps/s of MoveParticles, device-resident inputs (injected
-           particles staged in HBM), L2 flushed between steps
+value      particle-steps/s of MoveParticles, device-resident inputs (each
+           step's ions injected on the device), L2 flushed between steps
 e2e        the same through the C ABI with host buffers: the step's injected
            particles H2D from host memory, node density D2H each step
 e2e_full_step    the whole step through the C ABI (adds computePhi, updateEf
@@ -123,23 +123,20 @@ def run_form(form, args, cfg, deck, pop, inj_batches, device, rank, world, torch
     qm = mp.QE / (16 * mp.AMU)
     dt, spwt = cfg["dt"], cfg["spwt"] / world
     stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
-    # device-staged injections
-    staged = []
-    for (p, v, c) in inj_batches:
-        staged.append((torch.from_numpy(np.ascontiguousarray(p.T)).to(device),
-                       torch.from_numpy(np.ascontiguousarray(v.T)).to(device),
-                       torch.from_numpy(c).to(device), len(c)))
+    # device-resident steps inject on the device (the reference's counts, Philox
+    # Maxwellian sampling); the end-to-end steps upload the host injector's ions
+    inj_dev = mp.Injector(m, seed=rank)
+    P = deck.params
+    sigma = np.sqrt(KTI_EV * mp.QE / (16 * mp.AMU))
     torch.cuda.synchronize(device)
 
     def step(k, host):
-        p, v, c, n = staged[k % len(staged)]
         if host:
             hp, hv, hc = inj_batches[k % len(inj_batches)]
             ctx.append(hp, hv, hc, rewind=True, q_over_m=qm, half_dt=0.5 * dt)
             st = ctx.push(qm, dt, spwt, den_out=den_host)
         else:
-            ctx.append_device(p.data_ptr(), v.data_ptr(), c.data_ptr(), n, rewind=True, q_over_m=qm,
-                              half_dt=0.5 * dt)
+            ctx.inject_device(inj_dev, P.plasma_den, P.ion_velocity, dt, cfg["spwt"], sigma, qm, 1000 + rank, k)
             st = ctx.push(qm, dt, spwt)
         if world > 1:
             sharding.allreduce_density(ctx, device)
@@ -515,6 +512,9 @@ def main():
                        "ions_per_gpu": int(np.mean(nb)), "dt": cfg["dt"], "method": "lapack (1 Newton step)",
                        "form": "fp64", "l2": f"flushed ({FLUSH_BYTES >> 20} MiB write) between timed steps",
                        "tet_sort_every": SORT_PERIOD,
+                       "injection": "device (the reference's per-face counts; Philox4x32-10 positions and "
+                                    "0.1 eV Maxwellian velocities) in the device-resident steps; the host "
+                                    "injector's ions uploaded in the end-to-end steps",
                        "parallelism": f"particles sharded x{world}, density all-reduce" if world > 1 else "1 GPU"},
             "newton_step_ms": float(newton_ms),
             "full_step_particle_steps_per_s": psteps_all / step_s,

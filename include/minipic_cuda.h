@@ -296,6 +296,18 @@ int mp_injector_sample(mp_injector *inj, double plasma_den, double ion_velocity,
 int mp_injector_count(mp_injector *inj, double plasma_den, double ion_velocity, double dt, double spwt,
                       int64_t *n_next);
 int mp_injector_get_rem(mp_injector *inj, double *rem);
+/* InjectIons on the device (src/mini-pic.cpp:208-265): the reference's per-face
+ * counts, with the injector's shared remainder carried exactly as
+ * mp_injector_sample carries it, and positions (uniform on each inlet
+ * triangle, the reference's a+b>1 fold) and velocities (normal*ion_velocity
+ * plus a Maxwellian thermal part of standard deviation thermal_sigma per
+ * component; 0 = the reference's cold beam) drawn on the device with
+ * Philox4x32-10 keyed by seed at counter (particle, step) instead of the
+ * reference's mt19937 stream.  The particles are appended with the half-step
+ * rewind in the current device field (q_over_m, dt/2).  No particle crosses
+ * the host; *n_out (nullable) = particles injected. */
+int mp_inject_device(mp_ctx *ctx, mp_injector *inj, double plasma_den, double ion_velocity, double dt, double spwt,
+                     double thermal_sigma, double q_over_m, uint64_t seed, uint64_t step, int64_t *n_out);
 int mp_injector_set_rem(mp_injector *inj, double rem);
 
 /* ---- adjoint of K push + scatter steps ---------------------------------------

@@ -284,6 +284,7 @@ int mp_destroy(mp_ctx *ctx) {
     if (!ctx) return MP_OK;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     adjoint_free(ctx);
+    inject_free(ctx);
     void *dev[] = {ctx->tets, ctx->tets32, ctx->tet_x0, ctx->con, ctx->ef, ctx->node_volume, ctx->node_pos,
                    ctx->den, ctx->den_fixed, ctx->counters, ctx->scal, ctx->compact_off, ctx->sort_hist,
                    ctx->part_block[0], ctx->part_block[1], ctx->ID, ctx->LM, ctx->detJ, ctx->nx, ctx->g, ctx->uh,

@@ -13,6 +13,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "mp_injector.h"
 #include "mp_internal.h"
 
 namespace {
@@ -79,16 +80,6 @@ Quadrature make_quadrature() {
 }
 
 }  // namespace mp
-
-struct mp_injector {
-    int n_faces = 0;
-    std::vector<int> con;       // [n][3]
-    std::vector<double> u, v, normal, area, p0;
-    std::vector<int> cell;
-    std::mt19937 gen;
-    std::uniform_real_distribution<double> dist{0, 1.0};
-    double rem = 0;
-};
 
 extern "C" {
 

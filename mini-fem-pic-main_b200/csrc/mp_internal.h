@@ -165,6 +165,7 @@ struct mp_ctx {
     long long launches = 0;
 
     void *adjoint = nullptr;              // adjoint state (mp_adjoint.cu), created by mp_adjoint_setup
+    void *inject = nullptr;               // device injection state (mp_inject.cu)
 };
 
 namespace mp {
@@ -199,5 +200,6 @@ int fe_update_d(mp_ctx *ctx, double *l2_out);
 int fe_uh(mp_ctx *ctx);
 int fe_assemble(mp_ctx *ctx);
 void adjoint_free(mp_ctx *ctx);
+void inject_free(mp_ctx *ctx);
 
 }  // namespace mp

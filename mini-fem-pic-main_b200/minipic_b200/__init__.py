@@ -61,7 +61,7 @@ EXPORTED = [
     "mp_injector_get_rem", "mp_injector_set_rem", "mp_set_track_ids", "mp_kernel_launches",
     "mp_device_buffer", "mp_push_particles_noalloc", "mp_set_mixed_factor",
     "mp_adjoint_setup", "mp_adjoint_add_particles", "mp_adjoint_forward", "mp_adjoint_flux",
-    "mp_adjoint_backward", "mp_adjoint_tangent", "mp_set_walk_policy",
+    "mp_adjoint_backward", "mp_adjoint_tangent", "mp_set_walk_policy", "mp_inject_device",
 ]
 
 
@@ -154,6 +154,7 @@ def lib():
         L.mp_set_sort_period.argtypes = [vp, i32]
         L.mp_set_mixed_factor.argtypes = [vp, C.c_int]
         L.mp_set_walk_policy.argtypes = [vp, C.c_int]
+        L.mp_inject_device.argtypes = [vp, vp, d, d, d, d, d, d, C.c_uint64, C.c_uint64, C.POINTER(i64)]
         L.mp_adjoint_setup.argtypes = [vp, i32, i32, d, d, d, d, vp, vp, vp, C.c_int]
         L.mp_adjoint_add_particles.argtypes = [vp, i32, C.c_int, i64, vp, vp, vp]
         L.mp_adjoint_forward.argtypes = [vp, vp, d, C.c_int, vp, C.POINTER(AdjointStats)]
@@ -435,6 +436,13 @@ class Context:
     # options
     def set_walk_limit(self, n):
         self._c(lib().mp_set_walk_limit(self.h, n))
+
+    def inject_device(self, injector, plasma_den, ion_velocity, dt, spwt, thermal_sigma, q_over_m, seed, step):
+        """InjectIons on the device (Philox sampling, the reference's counts); returns the count."""
+        n = C.c_int64(0)
+        self._c(lib().mp_inject_device(self.h, injector.h, plasma_den, ion_velocity, dt, spwt, thermal_sigma,
+                                       q_over_m, seed, step, C.byref(n)))
+        return n.value
 
     def set_walk_policy(self, policy):
         """WALK_LIMIT_ERROR (default) or WALK_LIMIT_ABSORB: what a walk that reaches the hop limit does."""
