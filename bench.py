@@ -264,7 +264,8 @@ def mixed_vs_fp64_at_scale(args, device, torch, flush, steps=3, warmup=2):
         P = deck.params
         batches = [inj.sample(P.plasma_den, P.ion_velocity, cfg["dt"], cfg["spwt"]) for _ in range(warmup + steps)]
         ctxs = {}
-        for name, form in (("fp64", mp.FP64), ("mixed", mp.MIXED)):
+        for name, form, method in (("fp64", mp.FP64, mp.LAPACK), ("mixed", mp.MIXED, mp.LAPACK),
+                                   ("fp64_sparse_cg", mp.FP64, mp.SPARSE_CG)):
             c = mp.Context(deck.mesh, device=device)
             c.fe_setup(**fe)
             c.set_track_ids(True)  # for the cell comparison at the end
@@ -278,21 +279,21 @@ def mixed_vs_fp64_at_scale(args, device, torch, flush, steps=3, warmup=2):
             c.set_sort_period(SORT_PERIOD)
             if form == mp.MIXED:
                 c.set_form(mp.MIXED)
-            ctxs[name] = (c, form, torch.cuda.ExternalStream(c.stream(), device=device))
+            ctxs[name] = (c, form, method, torch.cuda.ExternalStream(c.stream(), device=device))
         del pos, vel, cell
         res = {k: {"step_ms": [], "newton_ms": [], "push_ms": [], "n": [], "refinements": [], "lost": []} for k in ctxs}
-        den_err, phi_err = [], []
+        den_err, phi_err, sparse_phi_err = [], [], []
         for k in range(warmup + steps):
             hp, hv, hc = batches[k]
             dens, uhs = {}, {}
-            for name, (c, form, stream) in ctxs.items():
+            for name, (c, form, method, stream) in ctxs.items():
                 flush.zero_()
                 torch.cuda.synchronize(device)
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
                 c.append(hp, hv, hc, rewind=True, q_over_m=qm, half_dt=0.5 * cfg["dt"])
                 st = c.push(qm, cfg["dt"], cfg["spwt"])
-                nt = c.compute_phi(mp.LAPACK, form)
+                nt = c.compute_phi(method, form)
                 c.update_ef()
                 e1.record(stream)
                 e1.synchronize()
@@ -310,21 +311,26 @@ def mixed_vs_fp64_at_scale(args, device, torch, flush, steps=3, warmup=2):
                 dens[name], uhs[name] = den, uh
             den_err.append(float(np.linalg.norm(dens["mixed"] - dens["fp64"]) / np.linalg.norm(dens["fp64"])))
             phi_err.append(float(np.abs(uhs["mixed"] - uhs["fp64"]).max()))
+            sparse_phi_err.append(float(np.abs(uhs["fp64_sparse_cg"] - uhs["fp64"]).max()))
         # the solver's own precision: one Newton step of each form from the same state
         # (d, the accumulated F1) and the same density, the FP64 context's
-        c64, cm = ctxs["fp64"][0], ctxs["mixed"][0]
+        c64, cm, csp = ctxs["fp64"][0], ctxs["mixed"][0], ctxs["fp64_sparse_cg"][0]
         for name in ("d", "F1"):
-            cm.fe_set(name, c64.fe_get(name))
+            v = c64.fe_get(name)
+            cm.fe_set(name, v)
+            csp.fe_set(name, v)
         c64.compute_phi(mp.LAPACK, mp.FP64, ion_den=dens["fp64"])
         cm.compute_phi(mp.LAPACK, mp.MIXED, ion_den=dens["fp64"])
+        nt_sp = csp.compute_phi(mp.SPARSE_CG, mp.FP64, ion_den=dens["fp64"])
         phi_solve_err = float(np.abs(cm.field()[1] - c64.field()[1]).max())
+        sparse_solve_err = float(np.abs(csp.field()[1] - c64.field()[1]).max())
         ga, gb = ctxs["fp64"][0].download(mp.ORDER_ID), ctxs["mixed"][0].download(mp.ORDER_ID)
         ids = np.union1d(ga["id"], gb["id"])
         ia = np.full(ids.size, -1)
         ib = np.full(ids.size, -1)
         ia[np.searchsorted(ids, ga["id"])] = ga["cell"]
         ib[np.searchsorted(ids, gb["id"])] = gb["cell"]
-        for c, _, _ in ctxs.values():
+        for c, _, _, _ in ctxs.values():
             c.close()
     out = {"workload": cfg["label"], "mesh_hexes": cfg["n"] ** 3, "tets": deck.mesh.n_tets,
            "unknowns": int(fe["neq"]), "ions": int(np.mean(res["fp64"]["n"])), "steps": steps, "warmup": warmup,
@@ -336,6 +342,12 @@ def mixed_vs_fp64_at_scale(args, device, torch, flush, steps=3, warmup=2):
                      "absorbed_at_walk_limit_per_step": float(np.mean(r["lost"]))}
     out["mixed_over_fp64_full_step"] = (out["mixed"]["full_step_particle_steps_per_s"] /
                                         out["fp64"]["full_step_particle_steps_per_s"])
+    out["fp64_sparse_cg"].pop("refinement_solves")
+    out["fp64_sparse_cg"]["cg_iterations"] = int(nt_sp.linear_iterations)
+    out["fp64_sparse_cg"]["errors_vs_fp64_lapack"] = {
+        "phi_solve_max_abs_V": sparse_solve_err, "phi_closed_loop_max_abs_V": max(sparse_phi_err),
+        "what": "the FP64 particles with the Newton step's J y = G solved by conjugate gradients on the sparse K "
+                "(||r|| <= 1e-12 ||G||) against the dense LDL^T FP64 step"}
     out["errors_vs_fp64"] = {"density_l2_rel": max(den_err),
                              "phi_solve_max_abs_V": phi_solve_err,
                              "phi_closed_loop_max_abs_V": max(phi_err),
@@ -344,6 +356,43 @@ def mixed_vs_fp64_at_scale(args, device, torch, flush, steps=3, warmup=2):
                                      "the same seeded run; phi_solve: the mixed Newton step against the FP64 one "
                                      "from the same state and density; phi_closed_loop: the two runs' potentials, "
                                      "which also carry their density difference"}
+    return out
+
+
+def sparse_field_at_scale(device, n=64, reps=3):
+    """The sparse field solve where the dense one cannot run: a 64^3 Kuhn box
+    minus the r = 0.02 m sphere at -10 V (255,822 unknowns; the dense K and J
+    would take 523 GB each) in sparse storage.  Node ion density: the plasma
+    density with 10 % seeded noise.  Times (CUDA events inside the library)
+    one SPARSE_CG Newton step from zero potential and the SPARSE_NEWTON loop,
+    each from the same state, and reports the conjugate-gradient iterations."""
+    with tempfile.TemporaryDirectory() as wd:
+        kd = kuhn.build(n, sphere=(50.0, 50.0, 50.0, 20.0))
+        kuhn.write(kd, wd, dt=5e-8, method="lapack")
+        deck = mp.Deck.load(wd)
+    fe = deck.fe_desc_arrays(workloads.SPHERE_POTENTIAL)
+    c = mp.Context(deck.mesh, device=device)
+    c.set_fe_storage(mp.FE_SPARSE)
+    c.fe_setup(**fe)
+    neq = c.neq
+    nnz = int(c.fe_sparse_matrix()[0][-1])
+    rng = np.random.default_rng(17)
+    ion = deck.params.plasma_den * (1 + 0.1 * rng.standard_normal(deck.mesh.n_nodes))
+    out = {"workload": f"kuhn{n}s sparse field solve", "unknowns": int(neq), "nonzeros": nnz,
+           "dense_K_bytes": 8 * neq * neq, "sparse_K_bytes": 12 * nnz}
+    for key, method in (("sparse_cg_newton_step", mp.SPARSE_CG), ("sparse_newton_loop", mp.SPARSE_NEWTON)):
+        ms, its, nits = [], [], []
+        for r in range(reps + 1):
+            c.fe_set("d", np.zeros(neq))
+            c.fe_set("F1", np.zeros(neq))
+            st = c.compute_phi(method, mp.FP64, ion_den=ion)
+            if r:
+                ms.append(st.ms_total)
+                its.append(st.linear_iterations)
+                nits.append(st.newton_iterations)
+        out[key] = {"ms": float(np.mean(ms)), "newton_iterations": int(max(nits)),
+                    "cg_iterations_last_solve": int(max(its))}
+    c.close()
     return out
 
 
@@ -470,9 +519,10 @@ def main():
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu:
             cpu = cpu_baseline(cfg, wd, pop)
-    scale = None
+    scale = sparse_big = None
     if rank == 0 and world == 1 and not args.no_scale and args.config == 1:
         scale = mixed_vs_fp64_at_scale(args, local, torch, flush)
+        sparse_big = sparse_field_at_scale(local)
 
     def agg(r):
         push_ms = np.array(r["push_ms"])
@@ -556,6 +606,8 @@ def main():
             line["cpu_baseline"] = cpu
         if scale is not None:
             line["mixed_vs_fp64_kuhn32s_50M"] = scale
+        if sparse_big is not None:
+            line["sparse_field_kuhn64s"] = sparse_big
         print(json.dumps(line))
     if world > 1:
         torch.distributed.barrier()

@@ -32,6 +32,8 @@
  *   mp_adjoint_*                  no reference counterpart: derivatives of K steps of
  *                                 MoveParticles + InjectIons (src/mini-pic.cpp:208-320)
  *                                 with respect to the node potential and the drift
+ *   mp_set_fe_storage,            sparse K (preAssembly's K, src/FESolver.cpp:434-485,
+ *   mp_fe_sparse_matrix           without its zeros) and the SPARSE_* methods
  */
 #ifndef MINIPIC_CUDA_H
 #define MINIPIC_CUDA_H
@@ -58,8 +60,23 @@ enum {
     MP_ERR_LIMIT = 10         /* size above the fixed maximum of an allocation-free entry point */
 };
 
-/* FESolver::Method, src/FESolver.h:26 */
-enum { MP_METHOD_NONLINEAR = 0, MP_METHOD_GAUSS_SEIDEL = 1, MP_METHOD_LAPACK = 2 };
+/* FESolver::Method, src/FESolver.h:26, and two sparse methods of this library:
+ * SPARSE_CG is the Lapack method's single Newton step (src/FESolver.cpp:301-317)
+ * with J y = G solved by Jacobi-preconditioned conjugate gradients in FP64 on
+ * the sparse K (||G - J y|| <= rtol ||G||, mp_set_sparse_solver);
+ * SPARSE_NEWTON is the NonLinear method's loop (src/FESolver.cpp:324-364: F1
+ * accumulating, up to 10 iterations, stop at ||y||/neq < 1e-2) with the same
+ * conjugate-gradient inner solves in place of Gauss-Seidel. */
+enum {
+    MP_METHOD_NONLINEAR = 0, MP_METHOD_GAUSS_SEIDEL = 1, MP_METHOD_LAPACK = 2,
+    MP_METHOD_SPARSE_CG = 3, MP_METHOD_SPARSE_NEWTON = 4
+};
+
+/* Storage of K for the field solve.  DENSE (the reference's neq x neq arrays,
+ * src/FESolver.cpp:80-127) keeps a sparse copy beside it, so every method
+ * runs; SPARSE keeps only the sparse K (about 15 nonzeros a row, 12 B each)
+ * and runs the SPARSE_* methods, for meshes whose dense K does not fit. */
+enum { MP_FE_STORAGE_DENSE = 0, MP_FE_STORAGE_SPARSE = 1 };
 
 /* Arithmetic forms. FP64 is the reference's method bit for bit on the particle
  * side; MIXED stores particles as FP32 offsets from the owning tet's vertex 0
@@ -247,6 +264,14 @@ int mp_push_particles_noalloc(const void *particles_in, void *particles_out, int
 
 /* ---- field solve ------------------------------------------------------------------ */
 int mp_fe_setup(mp_ctx *ctx, const mp_fe_desc *fe);
+/* Chooses the storage of K (MP_FE_STORAGE_*); call before mp_fe_setup. */
+int mp_set_fe_storage(mp_ctx *ctx, int storage);
+/* Conjugate-gradient stop: ||G - J y||_2 <= rtol ||G||_2 (default 1e-12) within
+ * max_iterations (default 20000; MP_ERR_NOT_CONVERGED past it). */
+int mp_set_sparse_solver(mp_ctx *ctx, double rtol, int32_t max_iterations);
+/* The sparse K as CSR (columns ascending): with row_ptr, col and val all NULL
+ * only *nnz is written; else row_ptr[neq + 1], col[nnz], val[nnz]. */
+int mp_fe_sparse_matrix(mp_ctx *ctx, int64_t *nnz, int64_t *row_ptr, int32_t *col, double *val);
 int mp_fe_upload(mp_ctx *ctx, int which, const double *values);
 int mp_fe_download(mp_ctx *ctx, int which, double *out);
 /* FESolver::computePhi: ion_den (host, nullable = the device density of the last
@@ -256,7 +281,7 @@ int mp_fe_build_f1(mp_ctx *ctx, const double *ion_den);
 int mp_fe_residual(mp_ctx *ctx);
 int mp_fe_build_j(mp_ctx *ctx, int method);
 /* Solves J y = G (G from mp_fe_residual, or b if non-NULL); y stays on the device
- * (MP_VEC_Y).  method MP_METHOD_GAUSS_SEIDEL or MP_METHOD_LAPACK. */
+ * (MP_VEC_Y).  method MP_METHOD_GAUSS_SEIDEL, MP_METHOD_LAPACK or MP_METHOD_SPARSE_CG. */
 int mp_fe_solve_linear(mp_ctx *ctx, int method, int form, const double *b, mp_newton_stats *stats);
 /* FESolver::updateEf from the device uh (or uh_host if non-NULL). */
 int mp_update_ef(mp_ctx *ctx, const double *uh_host);

@@ -285,6 +285,7 @@ int mp_destroy(mp_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     adjoint_free(ctx);
     inject_free(ctx);
+    sparse_free(ctx);
     void *dev[] = {ctx->tets, ctx->tets32, ctx->tet_x0, ctx->con, ctx->ef, ctx->node_volume, ctx->node_pos,
                    ctx->den, ctx->den_fixed, ctx->counters, ctx->scal, ctx->compact_off, ctx->sort_hist,
                    ctx->part_block[0], ctx->part_block[1], ctx->ID, ctx->LM, ctx->detJ, ctx->nx, ctx->g, ctx->uh,
@@ -593,8 +594,13 @@ int mp_fe_setup(mp_ctx *ctx, const mp_fe_desc *fe) {
         MP_CUDA(ctx, cudaMalloc(p, vec));
         MP_CUDA(ctx, cudaMemset(*p, 0, vec));
     }
-    MP_CUDA(ctx, cudaMalloc(&ctx->K, sizeof(double) * (size_t)ld * neq));
-    MP_CUDA(ctx, cudaMalloc(&ctx->J, sizeof(double) * (size_t)ld * neq));
+    ctx->K = ctx->J = nullptr;
+    ctx->j32_current = false;
+    const bool dense = ctx->fe_storage == MP_FE_STORAGE_DENSE;
+    if (dense) {
+        MP_CUDA(ctx, cudaMalloc(&ctx->K, sizeof(double) * (size_t)ld * neq));
+        MP_CUDA(ctx, cudaMalloc(&ctx->J, sizeof(double) * (size_t)ld * neq));
+    }
     cudaStream_t st = ctx->stream;
     MP_CUDA(ctx, cudaMemcpyAsync(ctx->ID, fe->ID, sizeof(int) * nn, cudaMemcpyHostToDevice, st));
     MP_CUDA(ctx, cudaMemcpyAsync(ctx->LM, LM.data(), sizeof(int) * 4 * nt, cudaMemcpyHostToDevice, st));
@@ -612,17 +618,26 @@ int mp_fe_setup(mp_ctx *ctx, const mp_fe_desc *fe) {
     ctx->n0 = fe->n0;
     ctx->phi0 = fe->phi0;
     ctx->kTe = fe->kTe;
+    int rc = sparse_setup(ctx, LM, cnt, eq_tet);
+    if (rc) return rc;
     if (fe->K_rows || fe->K_dense) {
         if (!fe->F0) return fail(ctx, MP_ERR_ARG, "K given without F0");
-        MP_CUDA(ctx, cudaMemset(ctx->K, 0, sizeof(double) * (size_t)ld * neq));
-        for (int i = 0; i < neq; i++) {
-            const double *row = fe->K_rows ? fe->K_rows[i] : fe->K_dense + (size_t)i * neq;
-            MP_CUDA(ctx, cudaMemcpy(ctx->K + (size_t)i * ld, row, sizeof(double) * neq, cudaMemcpyHostToDevice));
+        if (dense) {
+            MP_CUDA(ctx, cudaMemset(ctx->K, 0, sizeof(double) * (size_t)ld * neq));
+            for (int i = 0; i < neq; i++) {
+                const double *row = fe->K_rows ? fe->K_rows[i] : fe->K_dense + (size_t)i * neq;
+                MP_CUDA(ctx, cudaMemcpy(ctx->K + (size_t)i * ld, row, sizeof(double) * neq, cudaMemcpyHostToDevice));
+            }
+            rc = fe_sparse_from_dense(ctx);
+        } else {
+            rc = fe_sparse_from_host(ctx, fe->K_rows, fe->K_dense);
         }
+        if (rc) return rc;
         MP_CUDA(ctx, cudaMemcpy(ctx->F0, fe->F0, sizeof(double) * neq, cudaMemcpyHostToDevice));
     } else {
-        int rc = fe_assemble(ctx);
+        rc = dense ? fe_assemble(ctx) : fe_assemble_sparse(ctx);
         if (rc) return rc;
+        if (dense && (rc = fe_sparse_from_dense(ctx))) return rc;
     }
     MP_CUDA(ctx, cudaStreamSynchronize(st));
     ctx->fe_ready = true;
@@ -659,6 +674,7 @@ int mp_fe_download(mp_ctx *ctx, int which, double *out) {
     if (!ctx || !out) return MP_ERR_ARG;
     if (which == MP_MAT_K || which == MP_MAT_J) {
         if (!ctx->fe_ready) return fail(ctx, MP_ERR_STATE, "no FE setup");
+        if (!ctx->K) return fail(ctx, MP_ERR_STATE, "sparse storage: no dense matrix (mp_fe_sparse_matrix)");
         const long long ld = (ctx->neq + 31) & ~31ll;
         MP_CUDA(ctx, cudaMemcpy2DAsync(out, sizeof(double) * ctx->neq, which == MP_MAT_K ? ctx->K : ctx->J,
                                        sizeof(double) * ld, sizeof(double) * ctx->neq, ctx->neq,
@@ -740,6 +756,9 @@ int mp_fe_residual(mp_ctx *ctx) {
 int mp_fe_build_j(mp_ctx *ctx, int method) {
     if (!ctx) return MP_ERR_ARG;
     if (!ctx->fe_ready) return fail(ctx, MP_ERR_STATE, "no FE setup");
+    if (method < MP_METHOD_NONLINEAR || method > MP_METHOD_SPARSE_NEWTON) return MP_ERR_ARG;
+    if (!ctx->K && method <= MP_METHOD_LAPACK)
+        return fail(ctx, MP_ERR_STATE, "sparse storage: the dense J needs MP_FE_STORAGE_DENSE");
     int rc = fe_build_j(ctx, method);
     if (rc) return rc;
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -747,22 +766,29 @@ int mp_fe_build_j(mp_ctx *ctx, int method) {
 }
 
 int mp_fe_solve_linear(mp_ctx *ctx, int method, int form, const double *b, mp_newton_stats *st) {
-    if (!ctx || (method != MP_METHOD_GAUSS_SEIDEL && method != MP_METHOD_LAPACK)) return MP_ERR_ARG;
+    if (!ctx || (method != MP_METHOD_GAUSS_SEIDEL && method != MP_METHOD_LAPACK && method != MP_METHOD_SPARSE_CG))
+        return MP_ERR_ARG;
     if (!ctx->fe_ready) return fail(ctx, MP_ERR_STATE, "no FE setup");
+    if (!ctx->K && method != MP_METHOD_SPARSE_CG)
+        return fail(ctx, MP_ERR_STATE, "sparse storage: this method needs MP_FE_STORAGE_DENSE");
     if (b) MP_CUDA(ctx, cudaMemcpyAsync(ctx->G, b, sizeof(double) * ctx->neq, cudaMemcpyHostToDevice, ctx->stream));
     MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * ctx->neq, ctx->stream));
     if (st) std::memset(st, 0, sizeof(*st));
-    int rc = method == MP_METHOD_GAUSS_SEIDEL ? fe_solve_gs(ctx, st) : fe_solve_ldlt(ctx, form, st);
+    int rc = method == MP_METHOD_SPARSE_CG   ? fe_solve_cg(ctx, st)
+             : method == MP_METHOD_GAUSS_SEIDEL ? fe_solve_gs(ctx, st)
+                                                : fe_solve_ldlt(ctx, form, st);
     if (rc) return rc;
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return MP_OK;
 }
 
 int mp_compute_phi(mp_ctx *ctx, const double *ion_den, int method, int form, mp_newton_stats *st) {
-    if (!ctx || method < MP_METHOD_NONLINEAR || method > MP_METHOD_LAPACK ||
+    if (!ctx || method < MP_METHOD_NONLINEAR || method > MP_METHOD_SPARSE_NEWTON ||
         (form != MP_FORM_FP64 && form != MP_FORM_MIXED))
         return MP_ERR_ARG;
     if (!ctx->fe_ready) return fail(ctx, MP_ERR_STATE, "no FE setup");
+    const bool sparse = method == MP_METHOD_SPARSE_CG || method == MP_METHOD_SPARSE_NEWTON;
+    if (!ctx->K && !sparse) return fail(ctx, MP_ERR_STATE, "sparse storage: this method needs MP_FE_STORAGE_DENSE");
     mp_newton_stats local;
     if (!st) st = &local;
     std::memset(st, 0, sizeof(*st));
@@ -773,18 +799,21 @@ int mp_compute_phi(mp_ctx *ctx, const double *ion_den, int method, int form, mp_
     // solve(): y starts at zero and is reused across Newton iterations
     MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * ctx->neq, ctx->stream));
     double ms_factor = 0;
-    if (method == MP_METHOD_NONLINEAR) {
+    if (method == MP_METHOD_NONLINEAR || method == MP_METHOD_SPARSE_NEWTON) {
         // solveNonLinear, src/FESolver.cpp:324-364: up to 10 Newton iterations,
         // Gauss-Seidel inner solves in the FP64 form (the mixed form uses its
-        // refined LDL^T instead), stop when ||y||/neq < 1e-2.
+        // refined LDL^T instead, SPARSE_NEWTON conjugate gradients), stop when
+        // ||y||/neq < 1e-2.
         bool converged = false;
         double L2 = 0;
         int it;
         for (it = 0; it < 10; it++) {
             if ((rc = fe_build_f1(ctx, den))) return rc;
             if ((rc = fe_residual(ctx))) return rc;
-            if ((rc = fe_build_j(ctx, MP_METHOD_NONLINEAR, form))) return rc;
-            rc = form == MP_FORM_FP64 ? fe_solve_gs(ctx, st) : fe_solve_ldlt(ctx, form, st);
+            if ((rc = fe_build_j(ctx, method, form))) return rc;
+            rc = sparse                    ? fe_solve_cg(ctx, st)
+                 : form == MP_FORM_FP64 ? fe_solve_gs(ctx, st)
+                                        : fe_solve_ldlt(ctx, form, st);
             if (rc) return rc;
             ms_factor += st->ms_factor;
             if ((rc = fe_update_d(ctx, &L2))) return rc;
@@ -805,7 +834,9 @@ int mp_compute_phi(mp_ctx *ctx, const double *ion_den, int method, int form, mp_
         if ((rc = fe_build_f1(ctx, den))) return rc;
         if ((rc = fe_residual(ctx))) return rc;
         if ((rc = fe_build_j(ctx, method, method == MP_METHOD_GAUSS_SEIDEL ? MP_FORM_FP64 : form))) return rc;
-        rc = method == MP_METHOD_GAUSS_SEIDEL ? fe_solve_gs(ctx, st) : fe_solve_ldlt(ctx, form, st);
+        rc = method == MP_METHOD_SPARSE_CG      ? fe_solve_cg(ctx, st)
+             : method == MP_METHOD_GAUSS_SEIDEL ? fe_solve_gs(ctx, st)
+                                                : fe_solve_ldlt(ctx, form, st);
         if (rc) return rc;
         ms_factor = st->ms_factor;
         double L2 = 0;

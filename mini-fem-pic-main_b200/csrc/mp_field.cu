@@ -90,36 +90,9 @@ int fe_build_f1(mp_ctx *ctx, const double *den_dev) {
     return MP_OK;
 }
 
-// ---- residual G = K d - F0 - F1 (FESolver.cpp:333-335) ------------------------------
-// One warp per row; rows are 16-byte aligned (leading dimension padded).
-__global__ void k_residual(int neq, long long ld, const double *__restrict__ K, const double *__restrict__ d,
-                           const double *__restrict__ F0, const double *__restrict__ F1, double *G) {
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    if (warp >= neq) return;
-    const double *row = K + (long long)warp * ld;
-    double s = 0;
-    int n2 = neq & ~1;
-    for (int j = 2 * lane; j < n2; j += 64) {
-        double2 k = __ldg(reinterpret_cast<const double2 *>(row + j));
-        double2 x = __ldg(reinterpret_cast<const double2 *>(d + j));
-        s = fma(k.x, x.x, s);
-        s = fma(k.y, x.y, s);
-    }
-    if ((neq & 1) && lane == 0) s = fma(row[neq - 1], d[neq - 1], s);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) G[warp] = __dsub_rn(__dsub_rn(s, F0[warp]), F1[warp]);
-}
-
-int fe_residual(mp_ctx *ctx) {
-    long long ld = (ctx->neq + 31) & ~31ll;
-    int th = 256;
-    long long bl = ((long long)ctx->neq * 32 + th - 1) / th;
-    k_residual<<<(unsigned)bl, th, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->d, ctx->F0, ctx->F1, ctx->G), ++ctx->launches;
-    MP_CUDA(ctx, cudaGetLastError());
-    return MP_OK;
-}
+// ---- residual G = K d - F0 - F1 (FESolver.cpp:333-335): the sparse K's product,
+// summed in the reference's column order (mp_sparse.cu).
+int fe_residual(mp_ctx *ctx) { return fe_residual_sparse(ctx); }
 
 // ---- J = K, J[u][u] -= FP[u] (FESolver.cpp:367-431) ----------------------------------
 __global__ void k_copy_j(int neq, long long ld, const double *__restrict__ K, const double *__restrict__ FP,
@@ -154,7 +127,8 @@ __global__ void k_copy_j32(int neq, long long ld, const double *__restrict__ K, 
 }
 
 int fe_build_j(mp_ctx *ctx, int method, int form) {
-    (void)method;  // the full symmetric J serves both solvers (Lapack reads only one triangle)
+    // the full symmetric J serves both dense solvers (Lapack reads only one
+    // triangle); the sparse methods apply J = K - diag(FP) from K and FP
     int th = 256;
     k_node_terms<<<(ctx->n_nodes + th - 1) / th, th, 0, ctx->stream>>>(
         ctx->n_nodes, ctx->ID, nullptr, ctx->d, 0.0, -QE / EPS0, ctx->n0, ctx->phi0, ctx->kTe, 1 / ctx->kTe,
@@ -162,7 +136,9 @@ int fe_build_j(mp_ctx *ctx, int method, int form) {
     k_eq_gather<<<(ctx->neq + th - 1) / th, th, 0, ctx->stream>>>(ctx->neq, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a,
                                                                  ctx->detJ, ctx->work, ctx->FP, 0), ++ctx->launches;
     long long ld = (ctx->neq + 31) & ~31ll;
-    if (form == MP_FORM_MIXED) {
+    if (method == MP_METHOD_SPARSE_CG || method == MP_METHOD_SPARSE_NEWTON || !ctx->K) {
+        ctx->j32_current = false;
+    } else if (form == MP_FORM_MIXED) {
         if (!ctx->J32) MP_CUDA(ctx, cudaMalloc(&ctx->J32, sizeof(float) * (size_t)ld * ctx->neq));
         k_copy_j32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J32),
             ++ctx->launches;

@@ -160,6 +160,19 @@ struct mp_ctx {
     int *eq_ptr = nullptr, *eq_tet = nullptr;   // CSR equation -> (tet, a) sorted by tet
     unsigned char *eq_a = nullptr;
     double *gs_minv = nullptr;            // Gauss-Seidel: (D+L)^-1, [neq][neq]
+    // sparse K, sliced ELLPACK (slices of 32 rows): entry k of row P (columns
+    // ascending) at sp_ptr[P >> 5] + 32 * k + (P & 31); padding col = P, val = 0
+    int fe_storage = MP_FE_STORAGE_DENSE;
+    int *sp_len = nullptr;                // [neq] nonzeros of each row
+    long long *sp_ptr = nullptr;          // [slices + 1]
+    int *sp_col = nullptr;                // [sp_slots]
+    double *sp_val = nullptr;             // [sp_slots]
+    long long sp_nnz = 0, sp_slots = 0;
+    void *sparse_scratch = nullptr;       // conjugate-gradient work (mp_sparse.cu)
+    double cg_rtol = 1e-12;               // ||G - J y|| <= cg_rtol ||G||
+    int cg_max_it = 20000;
+    int cg_last_iterations = 0, cg_last_restarts = 0;
+    double cg_last_relres = 0;
 
     mp::Timer t0, t1, tp, ts;
     long long launches = 0;
@@ -199,6 +212,14 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st);
 int fe_update_d(mp_ctx *ctx, double *l2_out);
 int fe_uh(mp_ctx *ctx);
 int fe_assemble(mp_ctx *ctx);
+int sparse_setup(mp_ctx *ctx, const std::vector<int> &LM, const std::vector<int> &eq_ptr,
+                 const std::vector<int> &eq_tet);
+void sparse_free(mp_ctx *ctx);
+int fe_assemble_sparse(mp_ctx *ctx);
+int fe_sparse_from_dense(mp_ctx *ctx);
+int fe_sparse_from_host(mp_ctx *ctx, const double *const *rows, const double *dense);
+int fe_residual_sparse(mp_ctx *ctx);
+int fe_solve_cg(mp_ctx *ctx, mp_newton_stats *st);
 void adjoint_free(mp_ctx *ctx);
 void inject_free(mp_ctx *ctx);
 

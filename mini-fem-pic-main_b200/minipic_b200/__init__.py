@@ -34,7 +34,8 @@ MP_OK = 0
 STATUS = {0: "MP_OK", 1: "MP_ERR_ARG", 2: "MP_ERR_OOM", 3: "MP_ERR_CUDA", 4: "MP_ERR_WALK_LIMIT",
           5: "MP_ERR_NOT_CONVERGED", 6: "MP_ERR_SINGULAR", 7: "MP_ERR_STATE", 8: "MP_ERR_NO_DEVICE",
           9: "MP_ERR_TIMEOUT", 10: "MP_ERR_LIMIT"}
-NONLINEAR, GAUSS_SEIDEL, LAPACK = 0, 1, 2
+NONLINEAR, GAUSS_SEIDEL, LAPACK, SPARSE_CG, SPARSE_NEWTON = 0, 1, 2, 3, 4
+FE_DENSE, FE_SPARSE = 0, 1
 FP64, MIXED = 0, 1
 MIXED_TF32, MIXED_TF32X3 = 1, 3
 WALK_LIMIT_ERROR, WALK_LIMIT_ABSORB = 0, 1
@@ -62,6 +63,7 @@ EXPORTED = [
     "mp_device_buffer", "mp_push_particles_noalloc", "mp_set_mixed_factor",
     "mp_adjoint_setup", "mp_adjoint_add_particles", "mp_adjoint_forward", "mp_adjoint_flux",
     "mp_adjoint_backward", "mp_adjoint_tangent", "mp_set_walk_policy", "mp_inject_device",
+    "mp_set_fe_storage", "mp_set_sparse_solver", "mp_fe_sparse_matrix",
 ]
 
 
@@ -154,6 +156,9 @@ def lib():
         L.mp_set_sort_period.argtypes = [vp, i32]
         L.mp_set_mixed_factor.argtypes = [vp, C.c_int]
         L.mp_set_walk_policy.argtypes = [vp, C.c_int]
+        L.mp_set_fe_storage.argtypes = [vp, C.c_int]
+        L.mp_set_sparse_solver.argtypes = [vp, d, i32]
+        L.mp_fe_sparse_matrix.argtypes = [vp, C.POINTER(i64), vp, vp, vp]
         L.mp_inject_device.argtypes = [vp, vp, d, d, d, d, d, d, C.c_uint64, C.c_uint64, C.POINTER(i64)]
         L.mp_adjoint_setup.argtypes = [vp, i32, i32, d, d, d, d, vp, vp, vp, C.c_int]
         L.mp_adjoint_add_particles.argtypes = [vp, i32, C.c_int, i64, vp, vp, vp]
@@ -530,6 +535,25 @@ class Context:
         self._c(lib().mp_sort_by_tet(self.h))
 
     # field
+    def set_fe_storage(self, storage):
+        """FE_DENSE (default: dense K and J plus a sparse K) or FE_SPARSE (the
+        sparse K only; SPARSE_CG and SPARSE_NEWTON).  Before fe_setup."""
+        self._c(lib().mp_set_fe_storage(self.h, storage))
+
+    def set_sparse_solver(self, rtol=1e-12, max_iterations=20000):
+        """Conjugate-gradient stop: ||G - J y|| <= rtol ||G||."""
+        self._c(lib().mp_set_sparse_solver(self.h, float(rtol), int(max_iterations)))
+
+    def fe_sparse_matrix(self):
+        """The sparse K as CSR arrays (row_ptr, col, val), columns ascending."""
+        nnz = C.c_int64()
+        self._c(lib().mp_fe_sparse_matrix(self.h, C.byref(nnz), None, None, None))
+        row_ptr = np.zeros(self.neq + 1, dtype=np.int64)
+        col = np.zeros(nnz.value, dtype=np.int32)
+        val = np.zeros(nnz.value)
+        self._c(lib().mp_fe_sparse_matrix(self.h, C.byref(nnz), _p(row_ptr), _p(col), _p(val)))
+        return row_ptr, col, val
+
     def fe_setup(self, ID, nx, detJ, g, neq, n0, phi0, kTe, K=None, F0=None):
         d = FeDesc()
         self._fe_keep = [np.ascontiguousarray(ID, dtype=np.int32), np.ascontiguousarray(nx, dtype=np.float64),
