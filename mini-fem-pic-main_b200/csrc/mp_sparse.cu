@@ -590,6 +590,10 @@ int fe_solve_cg(mp_ctx *ctx, mp_newton_stats *st) {
     const int n = ctx->neq;
     if (n <= 0) return MP_OK;
     SparseScratch *s = scratch_of(ctx);
+    // one row a thread while the rows fit one block per SM: a thread's rows are
+    // worked one after the other, which costs more than the longer grid-wide
+    // rounds of more blocks (measured: 7.1 us an iteration at 8,379 unknowns
+    // on 17 blocks, 10.6 us on 5 blocks of 4 rows a thread)
     const int max_blocks = ctx->sm_count;
     int rpb = (n + max_blocks - 1) / max_blocks;
     rpb = std::max(CG_THREADS, (rpb + 31) & ~31);
