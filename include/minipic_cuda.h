@@ -34,6 +34,8 @@
  *                                 with respect to the node potential and the drift
  *   mp_set_fe_storage,            sparse K (preAssembly's K, src/FESolver.cpp:434-485,
  *   mp_fe_sparse_matrix           without its zeros) and the SPARSE_* methods
+ *   mp_*_geometry_device,         the three geometry helpers above, on the device
+ *   mp_inlet_faces_device
  */
 #ifndef MINIPIC_CUDA_H
 #define MINIPIC_CUDA_H
@@ -304,6 +306,22 @@ int mp_fe_geometry(int32_t n_nodes, const double *node_pos, const int32_t *node_
 int mp_inlet_faces(int32_t n_nodes, const double *node_pos, int32_t n_tets, const int32_t *con,
                    int32_t n_faces, const int32_t *face_con, int invert_normals,
                    int32_t *cell_con, double *u, double *v, double *normal, double *area);
+
+/* The three helpers above computed on device `device` (host arrays in and
+ * out; the same outputs bit for bit).  Face neighbours and inlet faces' tets
+ * come from the tets' faces sorted by node triple instead of the reference's
+ * scans over tets (src/meshes.cpp:180-227, 306-326).  MP_ERR_ARG for an index
+ * out of range, a face held by three tets, or an inlet face held by no tet or
+ * by two (where the reference exits); at most 2^29 tets. */
+int mp_mesh_geometry_device(int device, int32_t n_nodes, const double *node_pos, int32_t n_tets, int32_t *con,
+                            double *volume, double *alpha, double *beta, double *gamma, double *delta,
+                            int32_t *cell_con, double *node_volume, int32_t *node_open);
+int mp_inlet_faces_device(int device, int32_t n_nodes, const double *node_pos, int32_t n_tets,
+                          const int32_t *con, int32_t n_faces, const int32_t *face_con, int invert_normals,
+                          int32_t *cell_con, double *u, double *v, double *normal, double *area);
+int mp_fe_geometry_device(int device, int32_t n_nodes, const double *node_pos, const int32_t *node_type,
+                          int32_t n_tets, const int32_t *con, int32_t *ID, double *nx, double *detJ,
+                          int32_t *neq);
 
 /* InjectIons (src/mini-pic.cpp:208-265) with the reference's RNG stream
  * (std::mt19937 seeded 0, uniform_real_distribution<double>(0,1)). */

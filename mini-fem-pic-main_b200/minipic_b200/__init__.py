@@ -64,6 +64,7 @@ EXPORTED = [
     "mp_adjoint_setup", "mp_adjoint_add_particles", "mp_adjoint_forward", "mp_adjoint_flux",
     "mp_adjoint_backward", "mp_adjoint_tangent", "mp_set_walk_policy", "mp_inject_device",
     "mp_set_fe_storage", "mp_set_sparse_solver", "mp_fe_sparse_matrix",
+    "mp_mesh_geometry_device", "mp_inlet_faces_device", "mp_fe_geometry_device",
 ]
 
 
@@ -140,6 +141,9 @@ def lib():
         L.mp_fe_solve_linear.argtypes = [vp, C.c_int, C.c_int, vp, C.POINTER(NewtonStats)]
         L.mp_fe_setup.argtypes = [vp, C.POINTER(FeDesc)]
         L.mp_mesh_geometry.argtypes = [i32, vp, i32, vp] + [vp] * 8
+        L.mp_mesh_geometry_device.argtypes = [C.c_int, i32, vp, i32, vp] + [vp] * 8
+        L.mp_inlet_faces_device.argtypes = [C.c_int, i32, vp, i32, vp, i32, vp, C.c_int, vp, vp, vp, vp, vp]
+        L.mp_fe_geometry_device.argtypes = [C.c_int, i32, vp, vp, i32, vp, vp, vp, vp, vp]
         L.mp_fe_geometry.argtypes = [i32, vp, vp, i32, vp, vp, vp, vp, vp]
         L.mp_inlet_faces.argtypes = [i32, vp, i32, vp, i32, vp, C.c_int, vp, vp, vp, vp, vp]
         L.mp_injector_create.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, C.c_uint32, C.POINTER(vp)]
@@ -320,7 +324,9 @@ class Mesh:
 
     @classmethod
     def build(cls, node_pos: np.ndarray, tets: np.ndarray, inlet_nodes, inlet_tris, fixed_nodes,
-              invert_normals: bool = False) -> "Mesh":
+              invert_normals: bool = False, device: int | None = None) -> "Mesh":
+        """LoadVolumeMesh + LoadSurfaceMesh's geometry, on the host helpers or,
+        with `device`, on that GPU (the same arrays bit for bit)."""
         L = lib()
         node_pos = np.ascontiguousarray(node_pos, dtype=np.float64)
         con = np.ascontiguousarray(tets, dtype=np.int32).copy()
@@ -330,8 +336,12 @@ class Mesh:
         cc = np.zeros((nt, 4), dtype=np.int32)
         nvol = np.zeros(nn)
         nopen = np.zeros(nn, dtype=np.int32)
-        _check(L.mp_mesh_geometry(nn, _p(node_pos), nt, _p(con), _p(vol), _p(al), _p(be), _p(ga), _p(de),
-                                  _p(cc), _p(nvol), _p(nopen)))
+        if device is None:
+            _check(L.mp_mesh_geometry(nn, _p(node_pos), nt, _p(con), _p(vol), _p(al), _p(be), _p(ga), _p(de),
+                                      _p(cc), _p(nvol), _p(nopen)))
+        else:
+            _check(L.mp_mesh_geometry_device(device, nn, _p(node_pos), nt, _p(con), _p(vol), _p(al), _p(be),
+                                             _p(ga), _p(de), _p(cc), _p(nvol), _p(nopen)))
         ntype = np.where(nopen == 1, NODE_OPEN, NODE_NORMAL).astype(np.int32)
         ntype[np.asarray(inlet_nodes, dtype=np.int64)] = NODE_INLET
         ntype[np.asarray(fixed_nodes, dtype=np.int64)] = NODE_FIXED
@@ -340,8 +350,12 @@ class Mesh:
         fcell = np.zeros(nf, dtype=np.int32)
         u, v, nrm = np.zeros((nf, 3)), np.zeros((nf, 3)), np.zeros((nf, 3))
         area = np.zeros(nf)
-        _check(L.mp_inlet_faces(nn, _p(node_pos), nt, _p(con), nf, _p(tris), int(invert_normals), _p(fcell), _p(u),
-                                _p(v), _p(nrm), _p(area)))
+        if device is None:
+            _check(L.mp_inlet_faces(nn, _p(node_pos), nt, _p(con), nf, _p(tris), int(invert_normals), _p(fcell),
+                                    _p(u), _p(v), _p(nrm), _p(area)))
+        else:
+            _check(L.mp_inlet_faces_device(device, nn, _p(node_pos), nt, _p(con), nf, _p(tris), int(invert_normals),
+                                           _p(fcell), _p(u), _p(v), _p(nrm), _p(area)))
         return cls(node_pos, ntype, nvol, con, vol, al, be, ga, de, cc, tris, fcell, u, v, nrm, area)
 
     def desc(self) -> MeshDesc:
@@ -358,15 +372,17 @@ class Mesh:
         d.node_volume, d.node_volume_stride = _p(self.node_volume).value, 8
         return d
 
-    def fe_geometry(self):
-        """ID, NX, detJ, neq as FESolver's constructor computes them."""
+    def fe_geometry(self, device: int | None = None):
+        """ID, NX, detJ, neq as FESolver's constructor computes them (on the
+        host, or on GPU `device`)."""
         L = lib()
         ID = np.zeros(self.n_nodes, dtype=np.int32)
         nx = np.zeros((self.n_tets, 4, 3))
         detJ = np.zeros(self.n_tets)
         neq = C.c_int32(0)
-        _check(L.mp_fe_geometry(self.n_nodes, _p(self.node_pos), _p(self.node_type), self.n_tets, _p(self.con),
-                                _p(ID), _p(nx), _p(detJ), C.byref(neq)))
+        args = (self.n_nodes, _p(self.node_pos), _p(self.node_type), self.n_tets, _p(self.con), _p(ID), _p(nx),
+                _p(detJ), C.byref(neq))
+        _check(L.mp_fe_geometry(*args) if device is None else L.mp_fe_geometry_device(device, *args))
         return ID, nx, detJ, int(neq.value)
 
 
@@ -377,7 +393,7 @@ class Deck:
     sphere_nodes: np.ndarray
 
     @classmethod
-    def load(cls, directory: str) -> "Deck":
+    def load(cls, directory: str, device: int | None = None) -> "Deck":
         params = Parameters.read(os.path.join(directory, "system.param"))
         mf = {k: os.path.join(directory, v) for k, v in params.mesh_files.items()}
         pos, tets = read_volume_dat(mf["global_mesh"])
@@ -388,7 +404,7 @@ class Deck:
         if os.path.exists(sp):
             sphere_nodes, _ = read_surface_dat(sp)
         fixed = np.concatenate([wall_nodes, sphere_nodes])
-        mesh = Mesh.build(pos, tets, inlet_nodes, inlet_tris, fixed, params.invert_normals)
+        mesh = Mesh.build(pos, tets, inlet_nodes, inlet_tris, fixed, params.invert_normals, device=device)
         return cls(params, mesh, sphere_nodes)
 
     def dirichlet(self, sphere_potential: float | None = None) -> np.ndarray:
