@@ -36,6 +36,8 @@
  *   mp_fe_sparse_matrix           without its zeros) and the SPARSE_* methods
  *   mp_*_geometry_device,         the three geometry helpers above, on the device
  *   mp_inlet_faces_device
+ *   mp_output_mesh                OutputMesh, src/meshes.cpp:358-447 (asynchronous)
+ *   mp_output_particles           OutputParticles, src/particles.cpp:21-45
  */
 #ifndef MINIPIC_CUDA_H
 #define MINIPIC_CUDA_H
@@ -288,6 +290,23 @@ int mp_fe_solve_linear(mp_ctx *ctx, int method, int form, const double *b, mp_ne
 /* FESolver::updateEf from the device uh (or uh_host if non-NULL). */
 int mp_update_ef(mp_ctx *ctx, const double *uh_host);
 int mp_field_download(mp_ctx *ctx, double *d, double *uh, double *ef);
+
+/* ---- VTK output ---------------------------------------------------------------------- */
+/* OutputMesh (src/meshes.cpp:358-447): writes mesh_<ts+1, 4 digits>.vtu into
+ * `dir` (NULL or "" = the current directory) with the reference's ASCII text
+ * byte for byte, from the context's uh, ef and node density (the last push's)
+ * and the caller's node types (node_type_stride bytes apart; 40 for an array
+ * of the reference's Node).  Asynchronous: the call copies the arrays to
+ * pinned host memory on the context's stream, opens the file (MP_ERR_ARG if it
+ * cannot, where the reference exits) and returns; a writer thread formats and
+ * writes.  A later output call, mp_output_wait or mp_destroy joins it. */
+int mp_output_mesh(mp_ctx *ctx, int32_t ts, const char *dir, const int32_t *node_type, int64_t node_type_stride);
+/* OutputParticles (src/particles.cpp:21-45): the live particles' positions in
+ * the reference's order, written to `path` (the reference's is
+ * "particles.vtp") by the writer thread. */
+int mp_output_particles(mp_ctx *ctx, const char *path);
+/* Joins the writer; returns its status (MP_ERR_ARG if the write failed). */
+int mp_output_wait(mp_ctx *ctx);
 
 /* ---- host-side setup helpers (no device needed) ----------------------------------- */
 /* LoadVolumeMesh's geometry (src/meshes.cpp:80-262) from node positions in metres

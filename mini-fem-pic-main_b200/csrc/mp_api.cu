@@ -284,6 +284,7 @@ int mp_destroy(mp_ctx *ctx) {
     if (!ctx) return MP_OK;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     adjoint_free(ctx);
+    output_free(ctx);  // joins a writer still running
     inject_free(ctx);
     sparse_free(ctx);
     void *dev[] = {ctx->tets, ctx->tets32, ctx->tet_x0, ctx->con, ctx->ef, ctx->node_volume, ctx->node_pos,

@@ -179,6 +179,7 @@ struct mp_ctx {
 
     void *adjoint = nullptr;              // adjoint state (mp_adjoint.cu), created by mp_adjoint_setup
     void *inject = nullptr;               // device injection state (mp_inject.cu)
+    void *output = nullptr;               // VTK output state and writer thread (mp_output.cpp)
 };
 
 namespace mp {
@@ -222,5 +223,6 @@ int fe_residual_sparse(mp_ctx *ctx);
 int fe_solve_cg(mp_ctx *ctx, mp_newton_stats *st);
 void adjoint_free(mp_ctx *ctx);
 void inject_free(mp_ctx *ctx);
+void output_free(mp_ctx *ctx);
 
 }  // namespace mp

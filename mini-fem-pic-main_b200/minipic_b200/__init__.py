@@ -65,6 +65,7 @@ EXPORTED = [
     "mp_adjoint_backward", "mp_adjoint_tangent", "mp_set_walk_policy", "mp_inject_device",
     "mp_set_fe_storage", "mp_set_sparse_solver", "mp_fe_sparse_matrix",
     "mp_mesh_geometry_device", "mp_inlet_faces_device", "mp_fe_geometry_device",
+    "mp_output_mesh", "mp_output_particles", "mp_output_wait",
 ]
 
 
@@ -161,6 +162,9 @@ def lib():
         L.mp_set_mixed_factor.argtypes = [vp, C.c_int]
         L.mp_set_walk_policy.argtypes = [vp, C.c_int]
         L.mp_set_fe_storage.argtypes = [vp, C.c_int]
+        L.mp_output_mesh.argtypes = [vp, i32, C.c_char_p, vp, i64]
+        L.mp_output_particles.argtypes = [vp, C.c_char_p]
+        L.mp_output_wait.argtypes = [vp]
         L.mp_set_sparse_solver.argtypes = [vp, d, i32]
         L.mp_fe_sparse_matrix.argtypes = [vp, C.POINTER(i64), vp, vp, vp]
         L.mp_inject_device.argtypes = [vp, vp, d, d, d, d, d, d, C.c_uint64, C.c_uint64, C.POINTER(i64)]
@@ -628,6 +632,19 @@ class Context:
     def update_ef(self, uh=None):
         u = None if uh is None else np.ascontiguousarray(uh, dtype=np.float64)
         self._c(lib().mp_update_ef(self.h, _p(u)))
+
+    def output_mesh(self, ts: int, directory: str, node_type: np.ndarray) -> None:
+        """OutputMesh: mesh_<ts+1>.vtu in `directory`, written by a background
+        thread (output_wait joins it)."""
+        self._out_types = np.ascontiguousarray(node_type, dtype=np.int32)
+        self._c(lib().mp_output_mesh(self.h, int(ts), directory.encode(), _p(self._out_types), 4))
+
+    def output_particles(self, path: str) -> None:
+        """OutputParticles into `path`, written by a background thread."""
+        self._c(lib().mp_output_particles(self.h, path.encode()))
+
+    def output_wait(self) -> None:
+        self._c(lib().mp_output_wait(self.h))
 
     def field(self):
         d = np.zeros(self.neq) if self.neq else None

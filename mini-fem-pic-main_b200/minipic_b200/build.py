@@ -15,7 +15,7 @@ LIB = os.path.join(LIBDIR, "libminipic_cuda.so")
 INCLUDE = os.path.join(REPO, "include")
 
 CU_SOURCES = ["mp_api.cu", "mp_push.cu", "mp_field.cu", "mp_solve.cu", "mp_noalloc.cu", "mp_adjoint.cu", "mp_inject.cu", "mp_sparse.cu", "mp_mesh.cu"]
-CPP_SOURCES = ["mp_host.cpp"]
+CPP_SOURCES = ["mp_host.cpp", "mp_output.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -71,6 +71,7 @@ def lib(shim: bool = False):
             "ref_solve_lapack": (None, [vp, vp, vp]),
             "ref_time_move": (d, [vp, i, i, vp]), "ref_max_threads": (i, []),
             "ref_reseed": (None, [C.c_uint]),
+            "ref_output_mesh": (d, [vp, i, C.c_char_p]), "ref_output_particles": (d, [vp, C.c_char_p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

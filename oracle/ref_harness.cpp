@@ -23,6 +23,7 @@
 #include <vector>
 #include <omp.h>
 #include <random>
+#include <unistd.h>
 
 #include "FESolver.h"
 #include "maths.h"
@@ -388,6 +389,30 @@ int ref_max_threads() { return omp_get_max_threads(); }
 /* Restarts the reference's RNG stream (the process-wide mt19937 of maths.cpp),
  * so every simulation opened in one process injects like a fresh `mini-pic`. */
 void ref_reseed(unsigned seed) { mt_gen.seed(seed); }
+
+/* The reference's OutputMesh (src/meshes.cpp:358-447) and OutputParticles
+ * (src/particles.cpp:21-45) write into the current directory; these run them
+ * with `dir` as the current directory and return the seconds they took. */
+double ref_output_mesh(void *h, int ts, const char *dir) {
+    RefSim &S = *(RefSim *)h;
+    char here[4096];
+    if (!getcwd(here, sizeof here) || chdir(dir) != 0) return -1;
+    auto t0 = std::chrono::steady_clock::now();
+    OutputMesh(ts, S.volume, S.solver->uh, S.solver->ef, S.ions->den);
+    auto t1 = std::chrono::steady_clock::now();
+    if (chdir(here) != 0) return -1;
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+double ref_output_particles(void *h, const char *dir) {
+    RefSim &S = *(RefSim *)h;
+    char here[4096];
+    if (!getcwd(here, sizeof here) || chdir(dir) != 0) return -1;
+    auto t0 = std::chrono::steady_clock::now();
+    OutputParticles(S.ions->particles);
+    auto t1 = std::chrono::steady_clock::now();
+    if (chdir(here) != 0) return -1;
+    return std::chrono::duration<double>(t1 - t0).count();
+}
 
 
 #ifdef REF_WITH_SHIM
