@@ -393,7 +393,64 @@ def sparse_field_at_scale(device, n=64, reps=3):
         out[key] = {"ms": float(np.mean(ms)), "newton_iterations": int(max(nits)),
                     "cg_iterations_last_solve": int(max(its))}
     c.close()
+    # the mesh setup of the same mesh: the host helpers against the device ones
+    pos, fixed = kd.nodes_mm / 1000.0, np.concatenate([kd.wall_nodes, kd.sphere_nodes])
+    setup = {}
+    for key, dev in (("host_s", None), ("device_s", device), ("device_s", device)):
+        t0 = time.perf_counter()
+        m = mp.Mesh.build(pos, kd.tets, kd.inlet_nodes, kd.inlet_tris, fixed, device=dev)
+        m.fe_geometry(device=dev)
+        setup[key] = time.perf_counter() - t0  # the device entry is timed a second time, warm
+    out["mesh_setup"] = dict(setup, tets=int(m.n_tets),
+                             what="LoadVolumeMesh + LoadSurfaceMesh geometry + FESolver ID/NX/detJ, wall clock "
+                                  "including the host-device copies")
     return out
+
+
+def vtk_output_leg(device, cfg=CONFIGS[2]):
+    """OutputMesh of the 32^3 box minus sphere from the device buffers: the time
+    until the call returns (snapshot + writer start) and until the file is
+    complete; the reference's own OutputMesh on the same arrays when the
+    oracle library is present (reported beside, as its CPU baseline)."""
+    with tempfile.TemporaryDirectory() as wd:
+        kd = kuhn.build(cfg["n"], sphere=cfg["sphere"])
+        kuhn.write(kd, wd)
+        deck = mp.Deck.load(wd)
+        c = mp.Context(deck.mesh, device=device)
+        c.fe_setup(**deck.fe_desc_arrays(workloads.SPHERE_POTENTIAL))
+        rng = np.random.default_rng(3)
+        uh, den = rng.normal(size=deck.mesh.n_nodes), rng.normal(size=deck.mesh.n_nodes)
+        ef = rng.normal(size=(deck.mesh.n_tets, 3))
+        for name, v in (("uh", uh), ("den", den), ("ef", ef)):
+            c.fe_set(name, v)
+        c.output_mesh(0, wd, deck.mesh.node_type)
+        c.output_wait()
+        t0 = time.perf_counter()
+        c.output_mesh(1, wd, deck.mesh.node_type)
+        t1 = time.perf_counter()
+        c.output_wait()
+        t2 = time.perf_counter()
+        out = {"workload": cfg["label"] + " OutputMesh", "nodes": deck.mesh.n_nodes, "tets": deck.mesh.n_tets,
+               "bytes": os.path.getsize(os.path.join(wd, "mesh_0002.vtu")), "call_ms": (t1 - t0) * 1e3,
+               "file_complete_ms": (t2 - t0) * 1e3}
+        c.close()
+        out["reference_ms"] = reference_output_mesh_ms(wd, kd, uh, den, ef)
+    return out
+
+
+def reference_output_mesh_ms(wd, kd, uh, den, ef):
+    """CPU baseline of the VTK leg: the reference's OutputMesh (oracle/_ref)."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    s = ref.RefSim(wd, spwt=1.0, extra_fixed={os.path.join(wd, "sphere.dat"): (kd.sphere_nodes, -10.0)})
+    for name, v in (("uh", uh), ("den", den), ("ef", ef)):
+        s.set(name, v)
+    out_dir = os.path.join(wd, "reference")
+    os.makedirs(out_dir)
+    sec = s.L.ref_output_mesh(s.h, 1, out_dir.encode())
+    s.close()
+    return sec * 1e3 if sec >= 0 else None
 
 
 def cpu_baseline(cfg, workdir, pop, budget_s=20.0):
@@ -519,10 +576,11 @@ def main():
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu:
             cpu = cpu_baseline(cfg, wd, pop)
-    scale = sparse_big = None
+    scale = sparse_big = vtk = None
     if rank == 0 and world == 1 and not args.no_scale and args.config == 1:
         scale = mixed_vs_fp64_at_scale(args, local, torch, flush)
         sparse_big = sparse_field_at_scale(local)
+        vtk = vtk_output_leg(local)
 
     def agg(r):
         push_ms = np.array(r["push_ms"])
@@ -608,6 +666,8 @@ def main():
             line["mixed_vs_fp64_kuhn32s_50M"] = scale
         if sparse_big is not None:
             line["sparse_field_kuhn64s"] = sparse_big
+        if vtk is not None:
+            line["vtk_output"] = vtk
         print(json.dumps(line))
     if world > 1:
         torch.distributed.barrier()

@@ -147,6 +147,9 @@ def push_driver(args):
         ctx.close()
 
 
+METHODS = {"lapack": mp.LAPACK, "sparse_cg": mp.SPARSE_CG, "sparse_newton": mp.SPARSE_NEWTON}
+
+
 def newton_driver(args):
     cfg = dict(CONFIGS[args.config])
     if args.n:
@@ -158,15 +161,18 @@ def newton_driver(args):
         if cfg["sphere"]:
             absorb_cavity_walks(ctx)
         ctx.set_mixed_factor(mp.MIXED_TF32 if getattr(args, "mixed_factor", "tf32x3") == "tf32" else mp.MIXED_TF32X3)
+        if getattr(args, "storage", "dense") == "sparse":
+            ctx.set_fe_storage(mp.FE_SPARSE)
         ctx.fe_setup(**fe_arrays(cfg, deck))
         ctx.append(pos, vel, cell)
         ctx.push(mp.QE / (16 * mp.AMU), cfg["dt"], cfg["spwt"] * cfg["n_ions"] / len(cell))
         out = []
         for k in range(args.steps):
-            st = ctx.compute_phi(mp.LAPACK, form)
+            st = ctx.compute_phi(METHODS[getattr(args, "method", "lapack")], form)
             out.append({"step": k, "newton_ms": st.ms_total, "factor_ms": st.ms_factor,
                         "refinements": st.linear_iterations, "residual": st.linear_residual})
         print(json.dumps({"driver": "newton", "config": cfg["label"], "form": args.form,
+                          "method": getattr(args, "method", "lapack"), "storage": getattr(args, "storage", "dense"),
                           "mixed_factor": getattr(args, "mixed_factor", "tf32x3"),
                           "unknowns": int(fe_arrays(cfg, deck)["neq"]), "steps": out}))
         ctx.close()
@@ -182,6 +188,8 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="override the mesh's hexes per side (newton driver)")
     ap.add_argument("--mixed-factor", default="tf32x3", choices=["tf32", "tf32x3"],
                     help="tensor-core arithmetic of the mixed-form factorization (newton driver)")
+    ap.add_argument("--method", default="lapack", choices=sorted(METHODS), help="newton driver")
+    ap.add_argument("--storage", default="dense", choices=["dense", "sparse"], help="newton driver: storage of K")
     args = ap.parse_args()
     (push_driver if args.driver == "push" else newton_driver)(args)
 
