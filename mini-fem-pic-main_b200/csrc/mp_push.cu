@@ -255,7 +255,7 @@ __device__ __forceinline__ void issue_tile_f32(StageF32 *st, const PartsF32 &p, 
 }
 
 template <bool EXACT_CMP>
-__global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_fp64(PushF64Args a) {
+__global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_fp64(PushF64Args a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     StageF64 *stage = reinterpret_cast<StageF64 *>(smem_raw);
     __shared__ unsigned long long bars[STAGES];
@@ -348,7 +348,7 @@ __device__ __forceinline__ void load_x0(const double *__restrict__ x0, int cell,
     z = __ldg(x0 + 4ll * cell + 2);
 }
 
-__global__ void __launch_bounds__(PUSH_THREADS, 2) k_push_mixed(PushF32Args a) {
+__global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_mixed(PushF32Args a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     StageF32 *stage = reinterpret_cast<StageF32 *>(smem_raw);
     __shared__ unsigned long long bars[STAGES];
