@@ -4,6 +4,7 @@
 
 #include <cstdlib>
 #include <iostream>
+#include <vector>
 
 namespace {
 
@@ -36,6 +37,7 @@ void setup_fe(FESolver &solver, DeviceData &device) {
     fe.n0 = solver.n0;
     fe.phi0 = solver.phi0;
     fe.kTe = solver.kTe;
+    check(mp_set_fe_storage(device.ctx, device.fe_storage), device.ctx, "FE storage");
     check(mp_fe_setup(device.ctx, &fe), device.ctx, "FE setup");
     device.fe_ready = true;
 }
@@ -101,7 +103,12 @@ void MoveParticles(Species &ions, Volume &volume, FESolver &solver, const Parame
 void computePhiDevice(FESolver &solver, double *ion_den, FESolver::Method method, DeviceData &device) {
     setup_fe(solver, device);
     mp_newton_stats st{};
-    const int rc = mp_compute_phi(device.ctx, ion_den, (int)method, device.form, &st);
+    int m = (int)method;
+    if (device.fe_storage == MP_FE_STORAGE_SPARSE)
+        m = method == FESolver::NonLinear ? MP_METHOD_SPARSE_NEWTON
+            : method == FESolver::Lapack  ? MP_METHOD_SPARSE_CG
+                                          : m;  // Gauss-Seidel needs the dense J: reported as an error
+    const int rc = mp_compute_phi(device.ctx, ion_den, m, device.form, &st);
     if (rc == MP_ERR_NOT_CONVERGED) {
         // src/FESolver.cpp:360-361
         std::cerr << "NR failed to converge, L2 = " << st.l2 << std::endl;
@@ -116,3 +123,78 @@ void updateEfDevice(FESolver &solver, DeviceData &device) {
     check(mp_update_ef(device.ctx, solver.uh), device.ctx, "updateEf");
     check(mp_field_download(device.ctx, nullptr, nullptr, &solver.ef[0][0]), device.ctx, "field download");
 }
+
+void MeshGeometryDevice(Volume &volume) {
+    const int nn = (int)volume.nodes.size(), nt = (int)volume.elements.size();
+    std::vector<double> pos(3 * (size_t)nn), vol(nt), al(4 * (size_t)nt), be(4 * (size_t)nt), ga(4 * (size_t)nt),
+        de(4 * (size_t)nt), nvol(nn);
+    std::vector<int32_t> con(4 * (size_t)nt), cc(4 * (size_t)nt), open(nn);
+    for (int n = 0; n < nn; n++)
+        for (int d = 0; d < 3; d++) pos[3 * (size_t)n + d] = volume.nodes[n].pos[d];
+    for (int e = 0; e < nt; e++)
+        for (int v = 0; v < 4; v++) con[4 * (size_t)e + v] = volume.elements[e].con[v];
+    check(mp_mesh_geometry_device(0, nn, pos.data(), nt, con.data(), vol.data(), al.data(), be.data(), ga.data(),
+                                  de.data(), cc.data(), nvol.data(), open.data()),
+          nullptr, "mesh geometry");
+    for (int e = 0; e < nt; e++) {
+        Tetra &t = volume.elements[e];
+        t.volume = vol[e];
+        for (int v = 0; v < 4; v++) {
+            const size_t k = 4 * (size_t)e + v;
+            t.con[v] = con[k];
+            t.alpha[v] = al[k];
+            t.beta[v] = be[k];
+            t.gamma[v] = ga[k];
+            t.delta[v] = de[k];
+            t.cell_con[v] = cc[k];
+        }
+    }
+    for (int n = 0; n < nn; n++) {
+        volume.nodes[n].volume = nvol[n];
+        if (open[n]) volume.nodes[n].type = OPEN;
+    }
+}
+
+void InletFacesDevice(Volume &volume, bool invert_normals) {
+    const int nn = (int)volume.nodes.size(), nt = (int)volume.elements.size();
+    const int nf = (int)volume.inlet_faces.size();
+    std::vector<double> pos(3 * (size_t)nn), u(3 * (size_t)nf), v(3 * (size_t)nf), nrm(3 * (size_t)nf), area(nf);
+    std::vector<int32_t> con(4 * (size_t)nt), fc(3 * (size_t)nf), cell(nf);
+    for (int n = 0; n < nn; n++)
+        for (int d = 0; d < 3; d++) pos[3 * (size_t)n + d] = volume.nodes[n].pos[d];
+    for (int e = 0; e < nt; e++)
+        for (int k = 0; k < 4; k++) con[4 * (size_t)e + k] = volume.elements[e].con[k];
+    for (int f = 0; f < nf; f++)
+        for (int k = 0; k < 3; k++) fc[3 * (size_t)f + k] = volume.inlet_faces[f].con[k];
+    const int rc = mp_inlet_faces_device(0, nn, pos.data(), nt, con.data(), nf, fc.data(), invert_normals ? 1 : 0,
+                                         cell.data(), u.data(), v.data(), nrm.data(), area.data());
+    if (rc == MP_ERR_ARG) {
+        // src/meshes.cpp:318-326
+        std::cerr << "Inlet surface attached to no volume element or to more than one" << std::endl;
+        exit(-1);
+    }
+    check(rc, nullptr, "inlet faces");
+    for (int f = 0; f < nf; f++) {
+        Face &F = volume.inlet_faces[f];
+        F.cell_con = cell[f];
+        F.area = area[f];
+        for (int k = 0; k < 3; k++) {
+            F.u[k] = u[3 * (size_t)f + k];
+            F.v[k] = v[3 * (size_t)f + k];
+            F.normal[k] = nrm[3 * (size_t)f + k];
+        }
+    }
+}
+
+void OutputMeshDevice(int ts, Volume &volume, DeviceData &device) {
+    static_assert(sizeof(NodeType) == sizeof(int32_t), "NodeType is read as int32");
+    check(mp_output_mesh(device.ctx, ts, nullptr, reinterpret_cast<const int32_t *>(&volume.nodes[0].type),
+                         (int64_t)sizeof(Node)),
+          device.ctx, "OutputMesh");
+}
+
+void OutputParticlesDevice(DeviceData &device) {
+    check(mp_output_particles(device.ctx, "particles.vtp"), device.ctx, "OutputParticles");
+}
+
+void OutputWaitDevice(DeviceData &device) { check(mp_output_wait(device.ctx), device.ctx, "output"); }

@@ -31,6 +31,10 @@ struct DeviceData {
     int n_elements = 0;
     bool fe_ready = false;
     int form = MP_FORM_FP64;  /* MP_FORM_MIXED: FP32 particles and TF32 factorization */
+    /* MP_FE_STORAGE_SPARSE (set before the first computePhiDevice): K is kept
+     * sparse only, and computePhiDevice maps Lapack to MP_METHOD_SPARSE_CG and
+     * NonLinear to MP_METHOD_SPARSE_NEWTON (Gauss-Seidel is not available). */
+    int fe_storage = MP_FE_STORAGE_DENSE;
     DeviceData(Volume &volume);
     ~DeviceData();
     DeviceData(const DeviceData &) = delete;
@@ -52,5 +56,29 @@ void computePhiDevice(FESolver &solver, double *ion_den, FESolver::Method method
 /* FESolver::updateEf (src/FESolver.cpp:622-636) on the device from solver.uh;
  * the field is written back into solver.ef. */
 void updateEfDevice(FESolver &solver, DeviceData &device);
+
+/* LoadVolumeMesh's geometry (src/meshes.cpp:87-262) computed on the device for
+ * a Volume whose nodes (positions) and elements (con) are filled: the
+ * orientation fix, volumes, alpha..delta, cell_con, node volumes and the OPEN
+ * node types, written into the reference's records bit for bit as its own
+ * loader computes them.  A maintainer calls it where LoadVolumeMesh's
+ * geometry loops are. */
+void MeshGeometryDevice(Volume &volume);
+
+/* LoadSurfaceMesh's inlet part (src/meshes.cpp:300-353) on the device for the
+ * volume.inlet_faces whose con are filled: the owning tet, u, v, the unit
+ * normal and the area.  Exits like the reference when a face is held by no tet
+ * or by two. */
+void InletFacesDevice(Volume &volume, bool invert_normals);
+
+/* OutputMesh (src/meshes.cpp:358-447) from the device's potential, field and
+ * density (those of the last computePhiDevice, updateEfDevice and
+ * MoveParticles), byte for byte the reference's file; asynchronous (the file
+ * is complete after the next output call, OutputWaitDevice or ~DeviceData). */
+void OutputMeshDevice(int ts, Volume &volume, DeviceData &device);
+/* OutputParticles (src/particles.cpp:21-45): particles.vtp from the device's
+ * particles (those MoveParticles left), asynchronous like OutputMeshDevice. */
+void OutputParticlesDevice(DeviceData &device);
+void OutputWaitDevice(DeviceData &device);
 
 #endif

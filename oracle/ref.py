@@ -80,7 +80,10 @@ def lib(shim: bool = False):
         if shim:
             for name, (res, args) in {"ref_shim_device": (vp, [vp]), "ref_shim_free": (None, [vp]),
                                       "ref_shim_move": (None, [vp, vp]), "ref_shim_compute_phi": (None, [vp, vp, i]),
-                                      "ref_shim_update_ef": (None, [vp, vp])}.items():
+                                      "ref_shim_update_ef": (None, [vp, vp]),
+                                      "ref_shim_mesh_check": (l, [vp, vp]),
+                                      "ref_shim_output": (i, [vp, vp, i, C.c_char_p]),
+                                      "ref_shim_set_storage": (None, [vp, i])}.items():
                 f = getattr(L, name)
                 f.restype = res
                 f.argtypes = args

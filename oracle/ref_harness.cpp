@@ -17,6 +17,7 @@
  * non-convergence exactly like the reference; tests run those in a subprocess.
  */
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <cstring>
 #include <string>
@@ -430,6 +431,82 @@ void ref_shim_compute_phi(void *h, void *d, int method) {
     computePhiDevice(*s->solver, s->ions->den, (FESolver::Method)method, *(DeviceData *)d);
 }
 void ref_shim_update_ef(void *h, void *d) { updateEfDevice(*((RefSim *)h)->solver, *(DeviceData *)d); }
+
+/* The drop-in's MeshGeometryDevice + InletFacesDevice on a copy of the loaded
+ * Volume whose geometry is cleared and whose tets carry the mesh file's vertex
+ * order (con_file, 0-based: the reference's loader computes each volume in that
+ * order before it flips the orientation); returns how many values differ from
+ * what the reference's own loaders computed (0 = bit for bit).  Node types are
+ * compared as OPEN or not, for the nodes the surface loads did not retype. */
+long ref_shim_mesh_check(void *h, const int *con_file) {
+    RefSim &S = *(RefSim *)h;
+    Volume v;
+    v.nodes = S.volume.nodes;
+    v.elements = S.volume.elements;
+    v.inlet_faces = S.volume.inlet_faces;
+    for (size_t e = 0; e < v.elements.size(); e++)
+        for (int k = 0; k < 4; k++) v.elements[e].con[k] = con_file[4 * e + k];
+    for (Tetra &t : v.elements) {
+        t.volume = 0;
+        for (int k = 0; k < 4; k++) t.alpha[k] = t.beta[k] = t.gamma[k] = t.delta[k] = 0, t.cell_con[k] = -7;
+    }
+    for (Node &n : v.nodes) {
+        n.volume = 0;
+        if (n.type == OPEN) n.type = NORMAL;
+    }
+    for (Face &f : v.inlet_faces) {
+        f.area = 0;
+        f.cell_con = -7;
+        for (int k = 0; k < 3; k++) f.u[k] = f.v[k] = f.normal[k] = 0;
+    }
+    MeshGeometryDevice(v);
+    InletFacesDevice(v, S.params.invert_normals);
+    long cnt[12] = {};
+    for (size_t e = 0; e < v.elements.size(); e++) {
+        const Tetra &a = v.elements[e], &b = S.volume.elements[e];
+        cnt[0] += std::memcmp(&a.volume, &b.volume, sizeof(double)) != 0;
+        cnt[1] += std::memcmp(a.con, b.con, sizeof a.con) != 0;
+        cnt[2] += std::memcmp(a.alpha, b.alpha, sizeof a.alpha) != 0;
+        cnt[3] += std::memcmp(a.beta, b.beta, sizeof a.beta) != 0;
+        cnt[4] += std::memcmp(a.gamma, b.gamma, sizeof a.gamma) != 0;
+        cnt[5] += std::memcmp(a.delta, b.delta, sizeof a.delta) != 0;
+        cnt[6] += std::memcmp(a.cell_con, b.cell_con, sizeof a.cell_con) != 0;
+    }
+    for (size_t n = 0; n < v.nodes.size(); n++) {
+        const Node &a = v.nodes[n], &b = S.volume.nodes[n];
+        cnt[7] += std::memcmp(&a.volume, &b.volume, sizeof(double)) != 0;
+        if (b.type == NORMAL || b.type == OPEN) cnt[8] += (a.type == OPEN) != (b.type == OPEN);
+    }
+    for (size_t f = 0; f < v.inlet_faces.size(); f++) {
+        const Face &a = v.inlet_faces[f], &b = S.volume.inlet_faces[f];
+        cnt[9] += a.cell_con != b.cell_con;
+        cnt[10] += std::memcmp(&a.area, &b.area, sizeof(double)) != 0;
+        cnt[11] += std::memcmp(a.u, b.u, sizeof a.u) != 0 || std::memcmp(a.v, b.v, sizeof a.v) != 0 ||
+                   std::memcmp(a.normal, b.normal, sizeof a.normal) != 0;
+    }
+    long bad = 0;
+    for (long c : cnt) bad += c;
+    if (bad) {
+        static const char *names[12] = {"volume", "con", "alpha", "beta", "gamma", "delta", "cell_con",
+                                        "node_volume", "open", "inlet_cell", "inlet_area", "inlet_u_v_normal"};
+        for (int i = 0; i < 12; i++)
+            if (cnt[i]) fprintf(stderr, "mesh check: %s differs in %ld records\n", names[i], cnt[i]);
+    }
+    return bad;
+}
+
+void ref_shim_set_storage(void *d, int storage) { ((DeviceData *)d)->fe_storage = storage; }
+
+/* OutputMeshDevice + OutputParticlesDevice with `dir` as the current directory. */
+int ref_shim_output(void *h, void *d, int ts, const char *dir) {
+    RefSim &S = *(RefSim *)h;
+    char here[4096];
+    if (!getcwd(here, sizeof here) || chdir(dir) != 0) return -1;
+    OutputMeshDevice(ts, S.volume, *(DeviceData *)d);
+    OutputParticlesDevice(*(DeviceData *)d);
+    OutputWaitDevice(*(DeviceData *)d);
+    return chdir(here) == 0 ? 0 : -1;
+}
 #endif
 
 }  /* extern "C" */

@@ -14,11 +14,21 @@ comparison is open loop (the reference's own closed loop is not stable):
     bit for bit, in the reference's order;
   - node density within 1e-12 relative;
   - the potential and the E field from the device solve within 1e-9 relative
-    of dsysv_'s.
+    of dsysv_'s;
+  - after the last step, the drop-in's OutputMeshDevice / OutputParticlesDevice
+    files byte for byte those of the reference's OutputMesh / OutputParticles
+    on the same simulation's host arrays.
+A third simulation runs the drop-in with sparse storage (the Lapack method
+becomes the conjugate-gradient Newton step): potential within 1e-9 relative.
+The drop-in's MeshGeometryDevice + InletFacesDevice, run on a copy of the
+loaded Volume with its geometry cleared, reproduce the reference loaders'
+values bit for bit.
 """
 from __future__ import annotations
 
+import ctypes
 import os
+import tempfile
 
 import numpy as np
 import pytest
@@ -73,6 +83,49 @@ def test_drop_in_matches_reference_cpu_path(name):
             b.shim_update_ef()
             ea, eb = a.get("ef"), b.get("ef")
             assert np.abs(ea - eb).max() <= 1e-8 * np.abs(ea).max(), k
+        with tempfile.TemporaryDirectory() as d1, tempfile.TemporaryDirectory() as d2:
+            assert L.ref_shim_output(b.h, b.device, STEPS - 1, d1.encode()) == 0
+            assert L.ref_output_mesh(b.h, STEPS - 1, d2.encode()) >= 0
+            assert L.ref_output_particles(b.h, d2.encode()) >= 0
+            for f in (f"mesh_{STEPS:04d}.vtu", "particles.vtp"):
+                with open(os.path.join(d1, f), "rb") as x, open(os.path.join(d2, f), "rb") as y:
+                    assert x.read() == y.read(), f
+    finally:
+        b.close()
+        a.close()
+
+
+@pytest.mark.parametrize("name", ["kuhn4", "kuhn4s"])
+def test_drop_in_sparse_storage(name):
+    a, b = _sims(name)
+    L = a.L
+    try:
+        L.ref_shim_set_storage(b.device, mp.FE_SPARSE)
+        for k in range(3):
+            b.set("ef", a.get("ef"))
+            L.ref_reseed(1000 + k)
+            a.inject()
+            L.ref_reseed(1000 + k)
+            b.inject()
+            a.move(1)
+            b.shim_move()
+            a.compute_phi(ref.LAPACK)
+            b.shim_compute_phi(ref.LAPACK)
+            ua, ub = a.get("uh"), b.get("uh")
+            assert np.abs(ua - ub).max() <= 1e-9 * np.abs(ua).max(), k
+            a.update_ef()
+    finally:
+        b.close()
+        a.close()
+
+
+@pytest.mark.parametrize("name", ["kuhn4", "kuhn4s"])
+def test_drop_in_mesh_setup_on_device(name):
+    a, b = _sims(name)
+    try:
+        _, tets = mp.read_volume_dat(os.path.join(GOLDEN, name, "mesh.dat"))
+        con = np.ascontiguousarray(tets, dtype=np.int32)
+        assert a.L.ref_shim_mesh_check(a.h, con.ctypes.data_as(ctypes.c_void_p)) == 0
     finally:
         b.close()
         a.close()
