@@ -20,6 +20,13 @@ namespace mp {
 constexpr int PUSH_THREADS = 256;
 constexpr double FIXED_SCALE = 1099511627776.0;  // 2^40
 constexpr double NEAR_FACE = 1e-5;
+// Mixed form: a particle whose FP64 weights are all within ON_FACE of [0, 1]
+// lies on a face of the tet and stays in it.  The reference's weight formula
+// can round a point on the face shared by two tets to slightly below zero in
+// both (seen: -3.4e-15 and -3.4e-14 on a Kuhn diagonal plane), and the walk
+// would then hop between the two forever; FP32 offsets land exactly on such
+// planes often enough to meet this within a few million particle-steps.
+constexpr double ON_FACE = 1e-10;
 
 struct PushF64Args {
     PartsF64 p;
@@ -320,7 +327,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_mixed(PushF32Args a) {
                     inside = true;
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
-                        if (l64[k] < 0 || l64[k] > 1.0) inside = false;
+                        if (l64[k] < -ON_FACE || l64[k] > 1.0 + ON_FACE) inside = false;
                         lc[k] = (float)l64[k];
                     }
                     double m64 = l64[0];

@@ -217,6 +217,37 @@ def test_walk_limit_absorb_policy(deck6, form):
     assert out["cell"].size == 1 and out["cell"][0] == cell[1]
 
 
+def test_mixed_walk_point_on_shared_face(tmp_path):
+    """Mixed form: an ion exactly on the face shared by two Kuhn tets (the
+    x - x0 = z - z0 diagonal plane, FP32 offsets with rx == rz).  The
+    reference's weight formula puts it slightly outside both tets, so a walk
+    on those weights hops between them without end; the mixed form keeps a
+    point within 1e-10 of its tet's faces in the tet."""
+    from conftest import make_deck
+    _, path = make_deck(tmp_path, 20)
+    dk = mp.Deck.load(path)
+    m = dk.mesh
+    a, b = 47012, 47013
+    fa, fb = list(m.cell_con[a]).index(b), list(m.cell_con[b]).index(a)
+    assert m.con[a, 0] == m.con[b, 0]
+    x0 = m.node_pos[m.con[a, 0]]
+    r = np.array([0.0029650903306901455, 0.0030226900707930326, 0.0029650903306901455], dtype=np.float32)
+    X = x0 + r.astype(np.float64)
+
+    def lam(t):  # src/meshes.h:84-85, every operation rounded on its own
+        q = (1.0 / 6.0) * (((m.alpha[t] - X[0] * m.beta[t]) + X[1] * m.gamma[t]) - X[2] * m.delta[t])
+        return q / m.volume[t]
+
+    la, lb = lam(a), lam(b)
+    assert la[fa] < 0 and lb[fb] < 0 and la.argmin() == fa and lb.argmin() == fb
+    ctx = gpu_context(dk, fe=False)
+    ctx.set_form(mp.MIXED)
+    ctx.append(X[None, :], np.zeros((1, 3)), np.array([a], dtype=np.int32))
+    st = ctx.push(0.0, 5e-8, 1.0)
+    assert st.n_after == 1 and st.total_hops == 0
+    assert ctx.download(mp.ORDER_ID)["cell"][0] == a
+
+
 def test_append_rejects_bad_cell(deck4):
     kd, path = deck4
     dk = mp.Deck.load(path)
