@@ -63,47 +63,72 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
-// Position of the n-th (0-based) set bit of m; m must have more than n bits set.
-__device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
-    int base = 0;
-#pragma unroll
-    for (int w = 16; w > 0; w >>= 1) {
-        unsigned low = m & ((1u << w) - 1u);
-        int c = __popc(low);
-        if (n >= c) {
-            n -= c;
-            m >>= w;
-            base += w;
-        } else {
-            m = low;
-        }
-    }
-    return base;
-}
-
-
 // Sums v[0..3] over the lanes that share `key` (one tet), leaving the sums in
 // the group's lowest lane.  All 32 lanes must call it.  Returns true for the
 // lanes that hold a group sum.
+//
+// Pointer jumping over each group's member list: every lane starts pointing at
+// the next member above it and holds the sum of the members from itself up to
+// (not including) the one it points at; each round adds the pointed-to
+// lane's partial sum and takes over its pointer, so ceil(log2(group size))
+// rounds leave the whole group's sum in its lowest lane.  A round is one vote,
+// nine shuffles and four adds, and groups need not be contiguous (particles
+// that hopped since the last tet sort sit between their tet's others).  This
+// replaced a tree over group ranks that located the rank r + s member with a
+// bit search each round: FP64 push 0.0905 -> 0.0868 ms, mixed 0.0660 ->
+// 0.0592 ms on 2M ions sorted every 10 steps.  Summing runs of adjacent equal
+// keys instead (no match) was slower (0.14 ms): a tet's lanes split into
+// several runs once particles hop, and every run issues its own atomics.
 template <typename T>
 __device__ __forceinline__ bool group_sum4(int key, T v[4]) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    unsigned peers = __match_any_sync(FULL, key);
-    int r = __popc(peers & lanemask_lt());
-    int gsize = __popc(peers);
-    for (int s = 1; __any_sync(FULL, s < gsize); s <<= 1) {
-        int pr = r + s;
-        int src = pr < gsize ? nth_set_bit(peers, pr) : lane;
+    const unsigned peers = __match_any_sync(FULL, key);
+    const unsigned above = peers & (0xfffffffeu << lane);  // members above this lane
+    int nxt = above ? __ffs(above) - 1 : -1;
+    while (__any_sync(FULL, nxt >= 0)) {
+        const int src = nxt >= 0 ? nxt : lane;
         T t[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) t[i] = __shfl_sync(FULL, v[i], src);
-        if ((r & (2 * s - 1)) == 0 && pr < gsize) {
+        const int n2 = __shfl_sync(FULL, nxt, src);
+        if (nxt >= 0) {
 #pragma unroll
             for (int i = 0; i < 4; i++) v[i] += t[i];
+            nxt = n2;
         }
     }
-    return r == 0;
+    return (peers & ((1u << lane) - 1u)) == 0;
+}
+
+// Asynchronous global -> shared copies (cp.async, L2 only) for staging the
+// FP64 kernel's next particle chunk without holding it in registers.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// One warp's 32-particle chunk of the FP64 arrays (px, py, pz, vx, vy, vz, cell).
+struct ChunkF64 {
+    double d[6][32];
+    int cell[32];
+};
+
+// Stages chunk c of the FP64 particle arrays into b with 16-byte copies: lanes
+// 0-15 and 16-31 take alternate arrays, lanes 0-7 the cells.  The arrays start
+// on 256-byte boundaries and hold whole 256-particle tiles, so every copy is
+// aligned and inside the allocation, also for the last, partly filled chunk.
+__device__ __forceinline__ void stage_chunk_f64(const PartsF64 &p, long long c, ChunkF64 *b) {
+    const int lane = threadIdx.x & 31;
+    const int h = lane >> 4, q = lane & 15;
+    const long long base = c * 32 + 2 * q;
+    cp_async16(&b->d[h][2 * q], (h ? p.py : p.px) + base);
+    cp_async16(&b->d[2 + h][2 * q], (h ? p.vx : p.pz) + base);
+    cp_async16(&b->d[4 + h][2 * q], (h ? p.vz : p.vy) + base);
+    if (lane < 8) cp_async16(&b->cell[4 * lane], p.cell + c * 32 + 4 * lane);
 }
 
 // Step statistics of one thread, accumulated over all the tiles a persistent
@@ -172,13 +197,20 @@ __device__ __forceinline__ void scatter_warp(int state, int cell, const int con[
 
 // Work division of both push kernels: every warp runs its own 32-particle
 // chunks (chunk c = the warp's global index, then strides of all the grid's
-// warps) with no block-wide barrier, and loads the next chunk's particle into
-// registers (coalesced loads) before it computes the current one, so one
-// chunk's HBM reads are always in flight behind the tet-record gathers.  The
-// particles are updated in place.  This replaced 3-stage TMA bulk-copy staging
-// of 256-particle tiles with a block barrier per tile: the barrier was the
-// third stall reason, and without the staging buffers the L1 keeps more tet
-// records (FP64 push 0.100 -> 0.093 ms on 2M sorted ions).
+// warps) with no block-wide barrier, and fetches the next chunk before it
+// computes the current one, so one chunk's HBM reads are always in flight
+// behind the tet-record gathers.  The particles are updated in place.  This
+// replaced 3-stage TMA bulk-copy staging of 256-particle tiles with a block
+// barrier per tile: the barrier was the third stall reason, and without the
+// staging buffers the L1 keeps more tet records (FP64 push 0.100 -> 0.093 ms
+// on 2M sorted ions).
+//
+// The FP64 kernel fetches the next chunk with cp.async into a per-warp shared
+// slot (two slots, 26 KB per CTA) instead of registers: the 13 registers of a
+// register prefetch made it spill 92 bytes per thread at the 64-register
+// bound of 4 CTAs per SM (0.0868 -> 0.0837 ms on 2M sorted ions).  The mixed
+// kernel's prefetch needs 7 registers and does not spill; staging it was
+// slower (0.0592 -> 0.0626 ms).
 template <bool EXACT_CMP>
 __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_fp64(PushF64Args a) {
     const long long n = (long long)a.counters[C_N];
@@ -187,27 +219,24 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_fp64(PushF64Args a) {
     const long long n_chunks = (n + 31) >> 5;
     long long c = (long long)blockIdx.x * (PUSH_THREADS / 32) + (threadIdx.x >> 5);
     PushStats stats;
-    int cell_n = -1;
-    double xn = 0, yn = 0, zn = 0, vxn = 0, vyn = 0, vzn = 0;
-    if (c < n_chunks && c * 32 + lane < n) {
-        const long long i0 = c * 32 + lane;
-        cell_n = a.p.cell[i0];
-        xn = a.p.px[i0]; yn = a.p.py[i0]; zn = a.p.pz[i0];
-        vxn = a.p.vx[i0]; vyn = a.p.vy[i0]; vzn = a.p.vz[i0];
-    }
+    // two staging slots per warp: the chunk being pushed and the next one
+    __shared__ __align__(16) ChunkF64 stage[PUSH_THREADS / 32][2];
+    ChunkF64 *ws = stage[threadIdx.x >> 5];
+    if (c < n_chunks) stage_chunk_f64(a.p, c, ws);
+    cp_async_commit();
+    int slot = 0;
     for (; c < n_chunks; c += wstride) {
         const long long i = c * 32 + lane;
-        int cell = cell_n;
-        double x = xn, y = yn, z = zn, vx = vxn, vy = vyn, vz = vzn;
-        {
-            const long long in = (c + wstride) * 32 + lane;
-            cell_n = -1;
-            if (c + wstride < n_chunks && in < n) {
-                cell_n = a.p.cell[in];
-                xn = a.p.px[in]; yn = a.p.py[in]; zn = a.p.pz[in];
-                vxn = a.p.vx[in]; vyn = a.p.vy[in]; vzn = a.p.vz[in];
-            }
-        }
+        __syncwarp();  // every lane has read the slot the next chunk overwrites
+        if (c + wstride < n_chunks) stage_chunk_f64(a.p, c + wstride, ws + (slot ^ 1));
+        cp_async_commit();  // possibly empty: one group per chunk keeps the count
+        cp_async_wait<1>();  // this chunk's group has landed
+        __syncwarp();        // ... for every lane's copies
+        const ChunkF64 *cb = ws + slot;
+        slot ^= 1;
+        int cell = cb->cell[lane];
+        double x = cb->d[0][lane], y = cb->d[1][lane], z = cb->d[2][lane];
+        double vx = cb->d[3][lane], vy = cb->d[4][lane], vz = cb->d[5][lane];
         int state = 0, hops = 0, lost = 0;
         int con[4] = {0, 0, 0, 0};
         double lc[4] = {0, 0, 0, 0};
