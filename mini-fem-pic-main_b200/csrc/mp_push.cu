@@ -195,11 +195,16 @@ __device__ __forceinline__ void scatter_warp(int state, int cell, const int con[
     }
 }
 
-// Work division of both push kernels: every warp runs its own 32-particle
-// chunks (chunk c = the warp's global index, then strides of all the grid's
-// warps) with no block-wide barrier, and fetches the next chunk before it
-// computes the current one, so one chunk's HBM reads are always in flight
-// behind the tet-record gathers.  The particles are updated in place.  This
+// Work division of both push kernels: each CTA takes one contiguous block of
+// the (tet-sorted) particle array, and its 8 warps run its 32-particle chunks
+// interleaved (warp w: chunks w, w + 8, ... of the block) with no block-wide
+// barrier.  The CTA's warps thus walk the mesh together through a narrow band
+// of tets, whose records and hop neighbours stay in that SM's L1; striding the
+// warps over the whole array instead spread every SM over the whole mesh
+// (L1 hit rate 34 % FP64 / 49 % mixed; FP64 0.0839 -> 0.0762 ms, mixed
+// 0.0588 -> 0.0520 ms on 2M ions sorted every 10 steps).  Each warp fetches
+// its next chunk before it computes the current one, so one chunk's HBM reads
+// are always in flight behind the tet-record gathers.  The particles are updated in place.  This
 // replaced 3-stage TMA bulk-copy staging of 256-particle tiles with a block
 // barrier per tile: the barrier was the third stall reason, and without the
 // staging buffers the L1 keeps more tet records (FP64 push 0.100 -> 0.093 ms
@@ -215,9 +220,13 @@ template <bool EXACT_CMP>
 __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_fp64(PushF64Args a) {
     const long long n = (long long)a.counters[C_N];
     const int lane = threadIdx.x & 31;
-    const long long wstride = (long long)gridDim.x * (PUSH_THREADS / 32);
-    const long long n_chunks = (n + 31) >> 5;
-    long long c = (long long)blockIdx.x * (PUSH_THREADS / 32) + (threadIdx.x >> 5);
+    // this CTA's contiguous block of chunks [c, n_chunks), its warps interleaved
+    const long long n_all = (n + 31) >> 5;
+    const long long per = (n_all + gridDim.x - 1) / gridDim.x;
+    const long long cta0 = (long long)blockIdx.x * per;
+    const long long n_chunks = n_all < cta0 + per ? n_all : cta0 + per;
+    const long long wstride = PUSH_THREADS / 32;
+    long long c = cta0 + (threadIdx.x >> 5);
     PushStats stats;
     // two staging slots per warp: the chunk being pushed and the next one
     __shared__ __align__(16) ChunkF64 stage[PUSH_THREADS / 32][2];
@@ -301,9 +310,13 @@ __device__ __forceinline__ void load_x0(const double *__restrict__ x0, int cell,
 __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_mixed(PushF32Args a) {
     const long long n = (long long)a.counters[C_N];
     const int lane = threadIdx.x & 31;
-    const long long wstride = (long long)gridDim.x * (PUSH_THREADS / 32);
-    const long long n_chunks = (n + 31) >> 5;
-    long long c = (long long)blockIdx.x * (PUSH_THREADS / 32) + (threadIdx.x >> 5);
+    // this CTA's contiguous block of chunks [c, n_chunks), its warps interleaved
+    const long long n_all = (n + 31) >> 5;
+    const long long per = (n_all + gridDim.x - 1) / gridDim.x;
+    const long long cta0 = (long long)blockIdx.x * per;
+    const long long n_chunks = n_all < cta0 + per ? n_all : cta0 + per;
+    const long long wstride = PUSH_THREADS / 32;
+    long long c = cta0 + (threadIdx.x >> 5);
     PushStats stats;
     int cell_n = -1;
     float rxn = 0, ryn = 0, rzn = 0, vxn = 0, vyn = 0, vzn = 0;
