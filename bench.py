@@ -47,8 +47,8 @@ CONFIGS = workloads.CONFIGS
 make_workload = workloads.make_workload
 FLUSH_BYTES = 512 << 20
 # DRAM bytes of one k_push_fp64 launch on the 2M-ion workload, from ncu
-# (dram__bytes_read.sum 113.4 MB + dram__bytes_write.sum 50.5 MB)
-PUSH_TRAFFIC_BYTES = 163_911_936
+# (dram__bytes_read.sum 113.3 MB + dram__bytes_write.sum 45.6 MB)
+PUSH_TRAFFIC_BYTES = 158_962_176
 SORT_PERIOD = 10
 
 
