@@ -511,7 +511,11 @@ def reference_arm(args):
                 "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": {"workload": cfg["label"], "mesh_hexes": cfg["n"] ** 3,
-                                                "tets": deck.mesh.n_tets, "ions": int(len(cell)), "dt": cfg["dt"]},
+                                                "tets": deck.mesh.n_tets, "nodes": deck.mesh.n_nodes,
+                                                "unknowns": int(deck.fe_desc_arrays()["neq"]),
+                                                "ions_per_gpu": int(len(cell)), "dt": cfg["dt"],
+                                                "method": "lapack (1 Newton step)", "form": "fp64",
+                                                "device": f"host CPU, {threads} OpenMP threads"},
                 "newton_step_ms": newton_ms,
                 "full_step_particle_steps_per_s": full_rate,
                 "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
