@@ -183,6 +183,16 @@ int mp_set_walk_limit(mp_ctx *ctx, int32_t max_hops);
 int mp_set_scatter_mode(mp_ctx *ctx, int mode);
 int mp_set_walk_policy(mp_ctx *ctx, int policy);
 int mp_set_sort_period(mp_ctx *ctx, int32_t steps);
+/* Particle storage of the push (MoveParticles, src/mini-pic.cpp:268-320):
+ * MP_FORM_FP64 (default) is the reference's arithmetic bit for bit; with
+ * MP_FORM_MIXED positions are FP32 offsets from the owning tet's vertex 0 and
+ * velocities FP32, the inside test runs in FP32 and is redone with the
+ * reference's FP64 weights when the smallest weight is within 1e-5 of zero,
+ * and the density still accumulates in FP64.  In the mixed form a particle
+ * whose FP64 weights all lie within 1e-10 of [0, 1] stays in its tet: the
+ * reference's formula can put a point on a face shared by two tets outside
+ * both, and its walk (src/meshes.h:75-100) would then never end.  Converts the
+ * resident particles (holes removed first). */
 int mp_set_particle_form(mp_ctx *ctx, int form);
 /* Arithmetic of the mixed-form Newton factorization (MP_MIXED_TF32 or
  * MP_MIXED_TF32X3, the default).  No reference counterpart: the reference's
