@@ -166,6 +166,10 @@ typedef struct mp_newton_stats {
     double linear_residual;      /* ||b - J y|| / neq of the last linear solve */
     double ms_total;             /* device time of the call, ms */
     double ms_factor;            /* device time of the factorization, ms */
+    int32_t linear_failures;     /* Gauss-Seidel solves that ran out of sweeps above the tolerance
+                                    (the reference warns "GS failed to converge" and goes on,
+                                    src/FESolver.cpp:600) */
+    int32_t reserved;
 } mp_newton_stats;
 
 /* ---- context ---------------------------------------------------------------- */
@@ -271,7 +275,13 @@ int mp_sort_by_tet(mp_ctx *ctx);
  * MP_ERR_LIMIT; calls that overlap on the GPU race on the scratch and must be
  * serialised; the first call on a device looks the array up with that device
  * current and should come before any stream capture.  Walk limit 4096 hops
- * (MP_ERR_WALK_LIMIT). */
+ * (MP_ERR_WALK_LIMIT).  Every index in the caller's records is checked before
+ * use: a particle whose cell is outside [0, n_tets) (the reference's removed
+ * state cell_index = -1 included), or whose walk meets a neighbour index
+ * >= n_tets or a node index outside [0, n_nodes), stops there, adds nothing to
+ * den, is written out as it stands and the call returns MP_ERR_ARG.  After
+ * MP_ERR_TIMEOUT the contents of particles_out (and of particles_in when it is
+ * the same buffer) are undefined. */
 int mp_push_particles_noalloc(const void *particles_in, void *particles_out, int64_t n,
                               const void *tetra, int32_t n_tets, const double *ef, double *den,
                               int32_t n_nodes, double q_over_m, double dt, void *stream, int64_t *n_out);
@@ -295,8 +305,14 @@ int mp_fe_build_f1(mp_ctx *ctx, const double *ion_den);
 int mp_fe_residual(mp_ctx *ctx);
 int mp_fe_build_j(mp_ctx *ctx, int method);
 /* Solves J y = G (G from mp_fe_residual, or b if non-NULL); y stays on the device
- * (MP_VEC_Y).  method MP_METHOD_GAUSS_SEIDEL, MP_METHOD_LAPACK or MP_METHOD_SPARSE_CG. */
+ * (MP_VEC_Y).  method MP_METHOD_GAUSS_SEIDEL, MP_METHOD_LAPACK or MP_METHOD_SPARSE_CG.
+ * Gauss-Seidel that ends its sweeps with sqrt(sum r^2)/neq >= 1e-4 (solveLinear,
+ * src/FESolver.cpp:561-601) returns MP_ERR_NOT_CONVERGED with y holding the last
+ * iterate; inside mp_compute_phi the step goes on, as the reference's does, and
+ * the failure is counted in mp_newton_stats.linear_failures. */
 int mp_fe_solve_linear(mp_ctx *ctx, int method, int form, const double *b, mp_newton_stats *stats);
+/* Sweep limit of Gauss-Seidel (default 10000, the reference's). */
+int mp_set_gs_max_sweeps(mp_ctx *ctx, int32_t sweeps);
 /* FESolver::updateEf from the device uh (or uh_host if non-NULL). */
 int mp_update_ef(mp_ctx *ctx, const double *uh_host);
 int mp_field_download(mp_ctx *ctx, double *d, double *uh, double *ef);

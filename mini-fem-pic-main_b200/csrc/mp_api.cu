@@ -112,17 +112,16 @@ static int ensure_stage(mp_ctx *ctx, size_t bytes) {
     return MP_OK;
 }
 
-static void *g_dstage = nullptr;
-static size_t g_dstage_bytes = 0;
-
+// Device staging of host appends and downloads, owned by the context.
 static int ensure_dstage(mp_ctx *ctx, size_t bytes) {
-    if (bytes <= g_dstage_bytes) return MP_OK;
+    if (bytes <= ctx->dstage_bytes) return MP_OK;
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (g_dstage) cudaFree(g_dstage);
-    g_dstage = nullptr;
-    size_t b = std::max(bytes, g_dstage_bytes * 2);
-    MP_CUDA(ctx, cudaMalloc(&g_dstage, b));
-    g_dstage_bytes = b;
+    if (ctx->dstage) cudaFree(ctx->dstage);
+    ctx->dstage = nullptr;
+    size_t b = std::max(bytes, ctx->dstage_bytes * 2);
+    ctx->dstage_bytes = 0;
+    MP_CUDA(ctx, cudaMalloc(&ctx->dstage, b));
+    ctx->dstage_bytes = b;
     return MP_OK;
 }
 
@@ -284,6 +283,7 @@ int mp_destroy(mp_ctx *ctx) {
     if (!ctx) return MP_OK;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     adjoint_free(ctx);
+    solve_free(ctx);
     output_free(ctx);  // joins a writer still running
     inject_free(ctx);
     sparse_free(ctx);
@@ -291,7 +291,7 @@ int mp_destroy(mp_ctx *ctx) {
                    ctx->den, ctx->den_fixed, ctx->counters, ctx->scal, ctx->compact_off, ctx->sort_hist,
                    ctx->part_block[0], ctx->part_block[1], ctx->ID, ctx->LM, ctx->detJ, ctx->nx, ctx->g, ctx->uh,
                    ctx->d, ctx->F0, ctx->F1, ctx->G, ctx->y, ctx->fvec, ctx->FP, ctx->work, ctx->K, ctx->J,
-                   ctx->J32, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a, ctx->gs_minv, ctx->den_in};
+                   ctx->J32, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a, ctx->gs_minv, ctx->den_in, ctx->dstage};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
@@ -427,8 +427,8 @@ int mp_particles_append(mp_ctx *ctx, int64_t n, const double *pos, int64_t pos_s
         h[3 * n + i] = v[0]; h[4 * n + i] = v[1]; h[5 * n + i] = v[2];
         hc[i] = c;
     }
-    MP_CUDA(ctx, cudaMemcpyAsync(g_dstage, ctx->stage, bytes, cudaMemcpyHostToDevice, ctx->stream));
-    double *d = (double *)g_dstage;
+    MP_CUDA(ctx, cudaMemcpyAsync(ctx->dstage, ctx->stage, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    double *d = (double *)ctx->dstage;
     return mp_particles_append_device(ctx, n, d, d + 3 * n, (const int32_t *)(d + 6 * n), rewind, q_over_m,
                                       half_dt);
 }
@@ -450,12 +450,12 @@ int mp_particles_download(mp_ctx *ctx, int64_t n_max, double *pos, int64_t pos_s
     if (rc) return rc;
     rc = ensure_dstage(ctx, bytes);
     if (rc) return rc;
-    double *d = (double *)g_dstage;
+    double *d = (double *)ctx->dstage;
     int *dc = (int *)(d + 10 * n);
     long long *di = (long long *)(dc + n + (n & 1));
     rc = launch_download_pack(ctx, n, d, dc, di);
     if (rc) return rc;
-    MP_CUDA(ctx, cudaMemcpyAsync(ctx->stage, g_dstage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    MP_CUDA(ctx, cudaMemcpyAsync(ctx->stage, ctx->dstage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     const double *h = (const double *)ctx->stage;
     const int *hc = (const int *)(h + 10 * n);
@@ -774,12 +774,22 @@ int mp_fe_solve_linear(mp_ctx *ctx, int method, int form, const double *b, mp_ne
         return fail(ctx, MP_ERR_STATE, "sparse storage: this method needs MP_FE_STORAGE_DENSE");
     if (b) MP_CUDA(ctx, cudaMemcpyAsync(ctx->G, b, sizeof(double) * ctx->neq, cudaMemcpyHostToDevice, ctx->stream));
     MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * ctx->neq, ctx->stream));
-    if (st) std::memset(st, 0, sizeof(*st));
+    mp_newton_stats local;
+    if (!st) st = &local;
+    std::memset(st, 0, sizeof(*st));
     int rc = method == MP_METHOD_SPARSE_CG   ? fe_solve_cg(ctx, st)
              : method == MP_METHOD_GAUSS_SEIDEL ? fe_solve_gs(ctx, st)
                                                 : fe_solve_ldlt(ctx, form, st);
     if (rc) return rc;
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (st->linear_failures)
+        return fail(ctx, MP_ERR_NOT_CONVERGED, "GS failed to converge");
+    return MP_OK;
+}
+
+int mp_set_gs_max_sweeps(mp_ctx *ctx, int32_t sweeps) {
+    if (!ctx || sweeps < 1) return MP_ERR_ARG;
+    ctx->gs_max_sweeps = sweeps;
     return MP_OK;
 }
 

@@ -77,6 +77,7 @@ enum Flag : unsigned long long {
     FLAG_LOOKBACK_TIMEOUT = 2ull,
     FLAG_SINGULAR = 4ull,
     FLAG_NONFINITE = 8ull,
+    FLAG_BAD_INDEX = 16ull,   // a cell, neighbour or node index outside the mesh (caller-owned records)
 };
 
 // The per-quadrature-point shape function values used by buildF1Vector and
@@ -171,8 +172,18 @@ struct mp_ctx {
     void *sparse_scratch = nullptr;       // conjugate-gradient work (mp_sparse.cu)
     double cg_rtol = 1e-12;               // ||G - J y|| <= cg_rtol ||G||
     int cg_max_it = 20000;
+    int gs_max_sweeps = 10000;            // solveLinear's sweep limit (src/FESolver.cpp:575)
     int cg_last_iterations = 0, cg_last_restarts = 0;
     double cg_last_relres = 0;
+
+    // dense-solve scratch (mp_solve.cu): W panels, block inverses, ready words;
+    // sized for neq, allocated on the first factorization
+    void *solve_scratch = nullptr;
+    int solve_epoch = 0;                  // ready-word epoch of this context's triangular solves
+    bool ldlt_attr = false;               // >48 KB shared-memory attributes set for this context's device
+    // device staging of host appends and downloads
+    void *dstage = nullptr;
+    size_t dstage_bytes = 0;
 
     mp::Timer t0, t1, tp, ts;
     long long launches = 0;
@@ -221,6 +232,7 @@ int fe_sparse_from_dense(mp_ctx *ctx);
 int fe_sparse_from_host(mp_ctx *ctx, const double *const *rows, const double *dense);
 int fe_residual_sparse(mp_ctx *ctx);
 int fe_solve_cg(mp_ctx *ctx, mp_newton_stats *st);
+void solve_free(mp_ctx *ctx);
 void adjoint_free(mp_ctx *ctx);
 void inject_free(mp_ctx *ctx);
 void output_free(mp_ctx *ctx);

@@ -680,8 +680,6 @@ static bool operand_map(CUtensorMap *m, const float *base, long long rows, long 
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-static int g_solve_epoch = 0;
-
 // Super-panel width of the two-level LDL^T: the trailing matrix is read and
 // written once per SUPER_W columns (the HBM traffic that bounds the trailing
 // update), the panels inside a super-panel update only its remaining columns.
@@ -704,8 +702,7 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     const size_t panel_smem = sizeof(T) * (64 * (NB + 1) + NB * (NB + 1) + 2 * NB);
     const size_t upd_smem = sizeof(T) * 2 * NB * 68;
     const size_t f64_smem = sizeof(double) * 4 * WKC * WTILE;
-    static bool attr = false;
-    if (!attr) {
+    if (!ctx->ldlt_attr) {  // per context: the attributes belong to the context's device
         const int big = 96 * 1024;
         cudaFuncSetAttribute(k_ldlt_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
@@ -718,7 +715,7 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                              (int)tc::smem_bytes(false));
         cudaFuncSetAttribute(tc::k_update_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)tc::smem_bytes(true));
-        attr = true;
+        ctx->ldlt_attr = true;
     }
     unsigned long long *flags = ctx->counters + C_FLAGS;
     auto diag_and_panel = [&](int k0, int kb, T *W, int ldw) {
@@ -812,7 +809,7 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         }
     }
     const int nblk = (n + NB - 1) / NB;
-    const int epoch = ++g_solve_epoch;
+    const int epoch = ++ctx->solve_epoch;
     if (!factor) {
         int g = trsv_grid<T>(ctx, (const void *)k_trsv_fwd<T>, nblk);
         k_trsv_fwd<T><<<g, 256, 0, st>>>(n, ld, A, w.Linv, b, w.ready, epoch, flags), ++ctx->launches;

@@ -19,7 +19,15 @@
 //     that overlap on the GPU (two streams, or two host threads) race on it
 //     and must be serialised by the caller;
 //   * the first call on a device looks up the array's device address with that
-//     device current; make that first call before any stream capture.
+//     device current; make that first call before any stream capture;
+//   * the records are the caller's, so every index is checked before it is
+//     used: a particle whose cell lies outside [0, n_tets), or whose walk meets
+//     a neighbour index >= n_tets or a node index outside [0, n_nodes), stops
+//     where it is, adds nothing to den, is written out unchanged from that
+//     point, and the call returns MP_ERR_ARG (the reference's flagged state
+//     cell_index = -1 is removed before its next push, src/mini-pic.cpp:316);
+//   * after MP_ERR_TIMEOUT the contents of particles_out (and of particles_in
+//     when it is the same buffer) are undefined.
 #include <cuda/atomic>
 
 #include <mutex>
@@ -91,8 +99,8 @@ __device__ long long lookback(unsigned long long *w, long long tile, long long c
 // written stably to `out` (which may be `in`: a tile writes only below its own
 // end, after every earlier tile has read its input).
 __global__ void __launch_bounds__(THREADS) k_push_aos(const char *in, char *out, long long n, const char *tetra,
-                                                      const double *__restrict__ ef, double *den, double qm,
-                                                      double dt, unsigned long long *w) {
+                                                      int n_tets, const double *__restrict__ ef, double *den,
+                                                      int n_nodes, double qm, double dt, unsigned long long *w) {
     __shared__ long long s_tile, s_base;
     __shared__ int s_wc[THREADS / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -113,6 +121,14 @@ __global__ void __launch_bounds__(THREADS) k_push_aos(const char *in, char *out,
                 v[k] = ldd(p, P_VEL + 8 * k);
             }
             cell = ldi(p, P_CELL);
+            if (cell < 0 || cell >= n_tets) {
+                // not a particle of this mesh: written out as it came, nothing scattered
+                keep = true;
+                for (int k = 0; k < 4; k++) lc[k] = ldd(p, P_LC + 8 * k);
+                atomicOr(&w[W_FLAGS], mp::FLAG_BAD_INDEX);
+            }
+        }
+        if (i < n && !keep) {
             for (int k = 0; k < 3; k++) v[k] = __dadd_rn(v[k], __dmul_rn(__dmul_rn(qm, ef[3ll * cell + k]), dt));
             for (int k = 0; k < 3; k++) x[k] = __dadd_rn(x[k], __dmul_rn(v[k], dt));
             int hops = 0;
@@ -129,7 +145,17 @@ __global__ void __launch_bounds__(THREADS) k_push_aos(const char *in, char *out,
                 }
                 if (inside) {
                     keep = true;
-                    for (int q = 0; q < 4; q++) atomicAdd(&den[ldi(t, T_CON + 4 * q)], lc[q]);
+                    int nodes[4];
+                    bool ok = true;
+                    for (int q = 0; q < 4; q++) {
+                        nodes[q] = ldi(t, T_CON + 4 * q);
+                        ok = ok && nodes[q] >= 0 && nodes[q] < n_nodes;
+                    }
+                    if (ok) {
+                        for (int q = 0; q < 4; q++) atomicAdd(&den[nodes[q]], lc[q]);
+                    } else {
+                        atomicOr(&w[W_FLAGS], mp::FLAG_BAD_INDEX);
+                    }
                     break;
                 }
                 int mi = 0;
@@ -141,6 +167,11 @@ __global__ void __launch_bounds__(THREADS) k_push_aos(const char *in, char *out,
                     }
                 int nb = ldi(t, T_CELLCON + 4 * mi);
                 if (nb < 0) break;
+                if (nb >= n_tets) {
+                    keep = true;  // kept in the last valid tet, not scattered
+                    atomicOr(&w[W_FLAGS], mp::FLAG_BAD_INDEX);
+                    break;
+                }
                 if (hops >= HOP_LIMIT) {
                     keep = true;  // kept where the walk stopped, not scattered
                     atomicOr(&w[W_FLAGS], mp::FLAG_WALK_LIMIT);
@@ -222,7 +253,8 @@ extern "C" int mp_push_particles_noalloc(const void *particles_in, void *particl
         if (grid > tiles) grid = tiles;
         k_push_aos<<<(unsigned)grid, THREADS, 0, st>>>(static_cast<const char *>(particles_in),
                                                         static_cast<char *>(particles_out), n,
-                                                        static_cast<const char *>(tetra), ef, den, q_over_m, dt, w);
+                                                        static_cast<const char *>(tetra), n_tets, ef, den, n_nodes,
+                                                        q_over_m, dt, w);
         if (cudaGetLastError() != cudaSuccess) return MP_ERR_CUDA;
     }
     unsigned long long res[3] = {0, 0, 0};
@@ -230,6 +262,7 @@ extern "C" int mp_push_particles_noalloc(const void *particles_in, void *particl
     if (cudaStreamSynchronize(st) != cudaSuccess) return MP_ERR_CUDA;
     *n_out = (int64_t)res[W_KEPT];
     if (res[W_FLAGS] & mp::FLAG_LOOKBACK_TIMEOUT) return MP_ERR_TIMEOUT;
+    if (res[W_FLAGS] & mp::FLAG_BAD_INDEX) return MP_ERR_ARG;
     if (res[W_FLAGS] & mp::FLAG_WALK_LIMIT) return MP_ERR_WALK_LIMIT;
     return MP_OK;
 }

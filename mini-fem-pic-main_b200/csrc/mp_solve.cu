@@ -81,49 +81,70 @@ static int check_flags(mp_ctx *ctx, unsigned long long mask, unsigned long long 
     return MP_OK;
 }
 
-// Scratch of the solvers, allocated on first use.
+// Scratch of the dense solves, owned by the context and allocated on its
+// first factorization (again when neq changes).
 struct SolveScratch {
     double *dvec64 = nullptr, *W64 = nullptr, *s64 = nullptr, *r = nullptr, *Linv64 = nullptr;
     float *dvec32 = nullptr, *W32 = nullptr, *s32 = nullptr, *b32 = nullptr, *Linv32 = nullptr, *split32 = nullptr;
     int *ready = nullptr;
     int neq = 0;
 };
-static SolveScratch g_scr;
 
-static int ensure_scratch(mp_ctx *ctx) {
-    if (g_scr.neq == ctx->neq && g_scr.dvec64) return MP_OK;
-    int n = ctx->neq;
-    cudaFree(g_scr.dvec64); cudaFree(g_scr.W64); cudaFree(g_scr.s64); cudaFree(g_scr.r);
-    cudaFree(g_scr.dvec32); cudaFree(g_scr.W32); cudaFree(g_scr.s32); cudaFree(g_scr.b32);
-    cudaFree(g_scr.Linv64); cudaFree(g_scr.Linv32); cudaFree(g_scr.ready); cudaFree(g_scr.split32);
-    g_scr = SolveScratch();
-    MP_CUDA(ctx, cudaMalloc(&g_scr.dvec64, sizeof(double) * (n + 64)));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.W64, sizeof(double) * (size_t)(n + NB) * SUPER_W));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.s64, sizeof(double) * NB));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.r, sizeof(double) * (n + 64)));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.dvec32, sizeof(float) * (n + 64)));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.W32, sizeof(float) * (size_t)(n + NB) * SUPER_W));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.s32, sizeof(float) * NB));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.b32, sizeof(float) * (n + 64)));
+static void release(SolveScratch *s) {
+    void *p[] = {s->dvec64, s->W64, s->s64, s->r, s->dvec32, s->W32, s->s32, s->b32,
+                 s->Linv64, s->Linv32, s->ready, s->split32};
+    for (void *q : p)
+        if (q) cudaFree(q);
+    *s = SolveScratch();
+}
+
+void solve_free(mp_ctx *ctx) {
+    SolveScratch *s = static_cast<SolveScratch *>(ctx->solve_scratch);
+    if (!s) return;
+    release(s);
+    delete s;
+    ctx->solve_scratch = nullptr;
+}
+
+static int ensure_scratch(mp_ctx *ctx, SolveScratch **out) {
+    if (!ctx->solve_scratch) ctx->solve_scratch = new SolveScratch();
+    SolveScratch &s = *static_cast<SolveScratch *>(ctx->solve_scratch);
+    *out = &s;
+    if (s.neq == ctx->neq && s.dvec64) return MP_OK;
+    const int n = ctx->neq;
+    // the context's own stream may still read the old buffers
+    MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    release(&s);
+    MP_CUDA(ctx, cudaMalloc(&s.dvec64, sizeof(double) * (n + 64)));
+    MP_CUDA(ctx, cudaMalloc(&s.W64, sizeof(double) * (size_t)(n + NB) * SUPER_W));
+    MP_CUDA(ctx, cudaMalloc(&s.s64, sizeof(double) * NB));
+    MP_CUDA(ctx, cudaMalloc(&s.r, sizeof(double) * (n + 64)));
+    MP_CUDA(ctx, cudaMalloc(&s.dvec32, sizeof(float) * (n + 64)));
+    MP_CUDA(ctx, cudaMalloc(&s.W32, sizeof(float) * (size_t)(n + NB) * SUPER_W));
+    MP_CUDA(ctx, cudaMalloc(&s.s32, sizeof(float) * NB));
+    MP_CUDA(ctx, cudaMalloc(&s.b32, sizeof(float) * (n + 64)));
     const size_t nblk = (n + NB - 1) / NB;
-    MP_CUDA(ctx, cudaMalloc(&g_scr.Linv64, sizeof(double) * nblk * NB * NB));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.Linv32, sizeof(float) * nblk * NB * NB));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.split32, sizeof(float) * 4 * (size_t)n * SUPER_W));
-    MP_CUDA(ctx, cudaMalloc(&g_scr.ready, sizeof(int) * 2 * ((n + NB - 1) / NB + 1)));
-    MP_CUDA(ctx, cudaMemset(g_scr.ready, 0, sizeof(int) * 2 * ((n + NB - 1) / NB + 1)));
-    g_scr.neq = n;
+    MP_CUDA(ctx, cudaMalloc(&s.Linv64, sizeof(double) * nblk * NB * NB));
+    MP_CUDA(ctx, cudaMalloc(&s.Linv32, sizeof(float) * nblk * NB * NB));
+    MP_CUDA(ctx, cudaMalloc(&s.split32, sizeof(float) * 4 * (size_t)n * SUPER_W));
+    MP_CUDA(ctx, cudaMalloc(&s.ready, sizeof(int) * 2 * (nblk + 1)));
+    MP_CUDA(ctx, cudaMemsetAsync(s.ready, 0, sizeof(int) * 2 * (nblk + 1), ctx->stream));
+    ctx->solve_epoch = 0;  // fresh ready words hold epoch 0
+    s.neq = n;
     return MP_OK;
 }
 
 int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
-    int rc = ensure_scratch(ctx);
+    SolveScratch *sp = nullptr;
+    int rc = ensure_scratch(ctx, &sp);
     if (rc) return rc;
+    SolveScratch &sc = *sp;
     const int n = ctx->neq;
     const long long ld = (n + 31) & ~31ll;
     cudaEventRecord(ctx->t1.a, ctx->stream);
     if (form == MP_FORM_FP64) {
         MP_CUDA(ctx, cudaMemcpyAsync(ctx->y, ctx->G, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
-        LdltWork<double> w{g_scr.dvec64, g_scr.W64, g_scr.s64, g_scr.Linv64, g_scr.ready, nullptr};
+        LdltWork<double> w{sc.dvec64, sc.W64, sc.s64, sc.Linv64, sc.ready, nullptr};
         rc = ldlt_factor_solve<double>(ctx, ctx->J, ld, n, ctx->y, w, true);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
@@ -141,25 +162,25 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
             k_j_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(n, ld, ctx->J, ctx->J32), ++ctx->launches;
         ctx->j32_current = false;
         MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * n, ctx->stream));
-        LdltWork<float> w{g_scr.dvec32, g_scr.W32, g_scr.s32, g_scr.Linv32, g_scr.ready, g_scr.split32};
+        LdltWork<float> w{sc.dvec32, sc.W32, sc.s32, sc.Linv32, sc.ready, sc.split32};
         double rn = 0, bn = 0;
         // r = G (y = 0), in FP32 for the first solve, which also factors J32
-        rc = resid_norms(ctx, ctx->y, ctx->G, g_scr.r, g_scr.b32, &rn, &bn);
+        rc = resid_norms(ctx, ctx->y, ctx->G, sc.r, sc.b32, &rn, &bn);
         if (rc) return rc;
-        rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, g_scr.b32, w, true, ctx->mixed_factor);
+        rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, sc.b32, w, true, ctx->mixed_factor);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
-        k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, g_scr.b32, ctx->y), ++ctx->launches;
+        k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, sc.b32, ctx->y), ++ctx->launches;
         int it = 1;
         double prev = 1e300;
         for (; it < 60; it++) {
-            rc = resid_norms(ctx, ctx->y, ctx->G, g_scr.r, g_scr.b32, &rn, &bn);
+            rc = resid_norms(ctx, ctx->y, ctx->G, sc.r, sc.b32, &rn, &bn);
             if (rc) return rc;
             if (!(rn > 1e-14 * bn) || rn > 0.7 * prev) break;
             prev = rn;
-            rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, g_scr.b32, w, false);
+            rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, sc.b32, w, false);
             if (rc) return rc;
-            k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, g_scr.b32, ctx->y), ++ctx->launches;
+            k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, sc.b32, ctx->y), ++ctx->launches;
         }
         if (st) {
             st->linear_iterations = it;
@@ -256,7 +277,7 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st) {
     double L2 = 0;
     int it;
     bool converged = false;
-    for (it = 0; it < 10000; it++) {
+    for (it = 0; it < ctx->gs_max_sweeps; it++) {
         k_gs_sweep<<<1, 1024, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, ctx->y), ++ctx->launches;
         if (it % 25 == 0) {
             MP_CUDA(ctx, cudaMemsetAsync(ctx->scal + 3, 0, sizeof(double), ctx->stream));
@@ -273,8 +294,9 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st) {
     }
     MP_CUDA(ctx, cudaGetLastError());
     if (st) {
-        st->linear_iterations = converged ? it : it;
+        st->linear_iterations = it;
         st->linear_residual = L2;
+        if (!converged) st->linear_failures++;
     }
     return MP_OK;
 }

@@ -65,7 +65,7 @@ EXPORTED = [
     "mp_adjoint_backward", "mp_adjoint_tangent", "mp_set_walk_policy", "mp_inject_device",
     "mp_set_fe_storage", "mp_set_sparse_solver", "mp_fe_sparse_matrix",
     "mp_mesh_geometry_device", "mp_inlet_faces_device", "mp_fe_geometry_device",
-    "mp_output_mesh", "mp_output_particles", "mp_output_wait",
+    "mp_output_mesh", "mp_output_particles", "mp_output_wait", "mp_set_gs_max_sweeps",
 ]
 
 
@@ -106,7 +106,8 @@ class StepStats(C.Structure):
 
 class NewtonStats(C.Structure):
     _fields_ = [("newton_iterations", C.c_int32), ("linear_iterations", C.c_int32), ("l2", C.c_double),
-                ("linear_residual", C.c_double), ("ms_total", C.c_double), ("ms_factor", C.c_double)]
+                ("linear_residual", C.c_double), ("ms_total", C.c_double), ("ms_factor", C.c_double),
+                ("linear_failures", C.c_int32), ("reserved", C.c_int32)]
 
 
 class AdjointStats(C.Structure):
@@ -559,6 +560,10 @@ class Context:
         """FE_DENSE (default: dense K and J plus a sparse K) or FE_SPARSE (the
         sparse K only; SPARSE_CG and SPARSE_NEWTON).  Before fe_setup."""
         self._c(lib().mp_set_fe_storage(self.h, storage))
+
+    def set_gs_max_sweeps(self, sweeps=10000):
+        """Gauss-Seidel sweep limit (the reference's is 10000)."""
+        self._c(lib().mp_set_gs_max_sweeps(self.h, int(sweeps)))
 
     def set_sparse_solver(self, rtol=1e-12, max_iterations=20000):
         """Conjugate-gradient stop: ||G - J y|| <= rtol ||G||."""

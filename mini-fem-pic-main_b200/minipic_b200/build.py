@@ -67,7 +67,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             failed.append(c[-3] if c[0] == "g++" else c[-3])
     if failed:
         raise RuntimeError(f"compilation failed: {failed}")
-    link = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static" if False else "-cudart=static"]
+    link = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-cudart=static"]
     if verbose:
         print(" ".join(link))
     subprocess.run(link, check=True)

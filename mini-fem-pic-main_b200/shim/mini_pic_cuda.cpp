@@ -3,6 +3,7 @@
 #include "mini_pic_cuda.h"
 
 #include <cstdlib>
+#include <iomanip>
 #include <iostream>
 #include <vector>
 
@@ -109,6 +110,10 @@ void computePhiDevice(FESolver &solver, double *ion_den, FESolver::Method method
             : method == FESolver::Lapack  ? MP_METHOD_SPARSE_CG
                                           : m;  // Gauss-Seidel needs the dense J: reported as an error
     const int rc = mp_compute_phi(device.ctx, ion_den, m, device.form, &st);
+    // src/FESolver.cpp:600: each Gauss-Seidel solve that ran out of sweeps warns, the step goes on
+    for (int k = 0; k < st.linear_failures; k++)
+        std::cerr << " GS failed to converge in " << st.linear_iterations << " iterations, " << std::setprecision(3)
+                  << ": L2=" << st.linear_residual << std::endl;
     if (rc == MP_ERR_NOT_CONVERGED) {
         // src/FESolver.cpp:360-361
         std::cerr << "NR failed to converge, L2 = " << st.l2 << std::endl;

@@ -10,6 +10,9 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import subprocess
+import sys
+import tempfile
 
 import numpy as np
 
@@ -288,3 +291,27 @@ class RefSim:
 
 def max_threads() -> int:
     return lib().ref_max_threads()
+
+
+def compute_phi_isolated(deck_dir: str, method: int, d, F1, den, *, spwt: float = 200.0,
+                         extra_fixed: dict | None = None, timeout: float = 600.0) -> dict:
+    """The reference's computePhi from the state (d, F1, ion density) in a
+    child process (oracle/ref_isolated.py), since its NonLinear method may end
+    the process.  Returns exitcode, the reference's printed messages (log) and,
+    when it returned, d and uh."""
+    with tempfile.TemporaryDirectory() as wd:
+        inp, out = os.path.join(wd, "in.npz"), os.path.join(wd, "out.npz")
+        extra = {}
+        for path, (nodes, value) in (extra_fixed or {}).items():
+            extra = dict(fixed_file=path, fixed_nodes=np.asarray(nodes, dtype=np.int64), fixed_value=value)
+        np.savez(inp, method=method, spwt=spwt, d=np.asarray(d, dtype=np.float64),
+                 F1=np.asarray(F1, dtype=np.float64), den=np.asarray(den, dtype=np.float64), **extra)
+        root = os.path.dirname(HERE)
+        p = subprocess.run([sys.executable, "-m", "oracle.ref_isolated", deck_dir, inp, out], cwd=root,
+                           capture_output=True, text=True, timeout=timeout,
+                           env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
+        res = {"exitcode": p.returncode, "log": p.stdout + p.stderr}
+        if p.returncode == 0:
+            r = dict(np.load(out))
+            res.update(d=r["d"], uh=r["uh"], F1=r["F1"])
+    return res

@@ -195,3 +195,33 @@ def test_state_errors(deck4):
     with pytest.raises(mp.MpError) as e:
         ctx.compute_phi(mp.LAPACK)
     assert e.value.status == 7
+
+
+@needs_ref
+def test_gauss_seidel_out_of_sweeps_is_reported(deck6):
+    """solveLinear warns "GS failed to converge" when its sweeps run out above
+    the tolerance (src/FESolver.cpp:600) and the step goes on: mp_fe_solve_linear
+    returns MP_ERR_NOT_CONVERGED with y holding the last iterate (the
+    reference's after the same sweeps); computePhi completes and counts it."""
+    kd, path = deck6
+    dk, s, ctx = setup_pair(path, kd)
+    s.build_f1(s.get("den"))
+    G = s.residual()
+    s.build_j(1)
+    ctx.build_j(1)
+    ctx.set_gs_max_sweeps(1)
+    with pytest.raises(mp.MpError) as e:
+        ctx.solve_linear(mp.GAUSS_SEIDEL, mp.FP64, b=G)
+    assert e.value.status == 5
+    y = ctx.fe_get("y")
+    # one sweep from zero: the reference's first Gauss-Seidel iterate
+    A = s.matrix(1)
+    x = np.zeros_like(G)
+    for u in range(len(G)):
+        if abs(A[u, u]) < 1e-12:
+            continue
+        x[u] = (G[u] - (A[u, :u] @ x[:u] + A[u, u + 1:] @ x[u + 1:])) / A[u, u]
+    assert rel_err(y, x) < 1e-12
+    st = ctx.compute_phi(mp.GAUSS_SEIDEL, mp.FP64, ion_den=s.get("den"))
+    assert st.linear_failures == 1 and st.linear_iterations == 1
+    ctx.set_gs_max_sweeps(10000)

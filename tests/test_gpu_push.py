@@ -14,54 +14,11 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, gpu_context, ref_available, ref_sim, rel_err
+from conftest import DEN_RTOL, GOLDEN, den_close as _den_close, gpu_context, ref_available, run_open_loop
 import minipic_b200 as mp
 from oracle import port
 
 pytestmark = pytest.mark.gpu
-
-DEN_RTOL = 1e-12
-
-
-def _den_close(a, b):
-    scale = max(np.abs(b).max(), 1e-300)
-    return float(np.abs(a - b).max() / scale)
-
-
-def run_open_loop(path, kdeck, steps, spwt, *, sort_period=0, scatter=mp.SCATTER_ATOMIC, method=2, check_every=1):
-    dk = mp.Deck.load(path)
-    s = ref_sim(path, kdeck, spwt=spwt)
-    ctx = gpu_context(dk, sphere_potential=-10.0, fe=False)
-    ctx.set_sort_period(sort_period)
-    ctx.set_scatter_mode(scatter)
-    inj = mp.Injector(dk.mesh)
-    P = dk.params
-    qm, dt = s.q_over_m, P.dt
-    worst = 0.0
-    for ts in range(steps):
-        k = s.inject()
-        pos, vel, cell = inj.sample(P.plasma_den, P.ion_velocity, dt, spwt)
-        assert len(cell) == k
-        ctx.append(pos, vel, cell, rewind=True, q_over_m=qm, half_dt=0.5 * dt)
-        s.move(1)
-        den = np.zeros(dk.mesh.n_nodes)
-        st = ctx.push(qm, dt, spwt, den_out=den)
-        rp = s.particles()
-        assert st.n_after == len(rp)
-        if ts % check_every == 0 or ts == steps - 1:
-            g = ctx.download(mp.ORDER_ID)
-            assert np.array_equal(g["cell"], rp["cell_index"]), f"cell mismatch at step {ts}"
-            assert np.array_equal(g["pos"], rp["pos"]), f"pos mismatch at step {ts}"
-            assert np.array_equal(g["vel"], rp["vel"]), f"vel mismatch at step {ts}"
-            assert np.array_equal(g["lc"], rp["lc"]), f"lc mismatch at step {ts}"
-            assert np.all(np.diff(g["id"]) > 0)
-        e = _den_close(den, s.get("den"))
-        worst = max(worst, e)
-        assert e < DEN_RTOL, f"density rel error {e} at step {ts}"
-        s.compute_phi(method)
-        s.update_ef()
-        ctx.fe_set("ef", s.get("ef"))
-    return worst, s, ctx
 
 
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
