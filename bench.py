@@ -1,25 +1,36 @@
-"""Benchmark of the mini-pic hot path on B200: MoveParticles (push + tet walk +
-density scatter + removal + normalisation) and FESolver's Newton step.
+"""Benchmark of the mini-pic hot path on B200: InjectIons -> MoveParticles
+(push + tet walk + density scatter + removal + normalisation) -> computePhi
+(Poisson-Boltzmann Newton step) -> updateEf, in the mixed-precision form and
+the FP64 form side by side.
 
-    python bench.py [--gpus N --steps K --warmup W] [--config 1] [--impl reference]
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+                    [--legs all|none|kuhn20,nonlinear,adjoint,sparse64,vtk]
+    python bench.py --horizon 500     # mixed vs FP64 error growth over a long run
+    python bench.py --stress          # the combined-stress workload (40^3 box, 200M ions)
 
-Workload (default): the 20x20x20-hex Kuhn box (48,000 tets, 9,261 nodes,
-8,379 unknowns), O+ ions, n0 = 1e10 m^-3, 7 km/s drift + 0.1 eV Maxwellian,
-dt = 5e-8 s, spwt = 5 -> about 2M live ions, seeded synthetic population at
-steady state plus the reference injector's ~7,000 new ions per step.  A step
-is InjectIons -> MoveParticles -> computePhi (Lapack method: one Newton step,
-direct solve) -> updateEf.  FP64 form; the mixed form is measured beside it
-on the same seeded population with its errors against FP64.
+Headline workload (the metric's mixed-precision configuration): the 32^3-hex
+Kuhn box minus the centred r = 0.02 m sphere held at -10 V (189,972 tets,
+35,156 nodes, 32,244 unknowns; dense FP64 Jacobian 8.3 GB), O+ ions seeded at
+steady state (48.3M inside the domain: drift 7 km/s + 0.1 eV Maxwellian),
+spwt 0.2, dt 5e-8 s, the reference's per-face injection counts every step
+(about 175k ions), a tet re-sort every 10 steps.  A step is InjectIons ->
+MoveParticles -> computePhi (Lapack method: one Newton step, dense LDL^T) ->
+updateEf.  The synthetic seeded population stands in for a physical run.
 
-value      particle-steps/s of MoveParticles, device-resident inputs (each
-           step's ions injected on the device), L2 flushed between steps
-e2e        the same through the C ABI with host buffers: the step's injected
-           particles H2D from host memory, node density D2H each step
-e2e_full_step    the whole step through the C ABI (adds computePhi, updateEf
-           and the potential D2H)
-newton_step_ms   computePhi device time per step
-N > 1: weak scaling, every rank pushes its own 2M-ion shard; the node density
-is summed over ranks (NCCL all-reduce) before the replicated field solve.
+value        particle-steps/s of the mixed form's whole step (device-resident:
+             ions injected on the device), sum of particles pushed / sum of the
+             steps' device time (CUDA events on the context's stream)
+fp64         the same for the FP64 form in lockstep on the same population
+errors_vs_fp64   the mixed form against the FP64 form on the same seeded run
+e2e          the mixed whole step through the C ABI with host buffers: the
+             step's injected ions H2D from host memory, node density and
+             potential D2H into host memory
+roofline     the kernel class with the largest device time in the mixed step
+roofline_push    the push kernels on the 20^3 box (2M ions, no particle IDs)
+N > 1: weak scaling.  Every rank pushes its own seeded population with its own
+device injections (weights spwt/N, so the summed density is the single-GPU
+one); the node density is summed over ranks (NCCL all-reduce in place) before
+the replicated field solve.
 """
 from __future__ import annotations
 
@@ -29,7 +40,6 @@ import os
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -44,24 +54,36 @@ from minipic_b200 import kuhn, sharding, workloads  # noqa: E402
 METRIC = "particle-steps/sec and Newton-step ms on 1 B200: mixed vs FP64 at stated error"
 KTI_EV = workloads.KTI_EV
 CONFIGS = workloads.CONFIGS
-make_workload = workloads.make_workload
+HEADLINE = 2
 FLUSH_BYTES = 512 << 20
-# DRAM bytes of one k_push_fp64 launch on the 2M-ion workload, from ncu
-# (dram__bytes_read.sum 113.3 MB + dram__bytes_write.sum 45.6 MB)
-PUSH_TRAFFIC_BYTES = 158_962_176
 SORT_PERIOD = 10
+POP_SEED = 4321
+QM = mp.QE / (16 * mp.AMU)
+SIGMA = float(np.sqrt(KTI_EV * mp.QE / (16 * mp.AMU)))
+LEGS = ("kuhn20", "nonlinear", "adjoint", "sparse64", "vtk")
+KT_NAMES = {mp.KT_PUSH: "push", mp.KT_UPDATE: "trailing_update", mp.KT_DIAG: "diagonal_factor",
+            mp.KT_PANEL: "panel", mp.KT_TRSV: "triangular_solve"}
+KT_KERNEL = {mp.KT_PUSH: {mp.FP64: "k_push_fp64", mp.MIXED: "k_push_mixed"},
+             mp.KT_UPDATE: {mp.FP64: "k_update_f64", mp.MIXED: "tc::k_update_tc<true> (3xTF32, tcgen05)"},
+             mp.KT_DIAG: {mp.FP64: "k_ldlt_diag<double>", mp.MIXED: "k_ldlt_diag<float>"},
+             mp.KT_PANEL: {mp.FP64: "k_ldlt_panel<double>", mp.MIXED: "k_ldlt_panel<float>"},
+             mp.KT_TRSV: {mp.FP64: "k_trsv_fwd/bwd<double>", mp.MIXED: "k_trsv_fwd/bwd<float>"}}
 
 
 def peaks():
+    """HBM copy GB/s and dense bf16 TFLOP/s (burst, sustained) measured on this
+    pool's B200s, else the pool's earlier measurement."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "bf16_tflops_sustained": float(d.get("bf16_tflops_sustained", d["bf16_tflops"])),
+                "kind": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "kind": "fallback"}
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling of the SM clock and throttle reasons during a timed region."""
 
     def __init__(self, device):
         self.device = device
@@ -106,257 +128,329 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def run_form(form, args, cfg, deck, pop, inj_batches, device, rank, world, torch, flush, measure_e2e):
-    """Runs warm-up + timed steps for one arithmetic form; returns a dict."""
-    pos, vel, cell = pop
-    m = deck.mesh
-    ctx = mp.Context(m, device=device)
-    fe = deck.fe_desc_arrays()
-    ctx.fe_setup(**fe)
-    ctx.set_track_ids(False)
-    ctx.reserve(int(len(cell) * 1.3) + 100_000)
-    ctx.append(pos, vel, cell)
-    ctx.sort_by_tet()  # a steady-state population has been sorted before
-    ctx.set_sort_period(SORT_PERIOD)
-    if form == mp.MIXED:
-        ctx.set_form(mp.MIXED)
-    qm = mp.QE / (16 * mp.AMU)
-    dt, spwt = cfg["dt"], cfg["spwt"] / world
-    stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
-    # device-resident steps inject on the device (the reference's counts, Philox
-    # Maxwellian sampling); the end-to-end steps upload the host injector's ions
-    inj_dev = mp.Injector(m, seed=rank)
-    P = deck.params
-    sigma = np.sqrt(KTI_EV * mp.QE / (16 * mp.AMU))
-    torch.cuda.synchronize(device)
+def workload_config(cfg, n_tets, n_nodes, neq, n_ions):
+    """The workload description both arms print (same keys and values)."""
+    return {"workload": cfg["label"], "mesh_hexes": cfg["n"] ** 3, "tets": int(n_tets), "nodes": int(n_nodes),
+            "unknowns": int(neq), "ions": int(n_ions), "dt": cfg["dt"], "spwt": cfg["spwt"],
+            "sphere_potential_V": workloads.SPHERE_POTENTIAL if cfg["sphere"] else None,
+            "method": "lapack (one Newton step per step)",
+            "injection": "the reference's per-face counts every step",
+            "population": f"seeded steady state (seed {POP_SEED}): uniform, 7 km/s drift + {KTI_EV} eV Maxwellian"}
 
-    def step(k, host):
-        if host:
-            hp, hv, hc = inj_batches[k % len(inj_batches)]
-            ctx.append(hp, hv, hc, rewind=True, q_over_m=qm, half_dt=0.5 * dt)
-            st = ctx.push(qm, dt, spwt, den_out=den_host)
-        else:
-            ctx.inject_device(inj_dev, P.plasma_den, P.ion_velocity, dt, cfg["spwt"], sigma, qm, 1000 + rank, k)
-            st = ctx.push(qm, dt, spwt)
+
+def make_context(deck, fe, form, n_pop, device, track_ids, sphere):
+    c = mp.Context(deck.mesh, device=device)
+    c.fe_setup(**fe)
+    c.set_track_ids(track_ids)
+    if sphere:
+        # an ion stepping into the sphere lies in no tet; the reference's greedy walk
+        # can cycle around the cavity: walks end at 256 hops and the ion is absorbed
+        workloads.absorb_cavity_walks(c)
+    c.reserve(int(n_pop * 1.05) + 400_000)
+    return c
+
+
+def load_population(c, pos, vel, cell, form, chunk=8_000_000):
+    for lo in range(0, len(cell), chunk):
+        hi = min(len(cell), lo + chunk)
+        c.append(pos[lo:hi], vel[lo:hi], cell[lo:hi])
+    c.sort_by_tet()  # a steady-state population has been sorted before
+    c.set_sort_period(SORT_PERIOD)
+    if form == mp.MIXED:
+        c.set_form(mp.MIXED)
+
+
+def kernel_roofline(ctx, form, pk, sustained=True):
+    """The kernel classes' device time in the timed region and the roofline of
+    the one with the largest share."""
+    classes = {k: ctx.kernel_timing(k) for k in KT_NAMES}
+    total = sum(v["ms"] for v in classes.values()) or 1.0
+    share = {KT_NAMES[k]: {"launches": v["launches"], "ms": v["ms"], "share": v["ms"] / total}
+             for k, v in classes.items()}
+    top = max(classes, key=lambda k: classes[k]["ms"])
+    v = classes[top]
+    out = {"kernel": KT_KERNEL[top][form], "class": KT_NAMES[top], "launches": v["launches"],
+           "avg_launch_ms": v["ms"] / max(v["launches"], 1)}
+    if top == mp.KT_PUSH:
+        ach = v["work"] / (v["ms"] * 1e-3) / 1e9
+        out.update(bound="hbm", achieved=ach, peak=pk["hbm_gbs"], unit="GB/s", frac=ach / pk["hbm_gbs"],
+                   peak_kind=pk["kind"] + " HBM copy",
+                   algorithmic="(particles before + after the push) x %d B" % (52 if form == mp.FP64 else 28))
+    elif top == mp.KT_UPDATE:
+        ach = v["work"] / (v["ms"] * 1e-3) / 1e12
+        peak = pk["bf16_tflops_sustained"] if sustained else pk["bf16_tflops"]
+        out.update(bound="tensor", achieved=ach, peak=peak, unit="TFLOP/s", frac=ach / peak,
+                   peak_kind=pk["kind"] + (" bf16 dense, sustained" if sustained else " bf16 dense, burst"),
+                   algorithmic="2 flops per multiply-add of the trailing update's lower triangle")
+        if form == mp.MIXED:
+            out["note"] = ("kind::tf32 MMAs run at half the bf16 rate, and the 3xTF32 split issues three per "
+                           "term: issued TF32 rate = 3 x achieved")
+            out["tf32_issued_frac_of_half_bf16_peak"] = 3 * ach / (peak / 2)
+    else:
+        out.update(bound="latency", achieved=None, peak=None, unit=None, frac=None,
+                   note="a serial chain of small launches; no throughput bound applies")
+    out["traffic"] = None
+    out["classes"] = share
+    return out
+
+
+def run_headline(args, device, rank, world, torch, flush, pk):
+    """Mixed and FP64 forms in lockstep on the headline workload; then the
+    mixed form's end-to-end steps through the C ABI."""
+    cfg = CONFIGS[args.config]
+    sphere = cfg["sphere"] is not None
+    wd = tempfile.mkdtemp()
+    kd = workloads.write_deck(cfg, wd)
+    deck = mp.Deck.load(wd)
+    pos, vel, cell = workloads.seed_population(kd, cfg, POP_SEED + rank)
+    fe = workloads.fe_arrays(cfg, deck)
+    neq = int(fe["neq"])
+    n0 = len(cell)
+    P = deck.params
+    dt, spwt = cfg["dt"], cfg["spwt"]
+    spwt_push = spwt / world
+    forms = {"mixed": mp.MIXED, "fp64": mp.FP64}
+    ctxs = {}
+    for name, form in forms.items():
+        c = make_context(deck, fe, form, n0, device, True, sphere)
+        load_population(c, pos, vel, cell, form)
+        ctxs[name] = (c, form, torch.cuda.ExternalStream(c.stream(), device=device))
+    del pos, vel, cell
+    inj = {name: mp.Injector(deck.mesh, seed=rank) for name in forms}
+    res = {k: {"step_ms": [], "newton_ms": [], "push_ms": [], "n": [], "refinements": [], "lost": [], "hops": []}
+           for k in forms}
+    den_err, phi_err = [], []
+    launches0 = {k: v[0].launches() for k, v in ctxs.items()}
+
+    def step(name, k):
+        c, form, _ = ctxs[name]
+        c.inject_device(inj[name], P.plasma_den, P.ion_velocity, dt, spwt, SIGMA, QM, 1000 + rank, k)
+        st = c.push(QM, dt, spwt_push)
         if world > 1:
-            sharding.allreduce_density(ctx, device)
-        nt = ctx.compute_phi(mp.LAPACK, form)
-        ctx.update_ef()
-        if host:
-            ctx._c(mp.lib().mp_field_download(ctx.h, None, mp._p(uh_host), None))
+            sharding.allreduce_density(c, device)
+        nt = c.compute_phi(mp.LAPACK, form)
+        c.update_ef()
         return st, nt
 
-    den_host = np.zeros(m.n_nodes)
-    uh_host = np.zeros(m.n_nodes)
-    for k in range(args.warmup):
-        step(k, False)
-    torch.cuda.synchronize(device)
-    res = {"push_ms": [], "push_call_ms": [], "newton_ms": [], "factor_ms": [], "step_ms": [], "n_before": [],
-           "n_after": [], "hops": [], "near": []}
-    launches0 = ctx.launches()
-    for k in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize(device)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        st, nt = step(args.warmup + k, False)
-        e1.record(stream)
-        e1.synchronize()
-        res["push_ms"].append(st.ms_kernel)
-        res["push_call_ms"].append(st.ms_step)
-        res["newton_ms"].append(nt.ms_total)
-        res["factor_ms"].append(nt.ms_factor)
-        res["step_ms"].append(e0.elapsed_time(e1))
-        res["n_before"].append(st.n_before)
-        res["n_after"].append(st.n_after)
-        res["hops"].append(st.total_hops)
-        res["near"].append(st.near_face_fp64)
-    res["launches"] = ctx.launches() - launches0
-    if measure_e2e:
-        # through the C ABI with host buffers: the step's injected ions H2D from
-        # host memory (with the device-side velocity rewind), MoveParticles, the
-        # node density D2H into host memory; then the rest of the step (field
-        # solve, updateEf, potential D2H) for the full-step figure
-        e2e_ms, full_ms, h2d, d2h = [], [], [], []
-        for k in range(args.steps):
+    clocks = Clocks(device)
+    for k in range(args.warmup + args.steps):
+        timed = k >= args.warmup
+        if k == args.warmup:
+            for c, _, _ in ctxs.values():
+                c.set_kernel_timing(True)
+            launches0 = {n: v[0].launches() for n, v in ctxs.items()}
+            if world > 1:
+                torch.distributed.barrier()
+            clocks.start()
+        dens, uhs = {}, {}
+        for name, (c, form, stream) in ctxs.items():
             flush.zero_()
             torch.cuda.synchronize(device)
-            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-            hp, hv, hc = inj_batches[(args.warmup + args.steps + k) % len(inj_batches)]
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            ctx.append(hp, hv, hc, rewind=True, q_over_m=qm, half_dt=0.5 * dt)
-            st = ctx.push(qm, dt, spwt, den_out=den_host)
+            st, nt = step(name, k)
             e1.record(stream)
-            if world > 1:
-                sharding.allreduce_density(ctx, device)
-            ctx.compute_phi(mp.LAPACK, form)
-            ctx.update_ef()
-            ctx._c(mp.lib().mp_field_download(ctx.h, None, mp._p(uh_host), None))
-            e2.record(stream)
-            e2.synchronize()
-            e2e_ms.append(e0.elapsed_time(e1))
-            full_ms.append(e0.elapsed_time(e2))
-            h2d.append(hp.nbytes + hv.nbytes + hc.nbytes)
-            d2h.append(den_host.nbytes)
-            res.setdefault("e2e_push_n", []).append(st.n_before)
-        res["e2e_ms"] = e2e_ms
-        res["e2e_full_ms"] = full_ms
-        res["h2d"] = float(np.mean(h2d))
-        res["d2h"] = float(np.mean(d2h))
-        res["d2h_full"] = float(np.mean(d2h)) + uh_host.nbytes
-    res["ctx"] = ctx
-    return res
-
-
-def error_metrics(deck, pop, inj_batches, cfg, device, steps=5):
-    """Mixed vs FP64 on the same seeded run: density L2, differing cells, phi."""
-    pos, vel, cell = pop
-    out = []
-    qm = mp.QE / (16 * mp.AMU)
-    dt, spwt = cfg["dt"], cfg["spwt"]
-    ctxs = []
-    for form in (mp.FP64, mp.MIXED):
-        c = mp.Context(deck.mesh, device=device)
-        c.fe_setup(**deck.fe_desc_arrays())
-        c.append(pos, vel, cell)
-        if form == mp.MIXED:
-            c.set_form(mp.MIXED)
-        ctxs.append(c)
-    for k in range(steps):
-        p, v, cc = inj_batches[k % len(inj_batches)]
-        dens, uhs = [], []
-        for form, c in zip((mp.FP64, mp.MIXED), ctxs):
-            c.append(p, v, cc, rewind=True, q_over_m=qm, half_dt=0.5 * dt)
-            den = np.zeros(deck.mesh.n_nodes)
-            c.push(qm, dt, spwt, den_out=den)
-            c.compute_phi(mp.LAPACK, form)
-            c.update_ef()
-            _, uh, _ = c.field()
-            dens.append(den)
-            uhs.append(uh)
-        out.append((np.linalg.norm(dens[1] - dens[0]) / np.linalg.norm(dens[0]), np.abs(uhs[1] - uhs[0]).max()))
-    ga, gb = ctxs[0].download(mp.ORDER_ID), ctxs[1].download(mp.ORDER_ID)
+            e1.synchronize()
+            if timed:
+                r = res[name]
+                r["step_ms"].append(e0.elapsed_time(e1))
+                r["newton_ms"].append(nt.ms_total)
+                r["push_ms"].append(st.ms_kernel)
+                r["n"].append(st.n_before)
+                r["refinements"].append(nt.linear_iterations)
+                r["lost"].append(st.lost)
+                r["hops"].append(st.total_hops)
+            dens[name] = c.density()
+            uhs[name] = c.field()[1]
+        if timed:
+            den_err.append(float(np.linalg.norm(dens["mixed"] - dens["fp64"]) / np.linalg.norm(dens["fp64"])))
+            phi_err.append(float(np.abs(uhs["mixed"] - uhs["fp64"]).max()))
+    clk = clocks.stop()
+    if world > 1:
+        torch.distributed.barrier()
+    out = {"cfg": cfg, "deck": deck, "neq": neq, "n0": n0, "res": res, "clocks": clk,
+           "launches": {n: ctxs[n][0].launches() - launches0[n] for n in ctxs}}
+    out["roofline"] = {n: kernel_roofline(ctxs[n][0], ctxs[n][1], pk) for n in ctxs}
+    for c, _, _ in ctxs.values():
+        c.set_kernel_timing(False)
+    # the solver's own precision: one Newton step of each form from the same state
+    # (d, the accumulated F1) and the same density
+    c64, cm = ctxs["fp64"][0], ctxs["mixed"][0]
+    for nm in ("d", "F1"):
+        cm.fe_set(nm, c64.fe_get(nm))
+    den64 = c64.density()
+    c64.compute_phi(mp.LAPACK, mp.FP64, ion_den=den64)
+    cm.compute_phi(mp.LAPACK, mp.MIXED, ion_den=den64)
+    phi_solve = float(np.abs(cm.field()[1] - c64.field()[1]).max())
+    # cells of the same particles in the two forms
+    ga, gb = c64.download(mp.ORDER_ID), cm.download(mp.ORDER_ID)
     ids = np.union1d(ga["id"], gb["id"])
     ia = np.full(ids.size, -1)
     ib = np.full(ids.size, -1)
     ia[np.searchsorted(ids, ga["id"])] = ga["cell"]
     ib[np.searchsorted(ids, gb["id"])] = gb["cell"]
-    for c in ctxs:
+    del ga, gb
+    out["errors"] = {"density_l2_rel": max(den_err), "density_l2_rel_per_step": den_err,
+                     "phi_closed_loop_max_abs_V": max(phi_err), "phi_closed_loop_per_step_V": phi_err,
+                     "phi_solve_max_abs_V": phi_solve, "cells_differing_frac": float(np.mean(ia != ib)),
+                     "steps_compared": args.steps + args.warmup,
+                     "what": "the mixed form's density, potential and cells against the FP64 form's on the same "
+                             "seeded run (same population, same device injections); phi_solve: the mixed Newton "
+                             "step against the FP64 one from the same state and density"}
+    # e2e: the mixed form through the C ABI with host buffers
+    cm.set_kernel_timing(False)
+    host_inj = mp.Injector(deck.mesh, seed=100 + rank)
+    batches = [host_inj.sample(P.plasma_den, P.ion_velocity, dt, spwt) for _ in range(args.steps)]
+    stream = ctxs["mixed"][2]
+    den_host = np.zeros(deck.mesh.n_nodes)
+    uh_host = np.zeros(deck.mesh.n_nodes)
+    e2e_ms, e2e_n, h2d = [], [], []
+    for k in range(args.steps):
+        hp, hv, hc = batches[k]
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cm.append(hp, hv, hc, rewind=True, q_over_m=QM, half_dt=0.5 * dt)
+        st = cm.push(QM, dt, spwt_push, den_out=den_host)
+        if world > 1:
+            sharding.allreduce_density(cm, device)
+        cm.compute_phi(mp.LAPACK, mp.MIXED)
+        cm.update_ef()
+        cm._c(mp.lib().mp_field_download(cm.h, None, mp._p(uh_host), None))
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+        e2e_n.append(st.n_before)
+        h2d.append(hp.nbytes + hv.nbytes + hc.nbytes)
+    out["e2e"] = {"ms": e2e_ms, "n": e2e_n, "h2d": float(np.mean(h2d)), "d2h": float(den_host.nbytes + uh_host.nbytes)}
+    for c, _, _ in ctxs.values():
         c.close()
-    return {"density_l2_rel": float(max(e[0] for e in out)), "phi_max_abs_V": float(max(e[1] for e in out)),
-            "cells_differing_frac": float(np.mean(ia != ib)), "steps": steps}
+    return out
 
 
-def mixed_vs_fp64_at_scale(args, device, torch, flush, steps=3, warmup=2):
-    """The mixed-form workload (32^3 Kuhn box minus the r = 0.02 m sphere at
-    -10 V, ~50M ions): the FP64 and mixed forms run in lockstep on the same
-    seeded population and injections.  Per form: full-step particle-steps/s
-    (inject + push + scatter + computePhi + updateEf, device time), Newton-step
-    ms, push-kernel ms; the mixed form's errors against the FP64 form: node
-    density L2, max |phi| difference per step, and the fraction of particles
-    whose cell differs at the end."""
-    cfg = CONFIGS[2]
-    qm = mp.QE / (16 * mp.AMU)
+def run_kuhn20(args, device, torch, flush, pk):
+    """The FP64 throughput configuration (20^3 box, 2M ions): push-kernel
+    lines of both forms (particle IDs off, re-sort every 10 steps) with their
+    rooflines, and the Newton step of both forms."""
+    cfg = CONFIGS[1]
     with tempfile.TemporaryDirectory() as wd:
-        kd, deck, pos, vel, cell = make_workload(cfg, wd, seed=4321)
+        kd = workloads.write_deck(cfg, wd)
+        deck = mp.Deck.load(wd)
+        pos, vel, cell = workloads.seed_population(kd, cfg, 1234)
         fe = workloads.fe_arrays(cfg, deck)
-        inj = mp.Injector(deck.mesh, seed=0)
         P = deck.params
-        batches = [inj.sample(P.plasma_den, P.ion_velocity, cfg["dt"], cfg["spwt"]) for _ in range(warmup + steps)]
-        ctxs = {}
-        for name, form, method in (("fp64", mp.FP64, mp.LAPACK), ("mixed", mp.MIXED, mp.LAPACK),
-                                   ("fp64_sparse_cg", mp.FP64, mp.SPARSE_CG)):
-            c = mp.Context(deck.mesh, device=device)
-            c.fe_setup(**fe)
-            c.set_track_ids(True)  # for the cell comparison at the end
-            # an ion stepping into the sphere lies in no tet; the reference's greedy walk can
-            # cycle around the cavity without end: absorb such walks (counted) instead
-            c.set_walk_limit(256)
-            c.set_walk_policy(mp.WALK_LIMIT_ABSORB)
-            c.reserve(int(len(cell) * 1.05) + 100_000)
-            c.append(pos, vel, cell)
-            c.sort_by_tet()
-            c.set_sort_period(SORT_PERIOD)
-            if form == mp.MIXED:
-                c.set_form(mp.MIXED)
-            ctxs[name] = (c, form, method, torch.cuda.ExternalStream(c.stream(), device=device))
-        del pos, vel, cell
-        res = {k: {"step_ms": [], "newton_ms": [], "push_ms": [], "n": [], "refinements": [], "lost": []} for k in ctxs}
-        den_err, phi_err, sparse_phi_err = [], [], []
-        for k in range(warmup + steps):
-            hp, hv, hc = batches[k]
-            dens, uhs = {}, {}
-            for name, (c, form, method, stream) in ctxs.items():
+        out = {"workload": cfg["label"], "tets": deck.mesh.n_tets, "unknowns": int(fe["neq"]), "ions": len(cell)}
+        keep = None
+        for name, form in (("fp64", mp.FP64), ("mixed", mp.MIXED)):
+            c = make_context(deck, fe, form, len(cell), device, False, False)
+            load_population(c, pos, vel, cell, form)
+            inj = mp.Injector(deck.mesh, seed=0)
+            newton, push, psteps = [], [], 0
+            for k in range(args.warmup + args.steps):
+                if k == args.warmup:
+                    c.set_kernel_timing(True)
                 flush.zero_()
                 torch.cuda.synchronize(device)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                c.append(hp, hv, hc, rewind=True, q_over_m=qm, half_dt=0.5 * cfg["dt"])
-                st = c.push(qm, cfg["dt"], cfg["spwt"])
-                nt = c.compute_phi(method, form)
+                c.inject_device(inj, P.plasma_den, P.ion_velocity, cfg["dt"], cfg["spwt"], SIGMA, QM, 1000, k)
+                st = c.push(QM, cfg["dt"], cfg["spwt"])
+                nt = c.compute_phi(mp.LAPACK, form)
                 c.update_ef()
-                e1.record(stream)
-                e1.synchronize()
-                if k >= warmup:
-                    r = res[name]
-                    r["step_ms"].append(e0.elapsed_time(e1))
-                    r["newton_ms"].append(nt.ms_total)
-                    r["push_ms"].append(st.ms_kernel)
-                    r["n"].append(st.n_before)
-                    r["refinements"].append(nt.linear_iterations)
-                    r["lost"].append(st.lost)
-                den = np.zeros(deck.mesh.n_nodes)
-                c._c(mp.lib().mp_density_download(c.h, mp._p(den)))
-                _, uh, _ = c.field()
-                dens[name], uhs[name] = den, uh
-            den_err.append(float(np.linalg.norm(dens["mixed"] - dens["fp64"]) / np.linalg.norm(dens["fp64"])))
-            phi_err.append(float(np.abs(uhs["mixed"] - uhs["fp64"]).max()))
-            sparse_phi_err.append(float(np.abs(uhs["fp64_sparse_cg"] - uhs["fp64"]).max()))
-        # the solver's own precision: one Newton step of each form from the same state
-        # (d, the accumulated F1) and the same density, the FP64 context's
-        c64, cm, csp = ctxs["fp64"][0], ctxs["mixed"][0], ctxs["fp64_sparse_cg"][0]
-        for name in ("d", "F1"):
-            v = c64.fe_get(name)
-            cm.fe_set(name, v)
-            csp.fe_set(name, v)
-        c64.compute_phi(mp.LAPACK, mp.FP64, ion_den=dens["fp64"])
-        cm.compute_phi(mp.LAPACK, mp.MIXED, ion_den=dens["fp64"])
-        nt_sp = csp.compute_phi(mp.SPARSE_CG, mp.FP64, ion_den=dens["fp64"])
-        phi_solve_err = float(np.abs(cm.field()[1] - c64.field()[1]).max())
-        sparse_solve_err = float(np.abs(csp.field()[1] - c64.field()[1]).max())
-        ga, gb = ctxs["fp64"][0].download(mp.ORDER_ID), ctxs["mixed"][0].download(mp.ORDER_ID)
-        ids = np.union1d(ga["id"], gb["id"])
-        ia = np.full(ids.size, -1)
-        ib = np.full(ids.size, -1)
-        ia[np.searchsorted(ids, ga["id"])] = ga["cell"]
-        ib[np.searchsorted(ids, gb["id"])] = gb["cell"]
-        for c, _, _, _ in ctxs.values():
-            c.close()
-    out = {"workload": cfg["label"], "mesh_hexes": cfg["n"] ** 3, "tets": deck.mesh.n_tets,
-           "unknowns": int(fe["neq"]), "ions": int(np.mean(res["fp64"]["n"])), "steps": steps, "warmup": warmup,
-           "l2": f"flushed ({FLUSH_BYTES >> 20} MiB write) before each timed step"}
-    for name, r in res.items():
-        out[name] = {"full_step_particle_steps_per_s": float(np.sum(r["n"]) / (np.sum(r["step_ms"]) / 1e3)),
-                     "newton_step_ms": float(np.mean(r["newton_ms"])), "push_kernel_ms": float(np.mean(r["push_ms"])),
-                     "refinement_solves": int(max(r["refinements"])),
-                     "absorbed_at_walk_limit_per_step": float(np.mean(r["lost"]))}
-    out["mixed_over_fp64_full_step"] = (out["mixed"]["full_step_particle_steps_per_s"] /
-                                        out["fp64"]["full_step_particle_steps_per_s"])
-    out["fp64_sparse_cg"].pop("refinement_solves")
-    out["fp64_sparse_cg"]["cg_iterations"] = int(nt_sp.linear_iterations)
-    out["fp64_sparse_cg"]["errors_vs_fp64_lapack"] = {
-        "phi_solve_max_abs_V": sparse_solve_err, "phi_closed_loop_max_abs_V": max(sparse_phi_err),
-        "what": "the FP64 particles with the Newton step's J y = G solved by conjugate gradients on the sparse K "
-                "(||r|| <= 1e-12 ||G||) against the dense LDL^T FP64 step"}
-    out["errors_vs_fp64"] = {"density_l2_rel": max(den_err),
-                             "phi_solve_max_abs_V": phi_solve_err,
-                             "phi_closed_loop_max_abs_V": max(phi_err),
-                             "cells_differing_frac": float(np.mean(ia != ib)), "steps": warmup + steps,
-                             "what": "density and cells: the mixed form's particles against the FP64 form's on "
-                                     "the same seeded run; phi_solve: the mixed Newton step against the FP64 one "
-                                     "from the same state and density; phi_closed_loop: the two runs' potentials, "
-                                     "which also carry their density difference"}
-    return out
+                if k >= args.warmup:
+                    newton.append(nt.ms_total)
+                    push.append(st.ms_kernel)
+                    psteps += st.n_before
+            t = c.kernel_timing(mp.KT_PUSH)
+            ach = t["work"] / (t["ms"] * 1e-3) / 1e9
+            out[name] = {"push_particle_steps_per_s": psteps / (np.sum(push) / 1e3),
+                         "push_kernel_ms": float(np.mean(push)), "newton_step_ms": float(np.mean(newton)),
+                         "roofline": {"kernel": KT_KERNEL[mp.KT_PUSH][form], "bound": "hbm", "achieved": ach,
+                                      "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": ach / pk["hbm_gbs"],
+                                      "launches": t["launches"], "avg_launch_ms": t["ms"] / max(t["launches"], 1),
+                                      "peak_kind": pk["kind"] + " HBM copy",
+                                      "bytes_per_particle_step": 104 if form == mp.FP64 else 56,
+                                      "traffic": None}}
+            if name == "fp64":
+                keep = c
+            else:
+                c.close()
+        return out, keep, deck
+
+
+def run_nonlinear(ctx, deck):
+    """The NonLinear method (Newton with Gauss-Seidel inner solves) from the
+    state the 20^3 FP64 run left: one computePhi, its Newton iterations and
+    sweeps, and the sweep bandwidth (8 neq^2 bytes of J per sweep)."""
+    neq = ctx.neq
+    ctx.set_kernel_timing(False)
+    den = ctx.density()
+    st = mp.NewtonStats()
+    d0, f0 = ctx.fe_get("d"), ctx.fe_get("F1")
+    rc = mp.lib().mp_compute_phi(ctx.h, mp._p(np.ascontiguousarray(den)), mp.NONLINEAR, mp.FP64,
+                                 mp.C.byref(st))
+    ctx.fe_set("d", d0)
+    ctx.fe_set("F1", f0)
+    return {"workload": "kuhn20 NonLinear computePhi (FP64 Gauss-Seidel inner solves)", "status": int(rc),
+            "ms": st.ms_total, "newton_iterations": st.newton_iterations,
+            "gs_sweeps_last_solve": st.linear_iterations, "gs_solves_out_of_sweeps": st.linear_failures,
+            "l2": st.l2}
+
+
+def run_adjoint(args, device, torch, pk):
+    """The adjoint configuration: 16^3 box, 1M ions, K = 20 push + scatter
+    steps, checkpoints every 5; forward, reverse (vector-Jacobian product) and
+    tangent (Jacobian-vector product) device times."""
+    from minipic_b200 import adjoint as adj_mod
+    cfg = CONFIGS[3]
+    with tempfile.TemporaryDirectory() as wd:
+        deck, slots, K = workloads.make_adjoint_case(cfg, wd, seed=77)
+    m = deck.mesh
+    c = mp.Context(m, device=device)
+    c.fe_setup(**deck.fe_desc_arrays())
+    stream = torch.cuda.ExternalStream(c.stream(), device=device)
+    wall = (m.node_type == mp.NODE_FIXED).astype(np.uint8)
+    a = adj_mod.Adjoint(c, K, cfg["checkpoint_every"], QM, 16 * mp.AMU, cfg["dt"], cfg["spwt"],
+                        np.array([1.0, 0.0, 0.0]), wall)
+    workloads.load_adjoint(a, slots)
+    phi = workloads.adjoint_phi(m)
+    rng = np.random.default_rng(3)
+    gbar = rng.standard_normal(m.n_nodes)
+    dphi = rng.standard_normal(m.n_nodes)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), r
+
+    fw, bw, tg = [], [], []
+    for k in range(args.warmup + args.steps):
+        tf, (den, st) = timed(lambda: a.forward(phi, 7000.0))
+        tb, _ = timed(lambda: a.backward(gbar, 1.0))
+        tt, _ = timed(lambda: a.tangent(dphi, 1.0))
+        if k >= args.warmup:
+            fw.append(st.ms)
+            bw.append(tb)
+            tg.append(tt)
+    n_slots = int(st.slots)
+    slot_steps = float(np.sum((K - slots["first"])))
+    C = cfg["checkpoint_every"]
+    # forward: slot inputs read once (6 FP64 + cell + first step + flag = 57 B),
+    # a 52 B checkpoint every C steps, the outcome byte
+    fwd_bytes = n_slots * (57 + 52 * (K // C) + 1)
+    c.close()
+    return {"workload": cfg["label"], "slots": n_slots, "K": K, "checkpoint_every": C,
+            "slot_steps": slot_steps, "forward_ms": float(np.mean(fw)), "reverse_ms": float(np.mean(bw)),
+            "tangent_ms": float(np.mean(tg)),
+            "forward_slot_steps_per_s": slot_steps / (np.mean(fw) / 1e3),
+            "reverse_slot_steps_per_s": slot_steps / (np.mean(bw) / 1e3),
+            "forward_bytes_per_slot_step": fwd_bytes / slot_steps,
+            "forward_hbm_frac": fwd_bytes / (np.mean(fw) * 1e-3) / 1e9 / pk["hbm_gbs"],
+            "what": "one thread carries a slot through its steps in registers; the tet records and field are "
+                    "gathered from L2, so the kernels are gather-latency bound, not HBM bound",
+            "alive": int(st.alive), "wall_exits": int(st.wall_exits)}
 
 
 def sparse_field_at_scale(device, n=64, reps=3):
@@ -393,25 +487,13 @@ def sparse_field_at_scale(device, n=64, reps=3):
         out[key] = {"ms": float(np.mean(ms)), "newton_iterations": int(max(nits)),
                     "cg_iterations_last_solve": int(max(its))}
     c.close()
-    # the mesh setup of the same mesh: the host helpers against the device ones
-    pos, fixed = kd.nodes_mm / 1000.0, np.concatenate([kd.wall_nodes, kd.sphere_nodes])
-    setup = {}
-    for key, dev in (("host_s", None), ("device_s", device), ("device_s", device)):
-        t0 = time.perf_counter()
-        m = mp.Mesh.build(pos, kd.tets, kd.inlet_nodes, kd.inlet_tris, fixed, device=dev)
-        m.fe_geometry(device=dev)
-        setup[key] = time.perf_counter() - t0  # the device entry is timed a second time, warm
-    out["mesh_setup"] = dict(setup, tets=int(m.n_tets),
-                             what="LoadVolumeMesh + LoadSurfaceMesh geometry + FESolver ID/NX/detJ, wall clock "
-                                  "including the host-device copies")
     return out
 
 
 def vtk_output_leg(device, cfg=CONFIGS[2]):
     """OutputMesh of the 32^3 box minus sphere from the device buffers: the time
     until the call returns (snapshot + writer start) and until the file is
-    complete; the reference's own OutputMesh on the same arrays when the
-    oracle library is present (reported beside, as its CPU baseline)."""
+    complete."""
     with tempfile.TemporaryDirectory() as wd:
         kd = kuhn.build(cfg["n"], sphere=cfg["sphere"])
         kuhn.write(kd, wd)
@@ -419,9 +501,8 @@ def vtk_output_leg(device, cfg=CONFIGS[2]):
         c = mp.Context(deck.mesh, device=device)
         c.fe_setup(**deck.fe_desc_arrays(workloads.SPHERE_POTENTIAL))
         rng = np.random.default_rng(3)
-        uh, den = rng.normal(size=deck.mesh.n_nodes), rng.normal(size=deck.mesh.n_nodes)
-        ef = rng.normal(size=(deck.mesh.n_tets, 3))
-        for name, v in (("uh", uh), ("den", den), ("ef", ef)):
+        for name, v in (("uh", rng.normal(size=deck.mesh.n_nodes)), ("den", rng.normal(size=deck.mesh.n_nodes)),
+                        ("ef", rng.normal(size=(deck.mesh.n_tets, 3)))):
             c.fe_set(name, v)
         c.output_mesh(0, wd, deck.mesh.node_type)
         c.output_wait()
@@ -434,96 +515,168 @@ def vtk_output_leg(device, cfg=CONFIGS[2]):
                "bytes": os.path.getsize(os.path.join(wd, "mesh_0002.vtu")), "call_ms": (t1 - t0) * 1e3,
                "file_complete_ms": (t2 - t0) * 1e3}
         c.close()
-        out["reference_ms"] = reference_output_mesh_ms(wd, kd, uh, den, ef)
     return out
 
 
-def reference_output_mesh_ms(wd, kd, uh, den, ef):
-    """CPU baseline of the VTK leg: the reference's OutputMesh (oracle/_ref)."""
-    from oracle import ref
-    if not ref.available():
-        return None
-    s = ref.RefSim(wd, spwt=1.0, extra_fixed={os.path.join(wd, "sphere.dat"): (kd.sphere_nodes, -10.0)})
-    for name, v in (("uh", uh), ("den", den), ("ef", ef)):
-        s.set(name, v)
-    out_dir = os.path.join(wd, "reference")
-    os.makedirs(out_dir)
-    sec = s.L.ref_output_mesh(s.h, 1, out_dir.encode())
-    s.close()
-    return sec * 1e3 if sec >= 0 else None
+# ---- the reference's CPU path (oracle/_ref): the CPU baseline and the reference arm ----
 
-
-def cpu_baseline(cfg, workdir, pop, budget_s=20.0):
-    """The reference's own MoveParticles (oracle/_ref, OpenMP over all host
-    threads) on the same population; one Lapack Newton step if it fits."""
+def reference_sim(cfg, wd, kd, seed, spwt=None):
+    """The reference's own loaders, FESolver and Species on the configuration's
+    deck, with the same seeded population (no call into this library)."""
     from oracle import ref
-    if not ref.available():
-        return None
-    threads = os.cpu_count() or 1
-    s = ref.RefSim(workdir, spwt=cfg["spwt"])
-    pos, vel, cell = pop
+    extra = {}
+    if cfg["sphere"]:
+        extra = {os.path.join(wd, "sphere.dat"): (kd.sphere_nodes, workloads.SPHERE_POTENTIAL)}
+    s = ref.RefSim(wd, spwt=cfg["spwt"] if spwt is None else spwt, extra_fixed=extra)
+    pos, vel, cell = workloads.seed_population(kd, cfg, seed)
     parts = np.zeros(len(cell), dtype=ref.PARTICLE_DTYPE)
     parts["pos"], parts["vel"], parts["cell_index"] = pos, vel, cell
+    del pos, vel
     s.set_particles(parts)
-    rate1, sec1 = s.time_move(1, threads)
-    steps = int(max(1, min(50, budget_s / max(sec1, 1e-3))))
-    s.set_particles(parts)
-    rate, sec = s.time_move(steps, threads)
-    t0 = time.perf_counter()
-    s.compute_phi(ref.LAPACK)
-    s.update_ef()
-    newton_ms = (time.perf_counter() - t0) * 1e3
-    s.close()
-    return {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
-            "sample": f"{steps} MoveParticles steps on the full {len(cell)}-ion population "
-                      f"({sec:.1f} s) + 1 Lapack Newton step",
-            "newton_step_ms": newton_ms}
+    return s, len(cell)
+
+
+def cpu_baseline(config, budget_s=25.0):
+    """The reference's MoveParticles with its InjectIons (oracle/_ref, OpenMP
+    over all host threads) on the headline population, a bounded number of
+    steps; the reference's Newton step at this size (dense dsysv_ on 32,244
+    unknowns, minutes) is timed by the reference arm instead."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    cfg = CONFIGS[config]
+    threads = ref.max_threads()
+    with tempfile.TemporaryDirectory() as wd:
+        kd = workloads.write_deck(cfg, wd)
+        s, n0 = reference_sim(cfg, wd, kd, POP_SEED)
+        s.inject()
+        s.move(threads)  # first touch of the population
+        psteps, sec, steps = 0.0, 0.0, 0
+        while sec < budget_s and steps < 20:
+            t0 = time.perf_counter()
+            s.inject()
+            n_before = s.L.ref_n_particles(s.h)
+            s.move(threads)
+            sec += time.perf_counter() - t0
+            psteps += n_before
+            steps += 1
+        s.close()
+    return {"value": psteps / sec, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+            "sample": f"{steps} InjectIons + MoveParticles steps of the reference on the headline workload's "
+                      f"{n0}-ion population ({sec:.1f} s); the Newton step is excluded (the reference arm times it)"}
 
 
 def reference_arm(args):
-    """--impl reference: the reference's own CPU path (oracle/_ref) timed on the
-    host cores, same config/metric; rank 0 only."""
+    """--impl reference: the reference's own CPU path (oracle/_ref: its
+    translation units, OpenMP over the host threads, OpenBLAS dsysv_) on the
+    headline workload: W + K steps of InjectIons + MoveParticles on the full
+    population, and one Newton step (Lapack) + updateEf as the bounded sample
+    of the field solve.  Rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cfg = CONFIGS[args.config]
     from oracle import ref
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_oracle.so was not built"}))
         return
+    cfg = CONFIGS[args.config]
+    threads = ref.max_threads()
     with tempfile.TemporaryDirectory() as wd:
-        kd, deck, pos, vel, cell = make_workload(cfg, wd, seed=1234)
-        threads = os.cpu_count() or 1
-        s = ref.RefSim(wd, spwt=cfg["spwt"])
-        parts = np.zeros(len(cell), dtype=ref.PARTICLE_DTYPE)
-        parts["pos"], parts["vel"], parts["cell_index"] = pos, vel, cell
-        s.set_particles(parts)
-        for _ in range(max(1, args.warmup)):
+        kd = workloads.write_deck(cfg, wd)
+        s, n0 = reference_sim(cfg, wd, kd, POP_SEED)
+        push_s, psteps = [], []
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            s.inject()
+            nb = s.L.ref_n_particles(s.h)
             s.move(threads)
-        rate, sec = s.time_move(args.steps, threads)
-        n_live = len(s.particles())
+            if k >= args.warmup:
+                push_s.append(time.perf_counter() - t0)
+                psteps.append(nb)
         t0 = time.perf_counter()
         s.compute_phi(ref.LAPACK)
+        newton_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
         s.update_ef()
-        newton_ms = (time.perf_counter() - t0) * 1e3
-        full_rate = n_live / (sec / args.steps + newton_ms / 1e3)
-        line = {"metric": METRIC, "value": rate, "unit": "particle-steps/s", "impl": "reference",
-                "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": cfg["label"], "mesh_hexes": cfg["n"] ** 3,
-                                                "tets": deck.mesh.n_tets, "nodes": deck.mesh.n_nodes,
-                                                "unknowns": int(deck.fe_desc_arrays()["neq"]),
-                                                "ions_per_gpu": int(len(cell)), "dt": cfg["dt"],
-                                                "method": "lapack (1 Newton step)", "form": "fp64",
-                                                "device": f"host CPU, {threads} OpenMP threads"},
-                "newton_step_ms": newton_ms,
-                "full_step_particle_steps_per_s": full_rate,
-                "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
-                                 "sample": f"{args.steps} MoveParticles steps, OpenMP over {threads} threads"},
-                "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
+        ef_s = time.perf_counter() - t0
+        conf = workload_config(cfg, s.n_tets, s.n_nodes, s.neq, n0)
         s.close()
+    step_s = float(np.mean(push_s)) + newton_s + ef_s
+    value = float(np.mean(psteps)) / step_s
+    line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "impl": "reference",
+            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Kuhn-box ions at steady state; the reference's own injector)",
+            "config": conf, "device": f"host CPU, {threads} OpenMP threads (the reference's CPU path)",
+            "newton_step_ms": newton_s * 1e3, "push_step_ms": float(np.mean(push_s)) * 1e3,
+            "push_particle_steps_per_s": float(np.sum(psteps) / np.sum(push_s)),
+            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                             "sample": f"{args.steps} timed InjectIons + MoveParticles steps on the full population "
+                                       f"after {args.warmup} untimed, plus one Lapack Newton step (dsysv_ on "
+                                       f"{conf['unknowns']} unknowns) and updateEf; value = mean particles per "
+                                       f"step / (mean push step + Newton step + updateEf)"},
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+# ---- long runs ----
+
+def run_horizon(args, device, torch):
+    """Mixed vs FP64 over a long run of the headline workload: per step the
+    density L2 error and the closed-loop potential difference, every 50 steps
+    the fraction of particles in different cells."""
+    cfg = CONFIGS[args.config]
+    wd = tempfile.mkdtemp()
+    kd = workloads.write_deck(cfg, wd)
+    deck = mp.Deck.load(wd)
+    pos, vel, cell = workloads.seed_population(kd, cfg, POP_SEED)
+    fe = workloads.fe_arrays(cfg, deck)
+    P = deck.params
+    ctxs = {}
+    for name, form in (("fp64", mp.FP64), ("mixed", mp.MIXED)):
+        c = make_context(deck, fe, form, len(cell), device, True, cfg["sphere"] is not None)
+        load_population(c, pos, vel, cell, form)
+        ctxs[name] = c
+    del pos, vel, cell
+    inj = {n: mp.Injector(deck.mesh, seed=0) for n in ctxs}
+    rows = []
+    t_start = time.time()
+    for k in range(args.horizon):
+        den, uh, n = {}, {}, {}
+        for name, c in ctxs.items():
+            form = mp.FP64 if name == "fp64" else mp.MIXED
+            c.inject_device(inj[name], P.plasma_den, P.ion_velocity, cfg["dt"], cfg["spwt"], SIGMA, QM, 1000, k)
+            st = c.push(QM, cfg["dt"], cfg["spwt"])
+            c.compute_phi(mp.LAPACK, form)
+            c.update_ef()
+            den[name], uh[name], n[name] = c.density(), c.field()[1], st.n_after
+        row = {"step": k, "density_l2_rel": float(np.linalg.norm(den["mixed"] - den["fp64"]) /
+                                                  np.linalg.norm(den["fp64"])),
+               "phi_max_abs_V": float(np.abs(uh["mixed"] - uh["fp64"]).max()),
+               "n_fp64": n["fp64"], "n_mixed": n["mixed"]}
+        if k % 50 == 49 or k == args.horizon - 1:
+            ga, gb = ctxs["fp64"].download(mp.ORDER_ID), ctxs["mixed"].download(mp.ORDER_ID)
+            ids = np.union1d(ga["id"], gb["id"])
+            ia = np.full(ids.size, -1)
+            ib = np.full(ids.size, -1)
+            ia[np.searchsorted(ids, ga["id"])] = ga["cell"]
+            ib[np.searchsorted(ids, gb["id"])] = gb["cell"]
+            row["cells_differing_frac"] = float(np.mean(ia != ib))
+            del ga, gb
+        rows.append(row)
+    for c in ctxs.values():
+        c.close()
+    d = np.array([r["density_l2_rel"] for r in rows])
+    ph = np.array([r["phi_max_abs_V"] for r in rows])
+    cells = [(r["step"], r["cells_differing_frac"]) for r in rows if "cells_differing_frac" in r]
+    print(json.dumps({"horizon": args.horizon, "workload": cfg["label"], "wall_s": time.time() - t_start,
+                      "density_l2_rel": {"max": float(d.max()), "median": float(np.median(d)), "last": float(d[-1]),
+                                         "per_50": [float(d[i:i + 50].max()) for i in range(0, len(d), 50)]},
+                      "phi_closed_loop_max_abs_V": {"max": float(ph.max()), "median": float(np.median(ph)),
+                                                    "last": float(ph[-1]),
+                                                    "per_50": [float(ph[i:i + 50].max()) for i in range(0, len(ph), 50)]},
+                      "cells_differing_frac": cells,
+                      "ions_last": {"fp64": rows[-1]["n_fp64"], "mixed": rows[-1]["n_mixed"]}}))
 
 
 def main():
@@ -531,14 +684,17 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", type=int, default=1, choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-scale", action="store_true", help="skip the mixed-vs-FP64 run on the 32^3 sphere workload")
+    ap.add_argument("--config", type=int, default=HEADLINE, choices=sorted(CONFIGS),
+                    help="workload of the headline step (default: the mixed-precision configuration)")
+    ap.add_argument("--legs", default="all", help="secondary legs: all, none, or a comma list of " + ",".join(LEGS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--horizon", type=int, default=0, help="run the long mixed-vs-FP64 comparison instead")
+    ap.add_argument("--stress", action="store_true", help="run the combined-stress workload instead")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    legs = set(LEGS) if args.legs == "all" else set() if args.legs == "none" else set(args.legs.split(","))
     if args.impl == "reference":
         reference_arm(args)
         return
@@ -547,131 +703,96 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    if args.horizon:
+        run_horizon(args, local, torch)
+        return
+    if args.stress:
+        from minipic_b200 import stress
+        print(json.dumps(stress.run(args, local, torch, peaks())))
+        return
     if world > 1:
         import datetime
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
-    cfg = CONFIGS[args.config]
-    hbm_peak, peak_kind = peaks()
-    with tempfile.TemporaryDirectory() as wd:
-        kd, deck, pos, vel, cell = make_workload(cfg, wd, seed=1234 + rank)
-        pop = (pos, vel, cell)
-        inj = mp.Injector(deck.mesh, seed=rank)
-        P = deck.params
-        n_batches = args.warmup + 2 * args.steps
-        batches = []
-        for _ in range(n_batches):
-            p, v, c = inj.sample(P.plasma_den, P.ion_velocity, cfg["dt"], cfg["spwt"])
-            batches.append((np.ascontiguousarray(p), np.ascontiguousarray(v), np.ascontiguousarray(c)))
-        flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=local)
-        clocks = Clocks(local)
-        if world > 1:
-            torch.distributed.barrier()
-        clocks.start()
-        r64 = run_form(mp.FP64, args, cfg, deck, pop, batches, local, rank, world, torch, flush, True)
-        clk = clocks.stop()
-        r32 = None
-        if not args.no_mixed:
-            r32 = run_form(mp.MIXED, args, cfg, deck, pop, batches, local, rank, world, torch, flush, False)
-        errors = None
-        if not args.no_mixed and rank == 0 and world == 1:
-            errors = error_metrics(deck, pop, batches, cfg, local)
-        cpu = None
-        if rank == 0 and world == 1 and not args.no_cpu:
-            cpu = cpu_baseline(cfg, wd, pop)
-    scale = sparse_big = vtk = None
-    if rank == 0 and world == 1 and not args.no_scale and args.config == 1:
-        scale = mixed_vs_fp64_at_scale(args, local, torch, flush)
-        sparse_big = sparse_field_at_scale(local)
-        vtk = vtk_output_leg(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    pk = peaks()
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=local)
+    h = run_headline(args, local, rank, world, torch, flush, pk)
+    extra = {}
+    if rank == 0 and world == 1:
+        if "kuhn20" in legs or "nonlinear" in legs:
+            k20, ctx20, deck20 = run_kuhn20(args, local, torch, flush, pk)
+            extra["kuhn20_2M"] = k20
+            if "nonlinear" in legs:
+                extra["nonlinear_kuhn20"] = run_nonlinear(ctx20, deck20)
+            ctx20.close()
+        if "adjoint" in legs:
+            extra["adjoint_kuhn16_1M_K20"] = run_adjoint(args, local, torch, pk)
+        if "sparse64" in legs:
+            extra["sparse_field_kuhn64s"] = sparse_field_at_scale(local)
+        if "vtk" in legs:
+            extra["vtk_output"] = vtk_output_leg(local)
+    cpu = cpu_baseline(args.config) if (rank == 0 and world == 1 and not args.no_cpu) else None
 
-    def agg(r):
-        push_ms = np.array(r["push_ms"])
-        nb, na = np.array(r["n_before"], float), np.array(r["n_after"], float)
-        step_ms = np.array(r["step_ms"])
-        return push_ms, nb, na, step_ms
-
-    push_ms, nb, na, step_ms = agg(r64)
-    psteps = nb.sum()
-    push_call_s = np.sum(r64["push_call_ms"]) / 1e3
-    e2e_n = float(np.sum(r64["e2e_push_n"]))
-    stats = np.array([psteps, push_call_s, step_ms.sum() / 1e3, np.sum(r64["e2e_ms"]) / 1e3,
-                      np.mean(r64["newton_ms"]), e2e_n, np.sum(r64["e2e_full_ms"]) / 1e3], dtype=np.float64)
+    res = h["res"]
+    stats = []
+    for name in ("mixed", "fp64"):
+        r = res[name]
+        stats += [float(np.sum(r["n"])), float(np.sum(r["step_ms"]) / 1e3), float(np.mean(r["newton_ms"])),
+                  float(np.sum(r["push_ms"]) / 1e3)]
+    stats += [float(np.sum(h["e2e"]["n"])), float(np.sum(h["e2e"]["ms"]) / 1e3)]
     if world > 1:
-        t = torch.tensor(stats, device=local)
-        tmax = t.clone()
+        t = torch.tensor(stats, dtype=torch.float64, device=local)
+        tmax, tsum = t.clone(), t.clone()
         torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
-        tsum = t.clone()
         torch.distributed.all_reduce(tsum, op=torch.distributed.ReduceOp.SUM)
-        psteps_all, e2e_n_all = float(tsum[0]), float(tsum[5])
-        push_s, step_s, e2e_s, newton_ms = float(tmax[1]), float(tmax[2]), float(tmax[3]), float(tmax[4])
-        e2e_full_s = float(tmax[6])
+        tot = [float(tsum[i]) if i in (0, 4, 8) else float(tmax[i]) for i in range(len(stats))]
     else:
-        psteps_all, e2e_n_all = psteps, e2e_n
-        push_s, step_s, e2e_s, newton_ms, e2e_full_s = stats[1], stats[2], stats[3], stats[4], stats[6]
+        tot = stats
     if rank == 0:
-        bytes_per = 52.0  # pos 24 + vel 24 + tet 4, read and written once (FP64 SoA)
-        alg_bytes = (nb + na) * bytes_per
-        achieved = float(np.mean(alg_bytes / (push_ms * 1e-3)) / 1e9)
+        m_ps, m_s, m_newton, m_push, f_ps, f_s, f_newton, f_push, e_ps, e_s = tot
+        cfg, deck = h["cfg"], h["deck"]
+        conf = workload_config(cfg, deck.mesh.n_tets, deck.mesh.n_nodes, h["neq"], h["n0"])
+        rm, rf = res["mixed"], res["fp64"]
         line = {
-            "metric": METRIC, "value": psteps_all / push_s, "unit": "particle-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(step_s / args.steps * 1e3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded Kuhn-box ions at steady state + reference injector)",
-            "config": {"workload": cfg["label"], "mesh_hexes": cfg["n"] ** 3, "tets": deck.mesh.n_tets,
-                       "nodes": deck.mesh.n_nodes, "unknowns": int(deck.fe_desc_arrays()["neq"]),
-                       "ions_per_gpu": int(np.mean(nb)), "dt": cfg["dt"], "method": "lapack (1 Newton step)",
-                       "form": "fp64", "l2": f"flushed ({FLUSH_BYTES >> 20} MiB write) between timed steps",
-                       "tet_sort_every": SORT_PERIOD,
-                       "injection": "device (the reference's per-face counts; Philox4x32-10 positions and "
-                                    "0.1 eV Maxwellian velocities) in the device-resident steps; the host "
-                                    "injector's ions uploaded in the end-to-end steps",
-                       "parallelism": f"particles sharded x{world}, density all-reduce" if world > 1 else "1 GPU"},
-            "newton_step_ms": float(newton_ms),
-            "full_step_particle_steps_per_s": psteps_all / step_s,
-            "push_kernel_ms": float(np.mean(push_ms)),
-            "hops_per_particle_step": float(np.sum(r64["hops"]) / psteps),
-            "e2e": {"value": e2e_n_all / e2e_s, "unit": "particle-steps/s",
-                    "what": "MoveParticles through the C ABI: injected ions H2D from host memory, push + walk + "
-                            "scatter + normalisation, node density D2H to host memory",
-                    "h2d_bytes_per_step": int(r64["h2d"]), "d2h_bytes_per_step": int(r64["d2h"]),
-                    "ms_per_step": float(e2e_s / args.steps * 1e3)},
-            "e2e_full_step": {"value": e2e_n_all / e2e_full_s, "unit": "particle-steps/s",
-                              "what": "the whole step through the C ABI: InjectIons H2D, MoveParticles, computePhi "
-                                      "(Lapack, one Newton step), updateEf, density and potential D2H",
-                              "h2d_bytes_per_step": int(r64["h2d"]), "d2h_bytes_per_step": int(r64["d2h_full"]),
-                              "ms_per_step": float(e2e_full_s / args.steps * 1e3)},
-            "gpu_launches": int(r64["launches"]),
-            "roofline": {"kernel": "k_push_fp64", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                         "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": PUSH_TRAFFIC_BYTES,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_push_fp64 "
-                                           "launch on this workload",
-                         "peak_kind": peak_kind,
-                         "bytes_per_particle_step": 104},
-            "clocks": clk,
+            "metric": METRIC, "value": m_ps / m_s, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": m_s / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded Kuhn-box ions at steady state; device injection with the reference's counts)",
+            "config": conf,
+            "form": "mixed: FP32 tet-relative particles, FP64 near-face test and density, 3xTF32 tcgen05 LDL^T "
+                    "with FP64 refinement",
+            "parallelism": f"particles sharded x{world}, density all-reduce, field solve replicated"
+            if world > 1 else "1 GPU",
+            "l2": f"inputs larger than L2 (the particle arrays); {FLUSH_BYTES >> 20} MiB written between steps",
+            "newton_step_ms": m_newton,
+            "push_kernel_ms": m_push / args.steps * 1e3,
+            "fp64": {"value": f_ps / f_s, "unit": "particle-steps/s", "ms_per_step": f_s / args.steps * 1e3,
+                     "newton_step_ms": f_newton, "push_kernel_ms": f_push / args.steps * 1e3,
+                     "roofline": h["roofline"]["fp64"]},
+            "mixed_over_fp64": (m_ps / m_s) / (f_ps / f_s),
+            "errors_vs_fp64": h["errors"],
+            "refinement_solves": int(max(rm["refinements"])),
+            "absorbed_at_walk_limit_per_step": float(np.mean(rm["lost"])),
+            "hops_per_particle_step": float(np.sum(rm["hops"]) / max(np.sum(rm["n"]), 1)),
+            "e2e": {"value": e_ps / e_s, "unit": "particle-steps/s",
+                    "what": "the mixed whole step through the C ABI: the host injector's ions H2D from host "
+                            "memory (velocity rewind on the device), MoveParticles, computePhi, updateEf, node "
+                            "density and potential D2H to host memory",
+                    "h2d_bytes_per_step": int(h["e2e"]["h2d"]), "d2h_bytes_per_step": int(h["e2e"]["d2h"]),
+                    "ms_per_step": e_s / args.steps * 1e3},
+            "gpu_launches": int(h["launches"]["mixed"]),
+            "gpu_launches_fp64": int(h["launches"]["fp64"]),
+            "roofline": h["roofline"]["mixed"],
+            "clocks": h["clocks"],
         }
-        if r32 is not None:
-            pm, nb32, na32, sm32 = agg(r32)
-            ach32 = float(np.mean((nb32 + na32) * 28.0 / (pm * 1e-3)) / 1e9)
-            line["mixed"] = {
-                "value": float(nb32.sum() / (np.sum(r32["push_call_ms"]) / 1e3)),
-                "full_step_particle_steps_per_s": float(nb32.sum() / (sm32.sum() / 1e3)),
-                "newton_step_ms": float(np.mean(r32["newton_ms"])),
-                "push_kernel_ms": float(np.mean(pm)),
-                "roofline": {"kernel": "k_push_mixed", "bound": "hbm", "achieved": ach32, "peak": hbm_peak,
-                             "unit": "GB/s", "frac": ach32 / hbm_peak, "bytes_per_particle_step": 56},
-                "near_face_fp64_per_step": float(np.mean(r32["near"])),
-                "errors_vs_fp64": errors,
-            }
+        if "kuhn20_2M" in extra:
+            line["roofline_push"] = {"fp64": extra["kuhn20_2M"]["fp64"]["roofline"],
+                                     "mixed": extra["kuhn20_2M"]["mixed"]["roofline"],
+                                     "workload": "kuhn20_2M (20^3 box, 2M ions, particle IDs off)"}
+        line.update(extra)
         if cpu is not None:
             line["cpu_baseline"] = cpu
-        if scale is not None:
-            line["mixed_vs_fp64_kuhn32s_50M"] = scale
-        if sparse_big is not None:
-            line["sparse_field_kuhn64s"] = sparse_big
-        if vtk is not None:
-            line["vtk_output"] = vtk
         print(json.dumps(line))
     if world > 1:
         torch.distributed.barrier()

@@ -214,6 +214,22 @@ int mp_set_track_ids(mp_ctx *ctx, int on);
 int mp_device_buffer(mp_ctx *ctx, int which, void **ptr, int64_t *len);
 /* Kernels this context has launched since creation (for launch accounting). */
 int mp_kernel_launches(mp_ctx *ctx, int64_t *n);
+/* Device time of kernel classes, for roofline accounting (no reference
+ * counterpart; the reference's trace.csv times host functions, src/trace.cpp).
+ * While on, CUDA events bracket every launch of the classes below and each
+ * call reads them after its own synchronisation; turning it on resets the
+ * clocks.  work: algorithmic bytes for MP_KT_PUSH ((particles before + after
+ * the push) x the form's bytes per particle, 52 FP64 / 28 mixed), algorithmic
+ * flops for MP_KT_UPDATE (2 per multiply-add of the trailing update's lower
+ * triangle; the 3xTF32 split issues three tensor-core products per term and
+ * counts once), 0 for the latency-bound classes. */
+enum { MP_KT_PUSH = 0,    /* the push + walk + scatter kernel */
+       MP_KT_UPDATE = 1,  /* trailing updates of the LDL^T: tcgen05 (mixed) or register-tiled FP64 */
+       MP_KT_DIAG = 2,    /* diagonal-block factorizations */
+       MP_KT_PANEL = 3,   /* panels, in-panel column updates and operand splits */
+       MP_KT_TRSV = 4     /* triangular solves */ };
+int mp_set_kernel_timing(mp_ctx *ctx, int on);
+int mp_kernel_timing(mp_ctx *ctx, int kernel_class, int64_t *launches, double *ms, double *work);
 
 /* ---- particles ---------------------------------------------------------------- */
 int mp_particles_reserve(mp_ctx *ctx, int64_t capacity);

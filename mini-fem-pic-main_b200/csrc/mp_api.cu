@@ -25,6 +25,42 @@ int cuda_fail(mp_ctx *ctx, cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? MP_ERR_OOM : MP_ERR_CUDA;
 }
 
+int kt_begin(mp_ctx *ctx, int cls, double work) {
+    if (!ctx->ktime_on) return -1;
+    cudaEvent_t ev[2];
+    for (int k = 0; k < 2; k++) {
+        if (ctx->kevents.empty()) {
+            if (cudaEventCreate(&ev[k]) != cudaSuccess) return -1;
+        } else {
+            ev[k] = ctx->kevents.back();
+            ctx->kevents.pop_back();
+        }
+    }
+    cudaEventRecord(ev[0], ctx->stream);
+    ctx->kmarks.push_back(KernelMark{cls, work, ev[0], ev[1]});
+    return (int)ctx->kmarks.size() - 1;
+}
+
+void kt_end(mp_ctx *ctx, int mark) {
+    if (mark < 0 || mark >= (int)ctx->kmarks.size()) return;
+    cudaEventRecord(ctx->kmarks[mark].b, ctx->stream);
+}
+
+void kt_collect(mp_ctx *ctx) {
+    for (const KernelMark &m : ctx->kmarks) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, m.a, m.b) == cudaSuccess) {
+            KernelClock &c = ctx->kclock[m.cls];
+            c.launches++;
+            c.ms += ms;
+            c.work += m.work;
+        }
+        ctx->kevents.push_back(m.a);
+        ctx->kevents.push_back(m.b);
+    }
+    ctx->kmarks.clear();
+}
+
 template <typename T>
 static const T *strided(const void *base, int64_t stride, int64_t i) {
     return reinterpret_cast<const T *>(reinterpret_cast<const char *>(base) + stride * i);
@@ -300,6 +336,11 @@ int mp_destroy(mp_ctx *ctx) {
     cudaEvent_t ev[] = {ctx->t0.a, ctx->t0.b, ctx->t1.a, ctx->t1.b, ctx->tp.a, ctx->tp.b, ctx->ts.a, ctx->ts.b};
     for (auto e : ev)
         if (e) cudaEventDestroy(e);
+    for (const KernelMark &m : ctx->kmarks) {
+        cudaEventDestroy(m.a);
+        cudaEventDestroy(m.b);
+    }
+    for (cudaEvent_t e : ctx->kevents) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return MP_OK;
@@ -369,6 +410,26 @@ int mp_set_track_ids(mp_ctx *ctx, int on) {
 int mp_kernel_launches(mp_ctx *ctx, int64_t *n) {
     if (!ctx || !n) return MP_ERR_ARG;
     *n = ctx->launches;
+    return MP_OK;
+}
+
+int mp_set_kernel_timing(mp_ctx *ctx, int on) {
+    if (!ctx) return MP_ERR_ARG;
+    MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    kt_collect(ctx);
+    for (KernelClock &c : ctx->kclock) c = KernelClock();
+    ctx->ktime_on = on != 0;
+    return MP_OK;
+}
+
+int mp_kernel_timing(mp_ctx *ctx, int cls, int64_t *launches, double *ms, double *work) {
+    if (!ctx || cls < MP_KT_PUSH || cls > MP_KT_TRSV) return MP_ERR_ARG;
+    MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    kt_collect(ctx);
+    const KernelClock &c = ctx->kclock[cls];
+    if (launches) *launches = c.launches;
+    if (ms) *ms = c.ms;
+    if (work) *work = c.work;
     return MP_OK;
 }
 
@@ -505,6 +566,17 @@ int mp_push_scatter(mp_ctx *ctx, double q_over_m, double dt, double spwt, double
         MP_CUDA(ctx, cudaMemcpyAsync(den_out, ctx->den, sizeof(double) * ctx->n_nodes, cudaMemcpyDeviceToHost,
                                      ctx->stream));
     rc = sync_counters(ctx);
+    if (ctx->ktime_on) {
+        float ka = 0;
+        if (cudaEventElapsedTime(&ka, ctx->tp.a, ctx->tp.b) == cudaSuccess) {
+            KernelClock &c = ctx->kclock[MP_KT_PUSH];
+            c.launches++;
+            c.ms += ka;
+            const double bpp = ctx->form == MP_FORM_FP64 ? 52.0 : 28.0;
+            c.work += bpp * (double)(n_before + (ctx->n_host - ctx->dead_host));
+        }
+        kt_collect(ctx);
+    }
     if (stats) {
         stats->n_before = n_before;
         stats->n_after = ctx->n_host - ctx->dead_host;
@@ -595,13 +667,10 @@ int mp_fe_setup(mp_ctx *ctx, const mp_fe_desc *fe) {
         MP_CUDA(ctx, cudaMalloc(p, vec));
         MP_CUDA(ctx, cudaMemset(*p, 0, vec));
     }
-    ctx->K = ctx->J = nullptr;
-    ctx->j32_current = false;
+    ctx->K = ctx->J = nullptr;  // J: allocated when an FP64 dense J is first built
+    ctx->j32_current = ctx->j_current = false;
     const bool dense = ctx->fe_storage == MP_FE_STORAGE_DENSE;
-    if (dense) {
-        MP_CUDA(ctx, cudaMalloc(&ctx->K, sizeof(double) * (size_t)ld * neq));
-        MP_CUDA(ctx, cudaMalloc(&ctx->J, sizeof(double) * (size_t)ld * neq));
-    }
+    if (dense) MP_CUDA(ctx, cudaMalloc(&ctx->K, sizeof(double) * (size_t)ld * neq));
     cudaStream_t st = ctx->stream;
     MP_CUDA(ctx, cudaMemcpyAsync(ctx->ID, fe->ID, sizeof(int) * nn, cudaMemcpyHostToDevice, st));
     MP_CUDA(ctx, cudaMemcpyAsync(ctx->LM, LM.data(), sizeof(int) * 4 * nt, cudaMemcpyHostToDevice, st));
@@ -676,6 +745,7 @@ int mp_fe_download(mp_ctx *ctx, int which, double *out) {
     if (which == MP_MAT_K || which == MP_MAT_J) {
         if (!ctx->fe_ready) return fail(ctx, MP_ERR_STATE, "no FE setup");
         if (!ctx->K) return fail(ctx, MP_ERR_STATE, "sparse storage: no dense matrix (mp_fe_sparse_matrix)");
+        if (which == MP_MAT_J && !ctx->J) return fail(ctx, MP_ERR_STATE, "no FP64 J built yet (mp_fe_build_j)");
         const long long ld = (ctx->neq + 31) & ~31ll;
         MP_CUDA(ctx, cudaMemcpy2DAsync(out, sizeof(double) * ctx->neq, which == MP_MAT_K ? ctx->K : ctx->J,
                                        sizeof(double) * ld, sizeof(double) * ctx->neq, ctx->neq,
@@ -858,6 +928,7 @@ int mp_compute_phi(mp_ctx *ctx, const double *ion_den, int method, int form, mp_
     }
     cudaEventRecord(ctx->t0.b, ctx->stream);
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    kt_collect(ctx);
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->t0.a, ctx->t0.b);
     st->ms_total = ms;

@@ -126,6 +126,15 @@ __global__ void k_copy_j32(int neq, long long ld, const double *__restrict__ K, 
     }
 }
 
+int fe_j32_from_k(mp_ctx *ctx) {
+    const long long ld = (ctx->neq + 31) & ~31ll;
+    if (!ctx->J32) MP_CUDA(ctx, cudaMalloc(&ctx->J32, sizeof(float) * (size_t)ld * ctx->neq));
+    k_copy_j32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J32),
+        ++ctx->launches;
+    MP_CUDA(ctx, cudaGetLastError());
+    return MP_OK;
+}
+
 int fe_build_j(mp_ctx *ctx, int method, int form) {
     // the full symmetric J serves both dense solvers (Lapack reads only one
     // triangle); the sparse methods apply J = K - diag(FP) from K and FP
@@ -139,13 +148,16 @@ int fe_build_j(mp_ctx *ctx, int method, int form) {
     if (method == MP_METHOD_SPARSE_CG || method == MP_METHOD_SPARSE_NEWTON || !ctx->K) {
         ctx->j32_current = false;
     } else if (form == MP_FORM_MIXED) {
-        if (!ctx->J32) MP_CUDA(ctx, cudaMalloc(&ctx->J32, sizeof(float) * (size_t)ld * ctx->neq));
-        k_copy_j32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J32),
-            ++ctx->launches;
+        // the mixed form factors an FP32 copy and refines against K and FP: no FP64 J
+        int rc = fe_j32_from_k(ctx);
+        if (rc) return rc;
         ctx->j32_current = true;
     } else {
+        // the FP64 J (neq^2 doubles) is allocated on its first use
+        if (!ctx->J) MP_CUDA(ctx, cudaMalloc(&ctx->J, sizeof(double) * (size_t)ld * ctx->neq));
         k_copy_j<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J), ++ctx->launches;
         ctx->j32_current = false;
+        ctx->j_current = true;
     }
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;

@@ -92,6 +92,19 @@ struct Timer {
     cudaEvent_t a = nullptr, b = nullptr;
 };
 
+// Device time of kernel classes (mp_set_kernel_timing): launches, summed CUDA
+// event time, summed algorithmic work (bytes for the push, flops for the
+// trailing updates).
+struct KernelClock {
+    long long launches = 0;
+    double ms = 0, work = 0;
+};
+struct KernelMark {
+    int cls;
+    double work;
+    cudaEvent_t a, b;
+};
+
 }  // namespace mp
 
 struct mp_ctx {
@@ -156,6 +169,7 @@ struct mp_ctx {
     double *K = nullptr, *J = nullptr;    // [neq][neq] row-major
     float *J32 = nullptr;                 // [neq][neq] mixed-form factor
     bool j32_current = false;             // J32 holds the lower triangle of the current J
+    bool j_current = false;               // J holds the current J (not yet overwritten by its factor)
     double *scal = nullptr;               // device scalars for reductions
     double *scal_host = nullptr;          // pinned
     int *eq_ptr = nullptr, *eq_tet = nullptr;   // CSR equation -> (tet, a) sorted by tet
@@ -187,6 +201,11 @@ struct mp_ctx {
 
     mp::Timer t0, t1, tp, ts;
     long long launches = 0;
+    // kernel-class timing, off unless asked for (mp_set_kernel_timing)
+    bool ktime_on = false;
+    mp::KernelClock kclock[8];
+    std::vector<mp::KernelMark> kmarks;     // recorded, not yet read
+    std::vector<cudaEvent_t> kevents;       // free events
 
     void *adjoint = nullptr;              // adjoint state (mp_adjoint.cu), created by mp_adjoint_setup
     void *inject = nullptr;               // device injection state (mp_inject.cu)
@@ -196,6 +215,13 @@ struct mp_ctx {
 namespace mp {
 
 int fail(mp_ctx *ctx, int code, const std::string &msg);
+
+// Kernel-class timing: kt_begin records an event before a launch (returns a
+// mark index, or -1 when timing is off), kt_end one after it; kt_collect reads
+// the marks whose events have completed (call after a stream synchronise).
+int kt_begin(mp_ctx *ctx, int cls, double work);
+void kt_end(mp_ctx *ctx, int mark);
+void kt_collect(mp_ctx *ctx);
 int cuda_fail(mp_ctx *ctx, cudaError_t e, const char *what);
 
 #define MP_CUDA(ctx, call)                                  \
@@ -219,6 +245,7 @@ int launch_update_ef(mp_ctx *ctx);
 int fe_build_f1(mp_ctx *ctx, const double *den_dev);
 int fe_residual(mp_ctx *ctx);
 int fe_build_j(mp_ctx *ctx, int method, int form = MP_FORM_FP64);
+int fe_j32_from_k(mp_ctx *ctx);
 int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st);
 int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st);
 int fe_update_d(mp_ctx *ctx, double *l2_out);

@@ -720,11 +720,22 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     unsigned long long *flags = ctx->counters + C_FLAGS;
     auto diag_and_panel = [&](int k0, int kb, T *W, int ldw) {
         T *Li = w.Linv + (size_t)(k0 / NB) * NB * NB;
+        int mk = kt_begin(ctx, MP_KT_DIAG, 0);
         k_ldlt_diag<T><<<1, 256, diag_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, b, flags), ++ctx->launches;
+        kt_end(ctx, mk);
         int k1 = k0 + kb;
-        if (k1 < n)
+        if (k1 < n) {
+            mk = kt_begin(ctx, MP_KT_PANEL, 0);
             k_ldlt_panel<T><<<(n - k1 + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b),
                 ++ctx->launches;
+            kt_end(ctx, mk);
+        }
+    };
+    // algorithmic flops of an update of rows [R0, n) x columns [R0, C1), lower part, depth K
+    auto update_flops = [&](int R0, int C1, int K) {
+        const double m = n - R0, wcol = C1 - R0;
+        const double pairs = C1 >= n ? m * (m + 1) / 2 : wcol * (wcol + 1) / 2 + (m - wcol) * wcol;
+        return 2.0 * K * pairs;
     };
     // A[i][j] -= sum_{k<K} L[i][K0+k] W[j][kofs+k] for rows [R0, n) and columns
     // [R0, C1): a strip inside a super-panel when C1 < n, else the lower
@@ -735,10 +746,12 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             const long long rb = (n - R0 + WTILE - 1) / WTILE;
             const int cb = strip ? (C1 - R0) / WTILE : 0;
             const long long ntiles = strip ? rb * cb : rb * (rb + 1) / 2;
+            const int mk = kt_begin(ctx, MP_KT_UPDATE, update_flops(R0, C1, K));
             k_update_f64<<<(unsigned)ntiles, 256, f64_smem, st>>>(n, ld, reinterpret_cast<double *>(A), K0, K, R0,
                                                                  reinterpret_cast<const double *>(w.W) + kofs,
                                                                  SUPER_W, cb),
                 ++ctx->launches;
+            kt_end(ctx, mk);
             return MP_OK;
         }
         const long long rb = (n - R0 + tc::TILE - 1) / tc::TILE;
@@ -756,8 +769,10 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             float *Lh = w.split, *Ll = w.split + plane, *Wh = w.split + 2 * plane, *Wl = w.split + 3 * plane;
             const int gl = (int)std::min<long long>(((n - R0) * (K / 4) + 255) / 256, (long long)ctx->sm_count * 8);
             const int gw = (int)std::min<long long>((wrows * (K / 4) + 255) / 256, (long long)ctx->sm_count * 8);
+            const int mk = kt_begin(ctx, MP_KT_PANEL, 0);
             tc::k_split_rows<<<gl, 256, 0, st>>>(Lsrc, ld, n - R0, K, Lh, Ll), ++ctx->launches;
             tc::k_split_rows<<<gw, 256, 0, st>>>(Wsrc, SUPER_W, wrows, K, Wh, Wl), ++ctx->launches;
+            kt_end(ctx, mk);
             ok = operand_map(&mLh, Lh, n - R0, K, tc::TILE, K) && operand_map(&mWh, Wh, wrows, K, tc::TILE_N, K) &&
                  operand_map(&mLl, Ll, n - R0, K, tc::TILE, K) && operand_map(&mWl, Wl, wrows, K, tc::TILE_N, K);
         } else {
@@ -769,9 +784,11 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         if (!ok) return fail(ctx, MP_ERR_CUDA, "cuTensorMapEncodeTiled failed for the tensor-core update");
         const int grid = (int)std::min<long long>(ntiles, (long long)ctx->sm_count);
         auto kern = split ? tc::k_update_tc<true> : tc::k_update_tc<false>;
+        const int mk = kt_begin(ctx, MP_KT_UPDATE, update_flops(R0, C1, K));
         kern<<<grid, tc::THREADS, tc::smem_bytes(split), st>>>(mLh, mWh, mLl, mWl, n, ld, Af, R0, ntiles, K / tc::KC,
                                                                cb, flags),
             ++ctx->launches;
+        kt_end(ctx, mk);
         return MP_OK;
     };
     if (factor) {
@@ -792,9 +809,11 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                     diag_and_panel(k0, kb, w.W + (k0 - S0), SUPER_W);
                     if (k1 < n && k1 < P1) {
                         dim3 g((P1 - k1 + 63) / 64, (n - k1 + 63) / 64);
+                        const int mk = kt_begin(ctx, MP_KT_PANEL, 0);
                         k_ldlt_update_cols<T><<<g, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W + (k0 - S0), SUPER_W,
                                                                         k1, P1),
                             ++ctx->launches;
+                        kt_end(ctx, mk);
                     }
                 }
                 if (P1 < S1) {  // a full panel with more of its super-panel to the right
@@ -810,12 +829,14 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     }
     const int nblk = (n + NB - 1) / NB;
     const int epoch = ++ctx->solve_epoch;
+    const int mk = kt_begin(ctx, MP_KT_TRSV, 0);
     if (!factor) {
         int g = trsv_grid<T>(ctx, (const void *)k_trsv_fwd<T>, nblk);
         k_trsv_fwd<T><<<g, 256, 0, st>>>(n, ld, A, w.Linv, b, w.ready, epoch, flags), ++ctx->launches;
     }
     int g = trsv_grid<T>(ctx, (const void *)k_trsv_bwd<T>, nblk);
     k_trsv_bwd<T><<<g, 256, 0, st>>>(n, ld, A, w.Linv, w.dvec, b, w.ready + nblk, epoch, flags), ++ctx->launches;
+    kt_end(ctx, mk);
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }

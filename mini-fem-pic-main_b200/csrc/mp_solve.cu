@@ -2,6 +2,7 @@
 // factor + FP64 iterative refinement for the mixed form) and the reference's
 // Gauss-Seidel iteration (FESolver::solveLinear, src/FESolver.cpp:561-601).
 #include <cmath>
+#include <utility>
 
 #include "mp_internal.h"
 #include "mp_ldlt.cuh"
@@ -37,13 +38,6 @@ __global__ void k_resid_j(int neq, long long ld, const double *__restrict__ K, c
         atomicAdd(&sums[0], rr * rr);
         atomicAdd(&sums[1], b[warp] * b[warp]);
     }
-}
-
-__global__ void k_j_to_f32(int neq, long long ld, const double *__restrict__ J, float *J32) {
-    long long total = (long long)neq * ld;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x)
-        J32[i] = (float)J[i];
 }
 
 __global__ void k_axpy_f32(int n, const float *__restrict__ c, double *y) {
@@ -143,6 +137,8 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
     const long long ld = (n + 31) & ~31ll;
     cudaEventRecord(ctx->t1.a, ctx->stream);
     if (form == MP_FORM_FP64) {
+        if (!ctx->J || !ctx->j_current) return fail(ctx, MP_ERR_STATE, "no current FP64 J (build it first)");
+        ctx->j_current = false;  // the factorization overwrites J
         MP_CUDA(ctx, cudaMemcpyAsync(ctx->y, ctx->G, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
         LdltWork<double> w{sc.dvec64, sc.W64, sc.s64, sc.Linv64, sc.ready, nullptr};
         rc = ldlt_factor_solve<double>(ctx, ctx->J, ld, n, ctx->y, w, true);
@@ -156,10 +152,9 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
             st->linear_residual = rn / n;
         }
     } else {
-        if (!ctx->J32) MP_CUDA(ctx, cudaMalloc(&ctx->J32, sizeof(float) * (size_t)ld * n));
-        // the factorization overwrites J32: it is current once per build of J
-        if (!ctx->j32_current)
-            k_j_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(n, ld, ctx->J, ctx->J32), ++ctx->launches;
+        // the factorization overwrites J32: it is current once per build of J;
+        // otherwise it is rebuilt from K and the current FP
+        if (!ctx->j32_current && (rc = fe_j32_from_k(ctx))) return rc;
         ctx->j32_current = false;
         MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * n, ctx->stream));
         LdltWork<float> w{sc.dvec32, sc.W32, sc.s32, sc.Linv32, sc.ready, sc.split32};
@@ -202,52 +197,134 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
 }
 
 // ---- Gauss-Seidel ---------------------------------------------------------------------
-// One sweep of the reference's row-sequential Gauss-Seidel on the dense J, in
-// one CTA: rows go in blocks of 32; the 32 warps first take each row's dot
-// product with the current x over the columns outside the block (new values
-// left of it, old values right of it), then one warp finishes the block's
-// rows in order.  The iterate is the reference's, up to summation order.
-// Rows with |J_uu| < 1e-12 keep their value (src/FESolver.cpp:569).
-__global__ void __launch_bounds__(1024) k_gs_sweep(int neq, long long ld, const double *__restrict__ A,
-                                                   const double *__restrict__ b, double *x) {
-    __shared__ double s_t[32];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int r0 = 0; r0 < neq; r0 += 32) {
-        int rb = neq - r0 < 32 ? neq - r0 : 32;
-        // off-block partial sums: warp w handles row r0+w
-        if (warp < rb) {
-            const double *row = A + (long long)(r0 + warp) * ld;
-            double s = 0;
-            for (int j = lane; j < neq; j += 32)
-                if (j < r0 || j >= r0 + rb) s = fma(row[j], x[j], s);
+// One sweep of the reference's row-sequential Gauss-Seidel (solveLinear,
+// src/FESolver.cpp:567-578) is x_new = (D + L)^-1 (b - U x_old), with L, D, U
+// the strictly lower, diagonal and strictly upper parts of J; a row with
+// |J_uu| < 1e-12 keeps its value (src/FESolver.cpp:569).  The sweep runs as a
+// persistent wavefront over 64-row blocks (the triangular solves' scheme):
+// block k streams its rows once, summing the columns right of the diagonal
+// against x_old as soon as it starts and the columns of each earlier block
+// against x_new as that block publishes it (a ready word per block holding the
+// sweep's epoch, release/acquire), then applies the stored inverse of its
+// diagonal block of D + L: a 64 x 64 product instead of 64 dependent
+// substitutions.  x_old and x_new are separate buffers (sweeps alternate
+// them), so no block reads a value another block is rewriting.  The iterate is
+// the reference's up to summation order.
+
+// Inverse of each 64 x 64 diagonal block of D + L, rows with |J_uu| < 1e-12
+// (and rows past n) replaced by identity rows, so the block's row keeps its
+// value.  One CTA of 64 threads per block; thread j owns column j of the
+// inverse X, computed row by row (X_rj = (delta_rj - sum_{c<r} M_rc X_cj) / M_rr),
+// and row r of X replaces row r of M once the step has read it.
+__global__ void __launch_bounds__(64) k_gs_block_inverse(int n, long long ld, const double *__restrict__ A,
+                                                         double *Minv) {
+    __shared__ double sM[NB][NB + 1];
+    const int blk = blockIdx.x, r0 = blk * NB, j = threadIdx.x;
+    for (int r = 0; r < NB; r++) {
+        const int row = r0 + r;
+        double v = 0.0;
+        if (row < n && j <= r) v = A[(long long)row * ld + r0 + j];
+        sM[r][j] = v;
+    }
+    __syncthreads();
+    // identity rows for skipped (and padding) rows
+    const bool ident = r0 + j >= n || fabs(sM[j][j]) < 1e-12;
+    __syncthreads();
+    if (ident)
+        for (int c = 0; c < NB; c++) sM[j][c] = c == j ? 1.0 : 0.0;
+    __syncthreads();
+    for (int r = 0; r < NB; r++) {
+        double t = r == j ? 1.0 : 0.0;
+        for (int c = j; c < r; c++) t = fma(-sM[r][c], sM[c][j], t);
+        const double x = r < j ? 0.0 : t / sM[r][r];
+        __syncthreads();  // every thread has read row r of M
+        sM[r][j] = x;
+        __syncthreads();
+    }
+    double *out = Minv + (size_t)blk * NB * NB;
+    for (int r = 0; r < NB; r++) out[r * NB + j] = sM[r][j];
+}
+
+__global__ void __launch_bounds__(256) k_gs_sweep(int n, long long ld, const double *__restrict__ A,
+                                                  const double *__restrict__ b, const double *__restrict__ Minv,
+                                                  const double *x_old, double *x_new, int *ready, int epoch,
+                                                  unsigned long long *flags) {
+    __shared__ double sI[NB][NB + 1];
+    __shared__ double sc[NB];
+    __shared__ int s_cnt[8];
+    const int nblk = (n + NB - 1) / NB;
+    const int t = threadIdx.x;
+    const int r = t >> 2, q = t & 3;  // row of the block, quarter of each 64-column chunk
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
+        for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = __ldg(&Minv[(size_t)blk * NB * NB + idx]);
+        const int row = r0 + (r < kb ? r : 0);
+        const double *arow = A + (long long)row * ld + q * 16;
+        double acc = 0.0, ap[16], xv[16];
+        // columns right of the block: x_old, available now
+        for (int c = blk + 1; c < nblk; c++) {
+            const int c0 = c * NB + q * 16;
+            if (c0 + 16 <= n) {
+                load16<double, false>(arow + c * NB, ap);
+                load16<double, false>(x_old + c0, xv);
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) s_t[warp] = s;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            int u = r0 + lane;
-            double t = 0, diag = 1, xo = 0;
-            bool act = lane < rb;
-            if (act) {
-                const double *row = A + (long long)u * ld;
-                t = b[u] - s_t[lane];
-                diag = row[u];
-                xo = x[u];
-                // within-block columns right of the diagonal use the old values
-                for (int v = lane + 1; v < rb; v++) t -= row[r0 + v] * x[r0 + v];
+                for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
+            } else {
+                for (int k = 0; k < 16 && c0 + k < n; k++) acc = fma(arow[c * NB + k], x_old[c0 + k], acc);
             }
-            for (int j = 0; j < rb; j++) {
-                double xj = 0;
-                if (lane == j) {
-                    xj = fabs(diag) < 1e-12 ? xo : t / diag;
-                    x[u] = xj;
+        }
+        // the diagonal block's columns right of the diagonal: x_old
+        for (int k = 0; k < 16; k++) {
+            const int col = q * 16 + k;
+            if (col > r && col < kb) acc = fma(arow[blk * NB + k], x_old[r0 + col], acc);
+        }
+        // columns left of the block: x_new, block by block as they are published
+        int done = 0;
+        long long spins = 0;
+        if (done < blk) load16<double, false>(arow, ap);
+        while (done < blk) {
+            const int span = blk - done < 256 ? blk - done : 256;
+            const int cnt = ready_prefix(ready, done, span, 1, epoch, s_cnt);
+            if (cnt == 0) {
+                if (++spins > TRSV_SPIN_LIMIT) {
+                    if (t == 0) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
+                    break;
                 }
-                xj = __shfl_sync(0xffffffffu, xj, j);
-                if (act && lane > j) t -= A[(long long)u * ld + r0 + j] * xj;
+                __nanosleep(32);
+                continue;
             }
+            const int avail = done + cnt;
+            load16<double, true>(x_new + done * NB + q * 16, xv);
+#pragma unroll
+            for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
+            for (int c = done + 1; c < avail; c++) {
+                load16<double, false>(arow + c * NB, ap);
+                load16<double, true>(x_new + c * NB + q * 16, xv);
+#pragma unroll
+                for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
+            }
+            done = avail;
+            if (done < blk) load16<double, false>(arow + done * NB, ap);
+        }
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        if (q == 0) {
+            double cv = 0.0;
+            if (r < kb) {
+                const double d = A[(long long)(r0 + r) * ld + r0 + r];
+                cv = fabs(d) < 1e-12 ? x_old[r0 + r] : b[r0 + r] - acc;
+            }
+            sc[r] = cv;
         }
         __syncthreads();
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) v = fma(sI[r][q * 16 + k], sc[q * 16 + k], v);
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+        v += __shfl_xor_sync(0xffffffffu, v, 2);
+        if (q == 0 && r < kb) x_new[r0 + r] = v;
+        __syncthreads();
+        if (t == 0) st_release(ready + blk, epoch);
     }
 }
 
@@ -269,19 +346,33 @@ __global__ void k_gs_resid(int neq, long long ld, const double *__restrict__ A, 
 }
 
 int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st) {
+    if (!ctx->J || !ctx->j_current) return fail(ctx, MP_ERR_STATE, "no current FP64 J (build it first)");
+    SolveScratch *sp = nullptr;
+    int rc = ensure_scratch(ctx, &sp);
+    if (rc) return rc;
     const int n = ctx->neq;
     const long long ld = (n + 31) & ~31ll;
+    const int nblk = (n + NB - 1) / NB;
     const double tol = 1e-4;
-    int th = 256;
-    long long bl = ((long long)n * 32 + th - 1) / th;
+    const int th = 256;
+    const long long bl = ((long long)n * 32 + th - 1) / th;
+    unsigned long long *flags = ctx->counters + C_FLAGS;
+    // the inverses of the diagonal blocks of D + L (J is fixed for the solve)
+    k_gs_block_inverse<<<nblk, 64, 0, ctx->stream>>>(n, ld, ctx->J, sp->Linv64), ++ctx->launches;
+    const int grid = trsv_grid<double>(ctx, (const void *)k_gs_sweep, nblk);
+    double *xa = ctx->y, *xb = sp->r;  // sweeps alternate the two
     double L2 = 0;
     int it;
     bool converged = false;
     for (it = 0; it < ctx->gs_max_sweeps; it++) {
-        k_gs_sweep<<<1, 1024, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, ctx->y), ++ctx->launches;
+        const int mk = kt_begin(ctx, MP_KT_TRSV, 0);
+        k_gs_sweep<<<grid, 256, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, sp->Linv64, xa, xb, sp->ready,
+                                                  ++ctx->solve_epoch, flags), ++ctx->launches;
+        kt_end(ctx, mk);
+        std::swap(xa, xb);
         if (it % 25 == 0) {
             MP_CUDA(ctx, cudaMemsetAsync(ctx->scal + 3, 0, sizeof(double), ctx->stream));
-            k_gs_resid<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, ctx->y, ctx->scal + 3), ++ctx->launches;
+            k_gs_resid<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, xa, ctx->scal + 3), ++ctx->launches;
             MP_CUDA(ctx, cudaMemcpyAsync(ctx->scal_host + 3, ctx->scal + 3, sizeof(double), cudaMemcpyDeviceToHost,
                                          ctx->stream));
             MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -292,7 +383,13 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st) {
             }
         }
     }
+    if (xa != ctx->y)
+        MP_CUDA(ctx, cudaMemcpyAsync(ctx->y, xa, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
     MP_CUDA(ctx, cudaGetLastError());
+    unsigned long long bad = 0;
+    rc = check_flags(ctx, FLAG_LOOKBACK_TIMEOUT, &bad);
+    if (rc) return rc;
+    if (bad) return fail(ctx, MP_ERR_TIMEOUT, "a bounded wait in the Gauss-Seidel sweep gave up");
     if (st) {
         st->linear_iterations = it;
         st->linear_residual = L2;

@@ -66,7 +66,9 @@ EXPORTED = [
     "mp_set_fe_storage", "mp_set_sparse_solver", "mp_fe_sparse_matrix",
     "mp_mesh_geometry_device", "mp_inlet_faces_device", "mp_fe_geometry_device",
     "mp_output_mesh", "mp_output_particles", "mp_output_wait", "mp_set_gs_max_sweeps",
+    "mp_set_kernel_timing", "mp_kernel_timing",
 ]
+KT_PUSH, KT_UPDATE, KT_DIAG, KT_PANEL, KT_TRSV = 0, 1, 2, 3, 4
 
 
 class MpError(RuntimeError):
@@ -178,6 +180,9 @@ def lib():
         L.mp_set_particle_form.argtypes = [vp, C.c_int]
         L.mp_set_track_ids.argtypes = [vp, C.c_int]
         L.mp_kernel_launches.argtypes = [vp, C.POINTER(i64)]
+        L.mp_set_kernel_timing.argtypes = [vp, C.c_int]
+        L.mp_kernel_timing.argtypes = [vp, C.c_int, C.POINTER(i64), C.POINTER(d), C.POINTER(d)]
+        L.mp_set_gs_max_sweeps.argtypes = [vp, C.c_int32]
         L.mp_device_buffer.argtypes = [vp, C.c_int, C.POINTER(vp), C.POINTER(i64)]
         L.mp_push_particles_noalloc.argtypes = [vp, vp, i64, vp, i32, vp, vp, i32, d, d, vp, C.POINTER(i64)]
         L.mp_particles_reserve.argtypes = [vp, i64]
@@ -560,6 +565,16 @@ class Context:
         """FE_DENSE (default: dense K and J plus a sparse K) or FE_SPARSE (the
         sparse K only; SPARSE_CG and SPARSE_NEWTON).  Before fe_setup."""
         self._c(lib().mp_set_fe_storage(self.h, storage))
+
+    def set_kernel_timing(self, on=True):
+        """CUDA events around every launch of the kernel classes (KT_*); resets the clocks."""
+        self._c(lib().mp_set_kernel_timing(self.h, 1 if on else 0))
+
+    def kernel_timing(self, kclass: int) -> dict:
+        """launches, device ms and algorithmic work (bytes or flops) of a kernel class."""
+        n, ms, w = C.c_int64(0), C.c_double(0), C.c_double(0)
+        self._c(lib().mp_kernel_timing(self.h, int(kclass), C.byref(n), C.byref(ms), C.byref(w)))
+        return {"launches": int(n.value), "ms": float(ms.value), "work": float(w.value)}
 
     def set_gs_max_sweeps(self, sweeps=10000):
         """Gauss-Seidel sweep limit (the reference's is 10000)."""

@@ -41,27 +41,47 @@ CONFIGS = {
     2: dict(n=32, n_ions=50_000_000, dt=5e-8, spwt=0.2, sphere=(50.0, 50.0, 50.0, 20.0), label="kuhn32s_50M_mixed"),
     3: dict(n=16, n_ions=1_000_000, dt=1e-7, spwt=5.0, sphere=None, label="kuhn16_1M_adjoint_K20",
             adjoint_steps=20, checkpoint_every=5),
+    4: dict(n=40, n_ions=200_000_000, dt=5e-8, spwt=0.05, sphere=(50.0, 50.0, 50.0, 20.0),
+            label="kuhn40s_200M_stress", adjoint_steps=10, checkpoint_every=5, sort_period=10),
 }
 KTI_EV = 0.1
 SPHERE_POTENTIAL = -10.0
 
 
-def make_workload(cfg: dict, workdir: str, seed: int, n_ions: int | None = None):
-    """Writes the deck into workdir, loads it as the reference would, and seeds
-    the ion population.  Returns (kuhn deck, Deck, pos, vel, cell)."""
+def write_deck(cfg: dict, workdir: str):
+    """The configuration's Kuhn deck in the reference's own file format (numpy
+    only; no library call).  Returns the Kuhn deck."""
     kd = kuhn.build(cfg["n"], sphere=cfg["sphere"])
     kuhn.write(kd, workdir, dt=cfg["dt"], method="lapack")
-    deck = mp.Deck.load(workdir)
+    return kd
+
+
+def seed_population(kd, cfg: dict, seed: int, n_ions: int | None = None):
+    """The steady-state ion population (numpy only): uniform in the box, the
+    7 km/s drift along +x plus a 0.1 eV Maxwellian, each ion in the Kuhn tet
+    that contains it; ions that fall in the removed sphere are dropped.
+    Returns (pos, vel, cell)."""
     rng = np.random.default_rng(seed)
     n = cfg["n_ions"] if n_ions is None else n_ions
     L = kd.length_mm / 1000.0
     pos = rng.uniform(1e-6 * L, (1 - 1e-6) * L, size=(n, 3))
     sigma = np.sqrt(KTI_EV * mp.QE / (16 * mp.AMU))
     vel = rng.normal(0.0, sigma, size=(n, 3))
-    vel[:, 0] += deck.params.ion_velocity
+    vel[:, 0] += float(kd.params["ion_velocity"])
     cell = kuhn.locate(kd, pos).astype(np.int32)
     keep = cell >= 0
-    return kd, deck, np.ascontiguousarray(pos[keep]), np.ascontiguousarray(vel[keep]), cell[keep]
+    if keep.all():
+        return pos, vel, cell
+    return np.ascontiguousarray(pos[keep]), np.ascontiguousarray(vel[keep]), cell[keep]
+
+
+def make_workload(cfg: dict, workdir: str, seed: int, n_ions: int | None = None):
+    """Writes the deck into workdir, loads it as the reference would, and seeds
+    the ion population.  Returns (kuhn deck, Deck, pos, vel, cell)."""
+    kd = write_deck(cfg, workdir)
+    deck = mp.Deck.load(workdir)
+    pos, vel, cell = seed_population(kd, cfg, seed, n_ions)
+    return kd, deck, pos, vel, cell
 
 
 def absorb_cavity_walks(ctx):
