@@ -258,6 +258,7 @@ int fe_assemble_sparse(mp_ctx *ctx);
 int fe_sparse_from_dense(mp_ctx *ctx);
 int fe_sparse_from_host(mp_ctx *ctx, const double *const *rows, const double *dense);
 int fe_residual_sparse(mp_ctx *ctx);
+int fe_resid_j_sparse(mp_ctx *ctx, const double *y, const double *b, double *r, float *r32, double *sums);
 int fe_solve_cg(mp_ctx *ctx, mp_newton_stats *st);
 void solve_free(mp_ctx *ctx);
 void adjoint_free(mp_ctx *ctx);

@@ -45,13 +45,21 @@ __global__ void k_axpy_f32(int n, const float *__restrict__ c, double *y) {
     if (i < n) y[i] += (double)c[i];
 }
 
+// r = b - J y and the norms ||r||, ||b||: from the sparse copy of K (about 15
+// nonzeros a row) when the context holds one, else from the dense K.
 static int resid_norms(mp_ctx *ctx, const double *y, const double *b, double *r, float *r32, double *rn,
                        double *bn) {
     long long ld = (ctx->neq + 31) & ~31ll;
     MP_CUDA(ctx, cudaMemsetAsync(ctx->scal + 1, 0, 2 * sizeof(double), ctx->stream));
-    int th = 256;
-    long long bl = ((long long)ctx->neq * 32 + th - 1) / th;
-    k_resid_j<<<(unsigned)bl, th, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, y, b, r, r32, ctx->scal + 1), ++ctx->launches;
+    if (ctx->sp_val) {
+        int rc = fe_resid_j_sparse(ctx, y, b, r, r32, ctx->scal + 1);
+        if (rc) return rc;
+    } else {
+        int th = 256;
+        long long bl = ((long long)ctx->neq * 32 + th - 1) / th;
+        k_resid_j<<<(unsigned)bl, th, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, y, b, r, r32, ctx->scal + 1),
+            ++ctx->launches;
+    }
     MP_CUDA(ctx, cudaGetLastError());
     MP_CUDA(ctx, cudaMemcpyAsync(ctx->scal_host + 1, ctx->scal + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost,
                                  ctx->stream));

@@ -7,6 +7,8 @@ kTe = 2 eV, inlet x=0 at 0 V, wall x=0.1 at -5 V):
   1  20^3 hexes (48,000 tets), ~2M ions, dt 5e-8, spwt 5
   2  32^3 hexes minus a centred r=0.02 m sphere at -10 V, ~50M ions, dt 5e-8
   3  16^3 hexes (24,576 tets), ~1M ions, adjoint over K=20 steps, checkpoints every 5
+  4  40^3 hexes minus the sphere (371,004 tets, 62,788 unknowns), ~193M ions, spwt 0.05,
+     re-sort every 10 steps, adjoint over K=10 steps (the combined-stress workload, stress.py)
 The ion population is seeded at steady state: uniform in the box, drift plus
 a 0.1 eV Maxwellian (sigma = sqrt(kTi*QE/m) ~ 776 m/s), each ion in the Kuhn
 tet that contains it.
