@@ -374,8 +374,10 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st) {
     bool converged = false;
     for (it = 0; it < ctx->gs_max_sweeps; it++) {
         const int mk = kt_begin(ctx, MP_KT_TRSV, 0);
-        k_gs_sweep<<<grid, 256, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, sp->Linv64, xa, xb, sp->ready,
-                                                  ++ctx->solve_epoch, flags), ++ctx->launches;
+        MP_CUDA(ctx, launch_wavefront(k_gs_sweep, grid, ctx->stream, n, ld, (const double *)ctx->J,
+                                      (const double *)ctx->G, (const double *)sp->Linv64, (const double *)xa, xb,
+                                      sp->ready, ++ctx->solve_epoch, flags));
+        ++ctx->launches;
         kt_end(ctx, mk);
         std::swap(xa, xb);
         if (it % 25 == 0) {
