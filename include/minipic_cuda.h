@@ -217,8 +217,11 @@ int mp_kernel_launches(mp_ctx *ctx, int64_t *n);
 /* Device time of kernel classes, for roofline accounting (no reference
  * counterpart; the reference's trace.csv times host functions, src/trace.cpp).
  * While on, CUDA events bracket every launch of the classes below and each
- * call reads them after its own synchronisation; turning it on resets the
- * clocks.  work: algorithmic bytes for MP_KT_PUSH ((particles before + after
+ * call reads them after its own synchronisation; any call resets the clocks.
+ * on = 0: off; 1: every class; otherwise a mask of (1 << MP_KT_*) bits (the
+ * diagonal-block and panel classes launch hundreds of small kernels a step,
+ * whose event records slow the host's launch stream, so a timed run leaves
+ * them out).  work: algorithmic bytes for MP_KT_PUSH ((particles before + after
  * the push) x the form's bytes per particle, 52 FP64 / 28 mixed), algorithmic
  * flops for MP_KT_UPDATE (2 per multiply-add of the trailing update's lower
  * triangle; the 3xTF32 split issues three tensor-core products per term and

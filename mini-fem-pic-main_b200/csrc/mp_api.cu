@@ -26,7 +26,7 @@ int cuda_fail(mp_ctx *ctx, cudaError_t e, const char *what) {
 }
 
 int kt_begin(mp_ctx *ctx, int cls, double work) {
-    if (!ctx->ktime_on) return -1;
+    if (!(ctx->ktime_mask >> cls & 1u)) return -1;
     cudaEvent_t ev[2];
     for (int k = 0; k < 2; k++) {
         if (ctx->kevents.empty()) {
@@ -418,7 +418,7 @@ int mp_set_kernel_timing(mp_ctx *ctx, int on) {
     MP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     kt_collect(ctx);
     for (KernelClock &c : ctx->kclock) c = KernelClock();
-    ctx->ktime_on = on != 0;
+    ctx->ktime_mask = on == 1 ? 0x1Fu : (unsigned)on & 0x1Fu;
     return MP_OK;
 }
 
@@ -566,7 +566,7 @@ int mp_push_scatter(mp_ctx *ctx, double q_over_m, double dt, double spwt, double
         MP_CUDA(ctx, cudaMemcpyAsync(den_out, ctx->den, sizeof(double) * ctx->n_nodes, cudaMemcpyDeviceToHost,
                                      ctx->stream));
     rc = sync_counters(ctx);
-    if (ctx->ktime_on) {
+    if (ctx->ktime_mask & (1u << MP_KT_PUSH)) {
         float ka = 0;
         if (cudaEventElapsedTime(&ka, ctx->tp.a, ctx->tp.b) == cudaSuccess) {
             KernelClock &c = ctx->kclock[MP_KT_PUSH];

@@ -202,7 +202,7 @@ struct mp_ctx {
     mp::Timer t0, t1, tp, ts;
     long long launches = 0;
     // kernel-class timing, off unless asked for (mp_set_kernel_timing)
-    bool ktime_on = false;
+    unsigned ktime_mask = 0;              // bit k: kernel class k timed
     mp::KernelClock kclock[8];
     std::vector<mp::KernelMark> kmarks;     // recorded, not yet read
     std::vector<cudaEvent_t> kevents;       // free events

@@ -42,88 +42,152 @@ __device__ __forceinline__ bool bad_pivot(T d) {
 // for the panel and the triangular solves.  If b is non-null,
 // z_k = L_kk^-1 b_k (the forward substitution riding on the factorization).
 //
-// One CTA of 64 threads (two warps, so a step's barrier is cheap); thread i
-// holds row i of the block's lower triangle in registers (padded to 64 x 64
-// with an identity).  Elimination step j: every thread i >= j posts A_ij to a
-// shared column buffer (double-buffered by step parity: one barrier a step),
-// then thread i > j forms l_ij = A_ij / d_j and updates its row,
-// A_ic -= l_ij A_cj for j < c <= i, from the posted column.  The inverse
-// follows column by column: thread c runs X_ic = [i == c] - sum_{k<i} L_ik X_kc
-// over i with L read from shared memory, and the block's z = X b is a row
-// product.  All loops over the block's columns are unrolled so the rows stay in
-// registers.  Dynamic smem: L [64][65] (then X), column buffers [2][64], b [64].
+// 256 threads, the block in shared memory (padded to 64 x 64 with an identity).
+// Four sub-panels of SUB = 16 columns:
+//   factor the sub-panel (64 x 16): 16 elimination steps, one barrier each;
+//     thread (row i, column quad g) updates its 4 columns from the step's
+//     published column (double-buffered), and the rows of the sub-panel's
+//     16 x 16 diagonal block apply the same row operation to an identity,
+//     which leaves that block's inverse;
+//   rank-16 update of the trailing block, 4 x 4 register tiles per thread.
+// The off-diagonal blocks of Linv follow by block substitution:
+//   X_qp = -X_qq sum_{r=p}^{q-1} L_qr X_rp.
+// Dynamic smem: A [64][65], Linv [64][65], W [64][17], T [16][17], w [2][64], b [64].
+constexpr int SUB = 16;
+
 template <typename T>
-__global__ void __launch_bounds__(64) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
-                                                  T *b, unsigned long long *flags) {
+__global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
+                                                   T *b, unsigned long long *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T(*sL)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
-    T *col = reinterpret_cast<T *>(sL + NB);  // [2][NB]
-    T *sb = col + 2 * NB;
+    T(*sA)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
+    T(*sI)[NB + 1] = sA + NB;
+    T(*sW)[SUB + 1] = reinterpret_cast<T(*)[SUB + 1]>(sI + NB);
+    T(*sT)[SUB + 1] = sW + NB;
+    T *sw = reinterpret_cast<T *>(sT + SUB);  // [2][NB]
+    T *sb = sw + 2 * NB;
     const int t = threadIdx.x;
-    // coalesced load of the lower triangle (identity past kb)
-    for (int r = 0; r < NB; r++) {
-        T v = T(0);
-        if (r < kb && t < kb && t <= r) v = A[(long long)(k0 + r) * ld + k0 + t];
-        else if (r >= kb && t == r) v = T(1);
-        sL[r][t] = v;
-    }
-    sb[t] = (b && t < kb) ? b[k0 + t] : T(0);
-    __syncthreads();
-    T a[NB];
+    // load the lower triangle, pad with an identity past kb; Linv starts as the identity
+    {
+        T v[16];
 #pragma unroll
-    for (int c = 0; c < NB; c++) a[c] = sL[t][c];
-    bool singular = false;
-#pragma unroll 1
-    for (int j = 0; j < NB; j++) {
-        T *cj = col + (j & 1) * NB;
-        // post column j (the entries at and below the diagonal)
-        T aj = T(0);
-#pragma unroll
-        for (int c = 0; c < NB; c++)
-            if (c == j) aj = a[c];
-        if (t >= j) cj[t] = aj;
-        __syncthreads();
-        T d = cj[j];
-        if (bad_pivot(d)) {
-            singular = true;
-            d = T(1);
+        for (int q = 0; q < 16; q++) {
+            const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
+            v[q] = (r < kb && c < kb && c <= r) ? A[(long long)(k0 + r) * ld + k0 + c] : T(0);
         }
-        if (t > j) {
-            const T l = aj / d;
 #pragma unroll
-            for (int c = 0; c < NB; c++) {
-                if (c == j) a[c] = l;
-                else if (c > j && c <= t) a[c] -= l * cj[c];
+        for (int q = 0; q < 16; q++) {
+            const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
+            sA[r][c] = (r >= kb && r == c) ? T(1) : v[q];
+            sI[r][c] = r == c ? T(1) : T(0);
+        }
+    }
+    if (b && t < NB) sb[t] = t < kb ? b[k0 + t] : T(0);
+    __syncthreads();
+    if (t < NB) sw[t] = sA[t][0];  // publish column 0
+    __syncthreads();
+    const int i = t >> 2, g = t & 3;  // this thread's row and column quad in the sub-panel
+    bool singular = false;
+    for (int p = 0; p < NB / SUB; p++) {
+        const int c0 = p * SUB;
+        // ---- factor the sub-panel: columns [c0, c0+16), rows [c0, 64) ----
+        for (int j = c0; j < c0 + SUB; j++) {
+            const T *w = sw + (j & 1) * NB;
+            T d = w[j];
+            if (bad_pivot(d)) {
+                singular = true;
+                d = T(1);
+            }
+            const T rd = T(1) / d;
+            const T wi = w[i];
+            const T li = wi * rd;  // L[i][j] for i > j
+            if (i > j) {
+#pragma unroll
+                for (int cc = 0; cc < 4; cc++) {
+                    const int col = c0 + 4 * g + cc;
+                    if (col > j && col <= i) sA[i][col] -= li * w[col];
+                    if (col == j) sA[i][j] = li;
+                    // the sub-panel's diagonal block: the same row operation on the identity
+                    if (i < c0 + SUB && col <= j) sI[i][col] -= li * sI[j][col];
+                }
+            }
+            // publish column j+1 (final for this step once its own update above has run)
+            if (j + 1 < c0 + SUB && 4 * g <= j + 1 - c0 && j + 1 - c0 < 4 * g + 4) sw[((j + 1) & 1) * NB + i] = sA[i][j + 1];
+            __syncthreads();
+        }
+        if (p == NB / SUB - 1) break;
+        // ---- rank-16 update of the trailing block [c0+16, 64)^2 ----
+        const int e0 = c0 + SUB;
+        if (t < NB) {
+#pragma unroll
+            for (int jl = 0; jl < SUB; jl++) sW[t][jl] = sA[t][c0 + jl] * sA[c0 + jl][c0 + jl];
+        }
+        __syncthreads();
+        {
+            const int ti = t >> 4, tk = t & 15;
+            const int r0 = 4 * ti, q0 = 4 * tk;
+            if (r0 + 3 >= e0 && q0 + 3 >= e0 && q0 <= r0 + 3) {
+                T acc[4][4] = {};
+#pragma unroll
+                for (int jl = 0; jl < SUB; jl++) {
+                    T av[4], wv[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) av[u] = sA[r0 + u][c0 + jl];
+#pragma unroll
+                    for (int v = 0; v < 4; v++) wv[v] = sW[q0 + v][jl];
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+#pragma unroll
+                        for (int v = 0; v < 4; v++) acc[u][v] += av[u] * wv[v];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+#pragma unroll
+                    for (int v = 0; v < 4; v++) {
+                        const int r = r0 + u, q = q0 + v;
+                        if (r >= e0 && q >= e0 && q <= r) sA[r][q] -= acc[u][v];
+                    }
             }
         }
+        __syncthreads();
+        if (t < NB) sw[(e0 & 1) * NB + t] = sA[t][e0];  // publish the next sub-panel's first column
+        __syncthreads();
     }
     if (singular && t == 0) atomicOr(flags, FLAG_SINGULAR);
-    // L (strict lower) and D to shared memory, then to A
-    __syncthreads();
+    // ---- off-diagonal blocks of Linv, by block distance ----
+    for (int dist = 1; dist < NB / SUB; dist++) {
+        for (int p = 0; p + dist < NB / SUB; p++) {
+            const int q = p + dist;
+            const int a = t >> 4, c = t & 15;  // element (a, c) of the 16 x 16 block
+            // T = sum_{r=p}^{q-1} L_qr X_rp
+            T acc = 0;
+            for (int r = p; r < q; r++)
 #pragma unroll
-    for (int c = 0; c < NB; c++) sL[t][c] = c <= t ? a[c] : T(0);
-    __syncthreads();
-    for (int r = 0; r < kb; r++)
-        if (t <= r && t < kb) A[(long long)(k0 + r) * ld + k0 + t] = sL[r][t];
-    if (t < kb) dvec[k0 + t] = sL[t][t];
-    // X = L^-1, column t per thread
-    T x[NB];
+                for (int m = 0; m < SUB; m++) acc += sA[q * SUB + a][r * SUB + m] * sI[r * SUB + m][p * SUB + c];
+            sT[a][c] = acc;
+            __syncthreads();
+            // X_qp = -X_qq T (X_qq unit lower)
+            T x = 0;
 #pragma unroll
-    for (int i = 0; i < NB; i++) {
-        T v = i == t ? T(1) : T(0);
-#pragma unroll
-        for (int k = 0; k < i; k++) v -= sL[i][k] * x[k];
-        x[i] = v;
+            for (int m = 0; m < SUB; m++) x += sI[q * SUB + a][q * SUB + m] * sT[m][c];
+            sI[q * SUB + a][p * SUB + c] = -x;
+            __syncthreads();
+        }
     }
-    __syncthreads();
+    // ---- write back L, D, Linv; z = Linv b ----
 #pragma unroll
-    for (int i = 0; i < NB; i++) sL[i][t] = x[i];
-    __syncthreads();
-    for (int r = 0; r < NB; r++) Linv[r * NB + t] = (r < kb && t < kb) ? sL[r][t] : T(0);
-    if (b && t < kb) {
-        T z = 0;
-        for (int c = 0; c <= t; c++) z += sL[t][c] * sb[c];
-        b[k0 + t] = z;
+    for (int q = 0; q < 16; q++) {
+        const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
+        const bool in = r < kb && c < kb;
+        if (in && c <= r) A[(long long)(k0 + r) * ld + k0 + c] = sA[r][c];
+        Linv[r * NB + c] = in ? sI[r][c] : T(0);
+    }
+    if (t < kb) {
+        dvec[k0 + t] = sA[t][t];
+        if (b) {
+            T z = 0;
+            for (int pp = 0; pp <= t; pp++) z += sI[t][pp] * sb[pp];
+            b[k0 + t] = z;
+        }
     }
 }
 
@@ -644,7 +708,7 @@ template <typename T>
 int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> w, bool factor,
                       int tc_terms = 0) {
     cudaStream_t st = ctx->stream;
-    const size_t diag_smem = sizeof(T) * (NB * (NB + 1) + 3 * NB);
+    const size_t diag_smem = sizeof(T) * (2 * NB * (NB + 1) + NB * (SUB + 1) + SUB * (SUB + 1) + 3 * NB);
     const size_t panel_smem = sizeof(T) * (64 * (NB + 1) + NB * (NB + 1) + 2 * NB);
     const size_t upd_smem = sizeof(T) * 2 * NB * 68;
     const size_t f64_smem = sizeof(double) * 4 * WKC * WTILE;
@@ -667,7 +731,7 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     auto diag_and_panel = [&](int k0, int kb, T *W, int ldw) {
         T *Li = w.Linv + (size_t)(k0 / NB) * NB * NB;
         int mk = kt_begin(ctx, MP_KT_DIAG, 0);
-        k_ldlt_diag<T><<<1, NB, diag_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, b, flags), ++ctx->launches;
+        k_ldlt_diag<T><<<1, 256, diag_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, b, flags), ++ctx->launches;
         kt_end(ctx, mk);
         int k1 = k0 + kb;
         if (k1 < n) {

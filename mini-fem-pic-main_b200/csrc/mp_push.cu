@@ -34,7 +34,6 @@ struct PushF64Args {
     double *den;
     unsigned long long *den_fixed;
     unsigned long long *counters;
-    int n_tets;
     double qm, dt;
     int walk_limit;
     int absorb;  // hop limit reached: remove the particle (counted in C_LOST) instead of raising the error
@@ -50,7 +49,6 @@ struct PushF32Args {
     double *den;
     unsigned long long *den_fixed;
     unsigned long long *counters;
-    int n_tets;
     float qm_dt;                     // q/m * dt
     float dt;
     int walk_limit;
@@ -218,216 +216,71 @@ __device__ __forceinline__ void scatter_warp(int state, int cell, const int con[
 // bound of 4 CTAs per SM (0.0868 -> 0.0837 ms on 2M sorted ions).  The mixed
 // kernel's prefetch needs 7 registers and does not spill; staging it was
 // slower (0.0592 -> 0.0626 ms).
-// The CTA's tet band (see the mixed kernel below for the scheme): 192 B per
-// tet in this form.
-constexpr int F64_BAND_MAX = 200;
-constexpr int F64_MARGIN = 24;
-constexpr int HOPQ64 = 64;
-struct HopQueueF64 {
-    double x[HOPQ64], y[HOPQ64], z[HOPQ64];
-    int cell[HOPQ64], idx[HOPQ64];
-};
-
-struct F64Band {
-    const TetRec *s;  // shared copy of tets [lo, lo + n)
-    int lo, n;
-    __device__ __forceinline__ const TetRec *rec(const TetRec *__restrict__ g, int cell) const {
-        const unsigned o = (unsigned)(cell - lo);
-        return o < (unsigned)n ? s + o : g + cell;
-    }
-};
-
-// XtoLtet (src/meshes.h:75-100) on band or global records, every operation
-// rounded on its own in the reference's order.  Returns 1 inside, 0 left the
-// domain, -1 hop limit reached, or, with `defer` set, 4 when the particle is
-// outside its start tet (nothing else computed).  EXACT_CMP: the division-free
-// inside test (see walk_fp64).
-template <bool EXACT_CMP>
-__device__ __forceinline__ int walk_fp64_band(const F64Band &band, const TetRec *__restrict__ tets, int &cell,
-                                              double x, double y, double z, double lc[4], int limit, int &hops,
-                                              bool defer) {
-    for (;;) {
-        const TetRec *t = band.rec(tets, cell);
-        double q[4];
-        numerators_fp64_any(t, x, y, z, q);
-        const double vol = t->volume;
-        if (EXACT_CMP) {
-            bool inside = true;
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-                if (q[i] < 0 || q[i] > vol) inside = false;
-            if (inside) {
-                const double rv = __drcp_rn(vol);
-#pragma unroll
-                for (int i = 0; i < 4; i++) lc[i] = __dmul_rn(q[i], rv);
-                return 1;
-            }
-            if (defer) return 4;
-#pragma unroll
-            for (int i = 0; i < 4; i++) lc[i] = __ddiv_rn(q[i], vol);
-        } else {
-            bool inside = true;
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                lc[i] = __ddiv_rn(q[i], vol);
-                if (lc[i] < 0 || lc[i] > 1.0) inside = false;
-            }
-            if (inside) return 1;
-            if (defer) return 4;
-        }
-        int min_i = 0;
-        double min_lc = lc[0];
-#pragma unroll
-        for (int i = 1; i < 4; i++)
-            if (lc[i] < min_lc) {
-                min_lc = lc[i];
-                min_i = i;
-            }
-        const int nb = t->cell_con[min_i];
-        if (nb < 0) return 0;
-        if (hops >= limit) return -1;
-        cell = nb;
-        hops++;
-    }
-}
-
-// Walks up to 32 queued particles of this warp, writes their cells, scatters,
-// and shifts the rest of the queue down.  All 32 lanes call it.
-template <bool EXACT_CMP>
-__device__ __forceinline__ void drain_fp64(const PushF64Args &a, const F64Band &band, HopQueueF64 *q, int &qn,
-                                           PushStats &stats) {
-    const int lane = threadIdx.x & 31;
-    const int m = qn < 32 ? qn : 32;
-    int state = 0, hops = 0, lost = 0, cell = -1;
-    int con[4] = {0, 0, 0, 0};
-    double lc[4] = {0, 0, 0, 0};
-    if (lane < m) {
-        cell = q->cell[lane];
-        const int i = q->idx[lane];
-        const int w = walk_fp64_band<EXACT_CMP>(band, a.tets, cell, q->x[lane], q->y[lane], q->z[lane], lc,
-                                                a.walk_limit, hops, false);
-        if (w == 1) {
-            state = 1;
-            const int4 c4 = *reinterpret_cast<const int4 *>(band.rec(a.tets, cell)->con);
-            con[0] = c4.x; con[1] = c4.y; con[2] = c4.z; con[3] = c4.w;
-        } else if (w == -1 && a.absorb) {
-            state = 3;  // the point lies outside the mesh where the walk cannot end: absorbed
-            cell = -1;
-            lost = 1;
-        } else if (w == -1) {
-            state = 2;  // kept where the walk stopped, not scattered, error raised
-            atomicOr(&a.counters[C_FLAGS], FLAG_WALK_LIMIT);
-        } else {
-            state = 3;
-            cell = -1;
-        }
-        a.p.cell[i] = cell;
-        stats.add(state, hops, 0, lost);
-    }
-    scatter_warp<double>(state, cell, con, lc, a.den, a.den_fixed, a.fixed);
-    __syncwarp();
-    const int rest = qn - m;
-    if (lane < rest) {
-        q->x[lane] = q->x[m + lane]; q->y[lane] = q->y[m + lane]; q->z[lane] = q->z[m + lane];
-        q->cell[lane] = q->cell[m + lane]; q->idx[lane] = q->idx[m + lane];
-    }
-    __syncwarp();
-    qn = rest;
-}
-
-// FP64 push: the tet band staged in shared memory, particles that must leave
-// their tet queued per warp and walked 32 at a time (see the mixed kernel).
 template <bool EXACT_CMP>
 __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_fp64(PushF64Args a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ HopQueueF64 queues[PUSH_THREADS / 32];
-    __shared__ int s_lo, s_hi;
     const long long n = (long long)a.counters[C_N];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     // this CTA's contiguous block of chunks [c, n_chunks), its warps interleaved
     const long long n_all = (n + 31) >> 5;
     const long long per = (n_all + gridDim.x - 1) / gridDim.x;
     const long long cta0 = (long long)blockIdx.x * per;
     const long long n_chunks = n_all < cta0 + per ? n_all : cta0 + per;
     const long long wstride = PUSH_THREADS / 32;
-    if (threadIdx.x == 0) {
-        s_lo = 0x7fffffff;
-        s_hi = -1;
-    }
-    __syncthreads();
-    if (warp < 2 && cta0 < n_chunks) {
-        const long long ch = warp == 0 ? cta0 : n_chunks - 1;
-        const long long i = ch * 32 + lane;
-        const int c = i < n ? a.p.cell[i] : -1;
-        const int lo = __reduce_min_sync(0xffffffffu, c >= 0 ? c : 0x7fffffff);
-        const int hi = __reduce_max_sync(0xffffffffu, c);
-        if (lane == 0) {
-            atomicMin(&s_lo, lo);
-            atomicMax(&s_hi, hi);
-        }
-    }
-    __syncthreads();
-    F64Band band;
-    band.s = reinterpret_cast<const TetRec *>(smem_raw);
-    band.lo = 0;
-    band.n = 0;
-    if (s_hi >= 0 && s_lo <= s_hi) {
-        const int lo = s_lo - F64_MARGIN > 0 ? s_lo - F64_MARGIN : 0;
-        int hi = s_hi + F64_MARGIN < a.n_tets - 1 ? s_hi + F64_MARGIN : a.n_tets - 1;
-        if (hi - lo + 1 > F64_BAND_MAX) hi = lo + F64_BAND_MAX - 1;
-        band.lo = lo;
-        band.n = hi - lo + 1;
-        const int4 *src = reinterpret_cast<const int4 *>(a.tets + lo);
-        int4 *dst = reinterpret_cast<int4 *>(smem_raw);
-        const int words = band.n * (int)(sizeof(TetRec) / sizeof(int4));
-        for (int k = threadIdx.x; k < words; k += PUSH_THREADS) dst[k] = __ldg(src + k);
-    }
-    __syncthreads();
-    HopQueueF64 *q = &queues[warp];
-    int qn = 0;
+    long long c = cta0 + (threadIdx.x >> 5);
     PushStats stats;
-    for (long long c = cta0 + warp; c < n_chunks; c += wstride) {
+    // two staging slots per warp: the chunk being pushed and the next one
+    __shared__ __align__(16) ChunkF64 stage[PUSH_THREADS / 32][2];
+    ChunkF64 *ws = stage[threadIdx.x >> 5];
+    if (c < n_chunks) stage_chunk_f64(a.p, c, ws);
+    cp_async_commit();
+    int slot = 0;
+    for (; c < n_chunks; c += wstride) {
         const long long i = c * 32 + lane;
-        int cell = -1;
-        double x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 0;
-        if (i < n) {
-            cell = a.p.cell[i];
-            x = a.p.px[i]; y = a.p.py[i]; z = a.p.pz[i];
-            vx = a.p.vx[i]; vy = a.p.vy[i]; vz = a.p.vz[i];
-        }
-        int state = 0, hops = 0;
+        __syncwarp();  // every lane has read the slot the next chunk overwrites
+        if (c + wstride < n_chunks) stage_chunk_f64(a.p, c + wstride, ws + (slot ^ 1));
+        cp_async_commit();  // possibly empty: one group per chunk keeps the count
+        cp_async_wait<1>();  // this chunk's group has landed
+        __syncwarp();        // ... for every lane's copies
+        const ChunkF64 *cb = ws + slot;
+        slot ^= 1;
+        int cell = cb->cell[lane];
+        double x = cb->d[0][lane], y = cb->d[1][lane], z = cb->d[2][lane];
+        double vx = cb->d[3][lane], vy = cb->d[4][lane], vz = cb->d[5][lane];
+        int state = 0, hops = 0, lost = 0;
         int con[4] = {0, 0, 0, 0};
         double lc[4] = {0, 0, 0, 0};
         if (i < n && cell >= 0) {
-            const TetRec *t = band.rec(a.tets, cell);
+            const TetRec *t = a.tets + cell;
             // v += q_over_m*ef*dt ; x += v*dt  (src/mini-pic.cpp:291-295)
-            vx = __dadd_rn(vx, __dmul_rn(__dmul_rn(a.qm, t->ef[0]), a.dt));
-            vy = __dadd_rn(vy, __dmul_rn(__dmul_rn(a.qm, t->ef[1]), a.dt));
-            vz = __dadd_rn(vz, __dmul_rn(__dmul_rn(a.qm, t->ef[2]), a.dt));
+            vx = __dadd_rn(vx, __dmul_rn(__dmul_rn(a.qm, __ldg(&t->ef[0])), a.dt));
+            vy = __dadd_rn(vy, __dmul_rn(__dmul_rn(a.qm, __ldg(&t->ef[1])), a.dt));
+            vz = __dadd_rn(vz, __dmul_rn(__dmul_rn(a.qm, __ldg(&t->ef[2])), a.dt));
             x = __dadd_rn(x, __dmul_rn(vx, a.dt));
             y = __dadd_rn(y, __dmul_rn(vy, a.dt));
             z = __dadd_rn(z, __dmul_rn(vz, a.dt));
-            state = walk_fp64_band<EXACT_CMP>(band, a.tets, cell, x, y, z, lc, a.walk_limit, hops, true);
-            if (state == 1) {
-                const int4 c4 = *reinterpret_cast<const int4 *>(t->con);
+            int w = walk_fp64<EXACT_CMP>(a.tets, cell, x, y, z, lc, a.walk_limit, hops);
+            if (w == 1) {
+                state = 1;
+                const int4 c4 = __ldg(reinterpret_cast<const int4 *>(a.tets[cell].con));
                 con[0] = c4.x; con[1] = c4.y; con[2] = c4.z; con[3] = c4.w;
+            } else if (w == -1 && a.absorb) {
+                state = 3;  // the point lies outside the mesh where the walk cannot end: absorbed
+                cell = -1;
+                lost = 1;
+            } else if (w == -1) {
+                state = 2;  // kept where the walk stopped, not scattered, error raised
+                atomicOr(&a.counters[C_FLAGS], FLAG_WALK_LIMIT);
+            } else {
+                state = 3;
+                cell = -1;
             }
-            // the position is final whatever the walk finds; the cell of a queued particle is written later
             a.p.px[i] = x; a.p.py[i] = y; a.p.pz[i] = z;
             a.p.vx[i] = vx; a.p.vy[i] = vy; a.p.vz[i] = vz;
+            a.p.cell[i] = cell;
         }
-        const unsigned hop = __ballot_sync(0xffffffffu, state == 4);
-        if (state == 4) {
-            const int slot = qn + __popc(hop & lanemask_lt());
-            q->x[slot] = x; q->y[slot] = y; q->z[slot] = z;
-            q->cell[slot] = cell;
-            q->idx[slot] = (int)i;
-        }
-        qn += __popc(hop);
-        scatter_warp<double>(state == 1 ? 1 : 0, cell, con, lc, a.den, a.den_fixed, a.fixed);
-        if (qn >= 32) drain_fp64<EXACT_CMP>(a, band, q, qn, stats);
+        scatter_warp<double>(state, cell, con, lc, a.den, a.den_fixed, a.fixed);
+        stats.add(state, hops, 0, lost);
     }
-    while (qn > 0) drain_fp64<EXACT_CMP>(a, band, q, qn, stats);
     stats.flush(a.counters);
 }
 
@@ -454,201 +307,16 @@ __device__ __forceinline__ void load_x0(const double *__restrict__ x0, int cell,
     z = __ldg(x0 + 4ll * cell + 2);
 }
 
-// Tet band of a CTA: the records of the tets its block of tet-sorted particles
-// lives in (from the smallest cell of its first chunk to the largest of its
-// last, plus a margin for particles that moved since the last sort), staged in
-// shared memory once; a lookup inside the band reads shared memory, any other
-// reads global memory.  96 B per tet.
-constexpr int MIX_BAND_MAX = 384;
-constexpr int BAND_MARGIN = 24;
-// Per-warp queue of particles that must leave their tet: a warp walks queued
-// particles 32 at a time, so the hop path (argmin, neighbour's weights,
-// re-basing, FP64 re-tests) runs at full width instead of once per chunk for
-// the few lanes that hop.
-constexpr int HOPQ = 64;
-struct HopQueueF32 {
-    float rx[HOPQ], ry[HOPQ], rz[HOPQ];
-    int cell[HOPQ], idx[HOPQ];
-};
-
-struct MixedBand {
-    const TetRec32 *s;  // shared copy of tets [lo, lo + n)
-    int lo, n;
-    __device__ __forceinline__ const TetRec32 *rec(const TetRec32 *__restrict__ g, int cell) const {
-        const unsigned o = (unsigned)(cell - lo);
-        return o < (unsigned)n ? s + o : g + cell;
-    }
-};
-
-// The walk of one particle from `cell` (the reference's XtoLtet on FP32 weights
-// with the FP64 near-face re-test).  Returns 1 inside, 2 hop limit reached
-// (kept, error), 3 left the domain, 5 absorbed at the hop limit, or, when
-// `defer` is set and the particle is outside its start tet, 4 without
-// walking.  `count_near` = 0 skips counting the start tet's re-test (already
-// counted when the particle was queued).
-__device__ __forceinline__ int walk_mixed(const PushF32Args &a, const MixedBand &band, int &cell, float &rx,
-                                          float &ry, float &rz, float lc[4], int &hops, int &near, bool defer,
-                                          int count_near) {
-    for (;;) {
-        const TetRec32 *tc = band.rec(a.tets32, cell);
-        const float4 gx = *reinterpret_cast<const float4 *>(tc->gx);
-        const float4 gy = *reinterpret_cast<const float4 *>(tc->gy);
-        const float4 gz = *reinterpret_cast<const float4 *>(tc->gz);
-        lc[0] = 1.0f + fmaf(gx.x, rx, fmaf(gy.x, ry, gz.x * rz));
-        lc[1] = fmaf(gx.y, rx, fmaf(gy.y, ry, gz.y * rz));
-        lc[2] = fmaf(gx.z, rx, fmaf(gy.z, ry, gz.z * rz));
-        lc[3] = fmaf(gx.w, rx, fmaf(gy.w, ry, gz.w * rz));
-        const float mn = fminf(fminf(lc[0], lc[1]), fminf(lc[2], lc[3]));
-        const float mx = fmaxf(fmaxf(lc[0], lc[1]), fmaxf(lc[2], lc[3]));
-        // lambda > 1 implies another lambda < 0, so min alone picks the near-face cases
-        bool inside;
-        int min_i = 0;
-        if (fabsf(mn) < (float)NEAR_FACE) {
-            // decide in FP64 on the reconstructed absolute position
-            near += count_near;
-            count_near = 1;
-            double ox, oy, oz;
-            load_x0(a.x0, cell, ox, oy, oz);
-            const double x = ox + (double)rx, y = oy + (double)ry, z = oz + (double)rz;
-            double l64[4];
-            lambdas_fp64(a.tets + cell, x, y, z, l64);
-            inside = true;
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                if (l64[k] < -ON_FACE || l64[k] > 1.0 + ON_FACE) inside = false;
-                lc[k] = (float)l64[k];
-            }
-            if (inside) return 1;
-            if (defer) return 4;
-            double m64 = l64[0];
-#pragma unroll
-            for (int k = 1; k < 4; k++)
-                if (l64[k] < m64) {
-                    m64 = l64[k];
-                    min_i = k;
-                }
-        } else {
-            count_near = 1;
-            inside = mn >= 0.0f && mx <= 1.0f;
-            if (inside) return 1;
-            if (defer) return 4;
-            float m32 = lc[0];
-#pragma unroll
-            for (int k = 1; k < 4; k++)
-                if (lc[k] < m32) {
-                    m32 = lc[k];
-                    min_i = k;
-                }
-        }
-        const int nb = tc->cell_con[min_i];
-        if (nb < 0) {
-            cell = -1;
-            return 3;
-        }
-        if (hops >= a.walk_limit) {
-            if (a.absorb) {
-                cell = -1;
-                return 5;
-            }
-            atomicOr(&a.counters[C_FLAGS], FLAG_WALK_LIMIT);
-            return 2;
-        }
-        // re-base the offset on the new tet's vertex 0
-        double ax, ay, az, bx, by, bz;
-        load_x0(a.x0, cell, ax, ay, az);
-        load_x0(a.x0, nb, bx, by, bz);
-        rx = (float)((ax - bx) + (double)rx);
-        ry = (float)((ay - by) + (double)ry);
-        rz = (float)((az - bz) + (double)rz);
-        cell = nb;
-        hops++;
-    }
-}
-
-// Walks up to 32 queued particles of this warp (one per lane), writes their
-// offsets and cells, scatters, and shifts the rest of the queue down.  All
-// 32 lanes call it.
-__device__ __forceinline__ void drain_mixed(const PushF32Args &a, const MixedBand &band, HopQueueF32 *q,
-                                            int &qn, PushStats &stats) {
-    const int lane = threadIdx.x & 31;
-    const int m = qn < 32 ? qn : 32;
-    int state = 0, hops = 0, near = 0, cell = -1;
-    int con[4] = {0, 0, 0, 0};
-    float lc[4] = {0, 0, 0, 0};
-    if (lane < m) {
-        cell = q->cell[lane];
-        float rx = q->rx[lane], ry = q->ry[lane], rz = q->rz[lane];
-        const int i = q->idx[lane];
-        const int w = walk_mixed(a, band, cell, rx, ry, rz, lc, hops, near, false, 0);
-        state = w == 5 ? 3 : w;
-        if (state == 1) {
-            const int4 c4 = *reinterpret_cast<const int4 *>(band.rec(a.tets32, cell)->con);
-            con[0] = c4.x; con[1] = c4.y; con[2] = c4.z; con[3] = c4.w;
-        }
-        a.p.rx[i] = rx; a.p.ry[i] = ry; a.p.rz[i] = rz;
-        a.p.cell[i] = cell;
-        stats.add(state, hops, near, w == 5);
-    }
-    scatter_warp<float>(state, cell, con, lc, a.den, a.den_fixed, a.fixed);
-    __syncwarp();
-    const int rest = qn - m;
-    if (lane < rest) {
-        q->rx[lane] = q->rx[m + lane]; q->ry[lane] = q->ry[m + lane]; q->rz[lane] = q->rz[m + lane];
-        q->cell[lane] = q->cell[m + lane]; q->idx[lane] = q->idx[m + lane];
-    }
-    __syncwarp();
-    qn = rest;
-}
-
 __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_mixed(PushF32Args a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ HopQueueF32 queues[PUSH_THREADS / 32];
-    __shared__ int s_lo, s_hi;
     const long long n = (long long)a.counters[C_N];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     // this CTA's contiguous block of chunks [c, n_chunks), its warps interleaved
     const long long n_all = (n + 31) >> 5;
     const long long per = (n_all + gridDim.x - 1) / gridDim.x;
     const long long cta0 = (long long)blockIdx.x * per;
     const long long n_chunks = n_all < cta0 + per ? n_all : cta0 + per;
     const long long wstride = PUSH_THREADS / 32;
-    // the band: smallest cell of the first chunk .. largest of the last chunk
-    if (threadIdx.x == 0) {
-        s_lo = 0x7fffffff;
-        s_hi = -1;
-    }
-    __syncthreads();
-    if (warp < 2 && cta0 < n_chunks) {
-        const long long ch = warp == 0 ? cta0 : n_chunks - 1;
-        const long long i = ch * 32 + lane;
-        const int c = i < n ? a.p.cell[i] : -1;
-        const int lo = __reduce_min_sync(0xffffffffu, c >= 0 ? c : 0x7fffffff);
-        const int hi = __reduce_max_sync(0xffffffffu, c);
-        if (lane == 0) {
-            atomicMin(&s_lo, lo);
-            atomicMax(&s_hi, hi);
-        }
-    }
-    __syncthreads();
-    MixedBand band;
-    band.s = reinterpret_cast<const TetRec32 *>(smem_raw);
-    band.lo = 0;
-    band.n = 0;
-    if (s_hi >= 0 && s_lo <= s_hi) {
-        const int lo = s_lo - BAND_MARGIN > 0 ? s_lo - BAND_MARGIN : 0;
-        int hi = s_hi + BAND_MARGIN < a.n_tets - 1 ? s_hi + BAND_MARGIN : a.n_tets - 1;
-        if (hi - lo + 1 > MIX_BAND_MAX) hi = lo + MIX_BAND_MAX - 1;
-        band.lo = lo;
-        band.n = hi - lo + 1;
-        const int4 *src = reinterpret_cast<const int4 *>(a.tets32 + lo);
-        int4 *dst = reinterpret_cast<int4 *>(smem_raw);
-        const int words = band.n * (int)(sizeof(TetRec32) / sizeof(int4));
-        for (int k = threadIdx.x; k < words; k += PUSH_THREADS) dst[k] = __ldg(src + k);
-    }
-    __syncthreads();
-    HopQueueF32 *q = &queues[warp];
-    int qn = 0;
-    long long c = cta0 + warp;
+    long long c = cta0 + (threadIdx.x >> 5);
     PushStats stats;
     int cell_n = -1;
     float rxn = 0, ryn = 0, rzn = 0, vxn = 0, vyn = 0, vzn = 0;
@@ -671,39 +339,98 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_mixed(PushF32Args a) {
                 vxn = a.p.vx[in]; vyn = a.p.vy[in]; vzn = a.p.vz[in];
             }
         }
-        int state = 0, hops = 0, near = 0;
+        int state = 0, hops = 0, near = 0, lost = 0;
         int con[4] = {0, 0, 0, 0};
         float lc[4] = {0, 0, 0, 0};
         if (i < n && cell >= 0) {
-            const TetRec32 *t = band.rec(a.tets32, cell);
-            vx = fmaf(a.qm_dt, t->ef[0], vx);
-            vy = fmaf(a.qm_dt, t->ef[1], vy);
-            vz = fmaf(a.qm_dt, t->ef[2], vz);
+            const TetRec32 *t = a.tets32 + cell;
+            vx = fmaf(a.qm_dt, __ldg(&t->ef[0]), vx);
+            vy = fmaf(a.qm_dt, __ldg(&t->ef[1]), vy);
+            vz = fmaf(a.qm_dt, __ldg(&t->ef[2]), vz);
             rx = fmaf(vx, a.dt, rx);
             ry = fmaf(vy, a.dt, ry);
             rz = fmaf(vz, a.dt, rz);
-            state = walk_mixed(a, band, cell, rx, ry, rz, lc, hops, near, true, 1);
-            if (state == 1) {
-                const int4 c4 = *reinterpret_cast<const int4 *>(t->con);
-                con[0] = c4.x; con[1] = c4.y; con[2] = c4.z; con[3] = c4.w;
-                a.p.rx[i] = rx; a.p.ry[i] = ry; a.p.rz[i] = rz;
+            for (;;) {
+                const TetRec32 *tc = a.tets32 + cell;
+                lambdas_fp32(tc, rx, ry, rz, lc);
+                float mn = fminf(fminf(lc[0], lc[1]), fminf(lc[2], lc[3]));
+                float mx = fmaxf(fmaxf(lc[0], lc[1]), fmaxf(lc[2], lc[3]));
+                // lambda > 1 implies another lambda < 0, so min alone picks the near-face cases
+                bool inside;
+                int min_i = 0;
+                if (fabsf(mn) < (float)NEAR_FACE) {
+                    // decide in FP64 on the reconstructed absolute position
+                    near++;
+                    double ox, oy, oz;
+                    load_x0(a.x0, cell, ox, oy, oz);
+                    double x = ox + (double)rx, y = oy + (double)ry, z = oz + (double)rz;
+                    double l64[4];
+                    lambdas_fp64(a.tets + cell, x, y, z, l64);
+                    inside = true;
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        if (l64[k] < -ON_FACE || l64[k] > 1.0 + ON_FACE) inside = false;
+                        lc[k] = (float)l64[k];
+                    }
+                    double m64 = l64[0];
+#pragma unroll
+                    for (int k = 1; k < 4; k++)
+                        if (l64[k] < m64) {
+                            m64 = l64[k];
+                            min_i = k;
+                        }
+                } else {
+                    inside = mn >= 0.0f && mx <= 1.0f;
+                    float m32 = lc[0];
+#pragma unroll
+                    for (int k = 1; k < 4; k++)
+                        if (lc[k] < m32) {
+                            m32 = lc[k];
+                            min_i = k;
+                        }
+                }
+                if (inside) {
+                    state = 1;
+                    break;
+                }
+                int nb = __ldg(&tc->cell_con[min_i]);
+                if (nb < 0) {
+                    state = 3;
+                    cell = -1;
+                    break;
+                }
+                if (hops >= a.walk_limit) {
+                    if (a.absorb) {
+                        state = 3;
+                        cell = -1;
+                        lost = 1;
+                    } else {
+                        state = 2;
+                        atomicOr(&a.counters[C_FLAGS], FLAG_WALK_LIMIT);
+                    }
+                    break;
+                }
+                // re-base the offset on the new tet's vertex 0
+                double ax, ay, az, bx, by, bz;
+                load_x0(a.x0, cell, ax, ay, az);
+                load_x0(a.x0, nb, bx, by, bz);
+                rx = (float)((ax - bx) + (double)rx);
+                ry = (float)((ay - by) + (double)ry);
+                rz = (float)((az - bz) + (double)rz);
+                cell = nb;
+                hops++;
             }
+            if (state == 1) {
+                const int4 c4 = __ldg(reinterpret_cast<const int4 *>(a.tets32[cell].con));
+                con[0] = c4.x; con[1] = c4.y; con[2] = c4.z; con[3] = c4.w;
+            }
+            a.p.rx[i] = rx; a.p.ry[i] = ry; a.p.rz[i] = rz;
             a.p.vx[i] = vx; a.p.vy[i] = vy; a.p.vz[i] = vz;
+            a.p.cell[i] = cell;
         }
-        // queue the particles that must leave their tet
-        const unsigned hop = __ballot_sync(0xffffffffu, state == 4);
-        if (state == 4) {
-            const int slot = qn + __popc(hop & lanemask_lt());
-            q->rx[slot] = rx; q->ry[slot] = ry; q->rz[slot] = rz;
-            q->cell[slot] = cell;
-            q->idx[slot] = (int)i;
-        }
-        qn += __popc(hop);
-        scatter_warp<float>(state == 1 ? 1 : 0, cell, con, lc, a.den, a.den_fixed, a.fixed);
-        stats.add(state == 1 ? 1 : 0, 0, near, 0);
-        if (qn >= 32) drain_mixed(a, band, q, qn, stats);
+        scatter_warp<float>(state, cell, con, lc, a.den, a.den_fixed, a.fixed);
+        stats.add(state, hops, near, lost);
     }
-    while (qn > 0) drain_mixed(a, band, q, qn, stats);
     stats.flush(a.counters);
 }
 
@@ -735,8 +462,6 @@ int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
         MP_CUDA(ctx, cudaMemsetAsync(ctx->den, 0, ctx->n_nodes * sizeof(double), ctx->stream));
     long long blocks = (ctx->n_host + PUSH_THREADS - 1) / PUSH_THREADS;
     if (blocks < 1) blocks = 1;
-    // the push kernels queue particles by a 32-bit index
-    if (ctx->n_host > 0x7fffffffll) return fail(ctx, MP_ERR_ARG, "more than 2^31 - 1 particle slots");
     if (ctx->form == MP_FORM_FP64) {
         PushF64Args a;
         a.p = ctx->p64[ctx->cur];
@@ -744,7 +469,6 @@ int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
         a.den = ctx->den;
         a.den_fixed = ctx->den_fixed;
         a.counters = ctx->counters;
-        a.n_tets = ctx->n_tets;
         a.qm = q_over_m;
         a.dt = dt;
         a.walk_limit = ctx->walk_limit;
@@ -753,15 +477,10 @@ int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
         a.track_ids = ctx->track_ids;
         // division-free inside test when every tet volume is below 1 (see walk_fp64)
         auto kern = ctx->small_tets ? k_push_fp64<true> : k_push_fp64<false>;
-        const size_t band_smem = sizeof(TetRec) * F64_BAND_MAX;
-        if (!ctx->push_grid[0]) {
-            cudaFuncSetAttribute(k_push_fp64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band_smem);
-            cudaFuncSetAttribute(k_push_fp64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band_smem);
-            ctx->push_grid[0] = grid_for(ctx, (const void *)kern, PUSH_THREADS, band_smem);
-        }
+        if (!ctx->push_grid[0]) ctx->push_grid[0] = grid_for(ctx, (const void *)kern, PUSH_THREADS, 0);
         long long g = blocks < ctx->push_grid[0] ? blocks : ctx->push_grid[0];
         cudaEventRecord(ctx->tp.a, ctx->stream);
-        kern<<<(unsigned)g, PUSH_THREADS, band_smem, ctx->stream>>>(a), ++ctx->launches;
+        kern<<<(unsigned)g, PUSH_THREADS, 0, ctx->stream>>>(a), ++ctx->launches;
         cudaEventRecord(ctx->tp.b, ctx->stream);
     } else {
         PushF32Args a;
@@ -772,21 +491,16 @@ int launch_push(mp_ctx *ctx, double q_over_m, double dt) {
         a.den = ctx->den;
         a.den_fixed = ctx->den_fixed;
         a.counters = ctx->counters;
-        a.n_tets = ctx->n_tets;
         a.qm_dt = (float)(q_over_m * dt);
         a.dt = (float)dt;
         a.walk_limit = ctx->walk_limit;
         a.absorb = ctx->walk_absorb;
         a.fixed = ctx->scatter_mode == MP_SCATTER_FIXED64;
         a.track_ids = ctx->track_ids;
-        const size_t band_smem = sizeof(TetRec32) * MIX_BAND_MAX;
-        if (!ctx->push_grid[1]) {
-            cudaFuncSetAttribute(k_push_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band_smem);
-            ctx->push_grid[1] = grid_for(ctx, (const void *)k_push_mixed, PUSH_THREADS, band_smem);
-        }
+        if (!ctx->push_grid[1]) ctx->push_grid[1] = grid_for(ctx, (const void *)k_push_mixed, PUSH_THREADS, 0);
         long long g = blocks < ctx->push_grid[1] ? blocks : ctx->push_grid[1];
         cudaEventRecord(ctx->tp.a, ctx->stream);
-        k_push_mixed<<<(unsigned)g, PUSH_THREADS, band_smem, ctx->stream>>>(a), ++ctx->launches;
+        k_push_mixed<<<(unsigned)g, PUSH_THREADS, 0, ctx->stream>>>(a), ++ctx->launches;
         cudaEventRecord(ctx->tp.b, ctx->stream);
     }
     MP_CUDA(ctx, cudaGetLastError());

@@ -269,15 +269,32 @@ __global__ void __launch_bounds__(256) k_gs_sweep(int n, long long ld, const dou
         const int row = r0 + (r < kb ? r : 0);
         const double *arow = A + (long long)row * ld + q * 16;
         double acc = 0.0, ap[16], xv[16];
-        // columns right of the block: x_old, available now
-        for (int c = blk + 1; c < nblk; c++) {
-            const int c0 = c * NB + q * 16;
-            if (c0 + 16 <= n) {
-                load16<double, false>(arow + c * NB, ap);
-                load16<double, false>(x_old + c0, xv);
+        // columns right of the block: x_old, available now.  The next chunk's
+        // row piece and x piece are loaded while this one is summed, so two
+        // chunks per thread are in flight (a CTA streams 64 rows of J).
+        {
+            const int nfull = n / NB;  // chunks inside n
+            int c = blk + 1;
+            double apn[16], xvn[16];
+            if (c < nfull) {
+                load16<double, false>(arow + c * NB, apn);
+                load16<double, false>(x_old + c * NB + q * 16, xvn);
+            }
+            for (; c < nfull; c++) {
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    ap[k] = apn[k];
+                    xv[k] = xvn[k];
+                }
+                if (c + 1 < nfull) {
+                    load16<double, false>(arow + (c + 1) * NB, apn);
+                    load16<double, false>(x_old + (c + 1) * NB + q * 16, xvn);
+                }
 #pragma unroll
                 for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
-            } else {
+            }
+            for (; c < nblk; c++) {  // the last, partial chunk
+                const int c0 = c * NB + q * 16;
                 for (int k = 0; k < 16 && c0 + k < n; k++) acc = fma(arow[c * NB + k], x_old[c0 + k], acc);
             }
         }

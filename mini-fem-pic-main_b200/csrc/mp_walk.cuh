@@ -33,27 +33,6 @@ __device__ __forceinline__ void numerators_fp64(const TetRec *__restrict__ t, do
     }
 }
 
-// The same numerators from a record in shared or global memory (generic loads).
-__device__ __forceinline__ void numerators_fp64_any(const TetRec *t, double x, double y, double z, double q[4]) {
-    const double2 *a2 = reinterpret_cast<const double2 *>(t->alpha);
-    const double2 *b2 = reinterpret_cast<const double2 *>(t->beta);
-    const double2 *g2 = reinterpret_cast<const double2 *>(t->gamma);
-    const double2 *d2 = reinterpret_cast<const double2 *>(t->delta);
-    double al[4], be[4], ga[4], de[4];
-    double2 v;
-    v = a2[0]; al[0] = v.x; al[1] = v.y; v = a2[1]; al[2] = v.x; al[3] = v.y;
-    v = b2[0]; be[0] = v.x; be[1] = v.y; v = b2[1]; be[2] = v.x; be[3] = v.y;
-    v = g2[0]; ga[0] = v.x; ga[1] = v.y; v = g2[1]; ga[2] = v.x; ga[3] = v.y;
-    v = d2[0]; de[0] = v.x; de[1] = v.y; v = d2[1]; de[2] = v.x; de[3] = v.y;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        double w = __dsub_rn(al[i], __dmul_rn(x, be[i]));
-        w = __dadd_rn(w, __dmul_rn(y, ga[i]));
-        w = __dsub_rn(w, __dmul_rn(z, de[i]));
-        q[i] = __dmul_rn(ONE_SIXTH, w);
-    }
-}
-
 // The reference's lambda_i = q_i/volume, correctly rounded.
 __device__ __forceinline__ void lambdas_fp64(const TetRec *__restrict__ t, double x, double y, double z,
                                              double lc[4]) {

@@ -69,6 +69,8 @@ EXPORTED = [
     "mp_set_kernel_timing", "mp_kernel_timing",
 ]
 KT_PUSH, KT_UPDATE, KT_DIAG, KT_PANEL, KT_TRSV = 0, 1, 2, 3, 4
+# the classes a timed run brackets with events: few launches a step each
+KT_TIMED = (1 << KT_PUSH) | (1 << KT_UPDATE) | (1 << KT_TRSV)
 
 
 class MpError(RuntimeError):
@@ -567,8 +569,10 @@ class Context:
         self._c(lib().mp_set_fe_storage(self.h, storage))
 
     def set_kernel_timing(self, on=True):
-        """CUDA events around every launch of the kernel classes (KT_*); resets the clocks."""
-        self._c(lib().mp_set_kernel_timing(self.h, 1 if on else 0))
+        """CUDA events around every launch of the kernel classes (KT_*); resets
+        the clocks.  on: True (every class), False, or a bit mask of classes."""
+        mask = (1 if on else 0) if isinstance(on, bool) else int(on)
+        self._c(lib().mp_set_kernel_timing(self.h, mask))
 
     def kernel_timing(self, kclass: int) -> dict:
         """launches, device ms and algorithmic work (bytes or flops) of a kernel class."""

@@ -62,7 +62,7 @@ def _steps(c, form, cfg, deck, steps, warmup, torch, device, keep):
     out = {"step_ms": [], "newton_ms": [], "push_ms": [], "n": [], "lost": []}
     for k in range(warmup + steps):
         if k == warmup:
-            c.set_kernel_timing(True)
+            c.set_kernel_timing(mp.KT_TIMED)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         c.inject_device(inj, P.plasma_den, P.ion_velocity, cfg["dt"], cfg["spwt"], sigma, qm, 1000, k)

@@ -169,7 +169,8 @@ def push_driver(args):
         ctx.close()
 
 
-METHODS = {"lapack": mp.LAPACK, "sparse_cg": mp.SPARSE_CG, "sparse_newton": mp.SPARSE_NEWTON}
+METHODS = {"lapack": mp.LAPACK, "sparse_cg": mp.SPARSE_CG, "sparse_newton": mp.SPARSE_NEWTON,
+           "gs": mp.GAUSS_SEIDEL, "nonlinear": mp.NONLINEAR}
 
 
 def newton_driver(args):
@@ -189,14 +190,20 @@ def newton_driver(args):
         ctx.append(pos, vel, cell)
         ctx.push(mp.QE / (16 * mp.AMU), cfg["dt"], cfg["spwt"] * cfg["n_ions"] / len(cell))
         out = []
+        if getattr(args, "ktime", False):
+            ctx.set_kernel_timing(True)
         for k in range(args.steps):
             st = ctx.compute_phi(METHODS[getattr(args, "method", "lapack")], form)
             out.append({"step": k, "newton_ms": st.ms_total, "factor_ms": st.ms_factor,
-                        "refinements": st.linear_iterations, "residual": st.linear_residual})
+                        "newton_iterations": st.newton_iterations, "linear_iterations": st.linear_iterations,
+                        "linear_failures": st.linear_failures, "residual": st.linear_residual})
+        classes = {name: ctx.kernel_timing(kc) for name, kc in
+                   (("update", mp.KT_UPDATE), ("diag", mp.KT_DIAG), ("panel", mp.KT_PANEL), ("trsv", mp.KT_TRSV))
+                   } if getattr(args, "ktime", False) else None
         print(json.dumps({"driver": "newton", "config": cfg["label"], "form": args.form,
                           "method": getattr(args, "method", "lapack"), "storage": getattr(args, "storage", "dense"),
                           "mixed_factor": getattr(args, "mixed_factor", "tf32x3"),
-                          "unknowns": int(fe_arrays(cfg, deck)["neq"]), "steps": out}))
+                          "unknowns": int(fe_arrays(cfg, deck)["neq"]), "steps": out, "kernel_classes": classes}))
         ctx.close()
 
 
@@ -212,6 +219,7 @@ def main():
                     help="tensor-core arithmetic of the mixed-form factorization (newton driver)")
     ap.add_argument("--method", default="lapack", choices=sorted(METHODS), help="newton driver")
     ap.add_argument("--storage", default="dense", choices=["dense", "sparse"], help="newton driver: storage of K")
+    ap.add_argument("--ktime", action="store_true", help="newton driver: CUDA-event times of the kernel classes")
     args = ap.parse_args()
     (push_driver if args.driver == "push" else newton_driver)(args)
 
