@@ -489,6 +489,8 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(int n, long long ld, const T *
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
         for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = __ldg(&Linv[(size_t)blk * NB * NB + idx]);
+        // this block's right-hand side is no other block's output: read it before waiting
+        const T rhs = (q == 0 && r < kb) ? __ldcg(&x[r0 + r]) : T(0);
         const T *row = A + (long long)(r0 + (r < kb ? r : 0)) * ld + q * 16;
         T acc = 0, ap[16], xv[16];
         int done = 0;  // column chunks [0, done) accumulated
@@ -520,7 +522,7 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(int n, long long ld, const T *
         }
         acc += __shfl_xor_sync(0xffffffffu, acc, 1);
         acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        if (q == 0) srhs[r] = r < kb ? __ldcg(&x[r0 + r]) - acc : T(0);
+        if (q == 0) srhs[r] = r < kb ? rhs - acc : T(0);
         __syncthreads();
         T v = 0;
 #pragma unroll
@@ -564,6 +566,8 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(int n, long long ld, const T *
     for (int g = blockIdx.x; g < nblk; g += gridDim.x) {
         const int blk = nblk - 1 - g;
         const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
+        // D^-1 z of this block: final before the kernel started, read before waiting
+        const T rhs = (t < NB && t < kb) ? __ldcg(&x[r0 + t]) / dvec[r0 + t] : T(0);
         for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = __ldg(&Linv[(size_t)blk * NB * NB + idx]);
         T acc[4] = {0, 0, 0, 0}, ap[4][4];
         // rows c*NB + 4*part + e, columns r0 + 4*c4 .. +3 (zero past n; every block before the last is full)
@@ -619,7 +623,7 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(int n, long long ld, const T *
             T sum = 0;
 #pragma unroll
             for (int pp = 0; pp < 16; pp++) sum += spart[pp][t];
-            srhs[t] = t < kb ? __ldcg(&x[r0 + t]) / dvec[r0 + t] - sum : T(0);
+            srhs[t] = t < kb ? rhs - sum : T(0);
         }
         __syncthreads();
         // y = Linv^T srhs

@@ -136,6 +136,11 @@ static int ensure_scratch(mp_ctx *ctx, SolveScratch **out) {
     return MP_OK;
 }
 
+// Mixed-form refinement stop: ||G - J y|| <= REFINE_RTOL ||G|| (or the
+// residual stalls above 0.7 of the previous one): the FP64 factorization's
+// accuracy, so y matches dsysv_'s to the FP64 form's tolerance.
+constexpr double REFINE_RTOL = 1e-14;
+
 int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
     SolveScratch *sp = nullptr;
     int rc = ensure_scratch(ctx, &sp);
@@ -179,7 +184,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         for (; it < 60; it++) {
             rc = resid_norms(ctx, ctx->y, ctx->G, sc.r, sc.b32, &rn, &bn);
             if (rc) return rc;
-            if (!(rn > 1e-14 * bn) || rn > 0.7 * prev) break;
+            if (!(rn > REFINE_RTOL * bn) || rn > 0.7 * prev) break;
             prev = rn;
             rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, sc.b32, w, false);
             if (rc) return rc;
@@ -268,6 +273,8 @@ __global__ void __launch_bounds__(256) k_gs_sweep(int n, long long ld, const dou
         for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = __ldg(&Minv[(size_t)blk * NB * NB + idx]);
         const int row = r0 + (r < kb ? r : 0);
         const double *arow = A + (long long)row * ld + q * 16;
+        // this row's diagonal, old value and right-hand side, read before the wait
+        const double d_rr = A[(long long)row * ld + row], xo_r = x_old[row], b_r = b[row];
         double acc = 0.0, ap[16], xv[16];
         // columns right of the block: x_old, available now.  The next chunk's
         // row piece and x piece are loaded while this one is summed, so two
@@ -335,10 +342,7 @@ __global__ void __launch_bounds__(256) k_gs_sweep(int n, long long ld, const dou
         acc += __shfl_xor_sync(0xffffffffu, acc, 2);
         if (q == 0) {
             double cv = 0.0;
-            if (r < kb) {
-                const double d = A[(long long)(r0 + r) * ld + r0 + r];
-                cv = fabs(d) < 1e-12 ? x_old[r0 + r] : b[r0 + r] - acc;
-            }
+            if (r < kb) cv = fabs(d_rr) < 1e-12 ? xo_r : b_r - acc;
             sc[r] = cv;
         }
         __syncthreads();
