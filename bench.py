@@ -61,6 +61,13 @@ POP_SEED = 4321
 QM = mp.QE / (16 * mp.AMU)
 SIGMA = float(np.sqrt(KTI_EV * mp.QE / (16 * mp.AMU)))
 LEGS = ("kuhn20", "nonlinear", "adjoint", "sparse64", "vtk")
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one ncu capture
+# per kernel, per unit of its algorithmic work; a launch's traffic is scaled by
+# its units (profiles/k_update_tc_kuhn20_newton.md: 444.3 MB for a K = 1,024
+# trailing update of 55.4 GFLOP; profiles/k_push_*_kuhn20_2M.md: 160.5 MB and
+# 65.1 MB for 1.99M particles, in and out)
+TRAFFIC_PER_UNIT = {("tc", "update"): 444.3e6 / 55.4e9, ("fp64", "push"): 160.5e6 / (2 * 1.99e6),
+                    ("mixed", "push"): 65.1e6 / (2 * 1.99e6)}
 KT_NAMES = {mp.KT_PUSH: "push", mp.KT_UPDATE: "trailing_update", mp.KT_DIAG: "diagonal_factor",
             mp.KT_PANEL: "panel", mp.KT_TRSV: "triangular_solve"}
 KT_KERNEL = {mp.KT_PUSH: {mp.FP64: "k_push_fp64", mp.MIXED: "k_push_mixed"},
@@ -178,6 +185,10 @@ def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True):
         out.update(bound="hbm", achieved=ach, peak=pk["hbm_gbs"], unit="GB/s", frac=ach / pk["hbm_gbs"],
                    peak_kind=pk["kind"] + " HBM copy",
                    algorithmic="(particles before + after the push) x %d B" % (52 if form == mp.FP64 else 28))
+        key = ("fp64" if form == mp.FP64 else "mixed", "push")
+        bpp = 52.0 if form == mp.FP64 else 28.0
+        out["traffic"] = TRAFFIC_PER_UNIT[key] * v["work"] / bpp / max(v["launches"], 1)
+        out["traffic_source"] = "ncu DRAM bytes per particle (20^3 box, 2M ions) x this launch's particles"
     elif top == mp.KT_UPDATE:
         ach = v["work"] / (v["ms"] * 1e-3) / 1e12
         peak = pk["bf16_tflops_sustained"] if sustained else pk["bf16_tflops"]
@@ -188,11 +199,21 @@ def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True):
             out["note"] = ("kind::tf32 MMAs run at half the bf16 rate, and the 3xTF32 split issues three per "
                            "term: issued TF32 rate = 3 x achieved")
             out["tf32_issued_frac_of_half_bf16_peak"] = 3 * ach / (peak / 2)
+            out["traffic"] = TRAFFIC_PER_UNIT[("tc", "update")] * v["work"] / max(v["launches"], 1)
+            out["traffic_source"] = ("ncu DRAM bytes per flop of a K = 1,024 trailing update (8,379 unknowns) x "
+                                     "this workload's average flops per launch (the strips, K = 256, move more "
+                                     "bytes per flop: an estimate)")
     else:
         out.update(bound="latency", achieved=None, peak=None, unit=None, frac=None,
                    note="a serial chain of small launches; no throughput bound applies")
-    out["traffic"] = None
+    out.setdefault("traffic", None)
     out["classes"] = share
+    p = classes.get(mp.KT_PUSH)
+    if p and p["ms"] > 0:
+        gbs = p["work"] / (p["ms"] * 1e-3) / 1e9
+        out["push_kernel"] = {"kernel": KT_KERNEL[mp.KT_PUSH][form], "achieved": gbs, "unit": "GB/s",
+                              "frac": gbs / pk["hbm_gbs"], "avg_launch_ms": p["ms"] / max(p["launches"], 1),
+                              "bytes_per_particle_step": 104 if form == mp.FP64 else 56}
     return out
 
 
@@ -372,7 +393,11 @@ def run_kuhn20(args, device, torch, flush, pk):
                                       "launches": t["launches"], "avg_launch_ms": t["ms"] / max(t["launches"], 1),
                                       "peak_kind": pk["kind"] + " HBM copy",
                                       "bytes_per_particle_step": 104 if form == mp.FP64 else 56,
-                                      "traffic": None}}
+                                      "traffic": TRAFFIC_PER_UNIT[(name, "push")] * t["work"] /
+                                      (52.0 if form == mp.FP64 else 28.0) / max(t["launches"], 1),
+                                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per "
+                                                        "particle of one launch on this workload x the launch's "
+                                                        "particles"}}
             if name == "fp64":
                 keep = c
             else:
