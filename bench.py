@@ -336,9 +336,13 @@ def run_headline(args, device, rank, world, torch, flush, pk):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         cm.append(hp, hv, hc, rewind=True, q_over_m=QM, half_dt=0.5 * dt)
-        st = cm.push(QM, dt, spwt_push, den_out=den_host)
         if world > 1:
+            # the density read back is the one summed over ranks
+            st = cm.push(QM, dt, spwt_push)
             sharding.allreduce_density(cm, device)
+            cm._c(mp.lib().mp_density_download(cm.h, mp._p(den_host)))
+        else:
+            st = cm.push(QM, dt, spwt_push, den_out=den_host)
         cm.compute_phi(mp.LAPACK, mp.MIXED)
         cm.update_ef()
         cm._c(mp.lib().mp_field_download(cm.h, None, mp._p(uh_host), None))
