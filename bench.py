@@ -71,10 +71,10 @@ TRAFFIC_PER_UNIT = {("tc", "update"): 444.3e6 / 55.4e9, ("fp64", "push"): 160.5e
 KT_NAMES = {mp.KT_PUSH: "push", mp.KT_UPDATE: "trailing_update", mp.KT_DIAG: "diagonal_factor",
             mp.KT_PANEL: "panel", mp.KT_TRSV: "triangular_solve"}
 KT_KERNEL = {mp.KT_PUSH: {mp.FP64: "k_push_fp64", mp.MIXED: "k_push_mixed"},
-             mp.KT_UPDATE: {mp.FP64: "k_update_f64", mp.MIXED: "tc::k_update_tc<true> (3xTF32, tcgen05)"},
+             mp.KT_UPDATE: {mp.FP64: "k_update_f64", mp.MIXED: "tc::k_update_tc (tcgen05)"},
              mp.KT_DIAG: {mp.FP64: "k_ldlt_diag<double>", mp.MIXED: "k_ldlt_diag<float>"},
              mp.KT_PANEL: {mp.FP64: "k_ldlt_panel<double>", mp.MIXED: "k_ldlt_panel<float>"},
-             mp.KT_TRSV: {mp.FP64: "k_trsv_fwd/bwd<double>", mp.MIXED: "k_trsv_fwd/bwd<float>"}}
+             mp.KT_TRSV: {mp.FP64: "k_trsv_ll<double>", mp.MIXED: "k_trsv_ll<float>"}}
 
 
 def peaks():
@@ -167,7 +167,13 @@ def load_population(c, pos, vel, cell, form, chunk=8_000_000):
         c.set_form(mp.MIXED)
 
 
-def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True):
+def mixed_terms(neq):
+    """TF32 products per term of the mixed factorization's trailing update
+    under the library's default (MIXED_AUTO)."""
+    return 1 if neq >= mp.MIXED_TF32_FROM else 3
+
+
+def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True, neq=0):
     """The kernel classes' device time in the timed region and the roofline of
     the one with the largest share."""
     classes = {k: ctx.kernel_timing(k) for k in KT_NAMES if mp.KT_TIMED >> k & 1}
@@ -178,7 +184,11 @@ def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True):
         "what": "not bracketed by events in the timed run (hundreds of small launches a step)"}
     top = max(classes, key=lambda k: classes[k]["ms"])
     v = classes[top]
-    out = {"kernel": KT_KERNEL[top][form], "class": KT_NAMES[top], "launches": v["launches"],
+    terms = mixed_terms(neq)
+    kname = KT_KERNEL[top][form]
+    if top == mp.KT_UPDATE and form == mp.MIXED:
+        kname = "tc::k_update_tc<%s> (%s, tcgen05)" % (("true", "3xTF32") if terms == 3 else ("false", "TF32"))
+    out = {"kernel": kname, "class": KT_NAMES[top], "launches": v["launches"],
            "avg_launch_ms": v["ms"] / max(v["launches"], 1)}
     if top == mp.KT_PUSH:
         ach = v["work"] / (v["ms"] * 1e-3) / 1e9
@@ -196,9 +206,10 @@ def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True):
                    peak_kind=pk["kind"] + (" bf16 dense, sustained" if sustained else " bf16 dense, burst"),
                    algorithmic="2 flops per multiply-add of the trailing update's lower triangle")
         if form == mp.MIXED:
-            out["note"] = ("kind::tf32 MMAs run at half the bf16 rate, and the 3xTF32 split issues three per "
-                           "term: issued TF32 rate = 3 x achieved")
-            out["tf32_issued_frac_of_half_bf16_peak"] = 3 * ach / (peak / 2)
+            out["note"] = ("kind::tf32 MMAs run at half the bf16 rate" +
+                           (", and the 3xTF32 split issues three per term: issued TF32 rate = 3 x achieved"
+                            if terms == 3 else "; one TF32 product per term"))
+            out["tf32_issued_frac_of_half_bf16_peak"] = terms * ach / (peak / 2)
             out["traffic"] = TRAFFIC_PER_UNIT[("tc", "update")] * v["work"] / max(v["launches"], 1)
             out["traffic_source"] = ("ncu DRAM bytes per flop of a K = 1,024 trailing update (8,379 unknowns) x "
                                      "this workload's average flops per launch (the strips, K = 256, move more "
@@ -293,7 +304,7 @@ def run_headline(args, device, rank, world, torch, flush, pk):
         torch.distributed.barrier()
     out = {"cfg": cfg, "deck": deck, "neq": neq, "n0": n0, "res": res, "clocks": clk,
            "launches": {n: ctxs[n][0].launches() - launches0[n] for n in ctxs}}
-    out["roofline"] = {n: kernel_roofline(ctxs[n][0], ctxs[n][1], pk, float(np.sum(res[n]["step_ms"])))
+    out["roofline"] = {n: kernel_roofline(ctxs[n][0], ctxs[n][1], pk, float(np.sum(res[n]["step_ms"])), neq=neq)
                        for n in ctxs}
     for c, _, _ in ctxs.values():
         c.set_kernel_timing(False)
@@ -823,8 +834,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded Kuhn-box ions at steady state; device injection with the reference's counts)",
             "config": conf,
-            "form": "mixed: FP32 tet-relative particles, FP64 near-face test and density, 3xTF32 tcgen05 LDL^T "
-                    "with FP64 refinement",
+            "form": "mixed: FP32 tet-relative particles, FP64 near-face test and density, %s tcgen05 LDL^T "
+                    "with FP64 refinement" % ("TF32" if mixed_terms(h["neq"]) == 1 else "3xTF32"),
             "parallelism": f"particles sharded x{world}, density all-reduce, field solve replicated"
             if world > 1 else "1 GPU",
             "l2": f"inputs larger than L2 (the particle arrays); {FLUSH_BYTES >> 20} MiB written between steps",

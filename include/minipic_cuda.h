@@ -91,7 +91,7 @@ enum { MP_FORM_FP64 = 0, MP_FORM_MIXED = 1 };
 /* Tensor-core arithmetic of the mixed form's FP32 factorization: one TF32
  * product per term, or the 3xTF32 split (hi*hi + hi*lo + lo*hi, about FP32
  * accuracy; fewer FP64 refinement iterations). */
-enum { MP_MIXED_TF32 = 1, MP_MIXED_TF32X3 = 3 };
+enum { MP_MIXED_AUTO = 0, MP_MIXED_TF32 = 1, MP_MIXED_TF32X3 = 3 };
 
 /* What a walk that reaches the hop limit does.  In a mesh with a cavity (the
  * sphere workload) a particle that steps into the cavity lies in no tet, and
@@ -198,9 +198,15 @@ int mp_set_sort_period(mp_ctx *ctx, int32_t steps);
  * both, and its walk (src/meshes.h:75-100) would then never end.  Converts the
  * resident particles (holes removed first). */
 int mp_set_particle_form(mp_ctx *ctx, int form);
-/* Arithmetic of the mixed-form Newton factorization (MP_MIXED_TF32 or
- * MP_MIXED_TF32X3, the default).  No reference counterpart: the reference's
- * dsysv_ call (src/FESolver.cpp:528-558) is FP64 throughout. */
+/* Arithmetic of the mixed-form Newton factorization: MP_MIXED_TF32 (one TF32
+ * product per term; more FP64 refinement solves), MP_MIXED_TF32X3 (hi/lo split,
+ * three TF32 products a term; about FP32 accuracy, fewer refinement solves) or
+ * MP_MIXED_AUTO, the default: TF32X3 below MP_MIXED_TF32_FROM unknowns, where
+ * the refinement solves cost more than the trailing update saves, TF32 from
+ * there on.  Either way the solve is refined in FP64 to the same tolerance.  No
+ * reference counterpart: the reference's dsysv_ call (src/FESolver.cpp:528-558)
+ * is FP64 throughout. */
+#define MP_MIXED_TF32_FROM 16384
 int mp_set_mixed_factor(mp_ctx *ctx, int mode);
 /* Particle IDs (16 B per particle-step of traffic) are needed only to restore
  * injection order after tet re-sorting; without sorting the stable removal

@@ -134,7 +134,7 @@ struct mp_ctx {
     int walk_limit = 4096;
     bool walk_absorb = false;             // hop limit: absorb the particle instead of raising MP_ERR_WALK_LIMIT
     int sort_period = 0;
-    int mixed_factor = MP_MIXED_TF32X3;  // tensor-core terms of the mixed factorization
+    int mixed_factor = MP_MIXED_AUTO;    // tensor-core terms of the mixed factorization
     long long steps_since_sort = 0;
     bool track_ids = true;
     long long capacity = 0;
@@ -193,7 +193,7 @@ struct mp_ctx {
     // dense-solve scratch (mp_solve.cu): W panels, block inverses, ready words;
     // sized for neq, allocated on the first factorization
     void *solve_scratch = nullptr;
-    int solve_epoch = 0;                  // ready-word epoch of this context's triangular solves
+    int solve_epoch = 0;                  // epoch of this context's wavefront words (solves, sweeps)
     bool ldlt_attr = false;               // >48 KB shared-memory attributes set for this context's device
     // device staging of host appends and downloads
     void *dstage = nullptr;

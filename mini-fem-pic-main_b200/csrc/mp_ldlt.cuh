@@ -37,156 +37,132 @@ __device__ __forceinline__ bool bad_pivot(T d) {
     return !(fabs((double)d) > 0.0) || !isfinite((double)d);
 }
 
+// 4 consecutive values (16-byte aligned for float, 32 for double) as vector loads
+template <typename T>
+__device__ __forceinline__ void load4p(const T *p, T *v) {
+    if constexpr (sizeof(T) == 8) {
+        const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+        const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else {
+        const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    }
+}
+
 // Factor the kb x kb diagonal block at (k0,k0): L (strict lower) and D written
 // back, and Linv = L_kk^-1 (unit lower, row-major NB x NB, zero outside kb x kb)
 // for the panel and the triangular solves.  If b is non-null,
 // z_k = L_kk^-1 b_k (the forward substitution riding on the factorization).
+// The block is padded to 64 x 64 with an identity.
 //
-// 256 threads, the block in shared memory (padded to 64 x 64 with an identity).
-// Four sub-panels of SUB = 16 columns:
-//   factor the sub-panel (64 x 16): 16 elimination steps, one barrier each;
-//     thread (row i, column quad g) updates its 4 columns from the step's
-//     published column (double-buffered), and the rows of the sub-panel's
-//     16 x 16 diagonal block apply the same row operation to an identity,
-//     which leaves that block's inverse;
-//   rank-16 update of the trailing block, 4 x 4 register tiles per thread.
-// The off-diagonal blocks of Linv follow by block substitution:
-//   X_qp = -X_qq sum_{r=p}^{q-1} L_qr X_rp.
-// Dynamic smem: A [64][65], Linv [64][65], W [64][17], T [16][17], w [2][64], b [64].
-constexpr int SUB = 16;
-
+// The block and its inverse live in registers: thread
+// (ti, tc) of 256 holds the 4 x 4 tiles at rows 4ti.., columns 4tc.. of the
+// block and of Linv (and, for tc == 0, b at rows 4ti..).  Elimination step j,
+// one barrier: the owners of column j of the block, of row j of Linv and of
+// b_j publish them in shared memory (double-buffered), the owner of the pivot
+// also 1/d_j; every thread forms its rows' multipliers l_i = A_ij / d_j (i > j)
+// and updates its tiles, A_ic -= l_i A_cj (c > j) and Linv_ic -= l_i Linv_jc,
+// and b_i -= l_i b_j; the owners of column j keep l_i there (L).  The step
+// loop is unrolled by four so every register index is a constant.
 template <typename T>
-__global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
-                                                   T *b, unsigned long long *flags) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T(*sA)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
-    T(*sI)[NB + 1] = sA + NB;
-    T(*sW)[SUB + 1] = reinterpret_cast<T(*)[SUB + 1]>(sI + NB);
-    T(*sT)[SUB + 1] = sW + NB;
-    T *sw = reinterpret_cast<T *>(sT + SUB);  // [2][NB]
-    T *sb = sw + 2 * NB;
-    const int t = threadIdx.x;
-    // load the lower triangle, pad with an identity past kb; Linv starts as the identity
-    {
-        T v[16];
+__global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec,
+                                                      T *Linv, T *b, unsigned long long *flags) {
+    __shared__ __align__(16) T scol[2][NB];
+    __shared__ __align__(16) T srow[2][NB];
+    __shared__ T spiv[2][2];  // d_j, 1/d_j
+    __shared__ T sbj[2];
+    const int t = threadIdx.x, ti = t >> 4, tc = t & 15;
+    T a[4][4], li[4][4], bb[4];
 #pragma unroll
-        for (int q = 0; q < 16; q++) {
-            const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
-            v[q] = (r < kb && c < kb && c <= r) ? A[(long long)(k0 + r) * ld + k0 + c] : T(0);
+    for (int u = 0; u < 4; u++) {
+        const int r = 4 * ti + u;
+        const T *row = A + (long long)(k0 + r) * ld + k0 + 4 * tc;
+        T v4[4] = {T(0), T(0), T(0), T(0)};
+        if (r < kb) {
+            if (4 * tc + 3 < kb) {
+                load4p<T>(row, v4);
+            } else {
+#pragma unroll
+                for (int v = 0; v < 4; v++)
+                    if (4 * tc + v < kb) v4[v] = row[v];
+            }
         }
 #pragma unroll
-        for (int q = 0; q < 16; q++) {
-            const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
-            sA[r][c] = (r >= kb && r == c) ? T(1) : v[q];
-            sI[r][c] = r == c ? T(1) : T(0);
+        for (int v = 0; v < 4; v++) {
+            const int c = 4 * tc + v;
+            a[u][v] = r < kb ? (c <= r ? v4[v] : T(0)) : (r == c ? T(1) : T(0));
+            li[u][v] = r == c ? T(1) : T(0);
         }
+        bb[u] = (b && tc == 0 && r < kb) ? b[k0 + r] : T(0);
     }
-    if (b && t < NB) sb[t] = t < kb ? b[k0 + t] : T(0);
-    __syncthreads();
-    if (t < NB) sw[t] = sA[t][0];  // publish column 0
-    __syncthreads();
-    const int i = t >> 2, g = t & 3;  // this thread's row and column quad in the sub-panel
     bool singular = false;
-    for (int p = 0; p < NB / SUB; p++) {
-        const int c0 = p * SUB;
-        // ---- factor the sub-panel: columns [c0, c0+16), rows [c0, 64) ----
-        for (int j = c0; j < c0 + SUB; j++) {
-            const T *w = sw + (j & 1) * NB;
-            T d = w[j];
-            if (bad_pivot(d)) {
-                singular = true;
-                d = T(1);
-            }
-            const T rd = T(1) / d;
-            const T wi = w[i];
-            const T li = wi * rd;  // L[i][j] for i > j
-            if (i > j) {
+    int buf = 0;
+    for (int jj = 0; jj < NB / 4; jj++) {
 #pragma unroll
-                for (int cc = 0; cc < 4; cc++) {
-                    const int col = c0 + 4 * g + cc;
-                    if (col > j && col <= i) sA[i][col] -= li * w[col];
-                    if (col == j) sA[i][j] = li;
-                    // the sub-panel's diagonal block: the same row operation on the identity
-                    if (i < c0 + SUB && col <= j) sI[i][col] -= li * sI[j][col];
+        for (int jr = 0; jr < 4; jr++) {
+            const int j = 4 * jj + jr;
+            if (tc == jj) {
+#pragma unroll
+                for (int u = 0; u < 4; u++) scol[buf][4 * ti + u] = a[u][jr];
+                if (ti == jj) {
+                    T d = a[jr][jr];
+                    if (bad_pivot(d)) {
+                        singular = true;
+                        d = T(1);
+                    }
+                    spiv[buf][0] = d;
+                    spiv[buf][1] = T(1) / d;
                 }
             }
-            // publish column j+1 (final for this step once its own update above has run)
-            if (j + 1 < c0 + SUB && 4 * g <= j + 1 - c0 && j + 1 - c0 < 4 * g + 4) sw[((j + 1) & 1) * NB + i] = sA[i][j + 1];
+            if (ti == jj) {
+#pragma unroll
+                for (int v = 0; v < 4; v++) srow[buf][4 * tc + v] = li[jr][v];
+                if (tc == 0) sbj[buf] = bb[jr];
+            }
             __syncthreads();
-        }
-        if (p == NB / SUB - 1) break;
-        // ---- rank-16 update of the trailing block [c0+16, 64)^2 ----
-        const int e0 = c0 + SUB;
-        if (t < NB) {
+            const T rd = spiv[buf][1];
+            T l[4], w[4], lr[4];
 #pragma unroll
-            for (int jl = 0; jl < SUB; jl++) sW[t][jl] = sA[t][c0 + jl] * sA[c0 + jl][c0 + jl];
-        }
-        __syncthreads();
-        {
-            const int ti = t >> 4, tk = t & 15;
-            const int r0 = 4 * ti, q0 = 4 * tk;
-            if (r0 + 3 >= e0 && q0 + 3 >= e0 && q0 <= r0 + 3) {
-                T acc[4][4] = {};
+            for (int u = 0; u < 4; u++) {
+                l[u] = 4 * ti + u > j ? scol[buf][4 * ti + u] * rd : T(0);
+                w[u] = 4 * tc + u > j ? scol[buf][4 * tc + u] : T(0);
+                lr[u] = srow[buf][4 * tc + u];
+            }
 #pragma unroll
-                for (int jl = 0; jl < SUB; jl++) {
-                    T av[4], wv[4];
+            for (int u = 0; u < 4; u++)
 #pragma unroll
-                    for (int u = 0; u < 4; u++) av[u] = sA[r0 + u][c0 + jl];
-#pragma unroll
-                    for (int v = 0; v < 4; v++) wv[v] = sW[q0 + v][jl];
-#pragma unroll
-                    for (int u = 0; u < 4; u++)
-#pragma unroll
-                        for (int v = 0; v < 4; v++) acc[u][v] += av[u] * wv[v];
+                for (int v = 0; v < 4; v++) {
+                    a[u][v] = fma(-l[u], w[v], a[u][v]);
+                    li[u][v] = fma(-l[u], lr[v], li[u][v]);
                 }
+            if (tc == jj) {
 #pragma unroll
                 for (int u = 0; u < 4; u++)
-#pragma unroll
-                    for (int v = 0; v < 4; v++) {
-                        const int r = r0 + u, q = q0 + v;
-                        if (r >= e0 && q >= e0 && q <= r) sA[r][q] -= acc[u][v];
-                    }
+                    if (4 * ti + u > j) a[u][jr] = l[u];
             }
-        }
-        __syncthreads();
-        if (t < NB) sw[(e0 & 1) * NB + t] = sA[t][e0];  // publish the next sub-panel's first column
-        __syncthreads();
-    }
-    if (singular && t == 0) atomicOr(flags, FLAG_SINGULAR);
-    // ---- off-diagonal blocks of Linv, by block distance ----
-    for (int dist = 1; dist < NB / SUB; dist++) {
-        for (int p = 0; p + dist < NB / SUB; p++) {
-            const int q = p + dist;
-            const int a = t >> 4, c = t & 15;  // element (a, c) of the 16 x 16 block
-            // T = sum_{r=p}^{q-1} L_qr X_rp
-            T acc = 0;
-            for (int r = p; r < q; r++)
+            if (tc == 0) {
+                const T bj = sbj[buf];
 #pragma unroll
-                for (int m = 0; m < SUB; m++) acc += sA[q * SUB + a][r * SUB + m] * sI[r * SUB + m][p * SUB + c];
-            sT[a][c] = acc;
-            __syncthreads();
-            // X_qp = -X_qq T (X_qq unit lower)
-            T x = 0;
-#pragma unroll
-            for (int m = 0; m < SUB; m++) x += sI[q * SUB + a][q * SUB + m] * sT[m][c];
-            sI[q * SUB + a][p * SUB + c] = -x;
-            __syncthreads();
+                for (int u = 0; u < 4; u++) bb[u] = fma(-l[u], bj, bb[u]);
+            }
+            buf ^= 1;
         }
     }
-    // ---- write back L, D, Linv; z = Linv b ----
+    if (singular) atomicOr(flags, FLAG_SINGULAR);
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-        const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
-        const bool in = r < kb && c < kb;
-        if (in && c <= r) A[(long long)(k0 + r) * ld + k0 + c] = sA[r][c];
-        Linv[r * NB + c] = in ? sI[r][c] : T(0);
-    }
-    if (t < kb) {
-        dvec[k0 + t] = sA[t][t];
-        if (b) {
-            T z = 0;
-            for (int pp = 0; pp <= t; pp++) z += sI[t][pp] * sb[pp];
-            b[k0 + t] = z;
+    for (int u = 0; u < 4; u++) {
+        const int r = 4 * ti + u;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const int c = 4 * tc + v;
+            const bool in = r < kb && c < kb;
+            if (in && c <= r) A[(long long)(k0 + r) * ld + k0 + c] = a[u][v];
+            Linv[r * NB + c] = in ? li[u][v] : T(0);
+        }
+        if (r < kb) {
+            if (ti == tc) dvec[k0 + r] = a[u][u];
+            if (b && tc == 0) b[k0 + r] = bb[u];
         }
     }
 }
@@ -414,45 +390,107 @@ __global__ void __launch_bounds__(256, 1) k_update_f64(int n, long long ld, doub
 }
 
 // ---- triangular solves with an existing factor --------------------------------------
-// One persistent launch per direction.  CTA g takes row blocks g, g+G, ... (in
-// solve order); a block subtracts the contributions of the blocks already
-// solved (each published by a per-block ready word holding the solve's epoch,
-// stored with release semantics and polled with acquire loads), then applies
-// its diagonal block's stored inverse: the block's own solve is a 64 x 64
-// product, not a serial substitution.  Each poll takes every block already
-// published (up to 256) at once, and the operand chunk of the next awaited block
-// is loaded before the poll, so a block's wait ends one chunk behind the
-// wavefront.  The grid never exceeds the resident capacity, so the lowest
-// unsolved block always runs.  Waits are bounded (TRSV_SPIN_LIMIT empty polls);
-// a timeout sets the error flag.
+// One persistent cooperative launch per direction over 64-row blocks; CTA g
+// takes blocks g, g+G, ... in solve order, so the lowest unsolved block always
+// runs.  A solved block is published as low-latency words: each 8-byte word
+// holds 32 bits of a value and the solve's epoch in its upper half, written and
+// read as one relaxed gpu-scope 64-bit access (single-copy atomic), so a reader
+// that sees the epoch holds the value -- one L2 round trip per block instead of
+// a release flag followed by a load of the data.  One warp per CTA polls; the
+// others wait at the block barrier.
+//
+// A block sums the contributions of every solved block except its nearest
+// predecessor as they arrive (polling with a back-off that grows with its
+// distance from the front), applies its diagonal block's stored inverse, and
+// then waits for the predecessor alone, whose contribution is one 64 x 64
+// product with a coupling block computed once per factorization:
+//   forward  z_i = Linv_ii (b_i - sum_{j<i-1} L_ij z_j) - Mf_i z_{i-1},  Mf_i = Linv_ii L_{i,i-1}
+//   backward y_i = Linv_ii^T (D_i^-1 z_i - sum_{j>i+1} L_ji^T y_j) - Mb_i y_{i+1},
+//            Mb_i = Linv_ii^T L_{i+1,i}^T
+// so a step of the chain is a poll, 16 multiply-adds a thread, two shuffles and
+// a store.  Waits are bounded (TRSV_SPIN_LIMIT empty polls); a wait that gives
+// up sets the error flag and the block publishes what it has, so no other
+// block waits on it for long.
 constexpr long long TRSV_SPIN_LIMIT = 1ll << 20;
+constexpr int MS = NB + 4;  // row pitch of the shared inverse and coupling blocks: quad reads hit 32 banks
 
-__device__ __forceinline__ int ld_acquire(const int *p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ void st_ll(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_ll(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release(int *p, int v) {
-    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+
+// Words of block `blk`: FP32 one per value ([blk][64]); FP64 two, the low and
+// high halves in two planes ([blk][2][64]).
+template <typename T>
+__device__ __forceinline__ void ll_put(unsigned long long *ll, int blk, int r, T v, unsigned epoch) {
+    const unsigned long long e = (unsigned long long)epoch << 32;
+    if constexpr (sizeof(T) == 4) {
+        st_ll(ll + (size_t)blk * NB + r, e | __float_as_uint(v));
+    } else {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+        unsigned long long *p = ll + (size_t)blk * 2 * NB;
+        st_ll(p + r, e | (b & 0xffffffffull));
+        st_ll(p + NB + r, e | (b >> 32));
+    }
 }
 
-// Number of consecutive published blocks from `from` in direction `step`
-// (+1 or -1), at most `span`.  All threads call it; one round trip per call.
-__device__ __forceinline__ int ready_prefix(const int *ready, int from, int span, int step, int epoch, int *s_cnt) {
-    const int t = threadIdx.x;
-    const bool ok = t < span && ld_acquire(ready + from + step * t) == epoch;
-    const unsigned bal = __ballot_sync(0xffffffffu, ok);
-    if ((t & 31) == 0) s_cnt[t >> 5] = bal == 0xffffffffu ? 32 : __ffs(~bal) - 1;
-    __syncthreads();
-    int cnt = 0;
-    for (int w = 0; w < 8; w++) {
-        const int c = s_cnt[w];
-        cnt += c;
-        if (c < 32) break;
+// One poll of block c's 64 values by a whole warp; true (warp-uniform) when all
+// carry `epoch`, and then they are in dst[0..63].
+template <typename T>
+__device__ __forceinline__ bool ll_try(const unsigned long long *ll, int c, unsigned epoch, T *dst) {
+    const int lane = threadIdx.x & 31;
+    if constexpr (sizeof(T) == 4) {
+        const unsigned long long *p = ll + (size_t)c * NB;
+        const unsigned long long w0 = ld_ll(p + lane), w1 = ld_ll(p + 32 + lane);
+        const bool ok = (unsigned)(w0 >> 32) == epoch && (unsigned)(w1 >> 32) == epoch;
+        if (!__all_sync(0xffffffffu, ok)) return false;
+        dst[lane] = __uint_as_float((unsigned)w0);
+        dst[lane + 32] = __uint_as_float((unsigned)w1);
+    } else {
+        const unsigned long long *p = ll + (size_t)c * 2 * NB;
+        const unsigned long long l0 = ld_ll(p + lane), l1 = ld_ll(p + 32 + lane);
+        const unsigned long long h0 = ld_ll(p + NB + lane), h1 = ld_ll(p + NB + 32 + lane);
+        const bool ok = (unsigned)(l0 >> 32) == epoch && (unsigned)(l1 >> 32) == epoch &&
+                        (unsigned)(h0 >> 32) == epoch && (unsigned)(h1 >> 32) == epoch;
+        if (!__all_sync(0xffffffffu, ok)) return false;
+        dst[lane] = __longlong_as_double((long long)((h0 << 32) | (l0 & 0xffffffffull)));
+        dst[lane + 32] = __longlong_as_double((long long)((h1 << 32) | (l1 & 0xffffffffull)));
+    }
+    return true;
+}
+
+// All threads call it: warp 0 polls block c into dst (sleeping `backoff` ns
+// between empty polls), then the CTA meets at a barrier.  Returns false (and
+// raises the error flag) when the wait gave up.  `ok` is a shared slot that
+// alternates with dst, so a slot is rewritten only after every thread has
+// passed the next barrier.
+template <typename T>
+__device__ __forceinline__ bool wait_chunk(const unsigned long long *ll, int c, unsigned epoch, T *dst, int backoff,
+                                           int *ok, unsigned long long *flags) {
+    if (threadIdx.x < 32) {
+        bool got = false;
+        for (long long spins = 0; spins <= TRSV_SPIN_LIMIT; spins++) {
+            if (ll_try<T>(ll, c, epoch, dst)) {
+                got = true;
+                break;
+            }
+            if (backoff) __nanosleep(backoff);
+        }
+        if (threadIdx.x == 0) {
+            *ok = got ? 1 : 0;
+            if (!got) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
+        }
     }
     __syncthreads();
-    return cnt < span ? cnt : span;
+    return *ok != 0;
 }
+
+// sleep between empty polls for a block `dist` steps from the one it waits on
+__device__ __forceinline__ int poll_backoff(int dist) { return dist > 8 ? 512 : 64 * dist; }
 
 // 16 consecutive values (64-byte aligned for float, 128 for double) as vector loads
 template <typename T, bool CG>
@@ -476,184 +514,218 @@ __device__ __forceinline__ void load16(const T *p, T (&v)[16]) {
     }
 }
 
-// L z = b (unit lower, in place on x)
+
+// Shared memory of k_trsv_ll: inverse and coupling blocks, partial sums, two
+// poll buffers, the right-hand side, two poll results.
 template <typename T>
-__global__ void __launch_bounds__(256) k_trsv_fwd(int n, long long ld, const T *A, const T *Linv, T *x, int *ready,
-                                                  int epoch, unsigned long long *flags) {
-    __shared__ T sI[NB][NB + 1];
-    __shared__ T srhs[NB];
-    __shared__ int s_cnt[8];
-    const int nblk = (n + NB - 1) / NB;
-    const int t = threadIdx.x;
-    const int r = t >> 2, q = t & 3;  // row of the block, quarter of each 64-column chunk
-    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
-        const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
-        for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = __ldg(&Linv[(size_t)blk * NB * NB + idx]);
-        // this block's right-hand side is no other block's output: read it before waiting
-        const T rhs = (q == 0 && r < kb) ? __ldcg(&x[r0 + r]) : T(0);
-        const T *row = A + (long long)(r0 + (r < kb ? r : 0)) * ld + q * 16;
-        T acc = 0, ap[16], xv[16];
-        int done = 0;  // column chunks [0, done) accumulated
-        if (done < blk) load16<T, false>(row, ap);
-        long long spins = 0;
-        while (done < blk) {
-            const int span = blk - done < 256 ? blk - done : 256;
-            const int cnt = ready_prefix(ready, done, span, 1, epoch, s_cnt);
-            if (cnt == 0) {
-                if (++spins > TRSV_SPIN_LIMIT) {
-                    if (t == 0) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
-                    break;
-                }
-                __nanosleep(32);
-                continue;
-            }
-            const int avail = done + cnt;
-            load16<T, true>(x + done * NB + q * 16, xv);
-#pragma unroll
-            for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
-            for (int c = done + 1; c < avail; c++) {
-                load16<T, false>(row + c * NB, ap);
-                load16<T, true>(x + c * NB + q * 16, xv);
-#pragma unroll
-                for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
-            }
-            done = avail;
-            if (done < blk) load16<T, false>(row + done * NB, ap);
-        }
-        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        if (q == 0) srhs[r] = r < kb ? rhs - acc : T(0);
-        __syncthreads();
-        T v = 0;
-#pragma unroll
-        for (int k = 0; k < 16; k++) v = fma(sI[r][q * 16 + k], srhs[q * 16 + k], v);
-        v += __shfl_xor_sync(0xffffffffu, v, 1);
-        v += __shfl_xor_sync(0xffffffffu, v, 2);
-        if (q == 0 && r < kb) x[r0 + r] = v;
-        __syncthreads();
-        if (t == 0) st_release(ready + blk, epoch);
-    }
+constexpr size_t trsv_smem() {
+    return sizeof(T) * (2 * NB * MS + 16 * (NB + 1) + 3 * NB) + 2 * sizeof(int);
 }
 
-// 4 consecutive values (16-byte aligned for float, 32 for double) as vector loads
-template <typename T, bool CG>
-__device__ __forceinline__ void load4(const T *p, T (&v)[4]) {
-    if constexpr (sizeof(T) == 8) {
-        const double2 a = CG ? __ldcg(reinterpret_cast<const double2 *>(p)) : __ldg(reinterpret_cast<const double2 *>(p));
-        const double2 b = CG ? __ldcg(reinterpret_cast<const double2 *>(p) + 1)
-                             : __ldg(reinterpret_cast<const double2 *>(p) + 1);
-        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-    } else {
-        const float4 a = CG ? __ldcg(reinterpret_cast<const float4 *>(p)) : __ldg(reinterpret_cast<const float4 *>(p));
-        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-    }
-}
-
-// L^T y = D^-1 z (unit upper after scaling, in place on x), blocks from the last.
-// Thread (column quad c4, row quad part) takes a 4 x 4 piece of every later
-// 64 x 64 chunk with vector loads; the 16 partial sums of each column meet in
-// shared memory.
-template <typename T>
-__global__ void __launch_bounds__(256) k_trsv_bwd(int n, long long ld, const T *A, const T *Linv, const T *dvec, T *x,
-                                                  int *ready, int epoch, unsigned long long *flags) {
-    __shared__ T sI[NB][NB + 1];
-    __shared__ T srhs[NB];
-    __shared__ T spart[16][NB + 1];
-    __shared__ int s_cnt[8];
+// DIR = +1: L z = b (unit lower, in place on x); DIR = -1: L^T y = D^-1 z (in
+// place on x).  Mc holds the direction's coupling blocks; ll its words.
+template <typename T, int DIR>
+__global__ void __launch_bounds__(256) k_trsv_ll(int n, long long ld, const T *__restrict__ A,
+                                                 const T *__restrict__ Linv, const T *__restrict__ Mc,
+                                                 const T *__restrict__ dvec, T *x, unsigned long long *ll,
+                                                 unsigned epoch, unsigned long long *flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T(*sI)[MS] = reinterpret_cast<T(*)[MS]>(smem_raw);
+    T(*sC)[MS] = sI + NB;
+    T(*spart)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(sC + NB);
+    T *sx = reinterpret_cast<T *>(spart + 16);  // [2][NB]
+    T *srhs = sx + 2 * NB;
+    int *sok = reinterpret_cast<int *>(srhs + NB);  // [2]
     const int nblk = (n + NB - 1) / NB;
     const int t = threadIdx.x;
-    const int c4 = t & 15, part = t >> 4;  // columns 4*c4 .. +3 of this block, rows 4*part .. +3 of each chunk
+    const int r = t >> 2, q = t & 3;       // forward sums and the chain step: row r, columns 4k + q / 16q + k
+    const int c4 = t & 15, part = t >> 4;  // backward sums: columns 4c4 .. +3, chunk rows 4part .. +3
+    int par = 0;
     for (int g = blockIdx.x; g < nblk; g += gridDim.x) {
-        const int blk = nblk - 1 - g;
+        const int blk = DIR > 0 ? g : nblk - 1 - g;
         const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
-        // D^-1 z of this block: final before the kernel started, read before waiting
-        const T rhs = (t < NB && t < kb) ? __ldcg(&x[r0 + t]) / dvec[r0 + t] : T(0);
-        for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = __ldg(&Linv[(size_t)blk * NB * NB + idx]);
-        T acc[4] = {0, 0, 0, 0}, ap[4][4];
-        // rows c*NB + 4*part + e, columns r0 + 4*c4 .. +3 (zero past n; every block before the last is full)
-        auto fetch = [&](int c) {
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                const int i = c * NB + 4 * part + e;
-                if (i < n) {
-                    load4<T, false>(A + (long long)i * ld + r0 + 4 * c4, ap[e]);
+        const int pred = blk - DIR;
+        const bool has_pred = pred >= 0 && pred < nblk;
+        for (int idx = t; idx < NB * NB; idx += 256) {
+            sI[idx >> 6][idx & 63] = __ldg(&Linv[(size_t)blk * NB * NB + idx]);
+            sC[idx >> 6][idx & 63] = has_pred ? __ldg(&Mc[(size_t)blk * NB * NB + idx]) : T(0);
+        }
+        // this block's right-hand side is no other block's output: read it before any wait
+        if (t < NB) srhs[t] = t < kb ? (DIR > 0 ? __ldcg(&x[r0 + t]) : __ldcg(&x[r0 + t]) / dvec[r0 + t]) : T(0);
+        // far blocks: forward 0 .. blk-2, backward nblk-1 .. blk+2
+        const int nfar = DIR > 0 ? (blk > 1 ? blk - 1 : 0) : (nblk - 2 - blk > 0 ? nblk - 2 - blk : 0);
+        T acc = 0, acc4[4] = {0, 0, 0, 0}, ap[16];
+        auto fetch = [&](int j) {
+            if (DIR > 0) {
+                if (r < kb) {
+                    load16<T, false>(A + (long long)(r0 + r) * ld + j * NB + q * 16, ap);
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 4; j++) ap[e][j] = T(0);
+                    for (int k = 0; k < 16; k++) ap[k] = T(0);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int i = j * NB + 4 * part + e;
+                    if (i < n) {
+                        load4p<T>(A + (long long)i * ld + r0 + 4 * c4, ap + 4 * e);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 4; k++) ap[4 * e + k] = T(0);
+                    }
                 }
             }
         };
-        int done = nblk - 1;  // chunks (done, nblk) accumulated
-        if (done > blk) fetch(done);
-        long long spins = 0;
-        while (done > blk) {
-            const int span = done - blk < 256 ? done - blk : 256;
-            const int cnt = ready_prefix(ready, done, span, -1, epoch, s_cnt);
-            if (cnt == 0) {
-                if (++spins > TRSV_SPIN_LIMIT) {
-                    if (t == 0) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
-                    break;
+        bool ok = true;
+        if (nfar > 0) fetch(DIR > 0 ? 0 : nblk - 1);
+        for (int s = 0; s < nfar; s++) {
+            const int j = DIR > 0 ? s : nblk - 1 - s;
+            T *buf = sx + par * NB;
+            ok = wait_chunk<T>(ll, j, epoch, buf, poll_backoff(nfar - s), sok + par, flags);
+            par ^= 1;
+            if (!ok) break;
+            if (DIR > 0) {
+#pragma unroll
+                for (int k = 0; k < 16; k++) acc = fma(ap[k], buf[q * 16 + k], acc);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const T xe = buf[4 * part + e];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) acc4[k] = fma(ap[4 * e + k], xe, acc4[k]);
                 }
-                __nanosleep(32);
-                continue;
             }
-            const int avail = done - cnt;
-            for (int c = done; c > avail; c--) {
-                if (c != done) fetch(c);
-                const int i0 = c * NB + 4 * part;
-                T xv[4];
-                if (i0 + 3 < n) {
-                    load4<T, true>(x + i0, xv);
-                } else {
-#pragma unroll
-                    for (int e = 0; e < 4; e++) xv[e] = i0 + e < n ? __ldcg(&x[i0 + e]) : T(0);
-                }
-#pragma unroll
-                for (int e = 0; e < 4; e++)
-#pragma unroll
-                    for (int j = 0; j < 4; j++) acc[j] = fma(ap[e][j], xv[e], acc[j]);
-            }
-            done = avail;
-            if (done > blk) fetch(done);
+            if (s + 1 < nfar) fetch(DIR > 0 ? j + 1 : j - 1);
         }
+        if (DIR > 0) {
+            acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+            acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+            if (q == 0) spart[0][r] = acc;
+        } else {
 #pragma unroll
-        for (int j = 0; j < 4; j++) spart[part][4 * c4 + j] = acc[j];
+            for (int k = 0; k < 4; k++) spart[part][4 * c4 + k] = acc4[k];
+        }
         __syncthreads();
         if (t < NB) {
             T sum = 0;
+            if (DIR > 0) {
+                sum = spart[0][t];
+            } else {
 #pragma unroll
-            for (int pp = 0; pp < 16; pp++) sum += spart[pp][t];
-            srhs[t] = t < kb ? rhs - sum : T(0);
+                for (int p = 0; p < 16; p++) sum += spart[p][t];
+            }
+            srhs[t] -= sum;
         }
         __syncthreads();
-        // y = Linv^T srhs
-        T v[4] = {0, 0, 0, 0};
+        // y = Linv srhs (forward) or Linv^T srhs (backward), row r split over the quad
+        T y = 0;
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const T rr = srhs[4 * part + e];
-#pragma unroll
-            for (int j = 0; j < 4; j++) v[j] = fma(sI[4 * part + e][4 * c4 + j], rr, v[j]);
+        for (int k = 0; k < 16; k++) {
+            const int c = 4 * k + q;
+            y = fma(DIR > 0 ? sI[r][c] : sI[c][r], srhs[c], y);
         }
+        y += __shfl_xor_sync(0xffffffffu, y, 1);
+        y += __shfl_xor_sync(0xffffffffu, y, 2);
+        // the chain step: the nearest predecessor through the coupling block
+        T xr = y;
+        if (has_pred && ok) {
+            T *buf = sx + par * NB;
+            ok = wait_chunk<T>(ll, pred, epoch, buf, 0, sok + par, flags);
+            par ^= 1;
+            if (ok) {
+                T v = 0;
 #pragma unroll
-        for (int j = 0; j < 4; j++) spart[part][4 * c4 + j] = v[j];
-        __syncthreads();
-        if (t < kb) {
-            T sum = 0;
-#pragma unroll
-            for (int pp = 0; pp < 16; pp++) sum += spart[pp][t];
-            x[r0 + t] = sum;
+                for (int k = 0; k < 16; k++) {
+                    const int c = 4 * k + q;
+                    v = fma(sC[r][c], buf[c], v);
+                }
+                v += __shfl_xor_sync(0xffffffffu, v, 1);
+                v += __shfl_xor_sync(0xffffffffu, v, 2);
+                xr = y - v;
+            }
+        }
+        if (q == 0) {
+            ll_put<T>(ll, blk, r, r < kb ? xr : T(0), epoch);
+            if (r < kb) x[r0 + r] = xr;
+        }
+        __syncthreads();  // shared memory is reused by this CTA's next block
+    }
+}
+
+// Coupling blocks of the wavefront solves, one CTA per block: Mf_i = Linv_ii
+// L_{i,i-1} (i > 0) and, when Mb is given, Mb_i = Linv_ii^T L_{i+1,i}^T (i <
+// nblk-1).  With skip_tiny, rows of L_{i,i-1} whose diagonal entry of A has
+// magnitude below 1e-12 count as zero (the Gauss-Seidel sweep keeps those rows'
+// values).  Dynamic smem: two [64][65] blocks.
+template <typename T>
+__global__ void __launch_bounds__(256) k_trsv_couplings(int n, long long ld, const T *__restrict__ A,
+                                                        const T *__restrict__ Linv, T *Mf, T *Mb, int skip_tiny) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T(*sI)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
+    T(*sL)[NB + 1] = sI + NB;
+    const int nblk = (n + NB - 1) / NB, blk = blockIdx.x, r0 = blk * NB, t = threadIdx.x;
+    const int tx = t & 15, ty = t >> 4;
+    for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = Linv[(size_t)blk * NB * NB + idx];
+    if (blk > 0) {
+        for (int idx = t; idx < NB * NB; idx += 256) {
+            const int rr = idx >> 6, cc = idx & 63, row = r0 + rr;
+            bool keep = row < n;
+            if (keep && skip_tiny) keep = fabs((double)A[(long long)row * ld + row]) >= 1e-12;
+            sL[rr][cc] = keep ? A[(long long)row * ld + r0 - NB + cc] : T(0);
         }
         __syncthreads();
-        if (t == 0) st_release(ready + blk, epoch);
+        T acc[4][4] = {};
+        for (int k = 0; k < NB; k++) {
+            T a[4], b[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) a[u] = sI[4 * ty + u][k];
+#pragma unroll
+            for (int v = 0; v < 4; v++) b[v] = sL[k][4 * tx + v];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+        }
+        T *out = Mf + (size_t)blk * NB * NB;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) out[(4 * ty + u) * NB + 4 * tx + v] = acc[u][v];
+        __syncthreads();
+    }
+    if (Mb && blk + 1 < nblk) {
+        for (int idx = t; idx < NB * NB; idx += 256) {
+            const int rr = idx >> 6, cc = idx & 63, row = r0 + NB + rr;
+            sL[rr][cc] = row < n ? A[(long long)row * ld + r0 + cc] : T(0);
+        }
+        __syncthreads();
+        T acc[4][4] = {};
+        for (int k = 0; k < NB; k++) {
+            T a[4], b[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) a[u] = sI[k][4 * ty + u];
+#pragma unroll
+            for (int v = 0; v < 4; v++) b[v] = sL[4 * tx + v][k];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+        }
+        T *out = Mb + (size_t)blk * NB * NB;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) out[(4 * ty + u) * NB + 4 * tx + v] = acc[u][v];
     }
 }
 
 template <typename T>
 struct LdltWork {
     T *dvec, *W, *s;
-    T *Linv;       // [blocks][NB][NB] inverses of the diagonal blocks' L (the solves use them)
-    int *ready;    // [2][blocks] per-block ready words of the two solves
-    float *split;  // tensor-core path: [4][n][SUPER_W] hi/lo copies of the update's L and W rows
+    T *Linv;                 // [blocks][NB][NB] inverses of the diagonal blocks' L (the solves use them)
+    T *Mc;                   // [2][blocks][NB][NB] coupling blocks of the forward and backward solves
+    unsigned long long *ll;  // [2][blocks][2][NB] words the two solves publish their blocks in
+    float *split;            // tensor-core path: [4][n][SUPER_W] hi/lo copies of the update's L and W rows
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
@@ -694,32 +766,51 @@ constexpr int PANEL_W = 256, SUPER_W = 4 * PANEL_W;
 // launches, which the runtime schedules only as a whole grid (a second
 // context's kernels on the same GPU cannot hold part of it back).
 template <typename... Args>
-static cudaError_t launch_wavefront(void (*kernel)(Args...), int grid, cudaStream_t st, Args... args) {
+static cudaError_t launch_wavefront(void (*kernel)(Args...), int grid, size_t smem, cudaStream_t st,
+                                    Args... args) {
     void *argv[] = {(void *)&args...};
-    return cudaLaunchCooperativeKernel((const void *)kernel, dim3(grid), dim3(256), argv, 0, st);
+    return cudaLaunchCooperativeKernel((const void *)kernel, dim3(grid), dim3(256), argv, smem, st);
 }
 
-template <typename T>
-int trsv_grid(mp_ctx *ctx, const void *kernel, int nblk) {
+// CTAs of a wavefront launch over nblk blocks: at most one per block and never
+// more than can be resident at once (then the lowest unsolved block always runs).
+static int wavefront_grid(mp_ctx *ctx, const void *kernel, int nblk, size_t smem) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem);
     if (per_sm < 1) per_sm = 1;
-    int cap = per_sm * ctx->sm_count;  // every CTA resident: the wavefront cannot stall
+    int cap = per_sm * ctx->sm_count;
     return nblk < cap ? nblk : cap;
+}
+
+// Words of a wavefront solve: the epoch in the upper half of every word is the
+// context's solve count, so words left by earlier solves never match.  Returns
+// the next epoch; before the count would wrap, the words are cleared.
+static unsigned next_wavefront_epoch(mp_ctx *ctx, unsigned long long *ll, size_t words) {
+    if (ctx->solve_epoch >= 0x7ffffff0) {
+        cudaMemsetAsync(ll, 0, words * sizeof(unsigned long long), ctx->stream);
+        ctx->solve_epoch = 0;
+    }
+    return (unsigned)++ctx->solve_epoch;
+}
+
+// >48 KB dynamic shared memory of the wavefront kernels, set once per context
+template <typename T>
+static void wavefront_attrs() {
+    cudaFuncSetAttribute(k_trsv_ll<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsv_smem<T>());
+    cudaFuncSetAttribute(k_trsv_ll<T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsv_smem<T>());
+    cudaFuncSetAttribute(k_trsv_couplings<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(2 * NB * (NB + 1) * sizeof(T)));
 }
 
 template <typename T>
 int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> w, bool factor,
                       int tc_terms = 0) {
     cudaStream_t st = ctx->stream;
-    const size_t diag_smem = sizeof(T) * (2 * NB * (NB + 1) + NB * (SUB + 1) + SUB * (SUB + 1) + 3 * NB);
     const size_t panel_smem = sizeof(T) * (64 * (NB + 1) + NB * (NB + 1) + 2 * NB);
     const size_t upd_smem = sizeof(T) * 2 * NB * 68;
     const size_t f64_smem = sizeof(double) * 4 * WKC * WTILE;
     if (!ctx->ldlt_attr) {  // per context: the attributes belong to the context's device
         const int big = 96 * 1024;
-        cudaFuncSetAttribute(k_ldlt_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(k_ldlt_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_update_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
@@ -729,13 +820,15 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                              (int)tc::smem_bytes(false));
         cudaFuncSetAttribute(tc::k_update_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)tc::smem_bytes(true));
+        wavefront_attrs<float>();
+        wavefront_attrs<double>();
         ctx->ldlt_attr = true;
     }
     unsigned long long *flags = ctx->counters + C_FLAGS;
     auto diag_and_panel = [&](int k0, int kb, T *W, int ldw) {
         T *Li = w.Linv + (size_t)(k0 / NB) * NB * NB;
         int mk = kt_begin(ctx, MP_KT_DIAG, 0);
-        k_ldlt_diag<T><<<1, 256, diag_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, b, flags), ++ctx->launches;
+        k_ldlt_diag<T><<<1, 256, 0, st>>>(n, ld, A, k0, kb, w.dvec, Li, b, flags), ++ctx->launches;
         kt_end(ctx, mk);
         int k1 = k0 + kb;
         if (k1 < n) {
@@ -842,17 +935,26 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         }
     }
     const int nblk = (n + NB - 1) / NB;
-    const int epoch = ++ctx->solve_epoch;
+    const size_t blkw = (size_t)nblk * NB * NB, llw = (size_t)nblk * 2 * NB;
+    T *Mf = w.Mc, *Mb = w.Mc + blkw;
+    if (factor) {  // the coupling blocks of the solves belong to this factor
+        const int mk = kt_begin(ctx, MP_KT_TRSV, 0);
+        k_trsv_couplings<T><<<nblk, 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(n, ld, A, w.Linv, Mf, Mb, 0),
+            ++ctx->launches;
+        kt_end(ctx, mk);
+    }
+    const unsigned epoch = next_wavefront_epoch(ctx, w.ll, 2 * llw);
+    const size_t smem = trsv_smem<T>();
     const int mk = kt_begin(ctx, MP_KT_TRSV, 0);
     if (!factor) {
-        int g = trsv_grid<T>(ctx, (const void *)k_trsv_fwd<T>, nblk);
-        MP_CUDA(ctx, launch_wavefront(k_trsv_fwd<T>, g, st, n, ld, (const T *)A, (const T *)w.Linv, b, w.ready,
-                                      epoch, flags));
+        const int g = wavefront_grid(ctx, (const void *)k_trsv_ll<T, 1>, nblk, smem);
+        MP_CUDA(ctx, launch_wavefront(k_trsv_ll<T, 1>, g, smem, st, n, ld, (const T *)A, (const T *)w.Linv,
+                                      (const T *)Mf, (const T *)w.dvec, b, w.ll, epoch, flags));
         ++ctx->launches;
     }
-    int g = trsv_grid<T>(ctx, (const void *)k_trsv_bwd<T>, nblk);
-    MP_CUDA(ctx, launch_wavefront(k_trsv_bwd<T>, g, st, n, ld, (const T *)A, (const T *)w.Linv, (const T *)w.dvec,
-                                  b, w.ready + nblk, epoch, flags));
+    const int g = wavefront_grid(ctx, (const void *)k_trsv_ll<T, -1>, nblk, smem);
+    MP_CUDA(ctx, launch_wavefront(k_trsv_ll<T, -1>, g, smem, st, n, ld, (const T *)A, (const T *)w.Linv,
+                                  (const T *)Mb, (const T *)w.dvec, b, w.ll + llw, epoch, flags));
     ++ctx->launches;
     kt_end(ctx, mk);
     MP_CUDA(ctx, cudaGetLastError());

@@ -88,13 +88,16 @@ static int check_flags(mp_ctx *ctx, unsigned long long mask, unsigned long long 
 struct SolveScratch {
     double *dvec64 = nullptr, *W64 = nullptr, *s64 = nullptr, *r = nullptr, *Linv64 = nullptr;
     float *dvec32 = nullptr, *W32 = nullptr, *s32 = nullptr, *b32 = nullptr, *Linv32 = nullptr, *split32 = nullptr;
-    int *ready = nullptr;
+    double *Mc64 = nullptr;             // [2][blocks][NB][NB] coupling blocks (FP64 solves, Gauss-Seidel)
+    float *Mc32 = nullptr;              // [2][blocks][NB][NB] coupling blocks (FP32 solves)
+    unsigned long long *ll = nullptr;   // [2][blocks][2][NB] wavefront words
+    size_t ll_words = 0;
     int neq = 0;
 };
 
 static void release(SolveScratch *s) {
     void *p[] = {s->dvec64, s->W64, s->s64, s->r, s->dvec32, s->W32, s->s32, s->b32,
-                 s->Linv64, s->Linv32, s->ready, s->split32};
+                 s->Linv64, s->Linv32, s->Mc64, s->Mc32, s->ll, s->split32};
     for (void *q : p)
         if (q) cudaFree(q);
     *s = SolveScratch();
@@ -129,9 +132,12 @@ static int ensure_scratch(mp_ctx *ctx, SolveScratch **out) {
     MP_CUDA(ctx, cudaMalloc(&s.Linv64, sizeof(double) * nblk * NB * NB));
     MP_CUDA(ctx, cudaMalloc(&s.Linv32, sizeof(float) * nblk * NB * NB));
     MP_CUDA(ctx, cudaMalloc(&s.split32, sizeof(float) * 4 * (size_t)n * SUPER_W));
-    MP_CUDA(ctx, cudaMalloc(&s.ready, sizeof(int) * 2 * (nblk + 1)));
-    MP_CUDA(ctx, cudaMemsetAsync(s.ready, 0, sizeof(int) * 2 * (nblk + 1), ctx->stream));
-    ctx->solve_epoch = 0;  // fresh ready words hold epoch 0
+    MP_CUDA(ctx, cudaMalloc(&s.Mc64, sizeof(double) * 2 * nblk * NB * NB));
+    MP_CUDA(ctx, cudaMalloc(&s.Mc32, sizeof(float) * 2 * nblk * NB * NB));
+    s.ll_words = 2 * nblk * 2 * NB;
+    MP_CUDA(ctx, cudaMalloc(&s.ll, sizeof(unsigned long long) * s.ll_words));
+    MP_CUDA(ctx, cudaMemsetAsync(s.ll, 0, sizeof(unsigned long long) * s.ll_words, ctx->stream));
+    ctx->solve_epoch = 0;  // fresh words hold epoch 0, which no solve uses
     s.neq = n;
     return MP_OK;
 }
@@ -153,7 +159,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         if (!ctx->J || !ctx->j_current) return fail(ctx, MP_ERR_STATE, "no current FP64 J (build it first)");
         ctx->j_current = false;  // the factorization overwrites J
         MP_CUDA(ctx, cudaMemcpyAsync(ctx->y, ctx->G, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
-        LdltWork<double> w{sc.dvec64, sc.W64, sc.s64, sc.Linv64, sc.ready, nullptr};
+        LdltWork<double> w{sc.dvec64, sc.W64, sc.s64, sc.Linv64, sc.Mc64, sc.ll, nullptr};
         rc = ldlt_factor_solve<double>(ctx, ctx->J, ld, n, ctx->y, w, true);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
@@ -170,12 +176,15 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         if (!ctx->j32_current && (rc = fe_j32_from_k(ctx))) return rc;
         ctx->j32_current = false;
         MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * n, ctx->stream));
-        LdltWork<float> w{sc.dvec32, sc.W32, sc.s32, sc.Linv32, sc.ready, sc.split32};
+        LdltWork<float> w{sc.dvec32, sc.W32, sc.s32, sc.Linv32, sc.Mc32, sc.ll, sc.split32};
         double rn = 0, bn = 0;
         // r = G (y = 0), in FP32 for the first solve, which also factors J32
         rc = resid_norms(ctx, ctx->y, ctx->G, sc.r, sc.b32, &rn, &bn);
         if (rc) return rc;
-        rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, sc.b32, w, true, ctx->mixed_factor);
+        const int terms = ctx->mixed_factor != MP_MIXED_AUTO ? ctx->mixed_factor
+                          : n >= MP_MIXED_TF32_FROM       ? MP_MIXED_TF32
+                                                          : MP_MIXED_TF32X3;
+        rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, sc.b32, w, true, terms);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
         k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, sc.b32, ctx->y), ++ctx->launches;
@@ -216,13 +225,15 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
 // |J_uu| < 1e-12 keeps its value (src/FESolver.cpp:569).  The sweep runs as a
 // persistent wavefront over 64-row blocks (the triangular solves' scheme):
 // block k streams its rows once, summing the columns right of the diagonal
-// against x_old as soon as it starts and the columns of each earlier block
-// against x_new as that block publishes it (a ready word per block holding the
-// sweep's epoch, release/acquire), then applies the stored inverse of its
-// diagonal block of D + L: a 64 x 64 product instead of 64 dependent
-// substitutions.  x_old and x_new are separate buffers (sweeps alternate
-// them), so no block reads a value another block is rewriting.  The iterate is
-// the reference's up to summation order.
+// against x_old as soon as it starts and the columns of blocks 0 .. k-2
+// against x_new as those blocks publish it (wavefront words holding the
+// sweep's epoch), then applies the stored inverse Minv_kk of its diagonal block
+// of D + L -- a 64 x 64 product instead of 64 dependent substitutions -- and
+// last takes block k-1 through the coupling block Minv_kk J~_{k,k-1} (J~: J
+// without the skipped rows), so a step of the chain is one poll and one small
+// product.  x_old and x_new are separate buffers (sweeps alternate them), so no
+// block reads a value another block is rewriting.  The iterate is the
+// reference's up to summation order.
 
 // Inverse of each 64 x 64 diagonal block of D + L, rows with |J_uu| < 1e-12
 // (and rows past n) replaced by identity rows, so the block's row keeps its
@@ -258,102 +269,98 @@ __global__ void __launch_bounds__(64) k_gs_block_inverse(int n, long long ld, co
     for (int r = 0; r < NB; r++) out[r * NB + j] = sM[r][j];
 }
 
+// rup_i = b_i - sum_{j>i} J_ij x_old_j for every row: the x_old half of a sweep,
+// a bandwidth-bound pass over the strict upper triangle, one warp per row.
+__global__ void __launch_bounds__(256) k_gs_upper(int n, long long ld, const double *__restrict__ A,
+                                                  const double *__restrict__ b, const double *__restrict__ x_old,
+                                                  double *rup) {
+    const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const double *a = A + (long long)row * ld;
+    double s = 0.0;
+#pragma unroll 4
+    for (int j = row + 1 + lane; j < n; j += 32) s = fma(__ldg(a + j), __ldg(x_old + j), s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) rup[row] = b[row] - s;
+}
+
+// Shared memory of k_gs_sweep: the block inverse and the coupling block, two
+// poll buffers, the right-hand side, two poll results.
+constexpr size_t gs_smem() { return sizeof(double) * (2 * NB * MS + 3 * NB) + 2 * sizeof(int); }
+
+// The x_new half of a sweep: with rup = b - U x_old from k_gs_upper, block k
+// solves (D + L)_kk x_k = rup_k - sum_{j<k} J_kj x_new_j as a wavefront.
 __global__ void __launch_bounds__(256) k_gs_sweep(int n, long long ld, const double *__restrict__ A,
-                                                  const double *__restrict__ b, const double *__restrict__ Minv,
-                                                  const double *x_old, double *x_new, int *ready, int epoch,
+                                                  const double *__restrict__ rup, const double *__restrict__ Minv,
+                                                  const double *__restrict__ Mc, const double *x_old, double *x_new,
+                                                  unsigned long long *ll, unsigned epoch,
                                                   unsigned long long *flags) {
-    __shared__ double sI[NB][NB + 1];
-    __shared__ double sc[NB];
-    __shared__ int s_cnt[8];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double(*sI)[MS] = reinterpret_cast<double(*)[MS]>(smem_raw);
+    double(*sC)[MS] = sI + NB;
+    double *sx = reinterpret_cast<double *>(sC + NB);  // [2][NB]
+    double *srhs = sx + 2 * NB;
+    int *sok = reinterpret_cast<int *>(srhs + NB);  // [2]
     const int nblk = (n + NB - 1) / NB;
     const int t = threadIdx.x;
-    const int r = t >> 2, q = t & 3;  // row of the block, quarter of each 64-column chunk
+    const int r = t >> 2, q = t & 3;  // row of the block; quarter of each 64-column chunk / columns 4k + q
+    int par = 0;
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
-        for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = __ldg(&Minv[(size_t)blk * NB * NB + idx]);
+        const bool has_pred = blk > 0;
+        for (int idx = t; idx < NB * NB; idx += 256) {
+            sI[idx >> 6][idx & 63] = __ldg(&Minv[(size_t)blk * NB * NB + idx]);
+            sC[idx >> 6][idx & 63] = has_pred ? __ldg(&Mc[(size_t)blk * NB * NB + idx]) : 0.0;
+        }
         const int row = r0 + (r < kb ? r : 0);
         const double *arow = A + (long long)row * ld + q * 16;
-        // this row's diagonal, old value and right-hand side, read before the wait
-        const double d_rr = A[(long long)row * ld + row], xo_r = x_old[row], b_r = b[row];
-        double acc = 0.0, ap[16], xv[16];
-        // columns right of the block: x_old, available now.  The next chunk's
-        // row piece and x piece are loaded while this one is summed, so two
-        // chunks per thread are in flight (a CTA streams 64 rows of J).
-        {
-            const int nfull = n / NB;  // chunks inside n
-            int c = blk + 1;
-            double apn[16], xvn[16];
-            if (c < nfull) {
-                load16<double, false>(arow + c * NB, apn);
-                load16<double, false>(x_old + c * NB + q * 16, xvn);
-            }
-            for (; c < nfull; c++) {
+        // this row's diagonal, old value and x_old half, read before any wait
+        const double d_rr = A[(long long)row * ld + row], xo_r = x_old[row], ru_r = rup[row];
+        double acc = 0.0, ap[16];
+        // the diagonal block's columns right of the diagonal belong to the x_old
+        // half (in rup); columns of blocks 0 .. blk-2: x_new as they are published
+        const int nfar = blk > 1 ? blk - 1 : 0;
+        bool ok = true;
+        if (nfar > 0) load16<double, false>(arow, ap);
+        for (int s = 0; s < nfar; s++) {
+            double *buf = sx + par * NB;
+            ok = wait_chunk<double>(ll, s, epoch, buf, poll_backoff(nfar - s), sok + par, flags);
+            par ^= 1;
+            if (!ok) break;
 #pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    ap[k] = apn[k];
-                    xv[k] = xvn[k];
-                }
-                if (c + 1 < nfull) {
-                    load16<double, false>(arow + (c + 1) * NB, apn);
-                    load16<double, false>(x_old + (c + 1) * NB + q * 16, xvn);
-                }
-#pragma unroll
-                for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
-            }
-            for (; c < nblk; c++) {  // the last, partial chunk
-                const int c0 = c * NB + q * 16;
-                for (int k = 0; k < 16 && c0 + k < n; k++) acc = fma(arow[c * NB + k], x_old[c0 + k], acc);
-            }
-        }
-        // the diagonal block's columns right of the diagonal: x_old
-        for (int k = 0; k < 16; k++) {
-            const int col = q * 16 + k;
-            if (col > r && col < kb) acc = fma(arow[blk * NB + k], x_old[r0 + col], acc);
-        }
-        // columns left of the block: x_new, block by block as they are published
-        int done = 0;
-        long long spins = 0;
-        if (done < blk) load16<double, false>(arow, ap);
-        while (done < blk) {
-            const int span = blk - done < 256 ? blk - done : 256;
-            const int cnt = ready_prefix(ready, done, span, 1, epoch, s_cnt);
-            if (cnt == 0) {
-                if (++spins > TRSV_SPIN_LIMIT) {
-                    if (t == 0) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
-                    break;
-                }
-                __nanosleep(32);
-                continue;
-            }
-            const int avail = done + cnt;
-            load16<double, true>(x_new + done * NB + q * 16, xv);
-#pragma unroll
-            for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
-            for (int c = done + 1; c < avail; c++) {
-                load16<double, false>(arow + c * NB, ap);
-                load16<double, true>(x_new + c * NB + q * 16, xv);
-#pragma unroll
-                for (int k = 0; k < 16; k++) acc = fma(ap[k], xv[k], acc);
-            }
-            done = avail;
-            if (done < blk) load16<double, false>(arow + done * NB, ap);
+            for (int k = 0; k < 16; k++) acc = fma(ap[k], buf[q * 16 + k], acc);
+            if (s + 1 < nfar) load16<double, false>(arow + (s + 1) * NB, ap);
         }
         acc += __shfl_xor_sync(0xffffffffu, acc, 1);
         acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        if (q == 0) {
-            double cv = 0.0;
-            if (r < kb) cv = fabs(d_rr) < 1e-12 ? xo_r : b_r - acc;
-            sc[r] = cv;
-        }
+        if (q == 0) srhs[r] = r < kb ? (fabs(d_rr) < 1e-12 ? xo_r : ru_r - acc) : 0.0;
         __syncthreads();
-        double v = 0.0;
+        double y = 0.0;
 #pragma unroll
-        for (int k = 0; k < 16; k++) v = fma(sI[r][q * 16 + k], sc[q * 16 + k], v);
-        v += __shfl_xor_sync(0xffffffffu, v, 1);
-        v += __shfl_xor_sync(0xffffffffu, v, 2);
-        if (q == 0 && r < kb) x_new[r0 + r] = v;
-        __syncthreads();
-        if (t == 0) st_release(ready + blk, epoch);
+        for (int k = 0; k < 16; k++) y = fma(sI[r][4 * k + q], srhs[4 * k + q], y);
+        y += __shfl_xor_sync(0xffffffffu, y, 1);
+        y += __shfl_xor_sync(0xffffffffu, y, 2);
+        // block blk-1 through the coupling block Minv_kk J~_{k,k-1}
+        double xr = y;
+        if (has_pred && ok) {
+            double *buf = sx + par * NB;
+            ok = wait_chunk<double>(ll, blk - 1, epoch, buf, 0, sok + par, flags);
+            par ^= 1;
+            if (ok) {
+                double v = 0.0;
+#pragma unroll
+                for (int k = 0; k < 16; k++) v = fma(sC[r][4 * k + q], buf[4 * k + q], v);
+                v += __shfl_xor_sync(0xffffffffu, v, 1);
+                v += __shfl_xor_sync(0xffffffffu, v, 2);
+                xr = y - v;
+            }
+        }
+        if (q == 0) {
+            ll_put<double>(ll, blk, r, r < kb ? xr : 0.0, epoch);
+            if (r < kb) x_new[r0 + r] = xr;
+        }
+        __syncthreads();  // shared memory is reused by this CTA's next block
     }
 }
 
@@ -386,18 +393,28 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st) {
     const int th = 256;
     const long long bl = ((long long)n * 32 + th - 1) / th;
     unsigned long long *flags = ctx->counters + C_FLAGS;
-    // the inverses of the diagonal blocks of D + L (J is fixed for the solve)
+    // the inverses of the diagonal blocks of D + L and the coupling blocks
+    // Minv_kk J~_{k,k-1}, J~ without the rows the sweep skips (J is fixed for the solve)
     k_gs_block_inverse<<<nblk, 64, 0, ctx->stream>>>(n, ld, ctx->J, sp->Linv64), ++ctx->launches;
-    const int grid = trsv_grid<double>(ctx, (const void *)k_gs_sweep, nblk);
+    wavefront_attrs<double>();
+    k_trsv_couplings<double><<<nblk, 256, 2 * NB * (NB + 1) * sizeof(double), ctx->stream>>>(
+        n, ld, ctx->J, sp->Linv64, sp->Mc64, nullptr, 1),
+        ++ctx->launches;
+    const size_t smem = gs_smem();
+    cudaFuncSetAttribute(k_gs_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int grid = wavefront_grid(ctx, (const void *)k_gs_sweep, nblk, smem);
     double *xa = ctx->y, *xb = sp->r;  // sweeps alternate the two
+    double *rup = sp->dvec64;          // b - U x_old (the FP64 factor's D is not in use here)
     double L2 = 0;
     int it;
     bool converged = false;
     for (it = 0; it < ctx->gs_max_sweeps; it++) {
         const int mk = kt_begin(ctx, MP_KT_TRSV, 0);
-        MP_CUDA(ctx, launch_wavefront(k_gs_sweep, grid, ctx->stream, n, ld, (const double *)ctx->J,
-                                      (const double *)ctx->G, (const double *)sp->Linv64, (const double *)xa, xb,
-                                      sp->ready, ++ctx->solve_epoch, flags));
+        k_gs_upper<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, xa, rup), ++ctx->launches;
+        const unsigned epoch = next_wavefront_epoch(ctx, sp->ll, sp->ll_words);
+        MP_CUDA(ctx, launch_wavefront(k_gs_sweep, grid, smem, ctx->stream, n, ld, (const double *)ctx->J,
+                                      (const double *)rup, (const double *)sp->Linv64, (const double *)sp->Mc64,
+                                      (const double *)xa, xb, sp->ll, epoch, flags));
         ++ctx->launches;
         kt_end(ctx, mk);
         std::swap(xa, xb);
