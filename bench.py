@@ -63,11 +63,12 @@ SIGMA = float(np.sqrt(KTI_EV * mp.QE / (16 * mp.AMU)))
 LEGS = ("kuhn20", "nonlinear", "adjoint", "sparse64", "vtk")
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one ncu capture
 # per kernel, per unit of its algorithmic work; a launch's traffic is scaled by
-# its units (profiles/k_update_tc_kuhn20_newton.md: 444.3 MB for a K = 1,024
-# trailing update of 55.4 GFLOP; profiles/k_push_*_kuhn20_2M.md: 160.5 MB and
-# 65.1 MB for 1.99M particles, in and out)
-TRAFFIC_PER_UNIT = {("tc", "update"): 444.3e6 / 55.4e9, ("fp64", "push"): 160.5e6 / (2 * 1.99e6),
-                    ("mixed", "push"): 65.1e6 / (2 * 1.99e6)}
+# its units (a K = 1,024 trailing update of 55.4 GFLOP moves 444.3 MB in 3xTF32,
+# profiles/k_update_tc_kuhn20_newton.md, and 232.4 MB in TF32,
+# profiles/k_update_tc_tf32_kuhn20_newton.md; profiles/k_push_*_kuhn20_2M.md:
+# 160.5 MB and 65.1 MB for 1.99M particles, in and out)
+TRAFFIC_PER_UNIT = {("tc3", "update"): 444.3e6 / 55.4e9, ("tc1", "update"): 232.4e6 / 55.4e9,
+                    ("fp64", "push"): 160.5e6 / (2 * 1.99e6), ("mixed", "push"): 65.1e6 / (2 * 1.99e6)}
 KT_NAMES = {mp.KT_PUSH: "push", mp.KT_UPDATE: "trailing_update", mp.KT_DIAG: "diagonal_factor",
             mp.KT_PANEL: "panel", mp.KT_TRSV: "triangular_solve"}
 KT_KERNEL = {mp.KT_PUSH: {mp.FP64: "k_push_fp64", mp.MIXED: "k_push_mixed"},
@@ -210,7 +211,7 @@ def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True, neq=0):
                            (", and the 3xTF32 split issues three per term: issued TF32 rate = 3 x achieved"
                             if terms == 3 else "; one TF32 product per term"))
             out["tf32_issued_frac_of_half_bf16_peak"] = terms * ach / (peak / 2)
-            out["traffic"] = TRAFFIC_PER_UNIT[("tc", "update")] * v["work"] / max(v["launches"], 1)
+            out["traffic"] = TRAFFIC_PER_UNIT[("tc%d" % terms, "update")] * v["work"] / max(v["launches"], 1)
             out["traffic_source"] = ("ncu DRAM bytes per flop of a K = 1,024 trailing update (8,379 unknowns) x "
                                      "this workload's average flops per launch (the strips, K = 256, move more "
                                      "bytes per flop: an estimate)")

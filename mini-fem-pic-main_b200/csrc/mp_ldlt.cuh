@@ -719,6 +719,170 @@ __global__ void __launch_bounds__(256) k_trsv_couplings(int n, long long ld, con
     }
 }
 
+// ---- tensor-core panels of the FP32 factor ----------------------------------------------
+// The mixed form's panel products (W = A_ik Linv^T) and in-panel column updates
+// (A_ij -= L_ik W_jk^T) are 64 x 64 x 64 products; they run on mma.sync
+// m16n8k8 TF32 fragments with FP32 accumulation, in the same arithmetic as the
+// trailing update: TERMS = 1 rounds each operand to TF32, TERMS = 3 splits it
+// into hi = RN_tf32(x) and lo = RN_tf32(x - hi) and sums hi*hi + hi*lo + lo*hi.
+// Operands sit in shared memory with a row pitch of MS = 68 floats, so the
+// fragment reads of a warp (row 4g + t) hit 32 distinct banks.
+__device__ __forceinline__ unsigned tf32_rn(float x) {
+    unsigned r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void mma_m16n8k8(float (&c)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// One warp: acc[nt] (16 x 8 tiles nt = 0..3, rows m0 + 0..15, columns n0 + 8nt
+// + 0..7) += sum over k < 64 of sa[row][k] * sb[col][k].  Fragment layout of
+// m16n8k8 (g = lane / 4, t = lane % 4): A a0 (g, t), a1 (g+8, t), a2 (g, t+4),
+// a3 (g+8, t+4); B b0 (k = t, n = g), b1 (k = t+4, n = g); C c0 (g, 2t),
+// c1 (g, 2t+1), c2 (g+8, 2t), c3 (g+8, 2t+1).
+template <int TERMS>
+__device__ __forceinline__ void warp_mma_64(const float (*sa)[MS], const float (*sb)[MS], int m0, int n0,
+                                            float (&acc)[4][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll 2
+    for (int k0 = 0; k0 < NB; k0 += 8) {
+        const float af[4] = {sa[m0 + g][k0 + t], sa[m0 + g + 8][k0 + t], sa[m0 + g][k0 + t + 4],
+                             sa[m0 + g + 8][k0 + t + 4]};
+        unsigned ah[4], al[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            ah[i] = tf32_rn(af[i]);
+            if (TERMS == 3) al[i] = tf32_rn(af[i] - __uint_as_float(ah[i]));
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            const int c = n0 + 8 * nt + g;
+            const float bf[2] = {sb[c][k0 + t], sb[c][k0 + t + 4]};
+            unsigned bh[2], bl[2];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                bh[i] = tf32_rn(bf[i]);
+                if (TERMS == 3) bl[i] = tf32_rn(bf[i] - __uint_as_float(bh[i]));
+            }
+            if (TERMS == 3) {
+                mma_m16n8k8(acc[nt], al, bh);
+                mma_m16n8k8(acc[nt], ah, bl);
+            }
+            mma_m16n8k8(acc[nt], ah, bh);
+        }
+    }
+}
+
+// Panel of the FP32 factor (rows [r0, r0+64) below the diagonal block), as
+// k_ldlt_panel: W = A_ik Linv^T, L_ik = W D^-1, b_i -= L_ik z_k.  Warp w takes
+// rows 16(w/2) .. +15 and columns 32(w%2) .. +31 of the 64 x 64 product.
+template <int TERMS>
+__global__ void __launch_bounds__(256) k_ldlt_panel_tc(int n, long long ld, float *A, int k0, int kb,
+                                                       const float *dvec, const float *Linv, float *W, int ldw,
+                                                       float *b) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float(*sA)[MS] = reinterpret_cast<float(*)[MS]>(smem_raw);
+    float(*sI)[MS] = sA + NB;
+    float *sd = reinterpret_cast<float *>(sI + NB);
+    float *sz = sd + NB;
+    float(*sbs)[NB] = reinterpret_cast<float(*)[NB]>(sz + NB);  // [2][64] the two column halves' b sums
+    const int r0 = k0 + kb + blockIdx.x * 64, t = threadIdx.x;
+    {
+        float va[16], vi[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int idx = q * 256 + t, r = idx >> 6, c = idx & 63, row = r0 + r;
+            va[q] = (row < n && c < kb) ? A[(long long)row * ld + k0 + c] : 0.f;
+            vi[q] = (r < kb && c < kb) ? __ldg(&Linv[r * NB + c]) : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int idx = q * 256 + t;
+            sA[idx >> 6][idx & 63] = va[q];
+            sI[idx >> 6][idx & 63] = vi[q];
+        }
+    }
+    if (t < NB) {
+        sd[t] = t < kb ? dvec[k0 + t] : 1.f;
+        sz[t] = (b && t < kb) ? b[k0 + t] : 0.f;
+    }
+    __syncthreads();
+    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
+    const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
+    float acc[4][4] = {};
+    warp_mma_64<TERMS>(sA, sI, m0, n0, acc);
+    float bsum[2] = {0.f, 0.f};  // rows m0 + g and m0 + g + 8
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int rr = m0 + g + (e >> 1) * 8, c = n0 + 8 * nt + 2 * tq + (e & 1), row = r0 + rr;
+            if (row < n && c < kb) {
+                const float wv = acc[nt][e];
+                const float lv = wv / sd[c];
+                W[(long long)row * ldw + c] = wv;
+                A[(long long)row * ld + k0 + c] = lv;
+                bsum[e >> 1] += lv * sz[c];
+            }
+        }
+    if (b) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            float v = bsum[h];
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            if (tq == 0) sbs[w & 1][m0 + g + 8 * h] = v;
+        }
+        __syncthreads();
+        if (t < NB && r0 + t < n) b[r0 + t] -= sbs[0][t] + sbs[1][t];
+    }
+}
+
+// In-panel column update of the FP32 factor, as k_ldlt_update_cols:
+// A_ij -= L_ik W_jk^T for the 64 x 64 tile (blockIdx.y, blockIdx.x) of rows
+// [k1, n) x columns [k1, jend).
+template <int TERMS>
+__global__ void __launch_bounds__(256) k_ldlt_update_cols_tc(int n, long long ld, float *A, int k0, int kb,
+                                                             const float *W, int ldw, int k1, int jend) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float(*sL)[MS] = reinterpret_cast<float(*)[MS]>(smem_raw);
+    float(*sW)[MS] = sL + NB;
+    const int i0 = k1 + blockIdx.y * 64, j0 = k1 + blockIdx.x * 64, t = threadIdx.x;
+    if (j0 > i0 + 63 || j0 >= jend) return;  // tile entirely above the diagonal or outside the panel
+    {
+        float la[16], wa[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int idx = q * 256 + t, r = idx >> 6, p = idx & 63, ri = i0 + r, rj = j0 + r;
+            la[q] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : 0.f;
+            wa[q] = (p < kb && rj < jend) ? __ldg(&W[(long long)rj * ldw + p]) : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int idx = q * 256 + t;
+            sL[idx >> 6][idx & 63] = la[q];
+            sW[idx >> 6][idx & 63] = wa[q];
+        }
+    }
+    __syncthreads();
+    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
+    const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
+    float acc[4][4] = {};
+    warp_mma_64<TERMS>(sL, sW, m0, n0, acc);
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int i = i0 + m0 + g + (e >> 1) * 8, j = j0 + n0 + 8 * nt + 2 * tq + (e & 1);
+            if (i < n && j < jend && j <= i) A[(long long)i * ld + j] -= acc[nt][e];
+        }
+}
+
 template <typename T>
 struct LdltWork {
     T *dvec, *W, *s;
@@ -808,6 +972,8 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     cudaStream_t st = ctx->stream;
     const size_t panel_smem = sizeof(T) * (64 * (NB + 1) + NB * (NB + 1) + 2 * NB);
     const size_t upd_smem = sizeof(T) * 2 * NB * 68;
+    const size_t panel_tc_smem = sizeof(float) * (2 * NB * MS + 4 * NB);
+    const size_t cols_tc_smem = sizeof(float) * 2 * NB * MS;
     const size_t f64_smem = sizeof(double) * 4 * WKC * WTILE;
     if (!ctx->ldlt_attr) {  // per context: the attributes belong to the context's device
         const int big = 96 * 1024;
@@ -822,6 +988,9 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                              (int)tc::smem_bytes(true));
         wavefront_attrs<float>();
         wavefront_attrs<double>();
+        for (const void *f : {(const void *)k_ldlt_panel_tc<1>, (const void *)k_ldlt_panel_tc<3>,
+                              (const void *)k_ldlt_update_cols_tc<1>, (const void *)k_ldlt_update_cols_tc<3>})
+            cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         ctx->ldlt_attr = true;
     }
     unsigned long long *flags = ctx->counters + C_FLAGS;
@@ -833,8 +1002,16 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         int k1 = k0 + kb;
         if (k1 < n) {
             mk = kt_begin(ctx, MP_KT_PANEL, 0);
-            k_ldlt_panel<T><<<(n - k1 + 63) / 64, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b),
-                ++ctx->launches;
+            const unsigned gp = (n - k1 + 63) / 64;
+            if constexpr (std::is_same<T, float>::value) {
+                if (tc_terms == 3)
+                    k_ldlt_panel_tc<3><<<gp, 256, panel_tc_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b);
+                else
+                    k_ldlt_panel_tc<1><<<gp, 256, panel_tc_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b);
+            } else {
+                k_ldlt_panel<T><<<gp, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b);
+            }
+            ++ctx->launches;
             kt_end(ctx, mk);
         }
     };
@@ -917,9 +1094,18 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                     if (k1 < n && k1 < P1) {
                         dim3 g((P1 - k1 + 63) / 64, (n - k1 + 63) / 64);
                         const int mk = kt_begin(ctx, MP_KT_PANEL, 0);
-                        k_ldlt_update_cols<T><<<g, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W + (k0 - S0), SUPER_W,
-                                                                        k1, P1),
-                            ++ctx->launches;
+                        if constexpr (std::is_same<T, float>::value) {
+                            if (tc_terms == 3)
+                                k_ldlt_update_cols_tc<3><<<g, 256, cols_tc_smem, st>>>(n, ld, A, k0, kb,
+                                                                                      w.W + (k0 - S0), SUPER_W, k1, P1);
+                            else
+                                k_ldlt_update_cols_tc<1><<<g, 256, cols_tc_smem, st>>>(n, ld, A, k0, kb,
+                                                                                      w.W + (k0 - S0), SUPER_W, k1, P1);
+                        } else {
+                            k_ldlt_update_cols<T><<<g, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W + (k0 - S0),
+                                                                            SUPER_W, k1, P1);
+                        }
+                        ++ctx->launches;
                         kt_end(ctx, mk);
                     }
                 }
