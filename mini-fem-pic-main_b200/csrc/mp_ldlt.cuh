@@ -56,23 +56,55 @@ __device__ __forceinline__ void load4p(const T *p, T *v) {
 // z_k = L_kk^-1 b_k (the forward substitution riding on the factorization).
 // The block is padded to 64 x 64 with an identity.
 //
-// The block and its inverse live in registers: thread
-// (ti, tc) of 256 holds the 4 x 4 tiles at rows 4ti.., columns 4tc.. of the
-// block and of Linv (and, for tc == 0, b at rows 4ti..).  Elimination step j,
-// one barrier: the owners of column j of the block, of row j of Linv and of
-// b_j publish them in shared memory (double-buffered), the owner of the pivot
-// also 1/d_j; every thread forms its rows' multipliers l_i = A_ij / d_j (i > j)
-// and updates its tiles, A_ic -= l_i A_cj (c > j) and Linv_ic -= l_i Linv_jc,
-// and b_i -= l_i b_j; the owners of column j keep l_i there (L).  The step
-// loop is unrolled by four so every register index is a constant.
+// The block and its inverse live in registers: thread (ti, tc) of 256 holds
+// the 4 x 4 tiles at rows 4ti.., columns 4tc.. of the block and of Linv (and,
+// for tc == 0, b at rows 4ti..).  Step jj eliminates the four pivots j0 = 4jj
+// .. j0+3 behind one barrier:
+//   publish   the owners of the step's four columns (tc == jj) put them in
+//             shared memory, the owners of Linv's rows j0.. (ti == jj) those
+//             rows and b_j0.., and the owner of the 4 x 4 pivot block (ti ==
+//             tc == jj) factors it, P = L_P D_P L_P^T, and publishes L_P, D_P
+//             and 1/D_P;
+//   eliminate every thread forms, for its rows i > j0+3, z_i = L_P^-1 x_i from
+//             the row's four column values x_i and the multipliers
+//             l_im = z_im / d_m, and for its columns c the same z_c; its
+//             tile takes the rank-4 update A_ic -= sum_m l_im z_cm; the four
+//             Linv rows become L_P^-1 (rows) and every later row subtracts
+//             sum_m l_im (that row m); b likewise.  The owners of the step's
+//             columns keep l_im there (L), the pivot owner L_P and D_P.
+// Shared buffers alternate between steps, so one barrier a step suffices.
 template <typename T>
-__global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec,
-                                                      T *Linv, T *b, unsigned long long *flags) {
-    __shared__ __align__(16) T scol[2][NB];
-    __shared__ __align__(16) T srow[2][NB];
-    __shared__ T spiv[2][2];  // d_j, 1/d_j
-    __shared__ T sbj[2];
-    const int t = threadIdx.x, ti = t >> 4, tc = t & 15;
+__device__ __forceinline__ void ld4s(const T *p, T (&v)[4]) {
+    if constexpr (sizeof(T) == 8) {
+        const double2 x = reinterpret_cast<const double2 *>(p)[0], y = reinterpret_cast<const double2 *>(p)[1];
+        v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+    } else {
+        const float4 x = *reinterpret_cast<const float4 *>(p);
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    }
+}
+template <typename T>
+__device__ __forceinline__ void st4s(T *p, const T (&v)[4]) {
+    if constexpr (sizeof(T) == 8) {
+        reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+    } else {
+        *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
+                                                   T *b, unsigned long long *flags) {
+    __shared__ __align__(16) T scol[2][NB][4];  // the step's four columns, every row
+    __shared__ __align__(16) T srow[2][4][NB];  // Linv's rows j0 .. j0+3, every column
+    __shared__ __align__(16) T spiv[2][4][4];   // the factored pivot block: L_P below the diagonal, D_P on it
+    __shared__ __align__(16) T srd[2][4];       // 1 / D_P
+    __shared__ __align__(16) T sbp[2][4];       // b_j0 .. b_j0+3
+    // a warp holds two column tiles (tc) of all 16 row tiles (ti), so the
+    // column-dependent branches of a step (update the block, or Linv) are
+    // uniform over a warp
+    const int t = threadIdx.x, ti = t & 15, tc = t >> 4;
     T a[4][4], li[4][4], bb[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
@@ -97,56 +129,134 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, in
         bb[u] = (b && tc == 0 && r < kb) ? b[k0 + r] : T(0);
     }
     bool singular = false;
-    int buf = 0;
     for (int jj = 0; jj < NB / 4; jj++) {
+        const int buf = jj & 1;
+        // ---- publish ----
+        if (tc == jj) {
 #pragma unroll
-        for (int jr = 0; jr < 4; jr++) {
-            const int j = 4 * jj + jr;
-            if (tc == jj) {
+            for (int u = 0; u < 4; u++) st4s<T>(scol[buf][4 * ti + u], a[u]);
+            if (ti == jj) {
+                T P[4][4], rd[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) scol[buf][4 * ti + u] = a[u][jr];
-                if (ti == jj) {
-                    T d = a[jr][jr];
+                for (int m = 0; m < 4; m++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) P[m][c] = a[m][c];
+#pragma unroll
+                for (int m = 0; m < 4; m++) {
+                    T d = P[m][m];
                     if (bad_pivot(d)) {
                         singular = true;
                         d = T(1);
                     }
-                    spiv[buf][0] = d;
-                    spiv[buf][1] = T(1) / d;
-                }
-            }
-            if (ti == jj) {
+                    rd[m] = T(1) / d;
+                    T w[4];
 #pragma unroll
-                for (int v = 0; v < 4; v++) srow[buf][4 * tc + v] = li[jr][v];
-                if (tc == 0) sbj[buf] = bb[jr];
+                    for (int r = 0; r < 4; r++) w[r] = P[r][m];
+#pragma unroll
+                    for (int r = m + 1; r < 4; r++) {
+                        const T l = w[r] * rd[m];
+#pragma unroll
+                        for (int c = m + 1; c <= r; c++) P[r][c] = fma(-l, w[c], P[r][c]);
+                        P[r][m] = l;
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < 4; m++) st4s<T>(spiv[buf][m], P[m]);
+                st4s<T>(srd[buf], rd);
             }
-            __syncthreads();
-            const T rd = spiv[buf][1];
-            T l[4], w[4], lr[4];
+        }
+        if (ti == jj) {
+#pragma unroll
+            for (int m = 0; m < 4; m++) st4s<T>(&srow[buf][m][4 * tc], li[m]);
+            if (tc == 0) st4s<T>(sbp[buf], bb);
+        }
+        __syncthreads();
+        // ---- eliminate ----
+        T lp[4][4], rd[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++) ld4s<T>(spiv[buf][m], lp[m]);
+        ld4s<T>(srd[buf], rd);
+        // z = L_P^-1 x (L_P unit lower, from lp's strict lower part)
+        auto fwd = [&](const T (&x)[4], T (&z)[4]) {
+            z[0] = x[0];
+            z[1] = fma(-z[0], lp[1][0], x[1]);
+            z[2] = fma(-z[1], lp[2][1], fma(-z[0], lp[2][0], x[2]));
+            z[3] = fma(-z[2], lp[3][2], fma(-z[1], lp[3][1], fma(-z[0], lp[3][0], x[3])));
+        };
+        const bool rowact = ti > jj;
+        T L[4][4];
+        if (rowact) {
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                l[u] = 4 * ti + u > j ? scol[buf][4 * ti + u] * rd : T(0);
-                w[u] = 4 * tc + u > j ? scol[buf][4 * tc + u] : T(0);
-                lr[u] = srow[buf][4 * tc + u];
-            }
+                T x[4], z[4];
+                ld4s<T>(scol[buf][4 * ti + u], x);
+                fwd(x, z);
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+                for (int m = 0; m < 4; m++) L[u][m] = z[m] * rd[m];
+            }
+            if (tc > jj) {
 #pragma unroll
                 for (int v = 0; v < 4; v++) {
-                    a[u][v] = fma(-l[u], w[v], a[u][v]);
-                    li[u][v] = fma(-l[u], lr[v], li[u][v]);
+                    T x[4], z[4];
+                    ld4s<T>(scol[buf][4 * tc + v], x);
+                    fwd(x, z);
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+#pragma unroll
+                        for (int m = 0; m < 4; m++) a[u][v] = fma(-L[u][m], z[m], a[u][v]);
                 }
-            if (tc == jj) {
+            }
+        }
+        if (tc <= jj) {  // Linv's rows j0.. are zero right of column j0+3
+            T R[4][4];
+#pragma unroll
+            for (int m = 0; m < 4; m++) ld4s<T>(&srow[buf][m][4 * tc], R[m]);
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                R[1][v] = fma(-R[0][v], lp[1][0], R[1][v]);
+                R[2][v] = fma(-R[1][v], lp[2][1], fma(-R[0][v], lp[2][0], R[2][v]));
+                R[3][v] = fma(-R[2][v], lp[3][2], fma(-R[1][v], lp[3][1], fma(-R[0][v], lp[3][0], R[3][v])));
+            }
+            if (rowact) {
 #pragma unroll
                 for (int u = 0; u < 4; u++)
-                    if (4 * ti + u > j) a[u][jr] = l[u];
-            }
-            if (tc == 0) {
-                const T bj = sbj[buf];
 #pragma unroll
-                for (int u = 0; u < 4; u++) bb[u] = fma(-l[u], bj, bb[u]);
+                    for (int v = 0; v < 4; v++)
+#pragma unroll
+                        for (int m = 0; m < 4; m++) li[u][v] = fma(-L[u][m], R[m][v], li[u][v]);
+            } else if (ti == jj) {
+#pragma unroll
+                for (int m = 0; m < 4; m++)
+#pragma unroll
+                    for (int v = 0; v < 4; v++) li[m][v] = R[m][v];
             }
-            buf ^= 1;
+        }
+        if (tc == 0 && ti >= jj) {
+            T x[4], z[4];
+            ld4s<T>(sbp[buf], x);
+            fwd(x, z);
+            if (rowact) {
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+#pragma unroll
+                    for (int m = 0; m < 4; m++) bb[u] = fma(-L[u][m], z[m], bb[u]);
+            } else {
+#pragma unroll
+                for (int m = 0; m < 4; m++) bb[m] = z[m];
+            }
+        }
+        if (tc == jj) {
+            if (rowact) {
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+#pragma unroll
+                    for (int m = 0; m < 4; m++) a[u][m] = L[u][m];
+            } else if (ti == jj) {
+#pragma unroll
+                for (int m = 0; m < 4; m++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) a[m][c] = lp[m][c];
+            }
         }
     }
     if (singular) atomicOr(flags, FLAG_SINGULAR);
@@ -386,6 +496,106 @@ __global__ void __launch_bounds__(256, 1) k_update_f64(int n, long long ld, doub
             const long long col = j0 + tx + 16 * v;
             if (col < n && col <= row) A[row * ld + col] -= acc[u][v];
         }
+    }
+}
+
+// The same update on the FP64 tensor cores (mma.sync m8n8k4, FP64 in and out,
+// so the products and sums are FP64 operations as in the SIMT kernel).  Warp w
+// takes rows 32(w/2) .. +31 and columns 64(w%2) .. +63 of the 128 x 128 tile:
+// 4 x 8 MMA tiles of 8 x 8, 64 accumulators a thread.  Fragments of m8n8k4
+// (g = lane / 4, t = lane % 4): A (row g, k t), B (k t, column g), C (row g,
+// columns 2t, 2t+1).  The k-major shared operands have a pitch of WPITCH = 132
+// doubles (132 = 4 mod 16), so a half-warp's fragment reads hit 16 distinct
+// 8-byte banks.
+constexpr int WPITCH = WTILE + 4;
+__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(256, 1) k_update_f64_mma(int n, long long ld, double *A, int K0, int K, int R0,
+                                                           const double *__restrict__ W, int ldw, int colblocks) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double(*sL)[WKC][WPITCH] = reinterpret_cast<double(*)[WKC][WPITCH]>(smem_raw);
+    double(*sW)[WKC][WPITCH] = sL + 2;
+    long long bidx = blockIdx.x;
+    int bi, bj;
+    if (colblocks > 0) {
+        bi = (int)(bidx / colblocks);
+        bj = (int)(bidx % colblocks);
+    } else {
+        bi = (int)((sqrt(8.0 * (double)bidx + 1.0) - 1.0) * 0.5);
+        while ((long long)(bi + 1) * (bi + 2) / 2 <= bidx) bi++;
+        while ((long long)bi * (bi + 1) / 2 > bidx) bi--;
+        bj = (int)(bidx - (long long)bi * (bi + 1) / 2);
+    }
+    const long long i0 = R0 + (long long)bi * WTILE, j0 = R0 + (long long)bj * WTILE;
+    if (j0 > i0 + WTILE - 1) return;  // strip tile entirely above the diagonal
+    const int t = threadIdx.x;
+    // loader: row lr of the tile, k half lh (8 values)
+    const int lr = t >> 1, lh = t & 1;
+    const bool lrow = i0 + lr < n, wrow = j0 + lr < n;
+    const double *lsrc = A + (i0 + (lrow ? lr : 0)) * ld + K0 + lh * 8;
+    const double *wsrc = W + (j0 + (wrow ? lr : 0)) * (long long)ldw + lh * 8;
+    double2 pl[4], pw[4];
+    auto fetch = [&](int kc) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            pl[e] = lrow ? __ldg(reinterpret_cast<const double2 *>(lsrc + kc * WKC) + e) : make_double2(0.0, 0.0);
+            pw[e] = wrow ? __ldg(reinterpret_cast<const double2 *>(wsrc + kc * WKC) + e) : make_double2(0.0, 0.0);
+        }
+    };
+    auto stash = [&](int buf) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            sL[buf][lh * 8 + 2 * e][lr] = pl[e].x;
+            sL[buf][lh * 8 + 2 * e + 1][lr] = pl[e].y;
+            sW[buf][lh * 8 + 2 * e][lr] = pw[e].x;
+            sW[buf][lh * 8 + 2 * e + 1][lr] = pw[e].y;
+        }
+    };
+    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
+    const int wm0 = 32 * (w >> 1), wn0 = 64 * (w & 1);
+    double acc[4][8][2];
+#pragma unroll
+    for (int mi = 0; mi < 4; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 8; ni++) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    const int NKC = K / WKC;
+#pragma unroll 1
+    for (int kc = 0; kc < NKC; kc++) {
+        const int buf = kc & 1;
+        if (kc + 1 < NKC) fetch(kc + 1);
+#pragma unroll
+        for (int k4 = 0; k4 < WKC; k4 += 4) {
+            double a[4], b[8];
+#pragma unroll
+            for (int mi = 0; mi < 4; mi++) a[mi] = sL[buf][k4 + tq][wm0 + 8 * mi + g];
+#pragma unroll
+            for (int ni = 0; ni < 8; ni++) b[ni] = sW[buf][k4 + tq][wn0 + 8 * ni + g];
+#pragma unroll
+            for (int mi = 0; mi < 4; mi++)
+#pragma unroll
+                for (int ni = 0; ni < 8; ni++) dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+        }
+        if (kc + 1 < NKC) stash(buf ^ 1);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; mi++) {
+        const long long row = i0 + wm0 + 8 * mi + g;
+        if (row >= n) continue;
+#pragma unroll
+        for (int ni = 0; ni < 8; ni++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const long long col = j0 + wn0 + 8 * ni + 2 * tq + e;
+                if (col < n && col <= row) A[row * ld + col] -= acc[mi][ni][e];
+            }
     }
 }
 
@@ -652,26 +862,242 @@ __global__ void __launch_bounds__(256) k_trsv_ll(int n, long long ld, const T *_
     }
 }
 
-// Coupling blocks of the wavefront solves, one CTA per block: Mf_i = Linv_ii
-// L_{i,i-1} (i > 0) and, when Mb is given, Mb_i = Linv_ii^T L_{i+1,i}^T (i <
-// nblk-1).  With skip_tiny, rows of L_{i,i-1} whose diagonal entry of A has
-// magnitude below 1e-12 count as zero (the Gauss-Seidel sweep keeps those rows'
-// values).  Dynamic smem: two [64][65] blocks.
+// ---- banded wavefront solves -----------------------------------------------------------
+// The same solves with each CTA owning a band of two consecutive blocks in
+// solve order, b1 then b2, so the step from b1 to b2 is a block barrier inside
+// the CTA and only every second step of the chain crosses SMs.  With p the
+// block before b1 in solve order, C1 / C2 the direction's coupling blocks at
+// distance 1 and 2 (k_trsv_couplings) and y_b the block's inverse (forward
+// Linv, backward Linv^T) applied to its right-hand side less the blocks before
+// p, which the band sums as they are published:
+//   x_b1 = y_b1 - C1_b1 x_p,    x_b2 = (y_b2 - C2_b2 x_p) - C1_b2 x_b1.
+// Each band sums two blocks' rows per published chunk, so a band step asks
+// twice the loads of its CTA; the banded form is used from 256 blocks on (16,384
+// unknowns), where halving the chain's hops outweighs that.
+// Shared memory: the two inverses, C1_b1, C2_b2, C1_b2 ([64][MS] each), the
+// two blocks' partial sums, poll buffers, right-hand sides, x_b1.
+constexpr int BAND_FROM_BLOCKS = 256;
+template <typename T>
+constexpr size_t band_smem() {
+    return sizeof(T) * (5 * NB * MS + 2 * 16 * (NB + 1) + 5 * NB) + 2 * sizeof(int);
+}
+
+template <typename T, int DIR>
+__global__ void __launch_bounds__(256, 2)
+    k_trsv_band(int n, long long ld, const T *__restrict__ A, const T *__restrict__ Linv, const T *__restrict__ C1,
+                const T *__restrict__ C2, const T *__restrict__ dvec, T *x, unsigned long long *ll, unsigned epoch,
+                unsigned long long *flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T(*sI1)[MS] = reinterpret_cast<T(*)[MS]>(smem_raw);
+    T(*sI2)[MS] = sI1 + NB;
+    T(*sC11)[MS] = sI2 + NB;  // C1 of b1
+    T(*sC22)[MS] = sC11 + NB;  // C2 of b2
+    T(*sC12)[MS] = sC22 + NB;  // C1 of b2
+    T(*spart)[16][NB + 1] = reinterpret_cast<T(*)[16][NB + 1]>(sC12 + NB);  // [2][16][65]
+    T *sx = reinterpret_cast<T *>(spart + 2);                                // [2][NB]
+    T *srhs = sx + 2 * NB;                                                   // [2][NB]
+    T *sx1 = srhs + 2 * NB;                                                  // [NB]
+    int *sok = reinterpret_cast<int *>(sx1 + NB);                            // [2]
+    const int nblk = (n + NB - 1) / NB, nband = (nblk + 1) / 2;
+    const int t = threadIdx.x;
+    const int r = t >> 2, q = t & 3;       // forward sums and the chain steps: row r
+    const int c4 = t & 15, part = t >> 4;  // backward sums: columns 4c4 .. +3, chunk rows 4part .. +3
+    int par = 0;
+    for (int g = blockIdx.x; g < nband; g += gridDim.x) {
+        const int b1 = DIR > 0 ? 2 * g : nblk - 1 - 2 * g, b2 = b1 + DIR, p = b1 - DIR;
+        const bool two = b2 >= 0 && b2 < nblk, has_p = p >= 0 && p < nblk;
+        const int r01 = b1 * NB, kb1 = n - r01 < NB ? n - r01 : NB;
+        const int r02 = b2 * NB, kb2 = two ? (n - r02 < NB ? n - r02 : NB) : 0;
+        for (int idx = t; idx < NB * NB; idx += 256) {
+            const int rr = idx >> 6, cc = idx & 63;
+            sI1[rr][cc] = __ldg(&Linv[(size_t)b1 * NB * NB + idx]);
+            sC11[rr][cc] = has_p ? __ldg(&C1[(size_t)b1 * NB * NB + idx]) : T(0);
+            sI2[rr][cc] = two ? __ldg(&Linv[(size_t)b2 * NB * NB + idx]) : T(0);
+            sC22[rr][cc] = two && has_p ? __ldg(&C2[(size_t)b2 * NB * NB + idx]) : T(0);
+            sC12[rr][cc] = two ? __ldg(&C1[(size_t)b2 * NB * NB + idx]) : T(0);
+        }
+        // the band's right-hand sides are no other block's output: read them before any wait
+        if (t < 2 * NB) {
+            const int h = t >> 6, rr = t & 63, kb = h ? kb2 : kb1, row = (h ? r02 : r01) + rr;
+            T v = T(0);
+            if (rr < kb) v = DIR > 0 ? __ldcg(&x[row]) : __ldcg(&x[row]) / dvec[row];
+            srhs[t] = v;
+        }
+        // blocks before p: forward 0 .. b1-2, backward nblk-1 .. b1+2
+        const int nfar = DIR > 0 ? (b1 > 1 ? b1 - 1 : 0) : (nblk - 2 - b1 > 0 ? nblk - 2 - b1 : 0);
+        T acc1 = T(0), acc2 = T(0), a41[4] = {T(0), T(0), T(0), T(0)}, a42[4] = {T(0), T(0), T(0), T(0)};
+        T ap1[16], ap2[16];
+        auto fetch = [&](int j) {
+            if (DIR > 0) {
+                if (r < kb1) {
+                    load16<T, false>(A + (long long)(r01 + r) * ld + j * NB + q * 16, ap1);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 16; k++) ap1[k] = T(0);
+                }
+                if (r < kb2) {
+                    load16<T, false>(A + (long long)(r02 + r) * ld + j * NB + q * 16, ap2);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 16; k++) ap2[k] = T(0);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int i = j * NB + 4 * part + e;
+                    if (i < n) {
+                        load4p<T>(A + (long long)i * ld + r01 + 4 * c4, ap1 + 4 * e);
+                        if (two) {
+                            load4p<T>(A + (long long)i * ld + r02 + 4 * c4, ap2 + 4 * e);
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < 4; k++) ap2[4 * e + k] = T(0);
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 4; k++) ap1[4 * e + k] = ap2[4 * e + k] = T(0);
+                    }
+                }
+            }
+        };
+        bool ok = true;
+        if (nfar > 0) fetch(DIR > 0 ? 0 : nblk - 1);
+        for (int s = 0; s < nfar; s++) {
+            const int j = DIR > 0 ? s : nblk - 1 - s;
+            T *buf = sx + par * NB;
+            ok = wait_chunk<T>(ll, j, epoch, buf, poll_backoff(nfar - s), sok + par, flags);
+            par ^= 1;
+            if (!ok) break;
+            if (DIR > 0) {
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    const T xv = buf[q * 16 + k];
+                    acc1 = fma(ap1[k], xv, acc1);
+                    acc2 = fma(ap2[k], xv, acc2);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const T xe = buf[4 * part + e];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        a41[k] = fma(ap1[4 * e + k], xe, a41[k]);
+                        a42[k] = fma(ap2[4 * e + k], xe, a42[k]);
+                    }
+                }
+            }
+            if (s + 1 < nfar) fetch(DIR > 0 ? j + 1 : j - 1);
+        }
+        if (DIR > 0) {
+            acc1 += __shfl_xor_sync(0xffffffffu, acc1, 1);
+            acc1 += __shfl_xor_sync(0xffffffffu, acc1, 2);
+            acc2 += __shfl_xor_sync(0xffffffffu, acc2, 1);
+            acc2 += __shfl_xor_sync(0xffffffffu, acc2, 2);
+            if (q == 0) {
+                spart[0][0][r] = acc1;
+                spart[1][0][r] = acc2;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                spart[0][part][4 * c4 + k] = a41[k];
+                spart[1][part][4 * c4 + k] = a42[k];
+            }
+        }
+        __syncthreads();
+        if (t < 2 * NB) {
+            const int h = t >> 6, rr = t & 63;
+            T sum = T(0);
+            if (DIR > 0) {
+                sum = spart[h][0][rr];
+            } else {
+#pragma unroll
+                for (int pp = 0; pp < 16; pp++) sum += spart[h][pp][rr];
+            }
+            srhs[t] -= sum;
+        }
+        __syncthreads();
+        T y1 = T(0), y2 = T(0);
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int c = 4 * k + q;
+            y1 = fma(DIR > 0 ? sI1[r][c] : sI1[c][r], srhs[c], y1);
+            y2 = fma(DIR > 0 ? sI2[r][c] : sI2[c][r], srhs[NB + c], y2);
+        }
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+        y2 += __shfl_xor_sync(0xffffffffu, y2, 1);
+        y2 += __shfl_xor_sync(0xffffffffu, y2, 2);
+        // the chain: p crosses SMs, b1 -> b2 stays in the CTA
+        T x1 = y1, t2 = y2;
+        if (has_p && ok) {
+            T *buf = sx + par * NB;
+            ok = wait_chunk<T>(ll, p, epoch, buf, 0, sok + par, flags);
+            par ^= 1;
+            if (ok) {
+                T v1 = T(0), v2 = T(0);
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    const int c = 4 * k + q;
+                    const T xv = buf[c];
+                    v1 = fma(sC11[r][c], xv, v1);
+                    v2 = fma(sC22[r][c], xv, v2);
+                }
+                v1 += __shfl_xor_sync(0xffffffffu, v1, 1);
+                v1 += __shfl_xor_sync(0xffffffffu, v1, 2);
+                v2 += __shfl_xor_sync(0xffffffffu, v2, 1);
+                v2 += __shfl_xor_sync(0xffffffffu, v2, 2);
+                x1 = y1 - v1;
+                t2 = y2 - v2;
+            }
+        }
+        if (q == 0) {
+            ll_put<T>(ll, b1, r, r < kb1 ? x1 : T(0), epoch);
+            if (r < kb1) x[r01 + r] = x1;
+            sx1[r] = r < kb1 ? x1 : T(0);
+        }
+        if (two) {
+            __syncthreads();
+            T v3 = T(0);
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int c = 4 * k + q;
+                v3 = fma(sC12[r][c], sx1[c], v3);
+            }
+            v3 += __shfl_xor_sync(0xffffffffu, v3, 1);
+            v3 += __shfl_xor_sync(0xffffffffu, v3, 2);
+            const T x2 = t2 - v3;
+            if (q == 0) {
+                ll_put<T>(ll, b2, r, r < kb2 ? x2 : T(0), epoch);
+                if (r < kb2) x[r02 + r] = x2;
+            }
+        }
+        __syncthreads();  // shared memory is reused by this CTA's next band
+    }
+}
+
+// Coupling blocks of the wavefront solves, one CTA per block, at block
+// distance d: Mf_i = Linv_ii L_{i,i-d} (i >= d) and, when Mb is given,
+// Mb_i = Linv_ii^T L_{i+d,i}^T (i < nblk-d).  With skip_tiny, rows of
+// L_{i,i-d} whose diagonal entry of A has magnitude below 1e-12 count as zero
+// (the Gauss-Seidel sweep keeps those rows' values).  Dynamic smem: two
+// [64][65] blocks.
 template <typename T>
 __global__ void __launch_bounds__(256) k_trsv_couplings(int n, long long ld, const T *__restrict__ A,
-                                                        const T *__restrict__ Linv, T *Mf, T *Mb, int skip_tiny) {
+                                                        const T *__restrict__ Linv, T *Mf, T *Mb, int skip_tiny,
+                                                        int dist) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T(*sI)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
     T(*sL)[NB + 1] = sI + NB;
     const int nblk = (n + NB - 1) / NB, blk = blockIdx.x, r0 = blk * NB, t = threadIdx.x;
     const int tx = t & 15, ty = t >> 4;
     for (int idx = t; idx < NB * NB; idx += 256) sI[idx >> 6][idx & 63] = Linv[(size_t)blk * NB * NB + idx];
-    if (blk > 0) {
+    if (blk >= dist) {
         for (int idx = t; idx < NB * NB; idx += 256) {
             const int rr = idx >> 6, cc = idx & 63, row = r0 + rr;
             bool keep = row < n;
             if (keep && skip_tiny) keep = fabs((double)A[(long long)row * ld + row]) >= 1e-12;
-            sL[rr][cc] = keep ? A[(long long)row * ld + r0 - NB + cc] : T(0);
+            sL[rr][cc] = keep ? A[(long long)row * ld + r0 - dist * NB + cc] : T(0);
         }
         __syncthreads();
         T acc[4][4] = {};
@@ -693,9 +1119,9 @@ __global__ void __launch_bounds__(256) k_trsv_couplings(int n, long long ld, con
             for (int v = 0; v < 4; v++) out[(4 * ty + u) * NB + 4 * tx + v] = acc[u][v];
         __syncthreads();
     }
-    if (Mb && blk + 1 < nblk) {
+    if (Mb && blk + dist < nblk) {
         for (int idx = t; idx < NB * NB; idx += 256) {
-            const int rr = idx >> 6, cc = idx & 63, row = r0 + NB + rr;
+            const int rr = idx >> 6, cc = idx & 63, row = r0 + dist * NB + rr;
             sL[rr][cc] = row < n ? A[(long long)row * ld + r0 + cc] : T(0);
         }
         __syncthreads();
@@ -887,7 +1313,7 @@ template <typename T>
 struct LdltWork {
     T *dvec, *W, *s;
     T *Linv;                 // [blocks][NB][NB] inverses of the diagonal blocks' L (the solves use them)
-    T *Mc;                   // [2][blocks][NB][NB] coupling blocks of the forward and backward solves
+    T *Mc;                   // [4][blocks][NB][NB] coupling blocks: forward, backward at distance 1, then 2
     unsigned long long *ll;  // [2][blocks][2][NB] words the two solves publish their blocks in
     float *split;            // tensor-core path: [4][n][SUPER_W] hi/lo copies of the update's L and W rows
 };
@@ -964,6 +1390,12 @@ static void wavefront_attrs() {
     cudaFuncSetAttribute(k_trsv_ll<T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsv_smem<T>());
     cudaFuncSetAttribute(k_trsv_couplings<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(2 * NB * (NB + 1) * sizeof(T)));
+    if constexpr (std::is_same<T, float>::value) {
+        cudaFuncSetAttribute(k_trsv_band<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)band_smem<float>());
+        cudaFuncSetAttribute(k_trsv_band<float, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)band_smem<float>());
+    }
 }
 
 template <typename T>
@@ -974,12 +1406,13 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     const size_t upd_smem = sizeof(T) * 2 * NB * 68;
     const size_t panel_tc_smem = sizeof(float) * (2 * NB * MS + 4 * NB);
     const size_t cols_tc_smem = sizeof(float) * 2 * NB * MS;
-    const size_t f64_smem = sizeof(double) * 4 * WKC * WTILE;
+    const size_t f64_smem = sizeof(double) * 4 * WKC * WPITCH;
     if (!ctx->ldlt_attr) {  // per context: the attributes belong to the context's device
         const int big = 96 * 1024;
         cudaFuncSetAttribute(k_ldlt_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_update_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(k_update_f64_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_update_cols<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_ldlt_update_cols<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(tc::k_update_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1031,9 +1464,9 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             const int cb = strip ? (C1 - R0) / WTILE : 0;
             const long long ntiles = strip ? rb * cb : rb * (rb + 1) / 2;
             const int mk = kt_begin(ctx, MP_KT_UPDATE, update_flops(R0, C1, K));
-            k_update_f64<<<(unsigned)ntiles, 256, f64_smem, st>>>(n, ld, reinterpret_cast<double *>(A), K0, K, R0,
-                                                                 reinterpret_cast<const double *>(w.W) + kofs,
-                                                                 SUPER_W, cb),
+            k_update_f64_mma<<<(unsigned)ntiles, 256, f64_smem, st>>>(n, ld, reinterpret_cast<double *>(A), K0, K,
+                                                                     R0, reinterpret_cast<const double *>(w.W) + kofs,
+                                                                     SUPER_W, cb),
                 ++ctx->launches;
             kt_end(ctx, mk);
             return MP_OK;
@@ -1122,26 +1555,49 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     }
     const int nblk = (n + NB - 1) / NB;
     const size_t blkw = (size_t)nblk * NB * NB, llw = (size_t)nblk * 2 * NB;
-    T *Mf = w.Mc, *Mb = w.Mc + blkw;
+    // coupling blocks: [forward, backward] at distance 1, then (FP32: banded
+    // solves) at distance 2
+    T *C1f = w.Mc, *C1b = w.Mc + blkw, *C2f = w.Mc + 2 * blkw, *C2b = w.Mc + 3 * blkw;
+    const bool banded = std::is_same<T, float>::value && nblk >= BAND_FROM_BLOCKS;
     if (factor) {  // the coupling blocks of the solves belong to this factor
         const int mk = kt_begin(ctx, MP_KT_TRSV, 0);
-        k_trsv_couplings<T><<<nblk, 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(n, ld, A, w.Linv, Mf, Mb, 0),
-            ++ctx->launches;
+        const size_t cs = 2 * NB * (NB + 1) * sizeof(T);
+        k_trsv_couplings<T><<<nblk, 256, cs, st>>>(n, ld, A, w.Linv, C1f, C1b, 0, 1), ++ctx->launches;
+        if (banded) k_trsv_couplings<T><<<nblk, 256, cs, st>>>(n, ld, A, w.Linv, C2f, C2b, 0, 2), ++ctx->launches;
         kt_end(ctx, mk);
     }
     const unsigned epoch = next_wavefront_epoch(ctx, w.ll, 2 * llw);
-    const size_t smem = trsv_smem<T>();
     const int mk = kt_begin(ctx, MP_KT_TRSV, 0);
-    if (!factor) {
-        const int g = wavefront_grid(ctx, (const void *)k_trsv_ll<T, 1>, nblk, smem);
-        MP_CUDA(ctx, launch_wavefront(k_trsv_ll<T, 1>, g, smem, st, n, ld, (const T *)A, (const T *)w.Linv,
-                                      (const T *)Mf, (const T *)w.dvec, b, w.ll, epoch, flags));
+    if (banded) {
+        if constexpr (std::is_same<T, float>::value) {
+            const int nband = (nblk + 1) / 2;
+            const size_t sm = band_smem<float>();
+            if (!factor) {
+                const int g = wavefront_grid(ctx, (const void *)k_trsv_band<float, 1>, nband, sm);
+                MP_CUDA(ctx, launch_wavefront(k_trsv_band<float, 1>, g, sm, st, n, ld, (const float *)A,
+                                              (const float *)w.Linv, (const float *)C1f, (const float *)C2f,
+                                              (const float *)w.dvec, b, w.ll, epoch, flags));
+                ++ctx->launches;
+            }
+            const int g = wavefront_grid(ctx, (const void *)k_trsv_band<float, -1>, nband, sm);
+            MP_CUDA(ctx, launch_wavefront(k_trsv_band<float, -1>, g, sm, st, n, ld, (const float *)A,
+                                          (const float *)w.Linv, (const float *)C1b, (const float *)C2b,
+                                          (const float *)w.dvec, b, w.ll + llw, epoch, flags));
+            ++ctx->launches;
+        }
+    } else {
+        const size_t smem = trsv_smem<T>();
+        if (!factor) {
+            const int g = wavefront_grid(ctx, (const void *)k_trsv_ll<T, 1>, nblk, smem);
+            MP_CUDA(ctx, launch_wavefront(k_trsv_ll<T, 1>, g, smem, st, n, ld, (const T *)A, (const T *)w.Linv,
+                                          (const T *)C1f, (const T *)w.dvec, b, w.ll, epoch, flags));
+            ++ctx->launches;
+        }
+        const int g = wavefront_grid(ctx, (const void *)k_trsv_ll<T, -1>, nblk, smem);
+        MP_CUDA(ctx, launch_wavefront(k_trsv_ll<T, -1>, g, smem, st, n, ld, (const T *)A, (const T *)w.Linv,
+                                      (const T *)C1b, (const T *)w.dvec, b, w.ll + llw, epoch, flags));
         ++ctx->launches;
     }
-    const int g = wavefront_grid(ctx, (const void *)k_trsv_ll<T, -1>, nblk, smem);
-    MP_CUDA(ctx, launch_wavefront(k_trsv_ll<T, -1>, g, smem, st, n, ld, (const T *)A, (const T *)w.Linv,
-                                  (const T *)Mb, (const T *)w.dvec, b, w.ll + llw, epoch, flags));
-    ++ctx->launches;
     kt_end(ctx, mk);
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;

@@ -89,7 +89,7 @@ struct SolveScratch {
     double *dvec64 = nullptr, *W64 = nullptr, *s64 = nullptr, *r = nullptr, *Linv64 = nullptr;
     float *dvec32 = nullptr, *W32 = nullptr, *s32 = nullptr, *b32 = nullptr, *Linv32 = nullptr, *split32 = nullptr;
     double *Mc64 = nullptr;             // [2][blocks][NB][NB] coupling blocks (FP64 solves, Gauss-Seidel)
-    float *Mc32 = nullptr;              // [2][blocks][NB][NB] coupling blocks (FP32 solves)
+    float *Mc32 = nullptr;              // [4][blocks][NB][NB] coupling blocks (FP32 banded solves)
     unsigned long long *ll = nullptr;   // [2][blocks][2][NB] wavefront words
     size_t ll_words = 0;
     int neq = 0;
@@ -133,7 +133,7 @@ static int ensure_scratch(mp_ctx *ctx, SolveScratch **out) {
     MP_CUDA(ctx, cudaMalloc(&s.Linv32, sizeof(float) * nblk * NB * NB));
     MP_CUDA(ctx, cudaMalloc(&s.split32, sizeof(float) * 4 * (size_t)n * SUPER_W));
     MP_CUDA(ctx, cudaMalloc(&s.Mc64, sizeof(double) * 2 * nblk * NB * NB));
-    MP_CUDA(ctx, cudaMalloc(&s.Mc32, sizeof(float) * 2 * nblk * NB * NB));
+    MP_CUDA(ctx, cudaMalloc(&s.Mc32, sizeof(float) * 4 * nblk * NB * NB));
     s.ll_words = 2 * nblk * 2 * NB;
     MP_CUDA(ctx, cudaMalloc(&s.ll, sizeof(unsigned long long) * s.ll_words));
     MP_CUDA(ctx, cudaMemsetAsync(s.ll, 0, sizeof(unsigned long long) * s.ll_words, ctx->stream));
@@ -398,7 +398,7 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st) {
     k_gs_block_inverse<<<nblk, 64, 0, ctx->stream>>>(n, ld, ctx->J, sp->Linv64), ++ctx->launches;
     wavefront_attrs<double>();
     k_trsv_couplings<double><<<nblk, 256, 2 * NB * (NB + 1) * sizeof(double), ctx->stream>>>(
-        n, ld, ctx->J, sp->Linv64, sp->Mc64, nullptr, 1),
+        n, ld, ctx->J, sp->Linv64, sp->Mc64, nullptr, 1, 1),
         ++ctx->launches;
     const size_t smem = gs_smem();
     cudaFuncSetAttribute(k_gs_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
