@@ -93,9 +93,12 @@ __device__ __forceinline__ void st4s(T *p, const T (&v)[4]) {
     }
 }
 
+// The block is read with coherent loads: the in-panel column update of the
+// previous block runs this on the CTA that has just updated the block
+// (k_ldlt_update_cols*, kbn > 0).  All 256 threads of the CTA call it.
 template <typename T>
-__global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
-                                                   T *b, unsigned long long *flags) {
+__device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv, T *b,
+                                           unsigned long long *flags) {
     __shared__ __align__(16) T scol[2][NB][4];  // the step's four columns, every row
     __shared__ __align__(16) T srow[2][4][NB];  // Linv's rows j0 .. j0+3, every column
     __shared__ __align__(16) T spiv[2][4][4];   // the factored pivot block: L_P below the diagonal, D_P on it
@@ -112,13 +115,9 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, in
         const T *row = A + (long long)(k0 + r) * ld + k0 + 4 * tc;
         T v4[4] = {T(0), T(0), T(0), T(0)};
         if (r < kb) {
-            if (4 * tc + 3 < kb) {
-                load4p<T>(row, v4);
-            } else {
 #pragma unroll
-                for (int v = 0; v < 4; v++)
-                    if (4 * tc + v < kb) v4[v] = row[v];
-            }
+            for (int v = 0; v < 4; v++)
+                if (4 * tc + v < kb) v4[v] = __ldcg(row + v);
         }
 #pragma unroll
         for (int v = 0; v < 4; v++) {
@@ -126,7 +125,7 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, in
             a[u][v] = r < kb ? (c <= r ? v4[v] : T(0)) : (r == c ? T(1) : T(0));
             li[u][v] = r == c ? T(1) : T(0);
         }
-        bb[u] = (b && tc == 0 && r < kb) ? b[k0 + r] : T(0);
+        bb[u] = (b && tc == 0 && r < kb) ? __ldcg(&b[k0 + r]) : T(0);
     }
     bool singular = false;
     for (int jj = 0; jj < NB / 4; jj++) {
@@ -277,6 +276,29 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, in
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
+                                                   T *b, unsigned long long *flags) {
+    diag_block<T>(n, ld, A, k0, kb, dvec, Linv, b, flags);
+}
+
+// The next block's diagonal factor, run by the CTA of an in-panel column
+// update that owns the next diagonal tile (grid tile (0, 0)) once that tile is
+// stored: it overlaps the rest of the update and saves a launch per block.
+struct NextDiag {
+    int k0, kb;  // kb == 0: none
+    void *dvec, *Linv, *b;
+    unsigned long long *flags;
+};
+template <typename T>
+__device__ __forceinline__ void fused_next_diag(int n, long long ld, T *A, const NextDiag &nd) {
+    if (nd.kb > 0 && blockIdx.x == 0 && blockIdx.y == 0) {
+        __syncthreads();  // the tile's stores by every thread of this CTA come first
+        diag_block<T>(n, ld, A, nd.k0, nd.kb, static_cast<T *>(nd.dvec), static_cast<T *>(nd.Linv),
+                      static_cast<T *>(nd.b), nd.flags);
+    }
+}
+
 // Panel: rows [r0, r0+64) below the diagonal block.  W = A_ik L_kk^-T (a small
 // product with Linv), L_ik = W D^-1, and b_i -= L_ik z_k.  Dynamic smem: the
 // rows' panel [64][NB+1] and Linv [NB][NB+1].
@@ -358,7 +380,7 @@ __global__ void __launch_bounds__(256) k_ldlt_panel(int n, long long ld, T *A, i
 // A_ij -= L_i W_j^T for rows i in [k1, n), 64x64 tiles, grid (col tile, row tile).
 template <typename T>
 __global__ void __launch_bounds__(256) k_ldlt_update_cols(int n, long long ld, T *A, int k0, int kb, const T *W,
-                                                          int ldw, int k1, int jend) {
+                                                          int ldw, int k1, int jend, NextDiag nd) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *sLt = reinterpret_cast<T *>(smem_raw);
     T *sWt = sLt + NB * 68;
@@ -406,6 +428,7 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols(int n, long long ld, T
             if (j < jend && j <= i) A[(long long)i * ld + j] -= acc[u][v];
         }
     }
+    fused_next_diag<T>(n, ld, A, nd);
 }
 
 // FP64 form: A[i][j] -= sum_{k<K} L[i][k] W[j][k] for rows/cols from R0, with
@@ -1274,7 +1297,8 @@ __global__ void __launch_bounds__(256) k_ldlt_panel_tc(int n, long long ld, floa
 // [k1, n) x columns [k1, jend).
 template <int TERMS>
 __global__ void __launch_bounds__(256) k_ldlt_update_cols_tc(int n, long long ld, float *A, int k0, int kb,
-                                                             const float *W, int ldw, int k1, int jend) {
+                                                             const float *W, int ldw, int k1, int jend,
+                                                             NextDiag nd) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float(*sL)[MS] = reinterpret_cast<float(*)[MS]>(smem_raw);
     float(*sW)[MS] = sL + NB;
@@ -1307,6 +1331,7 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols_tc(int n, long long ld
             const int i = i0 + m0 + g + (e >> 1) * 8, j = j0 + n0 + 8 * nt + 2 * tq + (e & 1);
             if (i < n && j < jend && j <= i) A[(long long)i * ld + j] -= acc[nt][e];
         }
+    fused_next_diag<float>(n, ld, A, nd);
 }
 
 template <typename T>
@@ -1427,11 +1452,16 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         ctx->ldlt_attr = true;
     }
     unsigned long long *flags = ctx->counters + C_FLAGS;
-    auto diag_and_panel = [&](int k0, int kb, T *W, int ldw) {
+    // the diagonal factor of block k0 (unless the previous block's in-panel
+    // column update ran it), then the panel below it
+    auto diag_and_panel = [&](int k0, int kb, T *W, int ldw, bool diag_done) {
         T *Li = w.Linv + (size_t)(k0 / NB) * NB * NB;
-        int mk = kt_begin(ctx, MP_KT_DIAG, 0);
-        k_ldlt_diag<T><<<1, 256, 0, st>>>(n, ld, A, k0, kb, w.dvec, Li, b, flags), ++ctx->launches;
-        kt_end(ctx, mk);
+        int mk;
+        if (!diag_done) {
+            mk = kt_begin(ctx, MP_KT_DIAG, 0);
+            k_ldlt_diag<T><<<1, 256, 0, st>>>(n, ld, A, k0, kb, w.dvec, Li, b, flags), ++ctx->launches;
+            kt_end(ctx, mk);
+        }
         int k1 = k0 + kb;
         if (k1 < n) {
             mk = kt_begin(ctx, MP_KT_PANEL, 0);
@@ -1520,23 +1550,29 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             const int S1 = S0 + SUPER_W < n ? S0 + SUPER_W : n;
             for (int P0 = S0; P0 < S1; P0 += PANEL_W) {
                 const int P1 = P0 + PANEL_W < S1 ? P0 + PANEL_W : S1;
+                bool diag_done = false;
                 for (int k0 = P0; k0 < P1; k0 += NB) {
                     const int kb = P1 - k0 < NB ? P1 - k0 : NB;
                     const int k1 = k0 + kb;
-                    diag_and_panel(k0, kb, w.W + (k0 - S0), SUPER_W);
+                    diag_and_panel(k0, kb, w.W + (k0 - S0), SUPER_W, diag_done);
+                    diag_done = false;
                     if (k1 < n && k1 < P1) {
+                        // the update's CTA on the next diagonal tile factors that block
+                        const int kbn = P1 - k1 < NB ? P1 - k1 : NB;
+                        const NextDiag nd{k1, kbn, w.dvec, w.Linv + (size_t)(k1 / NB) * NB * NB, b, flags};
+                        diag_done = true;
                         dim3 g((P1 - k1 + 63) / 64, (n - k1 + 63) / 64);
                         const int mk = kt_begin(ctx, MP_KT_PANEL, 0);
                         if constexpr (std::is_same<T, float>::value) {
                             if (tc_terms == 3)
-                                k_ldlt_update_cols_tc<3><<<g, 256, cols_tc_smem, st>>>(n, ld, A, k0, kb,
-                                                                                      w.W + (k0 - S0), SUPER_W, k1, P1);
+                                k_ldlt_update_cols_tc<3><<<g, 256, cols_tc_smem, st>>>(
+                                    n, ld, A, k0, kb, w.W + (k0 - S0), SUPER_W, k1, P1, nd);
                             else
-                                k_ldlt_update_cols_tc<1><<<g, 256, cols_tc_smem, st>>>(n, ld, A, k0, kb,
-                                                                                      w.W + (k0 - S0), SUPER_W, k1, P1);
+                                k_ldlt_update_cols_tc<1><<<g, 256, cols_tc_smem, st>>>(
+                                    n, ld, A, k0, kb, w.W + (k0 - S0), SUPER_W, k1, P1, nd);
                         } else {
                             k_ldlt_update_cols<T><<<g, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W + (k0 - S0),
-                                                                            SUPER_W, k1, P1);
+                                                                            SUPER_W, k1, P1, nd);
                         }
                         ++ctx->launches;
                         kt_end(ctx, mk);

@@ -364,6 +364,163 @@ __global__ void __launch_bounds__(256) k_gs_sweep(int n, long long ld, const dou
     }
 }
 
+// S Gauss-Seidel sweeps in one cooperative launch, one CTA per 64-row block
+// (used when every block's CTA is resident).  J is symmetric and stored in
+// full, so block i reads every other block j's contribution J_ij x_j as the
+// 64 x 64 tile of j's row band at i's columns (J_ji, transposed): when block j
+// publishes a sweep's values, all other blocks read one contiguous row band of
+// J.  In sweep s, block i sums the blocks j < i-1 of sweep s as they are
+// published, applies Minv_ii, takes block i-1 through the coupling block,
+// publishes x_i, and then sums its own diagonal block's strictly upper part
+// against x_i and the blocks j > i of sweep s, which is the x_old half of its
+// sweep s+1 -- so sweep s+1 needs no separate pass and starts as soon as the
+// last block of sweep s is published.  The first
+// sweep's x_old half comes in rup0 = b - U x.  One word per value and sweep
+// epoch suffices: a block publishes sweep s+1 only after every reader of its
+// sweep-s words has moved on.  x is updated in place (only the owning block
+// reads its own rows).
+constexpr size_t gs_sweeps_smem() { return sizeof(double) * (2 * NB * MS + 16 * (NB + 1) + 7 * NB) + 2 * sizeof(int); }
+
+__global__ void __launch_bounds__(256, 2) k_gs_sweeps(int n, long long ld, const double *__restrict__ A,
+                                                      const double *__restrict__ b, const double *__restrict__ rup0,
+                                                      const double *__restrict__ Minv, const double *__restrict__ Mc,
+                                                      double *x, unsigned long long *ll, unsigned epoch0, int S,
+                                                      unsigned long long *flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double(*sI)[MS] = reinterpret_cast<double(*)[MS]>(smem_raw);
+    double(*sC)[MS] = sI + NB;
+    double(*spart)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sC + NB);  // [16][65]
+    double *sx = reinterpret_cast<double *>(spart + 16);                     // [2][NB] poll buffers
+    double *srhs = sx + 2 * NB;                                              // this sweep's right-hand side
+    double *sb = srhs + NB;                                                  // b of the block's rows
+    double *snext = sb + NB;                                                 // b - U x_s: the next sweep's
+    double *sxo = snext + NB;                                                // the rows' current values
+    double *sdu = sxo + NB;                                                  // diagonal block's upper part x x_i
+    int *sok = reinterpret_cast<int *>(sdu + NB);                            // [2]
+    const int nblk = (n + NB - 1) / NB, blk = blockIdx.x;
+    const int r0 = blk * NB, kb = n - r0 < NB ? n - r0 : NB;
+    const int t = threadIdx.x;
+    const int r = t >> 2, q = t & 3;       // the chain step: row r, columns 4k + q
+    const int c4 = t & 15, part = t >> 4;  // tiles: block rows 4c4 .. +3, band rows 4part .. +3
+    const bool has_pred = blk > 0;
+    for (int idx = t; idx < NB * NB; idx += 256) {
+        sI[idx >> 6][idx & 63] = __ldg(&Minv[(size_t)blk * NB * NB + idx]);
+        sC[idx >> 6][idx & 63] = has_pred ? __ldg(&Mc[(size_t)blk * NB * NB + idx]) : 0.0;
+    }
+    // row r's strictly upper coefficients inside the diagonal block, columns 4k + q
+    double du[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        const int c = 4 * k + q;
+        du[k] = (r < kb && c > r && c < kb) ? A[(long long)(r0 + r) * ld + r0 + c] : 0.0;
+    }
+    bool skip = false;  // thread t < 64: row t keeps its value (|J_tt| < 1e-12)
+    if (t < NB) {
+        const bool in = t < kb;
+        sb[t] = in ? b[r0 + t] : 0.0;
+        snext[t] = in ? rup0[r0 + t] : 0.0;
+        sxo[t] = in ? x[r0 + t] : 0.0;
+        skip = in && fabs(A[(long long)(r0 + t) * ld + r0 + t]) < 1e-12;
+    }
+    // the 4 x 4 piece of the tile of band j at this block's columns
+    double ap[16];
+    auto fetch = [&](int j) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int i = j * NB + 4 * part + e;
+            if (i < n && 4 * c4 + 3 < kb) {
+                load4p<double>(A + (long long)i * ld + r0 + 4 * c4, ap + 4 * e);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++) ap[4 * e + k] = (i < n && 4 * c4 + k < kb) ? A[(long long)i * ld + r0 + 4 * c4 + k] : 0.0;
+            }
+        }
+    };
+    // sums over bands j in [j0, j1) of sweep `ep` into spart; returns false if a wait gave up
+    int par = 0;
+    auto sum_bands = [&](int j0, int j1, unsigned ep, int crit) -> bool {
+        double acc4[4] = {0.0, 0.0, 0.0, 0.0};
+        bool ok = true;
+        if (j0 < j1) fetch(j0);
+        for (int j = j0; j < j1; j++) {
+            double *buf = sx + par * NB;
+            const int dist = crit > j ? crit - j : j - crit;
+            ok = wait_chunk<double>(ll, j, ep, buf, poll_backoff(dist), sok + par, flags);
+            par ^= 1;
+            if (!ok) break;
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const double xe = buf[4 * part + e];
+#pragma unroll
+                for (int k = 0; k < 4; k++) acc4[k] = fma(ap[4 * e + k], xe, acc4[k]);
+            }
+            if (j + 1 < j1) fetch(j + 1);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) spart[part][4 * c4 + k] = acc4[k];
+        __syncthreads();
+        return ok;
+    };
+    bool ok = true;
+    for (int s = 0; s < S && ok; s++) {
+        const unsigned ep = epoch0 + (unsigned)s;
+        // blocks 0 .. blk-2 of this sweep
+        ok = sum_bands(0, blk > 1 ? blk - 1 : 0, ep, blk - 1);
+        if (t < NB) {
+            double sum = 0.0;
+#pragma unroll
+            for (int p = 0; p < 16; p++) sum += spart[p][t];
+            srhs[t] = t < kb ? (skip ? sxo[t] : snext[t] - sum) : 0.0;
+        }
+        __syncthreads();
+        double y = 0.0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) y = fma(sI[r][4 * k + q], srhs[4 * k + q], y);
+        y += __shfl_xor_sync(0xffffffffu, y, 1);
+        y += __shfl_xor_sync(0xffffffffu, y, 2);
+        double xr = y;
+        if (has_pred && ok) {
+            double *buf = sx + par * NB;
+            ok = wait_chunk<double>(ll, blk - 1, ep, buf, 0, sok + par, flags);
+            par ^= 1;
+            if (ok) {
+                double v = 0.0;
+#pragma unroll
+                for (int k = 0; k < 16; k++) v = fma(sC[r][4 * k + q], buf[4 * k + q], v);
+                v += __shfl_xor_sync(0xffffffffu, v, 1);
+                v += __shfl_xor_sync(0xffffffffu, v, 2);
+                xr = y - v;
+            }
+        }
+        if (q == 0) {
+            ll_put<double>(ll, blk, r, r < kb ? xr : 0.0, ep);
+            if (r < kb) {
+                x[r0 + r] = xr;
+                sxo[r] = xr;
+            }
+        }
+        if (s + 1 < S && ok) {
+            // the next sweep's x_old half: this block's strictly upper part
+            // against x_i, then blocks blk+1 .. nblk-1 of this sweep
+            __syncthreads();  // sxo holds x_i
+            double v = 0.0;
+#pragma unroll
+            for (int k = 0; k < 16; k++) v = fma(du[k], sxo[4 * k + q], v);
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            if (q == 0) sdu[r] = v;
+            ok = sum_bands(blk + 1, nblk, ep, blk);
+            if (t < NB) {
+                double sum = 0.0;
+#pragma unroll
+                for (int p = 0; p < 16; p++) sum += spart[p][t];
+                snext[t] = sb[t] - sdu[t] - sum;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // L2 = sqrt(sum (b - A x)^2)/neq  (src/FESolver.cpp:580-590), partial sums into sums[0]
 __global__ void k_gs_resid(int neq, long long ld, const double *__restrict__ A, const double *__restrict__ b,
                            const double *__restrict__ x, double *sums) {
@@ -400,24 +557,44 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st) {
     k_trsv_couplings<double><<<nblk, 256, 2 * NB * (NB + 1) * sizeof(double), ctx->stream>>>(
         n, ld, ctx->J, sp->Linv64, sp->Mc64, nullptr, 1, 1),
         ++ctx->launches;
-    const size_t smem = gs_smem();
+    const size_t smem = gs_smem(), fsmem = gs_sweeps_smem();
     cudaFuncSetAttribute(k_gs_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_gs_sweeps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem);
     const int grid = wavefront_grid(ctx, (const void *)k_gs_sweep, nblk, smem);
-    double *xa = ctx->y, *xb = sp->r;  // sweeps alternate the two
+    // every block's CTA resident: the sweeps run fused, 25 a launch
+    const bool fused = wavefront_grid(ctx, (const void *)k_gs_sweeps, nblk, fsmem) == nblk;
+    double *xa = ctx->y, *xb = sp->r;  // per-sweep launches alternate the two
     double *rup = sp->dvec64;          // b - U x_old (the FP64 factor's D is not in use here)
     double L2 = 0;
-    int it;
+    int it = 0, done = 0;
     bool converged = false;
-    for (it = 0; it < ctx->gs_max_sweeps; it++) {
+    // the reference checks the residual after sweeps 1, 26, 51, ... (it % 25 == 0)
+    while (done < ctx->gs_max_sweeps) {
+        const int S = done == 0 ? 1 : std::min(25, ctx->gs_max_sweeps - done);
         const int mk = kt_begin(ctx, MP_KT_TRSV, 0);
-        k_gs_upper<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, xa, rup), ++ctx->launches;
-        const unsigned epoch = next_wavefront_epoch(ctx, sp->ll, sp->ll_words);
-        MP_CUDA(ctx, launch_wavefront(k_gs_sweep, grid, smem, ctx->stream, n, ld, (const double *)ctx->J,
-                                      (const double *)rup, (const double *)sp->Linv64, (const double *)sp->Mc64,
-                                      (const double *)xa, xb, sp->ll, epoch, flags));
-        ++ctx->launches;
+        if (fused) {
+            k_gs_upper<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, xa, rup), ++ctx->launches;
+            unsigned ep0 = next_wavefront_epoch(ctx, sp->ll, sp->ll_words);
+            ctx->solve_epoch += S - 1;  // the launch uses epochs ep0 .. ep0 + S - 1
+            MP_CUDA(ctx, launch_wavefront(k_gs_sweeps, nblk, fsmem, ctx->stream, n, ld, (const double *)ctx->J,
+                                          (const double *)ctx->G, (const double *)rup, (const double *)sp->Linv64,
+                                          (const double *)sp->Mc64, xa, sp->ll, ep0, S, flags));
+            ++ctx->launches;
+        } else {
+            for (int k = 0; k < S; k++) {
+                k_gs_upper<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, xa, rup), ++ctx->launches;
+                const unsigned epoch = next_wavefront_epoch(ctx, sp->ll, sp->ll_words);
+                MP_CUDA(ctx, launch_wavefront(k_gs_sweep, grid, smem, ctx->stream, n, ld, (const double *)ctx->J,
+                                              (const double *)rup, (const double *)sp->Linv64,
+                                              (const double *)sp->Mc64, (const double *)xa, xb, sp->ll, epoch,
+                                              flags));
+                ++ctx->launches;
+                std::swap(xa, xb);
+            }
+        }
         kt_end(ctx, mk);
-        std::swap(xa, xb);
+        done += S;
+        it = done - 1;
         if (it % 25 == 0) {
             MP_CUDA(ctx, cudaMemsetAsync(ctx->scal + 3, 0, sizeof(double), ctx->stream));
             k_gs_resid<<<(unsigned)bl, th, 0, ctx->stream>>>(n, ld, ctx->J, ctx->G, xa, ctx->scal + 3), ++ctx->launches;
@@ -431,6 +608,7 @@ int fe_solve_gs(mp_ctx *ctx, mp_newton_stats *st) {
             }
         }
     }
+    if (!converged) it = ctx->gs_max_sweeps;
     if (xa != ctx->y)
         MP_CUDA(ctx, cudaMemcpyAsync(ctx->y, xa, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
     MP_CUDA(ctx, cudaGetLastError());

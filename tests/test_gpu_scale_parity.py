@@ -15,6 +15,9 @@ compiled code (oracle/_ref):
   bit-identical, density within 1e-12;
 * the 8^3 box at its configuration (spwt 200, dt 1e-7) for 200 steps from an
   empty domain, open loop, checked every 10 steps;
+* the Gauss-Seidel solve (solveLinear, src/FESolver.cpp:561-601) on the 12^3
+  box (30 row blocks: the fused multi-sweep kernel's wavefront and the
+  transposed row-band reads), against the reference's: y within 1e-7;
 * the NonLinear method (solveNonLinear, src/FESolver.cpp:324-364) per step on
   states captured from the reference's own run: where the reference converges,
   the same Newton iteration count and d within the Gauss-Seidel tolerance;
@@ -78,6 +81,30 @@ def test_ldlt_past_one_superpanel_vs_dsysv(tmp_path, n):
             assert rel_err(uh, uh_ref) < 1e-9
         else:
             assert np.abs(uh - uh_ref).max() < 1e-8
+
+
+def test_gauss_seidel_many_blocks_vs_reference(tmp_path):
+    kd, path = make_deck(tmp_path, 12, dt=5e-8)
+    dk = mp.Deck.load(path)
+    s = ref_sim(path, kd, spwt=5.0)
+    rng = np.random.default_rng(7)
+    den = dk.params.plasma_den * (1.0 + 0.1 * rng.standard_normal(dk.mesh.n_nodes))
+    d0 = rng.normal(0.0, 0.05, s.neq)
+    zero = np.zeros(s.neq)
+    s.set("d", d0)
+    s.set("F1", zero)
+    s.build_f1(den)
+    G = s.residual()
+    s.build_j(1)
+    y_ref = s.solve_gs(G)
+    ctx = gpu_context(dk)
+    ctx.fe_set("d", d0)
+    ctx.fe_set("F1", zero)
+    ctx.build_f1(den)
+    ctx.build_j(1)
+    st = ctx.solve_linear(mp.GAUSS_SEIDEL, mp.FP64, b=G)
+    assert st.linear_failures == 0
+    assert rel_err(ctx.fe_get("y"), y_ref) < 1e-7
 
 
 def test_push_kuhn20_2M_open_loop_vs_reference(tmp_path):
