@@ -37,6 +37,16 @@ __device__ __forceinline__ bool bad_pivot(T d) {
     return !(fabs((double)d) > 0.0) || !isfinite((double)d);
 }
 
+// The factorization's 64-wide chain (diagonal factor, panel, in-panel column
+// update) goes out as programmatic dependent launches: a kernel lets the next
+// one be scheduled as soon as all of its own CTAs are running, and waits for
+// the previous kernel's completion and memory before it touches any data, so
+// the next kernel's CTAs are resident when the previous one ends.
+__device__ __forceinline__ void chain_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // 4 consecutive values (16-byte aligned for float, 32 for double) as vector loads
 template <typename T>
 __device__ __forceinline__ void load4p(const T *p, T *v) {
@@ -279,6 +289,7 @@ __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, in
 template <typename T>
 __global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
                                                    T *b, unsigned long long *flags) {
+    chain_enter();
     diag_block<T>(n, ld, A, k0, kb, dvec, Linv, b, flags);
 }
 
@@ -305,6 +316,7 @@ __device__ __forceinline__ void fused_next_diag(int n, long long ld, T *A, const
 template <typename T>
 __global__ void __launch_bounds__(256) k_ldlt_panel(int n, long long ld, T *A, int k0, int kb, const T *dvec,
                                                     const T *Linv, T *W, int ldw, T *b) {
+    chain_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T(*sA)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
     T(*sI)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw + sizeof(T) * 64 * (NB + 1));
@@ -381,6 +393,7 @@ __global__ void __launch_bounds__(256) k_ldlt_panel(int n, long long ld, T *A, i
 template <typename T>
 __global__ void __launch_bounds__(256) k_ldlt_update_cols(int n, long long ld, T *A, int k0, int kb, const T *W,
                                                           int ldw, int k1, int jend, NextDiag nd) {
+    chain_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *sLt = reinterpret_cast<T *>(smem_raw);
     T *sWt = sLt + NB * 68;
@@ -1234,6 +1247,7 @@ template <int TERMS>
 __global__ void __launch_bounds__(256) k_ldlt_panel_tc(int n, long long ld, float *A, int k0, int kb,
                                                        const float *dvec, const float *Linv, float *W, int ldw,
                                                        float *b) {
+    chain_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float(*sA)[MS] = reinterpret_cast<float(*)[MS]>(smem_raw);
     float(*sI)[MS] = sA + NB;
@@ -1299,6 +1313,7 @@ template <int TERMS>
 __global__ void __launch_bounds__(256) k_ldlt_update_cols_tc(int n, long long ld, float *A, int k0, int kb,
                                                              const float *W, int ldw, int k1, int jend,
                                                              NextDiag nd) {
+    chain_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float(*sL)[MS] = reinterpret_cast<float(*)[MS]>(smem_raw);
     float(*sW)[MS] = sL + NB;
@@ -1380,6 +1395,22 @@ constexpr int PANEL_W = 256, SUPER_W = 4 * PANEL_W;
 // publish, so every CTA must be resident at once: they go out as cooperative
 // launches, which the runtime schedules only as a whole grid (a second
 // context's kernels on the same GPU cannot hold part of it back).
+// A chain kernel (see chain_enter) as a programmatic dependent launch.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_chain(void (*kernel)(KArgs...), dim3 grid, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 template <typename... Args>
 static cudaError_t launch_wavefront(void (*kernel)(Args...), int grid, size_t smem, cudaStream_t st,
                                     Args... args) {
@@ -1454,12 +1485,13 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     unsigned long long *flags = ctx->counters + C_FLAGS;
     // the diagonal factor of block k0 (unless the previous block's in-panel
     // column update ran it), then the panel below it
-    auto diag_and_panel = [&](int k0, int kb, T *W, int ldw, bool diag_done) {
+    auto diag_and_panel = [&](int k0, int kb, T *W, int ldw, bool diag_done) -> int {
         T *Li = w.Linv + (size_t)(k0 / NB) * NB * NB;
         int mk;
         if (!diag_done) {
             mk = kt_begin(ctx, MP_KT_DIAG, 0);
-            k_ldlt_diag<T><<<1, 256, 0, st>>>(n, ld, A, k0, kb, w.dvec, Li, b, flags), ++ctx->launches;
+            MP_CUDA(ctx, launch_chain(k_ldlt_diag<T>, dim3(1), 0, st, n, ld, A, k0, kb, w.dvec, Li, b, flags));
+            ++ctx->launches;
             kt_end(ctx, mk);
         }
         int k1 = k0 + kb;
@@ -1467,16 +1499,16 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             mk = kt_begin(ctx, MP_KT_PANEL, 0);
             const unsigned gp = (n - k1 + 63) / 64;
             if constexpr (std::is_same<T, float>::value) {
-                if (tc_terms == 3)
-                    k_ldlt_panel_tc<3><<<gp, 256, panel_tc_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b);
-                else
-                    k_ldlt_panel_tc<1><<<gp, 256, panel_tc_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b);
+                MP_CUDA(ctx, launch_chain(tc_terms == 3 ? k_ldlt_panel_tc<3> : k_ldlt_panel_tc<1>, dim3(gp),
+                                          panel_tc_smem, st, n, ld, A, k0, kb, w.dvec, Li, W, ldw, b));
             } else {
-                k_ldlt_panel<T><<<gp, 256, panel_smem, st>>>(n, ld, A, k0, kb, w.dvec, Li, W, ldw, b);
+                MP_CUDA(ctx, launch_chain(k_ldlt_panel<T>, dim3(gp), panel_smem, st, n, ld, A, k0, kb, w.dvec, Li,
+                                          W, ldw, b));
             }
             ++ctx->launches;
             kt_end(ctx, mk);
         }
+        return MP_OK;
     };
     // algorithmic flops of an update of rows [R0, n) x columns [R0, C1), lower part, depth K
     auto update_flops = [&](int R0, int C1, int K) {
@@ -1554,7 +1586,8 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                 for (int k0 = P0; k0 < P1; k0 += NB) {
                     const int kb = P1 - k0 < NB ? P1 - k0 : NB;
                     const int k1 = k0 + kb;
-                    diag_and_panel(k0, kb, w.W + (k0 - S0), SUPER_W, diag_done);
+                    int rc = diag_and_panel(k0, kb, w.W + (k0 - S0), SUPER_W, diag_done);
+                    if (rc) return rc;
                     diag_done = false;
                     if (k1 < n && k1 < P1) {
                         // the update's CTA on the next diagonal tile factors that block
@@ -1564,15 +1597,12 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                         dim3 g((P1 - k1 + 63) / 64, (n - k1 + 63) / 64);
                         const int mk = kt_begin(ctx, MP_KT_PANEL, 0);
                         if constexpr (std::is_same<T, float>::value) {
-                            if (tc_terms == 3)
-                                k_ldlt_update_cols_tc<3><<<g, 256, cols_tc_smem, st>>>(
-                                    n, ld, A, k0, kb, w.W + (k0 - S0), SUPER_W, k1, P1, nd);
-                            else
-                                k_ldlt_update_cols_tc<1><<<g, 256, cols_tc_smem, st>>>(
-                                    n, ld, A, k0, kb, w.W + (k0 - S0), SUPER_W, k1, P1, nd);
+                            MP_CUDA(ctx, launch_chain(tc_terms == 3 ? k_ldlt_update_cols_tc<3> : k_ldlt_update_cols_tc<1>,
+                                                      g, cols_tc_smem, st, n, ld, A, k0, kb, w.W + (k0 - S0),
+                                                      SUPER_W, k1, P1, nd));
                         } else {
-                            k_ldlt_update_cols<T><<<g, 256, upd_smem, st>>>(n, ld, A, k0, kb, w.W + (k0 - S0),
-                                                                            SUPER_W, k1, P1, nd);
+                            MP_CUDA(ctx, launch_chain(k_ldlt_update_cols<T>, g, upd_smem, st, n, ld, A, k0, kb,
+                                                      w.W + (k0 - S0), SUPER_W, k1, P1, nd));
                         }
                         ++ctx->launches;
                         kt_end(ctx, mk);
