@@ -69,6 +69,9 @@ LEGS = ("kuhn20", "nonlinear", "adjoint", "sparse64", "vtk")
 # 160.5 MB and 65.1 MB for 1.99M particles, in and out)
 TRAFFIC_PER_UNIT = {("tc3", "update"): 444.3e6 / 55.4e9, ("tc1", "update"): 232.4e6 / 55.4e9,
                     ("fp64", "push"): 160.5e6 / (2 * 1.99e6), ("mixed", "push"): 65.1e6 / (2 * 1.99e6)}
+# FP64 tensor-pipe rate implied by one ncu capture of k_update_f64_mma (26.4
+# TFLOP/s at 76.6 % DMMA-pipe activity); this pool's peaks file has no FP64 figure
+FP64_TENSOR_TFLOPS = 26.4 / 0.766
 KT_NAMES = {mp.KT_PUSH: "push", mp.KT_UPDATE: "trailing_update", mp.KT_DIAG: "diagonal_factor",
             mp.KT_PANEL: "panel", mp.KT_TRSV: "triangular_solve"}
 KT_KERNEL = {mp.KT_PUSH: {mp.FP64: "k_push_fp64", mp.MIXED: "k_push_mixed"},
@@ -200,6 +203,14 @@ def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True, neq=0):
         bpp = 52.0 if form == mp.FP64 else 28.0
         out["traffic"] = TRAFFIC_PER_UNIT[key] * v["work"] / bpp / max(v["launches"], 1)
         out["traffic_source"] = "ncu DRAM bytes per particle (20^3 box, 2M ions) x this launch's particles"
+    elif top == mp.KT_UPDATE and form == mp.FP64:
+        ach = v["work"] / (v["ms"] * 1e-3) / 1e12
+        out.update(bound="tensor (FP64)", achieved=ach, peak=FP64_TENSOR_TFLOPS, unit="TFLOP/s",
+                   frac=ach / FP64_TENSOR_TFLOPS,
+                   peak_kind="FP64 tensor pipe: 26.4 TFLOP/s at 76.6 % pipe activity in one ncu capture "
+                             "(profiles/k_update_f64_kuhn20_newton.md); no measured FP64 peak on this pool",
+                   algorithmic="2 flops per multiply-add of the trailing update's lower triangle",
+                   frac_of_bf16_sustained=ach / pk["bf16_tflops_sustained"])
     elif top == mp.KT_UPDATE:
         ach = v["work"] / (v["ms"] * 1e-3) / 1e12
         peak = pk["bf16_tflops_sustained"] if sustained else pk["bf16_tflops"]

@@ -4,11 +4,14 @@
 //
 // Blocked right-looking LDL^T without pivoting on the lower triangle (row-major
 // storage, leading dimension padded to 32).  Per block column k of width NB:
-//   diag   : L_kk D_k L_kk^T = A_kk in shared memory (one CTA); z_k = L_kk^-1 b_k
+//   diag   : L_kk D_k L_kk^T = A_kk in registers (one CTA); z_k = L_kk^-1 b_k
 //   panel  : W_ik = A_ik L_kk^-T,  L_ik = W_ik D_k^-1, b_i -= L_ik z_k  (rows below)
 //   update : A_ij -= L_ik W_jk^T on the lower tiles of the trailing matrix,
 //            two-level: within each 256-wide outer panel only the panel's own
-//            columns, and the rest of the trailing matrix once per outer panel
+//            columns (mma.sync tiles, the next diagonal factor riding along),
+//            the rest of its 1,024-wide super-panel once per panel, and the
+//            trailing matrix once per super-panel (tcgen05 for the FP32 factor,
+//            FP64 mma.sync for the FP64 one)
 // The forward substitution rides on the panel pass; the backward substitution
 // L^T y = D^-1 z runs afterwards.
 //
@@ -308,140 +311,6 @@ __device__ __forceinline__ void fused_next_diag(int n, long long ld, T *A, const
         diag_block<T>(n, ld, A, nd.k0, nd.kb, static_cast<T *>(nd.dvec), static_cast<T *>(nd.Linv),
                       static_cast<T *>(nd.b), nd.flags);
     }
-}
-
-// Panel: rows [r0, r0+64) below the diagonal block.  W = A_ik L_kk^-T (a small
-// product with Linv), L_ik = W D^-1, and b_i -= L_ik z_k.  Dynamic smem: the
-// rows' panel [64][NB+1] and Linv [NB][NB+1].
-template <typename T>
-__global__ void __launch_bounds__(256) k_ldlt_panel(int n, long long ld, T *A, int k0, int kb, const T *dvec,
-                                                    const T *Linv, T *W, int ldw, T *b) {
-    chain_enter();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T(*sA)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
-    T(*sI)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw + sizeof(T) * 64 * (NB + 1));
-    T *sd = reinterpret_cast<T *>(smem_raw + sizeof(T) * 2 * 64 * (NB + 1));
-    T *sz = sd + NB;
-    const int r0 = k0 + kb + blockIdx.x * 64;
-    {
-        T va[16], vi[16];
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            int idx = q * 256 + threadIdx.x;
-            int r = idx >> 6, c = idx & 63;
-            int row = r0 + r;
-            va[q] = (row < n && c < kb) ? A[(long long)row * ld + k0 + c] : T(0);
-            vi[q] = (r < kb && c < kb) ? __ldg(&Linv[r * NB + c]) : T(0);
-        }
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            int idx = q * 256 + threadIdx.x;
-            sA[idx >> 6][idx & 63] = va[q];
-            sI[idx >> 6][idx & 63] = vi[q];
-        }
-    }
-    if (threadIdx.x < kb) {
-        sd[threadIdx.x] = dvec[k0 + threadIdx.x];
-        if (b) sz[threadIdx.x] = b[k0 + threadIdx.x];
-    }
-    __syncthreads();
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 4 rows x 4 cols each
-    T acc[4][4] = {};
-    for (int pp = 0; pp < kb; pp++) {
-        T a[4], w[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) a[u] = sA[ty * 4 + u][pp];
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-            int c = tx * 4 + v;
-            w[v] = (c < kb && pp <= c) ? sI[c][pp] : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-#pragma unroll
-            for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], w[v], acc[u][v]);
-    }
-    T bsum[4] = {0, 0, 0, 0};
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-        const int row = r0 + ty * 4 + u;
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-            const int c = tx * 4 + v;
-            if (row < n && c < kb) {
-                const T wv = acc[u][v];
-                const T lv = wv / sd[c];
-                W[(long long)row * ldw + c] = wv;
-                A[(long long)row * ld + k0 + c] = lv;
-                if (b) bsum[u] += lv * sz[c];
-            }
-        }
-    }
-    if (b) {
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            T v = bsum[u];
-            for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            const int row = r0 + ty * 4 + u;
-            if (tx == 0 && row < n) b[row] -= v;
-        }
-    }
-}
-
-// Update restricted to the columns [k1, jend) of the current outer panel:
-// A_ij -= L_i W_j^T for rows i in [k1, n), 64x64 tiles, grid (col tile, row tile).
-template <typename T>
-__global__ void __launch_bounds__(256) k_ldlt_update_cols(int n, long long ld, T *A, int k0, int kb, const T *W,
-                                                          int ldw, int k1, int jend, NextDiag nd) {
-    chain_enter();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *sLt = reinterpret_cast<T *>(smem_raw);
-    T *sWt = sLt + NB * 68;
-    const int i0 = k1 + blockIdx.y * 64, j0 = k1 + blockIdx.x * 64;
-    if (j0 > i0 + 63 || j0 >= jend) return;  // tile entirely above the diagonal or outside the panel
-    {
-        T la[16], wa[16];
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            int idx = q * 256 + threadIdx.x;
-            int r = idx / NB, p = idx % NB;
-            int ri = i0 + r, rj = j0 + r;
-            la[q] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : T(0);
-            wa[q] = (p < kb && rj < jend) ? __ldg(&W[(long long)rj * ldw + p]) : T(0);
-        }
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            int idx = q * 256 + threadIdx.x;
-            int r = idx / NB, p = idx % NB;
-            sLt[p * 68 + r] = la[q];
-            sWt[p * 68 + r] = wa[q];
-        }
-    }
-    __syncthreads();
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    T acc[4][4] = {};
-    for (int p = 0; p < kb; p++) {
-        T a[4], w[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) a[u] = sLt[p * 68 + ty * 4 + u];
-#pragma unroll
-        for (int v = 0; v < 4; v++) w[v] = sWt[p * 68 + tx * 4 + v];
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-#pragma unroll
-            for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], w[v], acc[u][v]);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-        int i = i0 + ty * 4 + u;
-        if (i >= n) continue;
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-            int j = j0 + tx * 4 + v;
-            if (j < jend && j <= i) A[(long long)i * ld + j] -= acc[u][v];
-        }
-    }
-    fused_next_diag<T>(n, ld, A, nd);
 }
 
 // FP64 form: A[i][j] -= sum_{k<K} L[i][k] W[j][k] for rows/cols from R0, with
@@ -1240,8 +1109,8 @@ __device__ __forceinline__ void warp_mma_64(const float (*sa)[MS], const float (
     }
 }
 
-// Panel of the FP32 factor (rows [r0, r0+64) below the diagonal block), as
-// k_ldlt_panel: W = A_ik Linv^T, L_ik = W D^-1, b_i -= L_ik z_k.  Warp w takes
+// Panel of the FP32 factor (rows [r0, r0+64) below the diagonal block):
+// W = A_ik Linv^T, L_ik = W D^-1, b_i -= L_ik z_k.  Warp w takes
 // rows 16(w/2) .. +15 and columns 32(w%2) .. +31 of the 64 x 64 product.
 template <int TERMS>
 __global__ void __launch_bounds__(256) k_ldlt_panel_tc(int n, long long ld, float *A, int k0, int kb,
@@ -1306,7 +1175,120 @@ __global__ void __launch_bounds__(256) k_ldlt_panel_tc(int n, long long ld, floa
     }
 }
 
-// In-panel column update of the FP32 factor, as k_ldlt_update_cols:
+// Panel of the FP64 factor on the FP64 tensor cores (mma.sync m8n8k4, FP64 in
+// and out): W = A_ik Linv^T, L_ik = W D^-1, b_i -= L_ik z_k.
+// Warp w takes rows 16(w/2) .. +15 and columns 32(w%2) .. +31 of the 64 x 64
+// product: 2 x 4 MMA tiles of 8 x 8.  Shared operands at a pitch of MS = 68
+// doubles (68 = 4 mod 16), so a half-warp's fragment reads hit 16 distinct
+// 8-byte banks.
+__global__ void __launch_bounds__(256) k_ldlt_panel_dmma(int n, long long ld, double *A, int k0, int kb,
+                                                         const double *dvec, const double *Linv, double *W, int ldw,
+                                                         double *b) {
+    chain_enter();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double(*sA)[MS] = reinterpret_cast<double(*)[MS]>(smem_raw);
+    double(*sI)[MS] = sA + NB;
+    double *sd = reinterpret_cast<double *>(sI + NB);
+    double *sz = sd + NB;
+    double(*sbs)[NB] = reinterpret_cast<double(*)[NB]>(sz + NB);  // [2][64] the two column halves' b sums
+    const int r0 = k0 + kb + blockIdx.x * 64, t = threadIdx.x;
+    for (int q = 0; q < 16; q++) {
+        const int idx = q * 256 + t, r = idx >> 6, c = idx & 63, row = r0 + r;
+        sA[r][c] = (row < n && c < kb) ? A[(long long)row * ld + k0 + c] : 0.0;
+        sI[r][c] = (r < kb && c < kb) ? __ldg(&Linv[r * NB + c]) : 0.0;
+    }
+    if (t < NB) {
+        sd[t] = t < kb ? dvec[k0 + t] : 1.0;
+        sz[t] = (b && t < kb) ? b[k0 + t] : 0.0;
+    }
+    __syncthreads();
+    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
+    const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
+    double acc[2][4][2] = {};
+#pragma unroll 4
+    for (int kk = 0; kk < NB; kk += 4) {
+        const double a0 = sA[m0 + g][kk + tq], a1 = sA[m0 + 8 + g][kk + tq];
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            const double bv = sI[n0 + 8 * nt + g][kk + tq];
+            dmma_8x8x4(acc[0][nt][0], acc[0][nt][1], a0, bv);
+            dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a1, bv);
+        }
+    }
+    double bsum[2] = {0.0, 0.0};  // rows m0 + g and m0 + 8 + g
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int rr = m0 + 8 * mi + g, c = n0 + 8 * nt + 2 * tq + e, row = r0 + rr;
+                if (row < n && c < kb) {
+                    const double wv = acc[mi][nt][e];
+                    const double lv = wv / sd[c];
+                    W[(long long)row * ldw + c] = wv;
+                    A[(long long)row * ld + k0 + c] = lv;
+                    bsum[mi] += lv * sz[c];
+                }
+            }
+    if (b) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            double v = bsum[h];
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            if (tq == 0) sbs[w & 1][m0 + 8 * h + g] = v;
+        }
+        __syncthreads();
+        if (t < NB && r0 + t < n) b[r0 + t] -= sbs[0][t] + sbs[1][t];
+    }
+}
+
+// In-panel column update of the FP64 factor on the FP64 tensor cores
+// (mma.sync m8n8k4): A_ij -= L_ik W_jk^T for the 64 x 64
+// tile (blockIdx.y, blockIdx.x) of rows [k1, n) x columns [k1, jend); the CTA
+// on the next diagonal tile then factors that block.
+__global__ void __launch_bounds__(256) k_ldlt_update_cols_dmma(int n, long long ld, double *A, int k0, int kb,
+                                                               const double *W, int ldw, int k1, int jend,
+                                                               NextDiag nd) {
+    chain_enter();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double(*sL)[MS] = reinterpret_cast<double(*)[MS]>(smem_raw);
+    double(*sW)[MS] = sL + NB;
+    const int i0 = k1 + blockIdx.y * 64, j0 = k1 + blockIdx.x * 64, t = threadIdx.x;
+    if (j0 > i0 + 63 || j0 >= jend) return;  // tile entirely above the diagonal or outside the panel
+    for (int q = 0; q < 16; q++) {
+        const int idx = q * 256 + t, r = idx >> 6, p = idx & 63, ri = i0 + r, rj = j0 + r;
+        sL[r][p] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : 0.0;
+        sW[r][p] = (p < kb && rj < jend) ? __ldg(&W[(long long)rj * ldw + p]) : 0.0;
+    }
+    __syncthreads();
+    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
+    const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
+    double acc[2][4][2] = {};
+#pragma unroll 4
+    for (int kk = 0; kk < NB; kk += 4) {
+        const double a0 = sL[m0 + g][kk + tq], a1 = sL[m0 + 8 + g][kk + tq];
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            const double bv = sW[n0 + 8 * nt + g][kk + tq];
+            dmma_8x8x4(acc[0][nt][0], acc[0][nt][1], a0, bv);
+            dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a1, bv);
+        }
+    }
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int i = i0 + m0 + 8 * mi + g, j = j0 + n0 + 8 * nt + 2 * tq + e;
+                if (i < n && j < jend && j <= i) A[(long long)i * ld + j] -= acc[mi][nt][e];
+            }
+    fused_next_diag<double>(n, ld, A, nd);
+}
+
+// In-panel column update of the FP32 factor:
 // A_ij -= L_ik W_jk^T for the 64 x 64 tile (blockIdx.y, blockIdx.x) of rows
 // [k1, n) x columns [k1, jend).
 template <int TERMS>
@@ -1458,19 +1440,15 @@ template <typename T>
 int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> w, bool factor,
                       int tc_terms = 0) {
     cudaStream_t st = ctx->stream;
-    const size_t panel_smem = sizeof(T) * (64 * (NB + 1) + NB * (NB + 1) + 2 * NB);
-    const size_t upd_smem = sizeof(T) * 2 * NB * 68;
     const size_t panel_tc_smem = sizeof(float) * (2 * NB * MS + 4 * NB);
+    const size_t panel_dmma_smem = sizeof(double) * (2 * NB * MS + 4 * NB);
+    const size_t cols_dmma_smem = sizeof(double) * 2 * NB * MS;
     const size_t cols_tc_smem = sizeof(float) * 2 * NB * MS;
     const size_t f64_smem = sizeof(double) * 4 * WKC * WPITCH;
     if (!ctx->ldlt_attr) {  // per context: the attributes belong to the context's device
         const int big = 96 * 1024;
-        cudaFuncSetAttribute(k_ldlt_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(k_ldlt_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_update_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_update_f64_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(k_ldlt_update_cols<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(k_ldlt_update_cols<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(tc::k_update_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)tc::smem_bytes(false));
         cudaFuncSetAttribute(tc::k_update_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1478,6 +1456,7 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         wavefront_attrs<float>();
         wavefront_attrs<double>();
         for (const void *f : {(const void *)k_ldlt_panel_tc<1>, (const void *)k_ldlt_panel_tc<3>,
+                              (const void *)k_ldlt_panel_dmma, (const void *)k_ldlt_update_cols_dmma,
                               (const void *)k_ldlt_update_cols_tc<1>, (const void *)k_ldlt_update_cols_tc<3>})
             cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         ctx->ldlt_attr = true;
@@ -1502,8 +1481,8 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                 MP_CUDA(ctx, launch_chain(tc_terms == 3 ? k_ldlt_panel_tc<3> : k_ldlt_panel_tc<1>, dim3(gp),
                                           panel_tc_smem, st, n, ld, A, k0, kb, w.dvec, Li, W, ldw, b));
             } else {
-                MP_CUDA(ctx, launch_chain(k_ldlt_panel<T>, dim3(gp), panel_smem, st, n, ld, A, k0, kb, w.dvec, Li,
-                                          W, ldw, b));
+                MP_CUDA(ctx, launch_chain(k_ldlt_panel_dmma, dim3(gp), panel_dmma_smem, st, n, ld, A, k0, kb, w.dvec,
+                                          Li, W, ldw, b));
             }
             ++ctx->launches;
             kt_end(ctx, mk);
@@ -1601,8 +1580,8 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                                                       g, cols_tc_smem, st, n, ld, A, k0, kb, w.W + (k0 - S0),
                                                       SUPER_W, k1, P1, nd));
                         } else {
-                            MP_CUDA(ctx, launch_chain(k_ldlt_update_cols<T>, g, upd_smem, st, n, ld, A, k0, kb,
-                                                      w.W + (k0 - S0), SUPER_W, k1, P1, nd));
+                            MP_CUDA(ctx, launch_chain(k_ldlt_update_cols_dmma, g, cols_dmma_smem, st, n, ld, A, k0,
+                                                      kb, w.W + (k0 - S0), SUPER_W, k1, P1, nd));
                         }
                         ++ctx->launches;
                         kt_end(ctx, mk);
@@ -1641,14 +1620,14 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             if (!factor) {
                 const int g = wavefront_grid(ctx, (const void *)k_trsv_band<float, 1>, nband, sm);
                 MP_CUDA(ctx, launch_wavefront(k_trsv_band<float, 1>, g, sm, st, n, ld, (const float *)A,
-                                              (const float *)w.Linv, (const float *)C1f, (const float *)C2f,
-                                              (const float *)w.dvec, b, w.ll, epoch, flags));
+                                                 (const float *)w.Linv, (const float *)C1f, (const float *)C2f,
+                                                 (const float *)w.dvec, b, w.ll, epoch, flags));
                 ++ctx->launches;
             }
             const int g = wavefront_grid(ctx, (const void *)k_trsv_band<float, -1>, nband, sm);
             MP_CUDA(ctx, launch_wavefront(k_trsv_band<float, -1>, g, sm, st, n, ld, (const float *)A,
-                                          (const float *)w.Linv, (const float *)C1b, (const float *)C2b,
-                                          (const float *)w.dvec, b, w.ll + llw, epoch, flags));
+                                             (const float *)w.Linv, (const float *)C1b, (const float *)C2b,
+                                             (const float *)w.dvec, b, w.ll + llw, epoch, flags));
             ++ctx->launches;
         }
     } else {
