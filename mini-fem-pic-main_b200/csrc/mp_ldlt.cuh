@@ -34,6 +34,7 @@
 namespace mp {
 
 constexpr int NB = 64;
+constexpr int MS = NB + 4;  // row pitch of shared 64-wide blocks: a warp's quad or fragment reads hit all banks
 
 template <typename T>
 __device__ __forceinline__ bool bad_pivot(T d) {
@@ -106,12 +107,13 @@ __device__ __forceinline__ void st4s(T *p, const T (&v)[4]) {
     }
 }
 
-// The block is read with coherent loads: the in-panel column update of the
-// previous block runs this on the CTA that has just updated the block
-// (k_ldlt_update_cols*, kbn > 0).  All 256 threads of the CTA call it.
+// The block is read with coherent loads, or from stile (shared memory, row
+// pitch MS) where the in-panel column update of the previous block, whose CTA
+// has just updated the block, hands it over (k_ldlt_update_cols_*, kbn > 0).
+// All 256 threads of the CTA call it.
 template <typename T>
 __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv, T *b,
-                                           unsigned long long *flags) {
+                                           unsigned long long *flags, const T *stile = nullptr) {
     __shared__ __align__(16) T scol[2][NB][4];  // the step's four columns, every row
     __shared__ __align__(16) T srow[2][4][NB];  // Linv's rows j0 .. j0+3, every column
     __shared__ __align__(16) T spiv[2][4][4];   // the factored pivot block: L_P below the diagonal, D_P on it
@@ -130,7 +132,7 @@ __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, in
         if (r < kb) {
 #pragma unroll
             for (int v = 0; v < 4; v++)
-                if (4 * tc + v < kb) v4[v] = __ldcg(row + v);
+                if (4 * tc + v < kb) v4[v] = stile ? stile[r * MS + 4 * tc + v] : __ldcg(row + v);
         }
 #pragma unroll
         for (int v = 0; v < 4; v++) {
@@ -305,11 +307,16 @@ struct NextDiag {
     unsigned long long *flags;
 };
 template <typename T>
-__device__ __forceinline__ void fused_next_diag(int n, long long ld, T *A, const NextDiag &nd) {
-    if (nd.kb > 0 && blockIdx.x == 0 && blockIdx.y == 0) {
-        __syncthreads();  // the tile's stores by every thread of this CTA come first
+__device__ __forceinline__ bool owns_next_diag(const NextDiag &nd) {
+    return nd.kb > 0 && blockIdx.x == 0 && blockIdx.y == 0;
+}
+// stile: the updated tile in shared memory (row pitch MS), lower part
+template <typename T>
+__device__ __forceinline__ void fused_next_diag(int n, long long ld, T *A, const NextDiag &nd, const T *stile) {
+    if (owns_next_diag<T>(nd)) {
+        __syncthreads();  // the tile is complete in shared memory
         diag_block<T>(n, ld, A, nd.k0, nd.kb, static_cast<T *>(nd.dvec), static_cast<T *>(nd.Linv),
-                      static_cast<T *>(nd.b), nd.flags);
+                      static_cast<T *>(nd.b), nd.flags, stile);
     }
 }
 
@@ -527,7 +534,6 @@ __global__ void __launch_bounds__(256, 1) k_update_f64_mma(int n, long long ld, 
 // up sets the error flag and the block publishes what it has, so no other
 // block waits on it for long.
 constexpr long long TRSV_SPIN_LIMIT = 1ll << 20;
-constexpr int MS = NB + 4;  // row pitch of the shared inverse and coupling blocks: quad reads hit 32 banks
 
 __device__ __forceinline__ void st_ll(unsigned long long *p, unsigned long long v) {
     asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
@@ -1276,16 +1282,24 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols_dmma(int n, long long 
             dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a1, bv);
         }
     }
+    // the CTA on the next diagonal tile keeps the updated tile in shared memory
+    // (over sL, once every warp is done with it) for the diagonal factor
+    const bool keep = owns_next_diag<double>(nd);
+    if (keep) __syncthreads();
 #pragma unroll
     for (int mi = 0; mi < 2; mi++)
 #pragma unroll
         for (int nt = 0; nt < 4; nt++)
 #pragma unroll
             for (int e = 0; e < 2; e++) {
-                const int i = i0 + m0 + 8 * mi + g, j = j0 + n0 + 8 * nt + 2 * tq + e;
-                if (i < n && j < jend && j <= i) A[(long long)i * ld + j] -= acc[mi][nt][e];
+                const int ii = m0 + 8 * mi + g, jj = n0 + 8 * nt + 2 * tq + e, i = i0 + ii, j = j0 + jj;
+                if (i < n && j < jend && j <= i) {
+                    const double v = A[(long long)i * ld + j] - acc[mi][nt][e];
+                    A[(long long)i * ld + j] = v;
+                    if (keep) sL[ii][jj] = v;
+                }
             }
-    fused_next_diag<double>(n, ld, A, nd);
+    fused_next_diag<double>(n, ld, A, nd, &sL[0][0]);
 }
 
 // In-panel column update of the FP32 factor:
@@ -1321,14 +1335,22 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols_tc(int n, long long ld
     const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
     float acc[4][4] = {};
     warp_mma_64<TERMS>(sL, sW, m0, n0, acc);
+    // the CTA on the next diagonal tile keeps the updated tile in shared memory
+    // (over sL, once every warp is done with it) for the diagonal factor
+    const bool keep = owns_next_diag<float>(nd);
+    if (keep) __syncthreads();
 #pragma unroll
     for (int nt = 0; nt < 4; nt++)
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-            const int i = i0 + m0 + g + (e >> 1) * 8, j = j0 + n0 + 8 * nt + 2 * tq + (e & 1);
-            if (i < n && j < jend && j <= i) A[(long long)i * ld + j] -= acc[nt][e];
+            const int ii = m0 + g + (e >> 1) * 8, jj = n0 + 8 * nt + 2 * tq + (e & 1), i = i0 + ii, j = j0 + jj;
+            if (i < n && j < jend && j <= i) {
+                const float v = A[(long long)i * ld + j] - acc[nt][e];
+                A[(long long)i * ld + j] = v;
+                if (keep) sL[ii][jj] = v;
+            }
         }
-    fused_next_diag<float>(n, ld, A, nd);
+    fused_next_diag<float>(n, ld, A, nd, &sL[0][0]);
 }
 
 template <typename T>
