@@ -327,7 +327,7 @@ int mp_destroy(mp_ctx *ctx) {
                    ctx->den, ctx->den_fixed, ctx->counters, ctx->scal, ctx->compact_off, ctx->sort_hist,
                    ctx->part_block[0], ctx->part_block[1], ctx->ID, ctx->LM, ctx->detJ, ctx->nx, ctx->g, ctx->uh,
                    ctx->d, ctx->F0, ctx->F1, ctx->G, ctx->y, ctx->fvec, ctx->FP, ctx->work, ctx->K, ctx->J,
-                   ctx->J32, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a, ctx->gs_minv, ctx->den_in, ctx->dstage};
+                   ctx->J32, ctx->K32, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a, ctx->gs_minv, ctx->den_in, ctx->dstage};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
@@ -647,10 +647,12 @@ int mp_fe_setup(mp_ctx *ctx, const mp_fe_desc *fe) {
         }
     // (re)allocate
     void *old[] = {ctx->ID, ctx->LM, ctx->detJ, ctx->nx, ctx->g, ctx->uh, ctx->d, ctx->F0, ctx->F1, ctx->G, ctx->y,
-                   ctx->fvec, ctx->FP, ctx->work, ctx->K, ctx->J, ctx->J32, ctx->eq_ptr, ctx->eq_tet, ctx->eq_a};
+                   ctx->fvec, ctx->FP, ctx->work, ctx->K, ctx->J, ctx->J32, ctx->K32, ctx->eq_ptr, ctx->eq_tet,
+                   ctx->eq_a};
     for (void *p : old)
         if (p) cudaFree(p);
-    ctx->J32 = nullptr;
+    ctx->J32 = ctx->K32 = nullptr;
+    ctx->k32_current = false;
     const long long ld = (neq + 31) & ~31ll;
     size_t vec = sizeof(double) * (size_t)(ld + 64);
     MP_CUDA(ctx, cudaMalloc(&ctx->ID, sizeof(int) * nn));

@@ -126,11 +126,64 @@ __global__ void k_copy_j32(int neq, long long ld, const double *__restrict__ K, 
     }
 }
 
+// K's lower triangle (in 4-wide groups, as k_copy_j32 writes J32) rounded to FP32
+__global__ void k_k32_from_k(int neq, long long ld, const double *__restrict__ K, float *K32) {
+    for (long long r = blockIdx.x; r < neq; r += gridDim.x) {
+        const double *kr = K + r * ld;
+        float *out = K32 + r * ld;
+        for (long long c = 4 * threadIdx.x; c <= r; c += 4 * blockDim.x) {
+            const double2 a = *reinterpret_cast<const double2 *>(kr + c);
+            const double2 b = *reinterpret_cast<const double2 *>(kr + c + 2);
+            *reinterpret_cast<float4 *>(out + c) = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+        }
+    }
+}
+
+// J32 = K - diag(FP) from the FP32 copy of K; the diagonal from the FP64 K and
+// FP, so J32 is the same as rounding the FP64 J (k_copy_j32)
+__global__ void k_copy_j32_from32(int neq, long long ld, const float *__restrict__ K32,
+                                  const double *__restrict__ K, const double *__restrict__ FP, float *J32) {
+    for (long long r = blockIdx.x; r < neq; r += gridDim.x) {
+        const float *kr = K32 + r * ld;
+        float *jr = J32 + r * ld;
+        for (long long c = 4 * threadIdx.x; c <= r; c += 4 * blockDim.x) {
+            float4 v = *reinterpret_cast<const float4 *>(kr + c);
+            if (r >= c && r < c + 4) {
+                const float dg = (float)__dsub_rn(K[r * ld + r], FP[r]);
+                if (r == c) v.x = dg;
+                else if (r == c + 1) v.y = dg;
+                else if (r == c + 2) v.z = dg;
+                else v.w = dg;
+            }
+            *reinterpret_cast<float4 *>(jr + c) = v;
+        }
+    }
+}
+
 int fe_j32_from_k(mp_ctx *ctx) {
     const long long ld = (ctx->neq + 31) & ~31ll;
     if (!ctx->J32) MP_CUDA(ctx, cudaMalloc(&ctx->J32, sizeof(float) * (size_t)ld * ctx->neq));
-    k_copy_j32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J32),
-        ++ctx->launches;
+    // K does not change between Newton steps: its FP32 copy is made once
+    if (!ctx->K32) {
+        if (cudaMalloc(&ctx->K32, sizeof(float) * (size_t)ld * ctx->neq) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->K32 = nullptr;  // no room: build J32 from the FP64 K each time
+        }
+        ctx->k32_current = false;
+    }
+    if (ctx->K32) {
+        if (!ctx->k32_current) {
+            k_k32_from_k<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->K32),
+                ++ctx->launches;
+            ctx->k32_current = true;
+        }
+        k_copy_j32_from32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K32, ctx->K, ctx->FP,
+                                                                       ctx->J32),
+            ++ctx->launches;
+    } else {
+        k_copy_j32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(ctx->neq, ld, ctx->K, ctx->FP, ctx->J32),
+            ++ctx->launches;
+    }
     MP_CUDA(ctx, cudaGetLastError());
     return MP_OK;
 }

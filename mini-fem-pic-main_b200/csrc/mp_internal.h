@@ -168,6 +168,8 @@ struct mp_ctx {
     double *fvec = nullptr, *FP = nullptr, *work = nullptr;  // [neq]
     double *K = nullptr, *J = nullptr;    // [neq][neq] row-major
     float *J32 = nullptr;                 // [neq][neq] mixed-form factor
+    float *K32 = nullptr;                 // [neq][neq] K's lower triangle in FP32 (the mixed form's J32 source)
+    bool k32_current = false;             // K32 holds the current K
     bool j32_current = false;             // J32 holds the lower triangle of the current J
     bool j_current = false;               // J holds the current J (not yet overwritten by its factor)
     double *scal = nullptr;               // device scalars for reductions

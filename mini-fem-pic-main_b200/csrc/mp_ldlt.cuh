@@ -610,6 +610,47 @@ __device__ __forceinline__ bool wait_chunk(const unsigned long long *ll, int c, 
     return *ok != 0;
 }
 
+// The chain's critical wait: every warp polls block c's words itself, so no
+// CTA barrier follows; this lane gets values lane (v0) and lane + 32 (v1).  A
+// wait that gives up raises the error flag and leaves zeros (the caller's
+// control flow does not depend on it, so every warp takes the same barriers).
+template <typename T>
+__device__ __forceinline__ void wait_warp(const unsigned long long *ll, int c, unsigned epoch, T &v0, T &v1,
+                                          unsigned long long *flags) {
+    const int lane = threadIdx.x & 31;
+    for (long long spins = 0; spins <= TRSV_SPIN_LIMIT; spins++) {
+        if constexpr (sizeof(T) == 4) {
+            const unsigned long long *p = ll + (size_t)c * NB;
+            const unsigned long long w0 = ld_ll(p + lane), w1 = ld_ll(p + 32 + lane);
+            const bool ok = (unsigned)(w0 >> 32) == epoch && (unsigned)(w1 >> 32) == epoch;
+            if (__all_sync(0xffffffffu, ok)) {
+                v0 = __uint_as_float((unsigned)w0);
+                v1 = __uint_as_float((unsigned)w1);
+                return;
+            }
+        } else {
+            const unsigned long long *p = ll + (size_t)c * 2 * NB;
+            const unsigned long long l0 = ld_ll(p + lane), l1 = ld_ll(p + 32 + lane);
+            const unsigned long long h0 = ld_ll(p + NB + lane), h1 = ld_ll(p + NB + 32 + lane);
+            const bool ok = (unsigned)(l0 >> 32) == epoch && (unsigned)(l1 >> 32) == epoch &&
+                            (unsigned)(h0 >> 32) == epoch && (unsigned)(h1 >> 32) == epoch;
+            if (__all_sync(0xffffffffu, ok)) {
+                v0 = __longlong_as_double((long long)((h0 << 32) | (l0 & 0xffffffffull)));
+                v1 = __longlong_as_double((long long)((h1 << 32) | (l1 & 0xffffffffull)));
+                return;
+            }
+        }
+    }
+    v0 = v1 = T(0);
+    if (lane == 0) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
+}
+
+// value 4k + q of a block held across the warp as (v0, v1) by wait_warp
+template <typename T, int K>
+__device__ __forceinline__ T warp_value(T v0, T v1, int q) {
+    return __shfl_sync(0xffffffffu, K < 8 ? v0 : v1, (4 * K + q) & 31);
+}
+
 // sleep between empty polls for a block `dist` steps from the one it waits on
 __device__ __forceinline__ int poll_backoff(int dist) { return dist > 8 ? 512 : 64 * dist; }
 
@@ -750,20 +791,16 @@ __global__ void __launch_bounds__(256) k_trsv_ll(int n, long long ld, const T *_
         // the chain step: the nearest predecessor through the coupling block
         T xr = y;
         if (has_pred && ok) {
-            T *buf = sx + par * NB;
-            ok = wait_chunk<T>(ll, pred, epoch, buf, 0, sok + par, flags);
-            par ^= 1;
-            if (ok) {
-                T v = 0;
-#pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    const int c = 4 * k + q;
-                    v = fma(sC[r][c], buf[c], v);
-                }
-                v += __shfl_xor_sync(0xffffffffu, v, 1);
-                v += __shfl_xor_sync(0xffffffffu, v, 2);
-                xr = y - v;
-            }
+            T p0, p1;
+            wait_warp<T>(ll, pred, epoch, p0, p1, flags);
+            T v = 0;
+#define MP_STEP(K) v = fma(sC[r][4 * K + q], warp_value<T, K>(p0, p1, q), v);
+            MP_STEP(0) MP_STEP(1) MP_STEP(2) MP_STEP(3) MP_STEP(4) MP_STEP(5) MP_STEP(6) MP_STEP(7)
+            MP_STEP(8) MP_STEP(9) MP_STEP(10) MP_STEP(11) MP_STEP(12) MP_STEP(13) MP_STEP(14) MP_STEP(15)
+#undef MP_STEP
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            xr = y - v;
         }
         if (q == 0) {
             ll_put<T>(ll, blk, r, r < kb ? xr : T(0), epoch);
@@ -942,25 +979,24 @@ __global__ void __launch_bounds__(256, 2)
         // the chain: p crosses SMs, b1 -> b2 stays in the CTA
         T x1 = y1, t2 = y2;
         if (has_p && ok) {
-            T *buf = sx + par * NB;
-            ok = wait_chunk<T>(ll, p, epoch, buf, 0, sok + par, flags);
-            par ^= 1;
-            if (ok) {
-                T v1 = T(0), v2 = T(0);
-#pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    const int c = 4 * k + q;
-                    const T xv = buf[c];
-                    v1 = fma(sC11[r][c], xv, v1);
-                    v2 = fma(sC22[r][c], xv, v2);
-                }
-                v1 += __shfl_xor_sync(0xffffffffu, v1, 1);
-                v1 += __shfl_xor_sync(0xffffffffu, v1, 2);
-                v2 += __shfl_xor_sync(0xffffffffu, v2, 1);
-                v2 += __shfl_xor_sync(0xffffffffu, v2, 2);
-                x1 = y1 - v1;
-                t2 = y2 - v2;
-            }
+            T p0, p1;
+            wait_warp<T>(ll, p, epoch, p0, p1, flags);
+            T v1 = T(0), v2 = T(0);
+#define MP_STEP(K)                                       \
+    {                                                    \
+        const T xv = warp_value<T, K>(p0, p1, q);        \
+        v1 = fma(sC11[r][4 * K + q], xv, v1);            \
+        v2 = fma(sC22[r][4 * K + q], xv, v2);            \
+    }
+            MP_STEP(0) MP_STEP(1) MP_STEP(2) MP_STEP(3) MP_STEP(4) MP_STEP(5) MP_STEP(6) MP_STEP(7)
+            MP_STEP(8) MP_STEP(9) MP_STEP(10) MP_STEP(11) MP_STEP(12) MP_STEP(13) MP_STEP(14) MP_STEP(15)
+#undef MP_STEP
+            v1 += __shfl_xor_sync(0xffffffffu, v1, 1);
+            v1 += __shfl_xor_sync(0xffffffffu, v1, 2);
+            v2 += __shfl_xor_sync(0xffffffffu, v2, 1);
+            v2 += __shfl_xor_sync(0xffffffffu, v2, 2);
+            x1 = y1 - v1;
+            t2 = y2 - v2;
         }
         if (q == 0) {
             ll_put<T>(ll, b1, r, r < kb1 ? x1 : T(0), epoch);

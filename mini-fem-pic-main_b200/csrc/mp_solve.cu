@@ -344,17 +344,16 @@ __global__ void __launch_bounds__(256) k_gs_sweep(int n, long long ld, const dou
         // block blk-1 through the coupling block Minv_kk J~_{k,k-1}
         double xr = y;
         if (has_pred && ok) {
-            double *buf = sx + par * NB;
-            ok = wait_chunk<double>(ll, blk - 1, epoch, buf, 0, sok + par, flags);
-            par ^= 1;
-            if (ok) {
-                double v = 0.0;
-#pragma unroll
-                for (int k = 0; k < 16; k++) v = fma(sC[r][4 * k + q], buf[4 * k + q], v);
-                v += __shfl_xor_sync(0xffffffffu, v, 1);
-                v += __shfl_xor_sync(0xffffffffu, v, 2);
-                xr = y - v;
-            }
+            double p0, p1;
+            wait_warp<double>(ll, blk - 1, epoch, p0, p1, flags);
+            double v = 0.0;
+#define MP_STEP(K) v = fma(sC[r][4 * K + q], warp_value<double, K>(p0, p1, q), v);
+            MP_STEP(0) MP_STEP(1) MP_STEP(2) MP_STEP(3) MP_STEP(4) MP_STEP(5) MP_STEP(6) MP_STEP(7)
+            MP_STEP(8) MP_STEP(9) MP_STEP(10) MP_STEP(11) MP_STEP(12) MP_STEP(13) MP_STEP(14) MP_STEP(15)
+#undef MP_STEP
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            xr = y - v;
         }
         if (q == 0) {
             ll_put<double>(ll, blk, r, r < kb ? xr : 0.0, epoch);
@@ -480,17 +479,16 @@ __global__ void __launch_bounds__(256, 2) k_gs_sweeps(int n, long long ld, const
         y += __shfl_xor_sync(0xffffffffu, y, 2);
         double xr = y;
         if (has_pred && ok) {
-            double *buf = sx + par * NB;
-            ok = wait_chunk<double>(ll, blk - 1, ep, buf, 0, sok + par, flags);
-            par ^= 1;
-            if (ok) {
-                double v = 0.0;
-#pragma unroll
-                for (int k = 0; k < 16; k++) v = fma(sC[r][4 * k + q], buf[4 * k + q], v);
-                v += __shfl_xor_sync(0xffffffffu, v, 1);
-                v += __shfl_xor_sync(0xffffffffu, v, 2);
-                xr = y - v;
-            }
+            double p0, p1;
+            wait_warp<double>(ll, blk - 1, ep, p0, p1, flags);
+            double v = 0.0;
+#define MP_STEP(K) v = fma(sC[r][4 * K + q], warp_value<double, K>(p0, p1, q), v);
+            MP_STEP(0) MP_STEP(1) MP_STEP(2) MP_STEP(3) MP_STEP(4) MP_STEP(5) MP_STEP(6) MP_STEP(7)
+            MP_STEP(8) MP_STEP(9) MP_STEP(10) MP_STEP(11) MP_STEP(12) MP_STEP(13) MP_STEP(14) MP_STEP(15)
+#undef MP_STEP
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            xr = y - v;
         }
         if (q == 0) {
             ll_put<double>(ll, blk, r, r < kb ? xr : 0.0, ep);
