@@ -172,9 +172,9 @@ def load_population(c, pos, vel, cell, form, chunk=8_000_000):
 
 
 def mixed_terms(neq):
-    """TF32 products per term of the mixed factorization's trailing update
-    under the library's default (MIXED_AUTO)."""
-    return 1 if neq >= mp.MIXED_TF32_FROM else 3
+    """Arithmetic of the mixed factorization's trailing update under the
+    library's default (MIXED_AUTO): 3 (3xTF32) or 2 (FP16 operands)."""
+    return mp.MIXED_FP16 if neq >= mp.MIXED_FP16_FROM else mp.MIXED_TF32X3
 
 
 def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True, neq=0):
@@ -191,7 +191,8 @@ def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True, neq=0):
     terms = mixed_terms(neq)
     kname = KT_KERNEL[top][form]
     if top == mp.KT_UPDATE and form == mp.MIXED:
-        kname = "tc::k_update_tc<%s> (%s, tcgen05)" % (("true", "3xTF32") if terms == 3 else ("false", "TF32"))
+        kname = ("tc::k_update_tc<1> (3xTF32, tcgen05 kind::tf32)" if terms == mp.MIXED_TF32X3 else
+                 "tc::k_update_tc<2> (FP16 operands, tcgen05 kind::f16)")
     out = {"kernel": kname, "class": KT_NAMES[top], "launches": v["launches"],
            "avg_launch_ms": v["ms"] / max(v["launches"], 1)}
     if top == mp.KT_PUSH:
@@ -217,11 +218,14 @@ def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True, neq=0):
         out.update(bound="tensor", achieved=ach, peak=peak, unit="TFLOP/s", frac=ach / peak,
                    peak_kind=pk["kind"] + (" bf16 dense, sustained" if sustained else " bf16 dense, burst"),
                    algorithmic="2 flops per multiply-add of the trailing update's lower triangle")
-        if form == mp.MIXED:
-            out["note"] = ("kind::tf32 MMAs run at half the bf16 rate" +
-                           (", and the 3xTF32 split issues three per term: issued TF32 rate = 3 x achieved"
-                            if terms == 3 else "; one TF32 product per term"))
-            out["tf32_issued_frac_of_half_bf16_peak"] = terms * ach / (peak / 2)
+        if form == mp.MIXED and terms == mp.MIXED_TF32X3:
+            out["note"] = ("kind::tf32 MMAs run at half the bf16 rate, and the 3xTF32 split issues three "
+                           "per term: issued TF32 rate = 3 x achieved")
+            out["tf32_issued_frac_of_half_bf16_peak"] = 3 * ach / (peak / 2)
+        elif form == mp.MIXED:
+            out["note"] = ("kind::f16 MMAs (the bf16 rate) on FP16 copies of the trailing updates' operands; "
+                           "the strips inside a super-panel (3.5 % of the flops at 32,244 unknowns) stay on TF32")
+        if form == mp.MIXED and ("tc%d" % terms, "update") in TRAFFIC_PER_UNIT:
             out["traffic"] = TRAFFIC_PER_UNIT[("tc%d" % terms, "update")] * v["work"] / max(v["launches"], 1)
             out["traffic_source"] = ("ncu DRAM bytes per flop of a K = 1,024 trailing update (8,379 unknowns) x "
                                      "this workload's average flops per launch (the strips, K = 256, move more "
@@ -848,7 +852,7 @@ def main():
             "data": "synthetic (seeded Kuhn-box ions at steady state; device injection with the reference's counts)",
             "config": conf,
             "form": "mixed: FP32 tet-relative particles, FP64 near-face test and density, %s tcgen05 LDL^T "
-                    "with FP64 refinement" % ("TF32" if mixed_terms(h["neq"]) == 1 else "3xTF32"),
+                    "with FP64 refinement" % ("FP16-operand" if mixed_terms(h["neq"]) == mp.MIXED_FP16 else "3xTF32"),
             "parallelism": f"particles sharded x{world}, density all-reduce, field solve replicated"
             if world > 1 else "1 GPU",
             "l2": f"inputs larger than L2 (the particle arrays); {FLUSH_BYTES >> 20} MiB written between steps",

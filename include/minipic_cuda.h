@@ -91,7 +91,7 @@ enum { MP_FORM_FP64 = 0, MP_FORM_MIXED = 1 };
 /* Tensor-core arithmetic of the mixed form's FP32 factorization: one TF32
  * product per term, or the 3xTF32 split (hi*hi + hi*lo + lo*hi, about FP32
  * accuracy; fewer FP64 refinement iterations). */
-enum { MP_MIXED_AUTO = 0, MP_MIXED_TF32 = 1, MP_MIXED_TF32X3 = 3 };
+enum { MP_MIXED_AUTO = 0, MP_MIXED_TF32 = 1, MP_MIXED_FP16 = 2, MP_MIXED_TF32X3 = 3 };
 
 /* What a walk that reaches the hop limit does.  In a mesh with a cavity (the
  * sphere workload) a particle that steps into the cavity lies in no tet, and
@@ -198,15 +198,22 @@ int mp_set_sort_period(mp_ctx *ctx, int32_t steps);
  * both, and its walk (src/meshes.h:75-100) would then never end.  Converts the
  * resident particles (holes removed first). */
 int mp_set_particle_form(mp_ctx *ctx, int form);
-/* Arithmetic of the mixed-form Newton factorization: MP_MIXED_TF32 (one TF32
- * product per term; more FP64 refinement solves), MP_MIXED_TF32X3 (hi/lo split,
- * three TF32 products a term; about FP32 accuracy, fewer refinement solves) or
- * MP_MIXED_AUTO, the default: TF32X3 below MP_MIXED_TF32_FROM unknowns, where
- * the refinement solves cost more than the trailing update saves, TF32 from
- * there on.  Either way the solve is refined in FP64 to the same tolerance.  No
+/* Arithmetic of the mixed-form Newton factorization:
+ *   MP_MIXED_TF32    one TF32 product per term (more FP64 refinement solves);
+ *   MP_MIXED_FP16    the trailing updates on FP16 copies of their operands,
+ *                    scaled by powers of two: the same 11 significant bits as
+ *                    TF32 (rounded to nearest) at half the operand bytes and
+ *                    twice the tensor rate; if a scaled operand would overflow
+ *                    FP16 the factorization is redone with TF32 operands;
+ *   MP_MIXED_TF32X3  hi/lo split, three TF32 products a term (about FP32
+ *                    accuracy, fewer refinement solves);
+ *   MP_MIXED_AUTO    the default: TF32X3 below MP_MIXED_FP16_FROM unknowns,
+ *                    where the refinement solves cost more than the trailing
+ *                    update saves, FP16 from there on.
+ * Either way the solve is refined in FP64 to the same tolerance.  No
  * reference counterpart: the reference's dsysv_ call (src/FESolver.cpp:528-558)
  * is FP64 throughout. */
-#define MP_MIXED_TF32_FROM 16384
+#define MP_MIXED_FP16_FROM 16384
 int mp_set_mixed_factor(mp_ctx *ctx, int mode);
 /* Particle IDs (16 B per particle-step of traffic) are needed only to restore
  * injection order after tet re-sorting; without sorting the stable removal

@@ -383,7 +383,8 @@ int mp_set_sort_period(mp_ctx *ctx, int32_t steps) {
 }
 
 int mp_set_mixed_factor(mp_ctx *ctx, int mode) {
-    if (!ctx || (mode != MP_MIXED_AUTO && mode != MP_MIXED_TF32 && mode != MP_MIXED_TF32X3)) return MP_ERR_ARG;
+    if (!ctx || (mode != MP_MIXED_AUTO && mode != MP_MIXED_TF32 && mode != MP_MIXED_FP16 && mode != MP_MIXED_TF32X3))
+        return MP_ERR_ARG;
     ctx->mixed_factor = mode;
     return MP_OK;
 }

@@ -78,6 +78,7 @@ enum Flag : unsigned long long {
     FLAG_SINGULAR = 4ull,
     FLAG_NONFINITE = 8ull,
     FLAG_BAD_INDEX = 16ull,   // a cell, neighbour or node index outside the mesh (caller-owned records)
+    FLAG_HALF_RANGE = 32ull,  // an FP16 operand of the mixed factorization's update would overflow
 };
 
 // The per-quadrature-point shape function values used by buildF1Vector and

@@ -1391,11 +1391,13 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols_tc(int n, long long ld
 
 template <typename T>
 struct LdltWork {
-    T *dvec, *W, *s;
+    T *dvec, *W;
+    T *s;                    // [NB]; s[0]: the inverse operand scale of an FP16 trailing update
     T *Linv;                 // [blocks][NB][NB] inverses of the diagonal blocks' L (the solves use them)
     T *Mc;                   // [4][blocks][NB][NB] coupling blocks: forward, backward at distance 1, then 2
     unsigned long long *ll;  // [2][blocks][2][NB] words the two solves publish their blocks in
     float *split;            // tensor-core path: [4][n][SUPER_W] hi/lo copies of the update's L and W rows
+                             // (3xTF32), or [2][n][SUPER_W] FP16 copies (FP16 operands)
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
@@ -1414,14 +1416,18 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // Map of a [rows][K] FP32 operand with row pitch `pitch` elements, loaded as
 // boxes of 32 (K) x box_rows rows with the 128-byte swizzle the UMMA
 // descriptors use.  base must be 16-byte aligned and pitch*4 a multiple of 16.
-static bool operand_map(CUtensorMap *m, const float *base, long long rows, long long pitch, int box_rows, int K) {
+// Boxes are one 128-byte swizzle row wide: 32 FP32 or 64 FP16 values.
+static bool operand_map(CUtensorMap *m, const void *base, long long rows, long long pitch, int box_rows, int K,
+                        bool half = false) {
     PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
-    if (!fn || rows < 1 || (reinterpret_cast<size_t>(base) & 15) || ((pitch * 4) & 15)) return false;
+    const long long esz = half ? 2 : 4;
+    if (!fn || rows < 1 || (reinterpret_cast<size_t>(base) & 15) || ((pitch * esz) & 15)) return false;
     cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
-    cuuint32_t box[2] = {(cuuint32_t)tc::KC, (cuuint32_t)box_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(pitch * esz)};
+    cuuint32_t box[2] = {(cuuint32_t)(128 / esz), (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box, estr,
+    return fn(m, half ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base),
+              dims, strides, box, estr,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -1507,10 +1513,12 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         const int big = 96 * 1024;
         cudaFuncSetAttribute(k_update_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_update_f64_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(tc::k_update_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tc::smem_bytes(false));
-        cudaFuncSetAttribute(tc::k_update_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tc::smem_bytes(true));
+        cudaFuncSetAttribute(tc::k_update_tc<tc::MODE_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tc::smem_bytes(tc::MODE_TF32));
+        cudaFuncSetAttribute(tc::k_update_tc<tc::MODE_TF32X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tc::smem_bytes(tc::MODE_TF32X3));
+        cudaFuncSetAttribute(tc::k_update_tc<tc::MODE_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tc::smem_bytes(tc::MODE_F16));
         wavefront_attrs<float>();
         wavefront_attrs<double>();
         for (const void *f : {(const void *)k_ldlt_panel_tc<1>, (const void *)k_ldlt_panel_tc<3>,
@@ -1574,7 +1582,10 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         const int cb = strip ? (C1 - R0) / tc::TILE_N : 0;
         const long long ntiles = strip ? rb * cb : tc::tile_count(rb);
         const long long wrows = (strip ? C1 : n) - R0;
-        const bool split = tc_terms == 3;
+        // the strips keep TF32 operands in the FP16 mode: their conversion
+        // would cost more than their MMAs save
+        const int mode = tc_terms == 3 ? tc::MODE_TF32X3 : (tc_terms == 2 && !strip ? tc::MODE_F16 : tc::MODE_TF32);
+        const bool split = mode == tc::MODE_TF32X3;
         float *Af = reinterpret_cast<float *>(A);
         const float *Wf = reinterpret_cast<const float *>(w.W);
         const float *Lsrc = Af + (long long)R0 * ld + K0, *Wsrc = Wf + (long long)R0 * SUPER_W + kofs;
@@ -1591,6 +1602,20 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             kt_end(ctx, mk);
             ok = operand_map(&mLh, Lh, n - R0, K, tc::TILE, K) && operand_map(&mWh, Wh, wrows, K, tc::TILE_N, K) &&
                  operand_map(&mLl, Ll, n - R0, K, tc::TILE, K) && operand_map(&mWl, Wl, wrows, K, tc::TILE_N, K);
+        } else if (mode == tc::MODE_F16) {
+            __half *Lh = reinterpret_cast<__half *>(w.split), *Wh = Lh + (size_t)n * SUPER_W;
+            const long long groups = (n - R0 + wrows) * (K / 8);
+            const int gh = (int)std::min<long long>((groups + 255) / 256, (long long)ctx->sm_count * 8);
+            const int mk = kt_begin(ctx, MP_KT_PANEL, 0);
+            tc::k_half_operands<<<gh, 256, 0, st>>>(Lsrc, ld, n - R0, Wsrc, SUPER_W, wrows, K,
+                                                    reinterpret_cast<const float *>(w.dvec) + K0, Lh, Wh,
+                                                    reinterpret_cast<float *>(w.s), flags),
+                ++ctx->launches;
+            kt_end(ctx, mk);
+            ok = operand_map(&mLh, Lh, n - R0, K, tc::TILE, K, true) &&
+                 operand_map(&mWh, Wh, wrows, K, tc::TILE_N, K, true);
+            mLl = mLh;
+            mWl = mWh;
         } else {
             ok = operand_map(&mLh, Lsrc, n - R0, ld, tc::TILE, K) &&
                  operand_map(&mWh, Wsrc, wrows, SUPER_W, tc::TILE_N, K);
@@ -1599,10 +1624,13 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         }
         if (!ok) return fail(ctx, MP_ERR_CUDA, "cuTensorMapEncodeTiled failed for the tensor-core update");
         const int grid = (int)std::min<long long>(ntiles, (long long)ctx->sm_count);
-        auto kern = split ? tc::k_update_tc<true> : tc::k_update_tc<false>;
+        auto kern = mode == tc::MODE_F16 ? tc::k_update_tc<tc::MODE_F16>
+                    : split            ? tc::k_update_tc<tc::MODE_TF32X3>
+                                       : tc::k_update_tc<tc::MODE_TF32>;
         const int mk = kt_begin(ctx, MP_KT_UPDATE, update_flops(R0, C1, K));
-        kern<<<grid, tc::THREADS, tc::smem_bytes(split), st>>>(mLh, mWh, mLl, mWl, n, ld, Af, R0, ntiles, K / tc::KC,
-                                                               cb, flags),
+        kern<<<grid, tc::THREADS, tc::smem_bytes(mode), st>>>(mLh, mWh, mLl, mWl, n, ld, Af, R0, ntiles,
+                                                              K / tc::kc_of(mode), cb,
+                                                              reinterpret_cast<const float *>(w.s), flags),
             ++ctx->launches;
         kt_end(ctx, mk);
         return MP_OK;
@@ -1613,7 +1641,8 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         // (diagonal block, panel, updates restricted to the panel's columns),
         // then updates the rest of its super-panel (a strip); the trailing
         // matrix gets one update per super-panel with K = SUPER_W: on the tensor
-        // cores for the FP32 factor (TF32, or 3xTF32 when tc_terms == 3),
+        // cores for the FP32 factor (TF32; 3xTF32 when tc_terms == 3; FP16
+        // operands for the trailing updates when tc_terms == 2),
         // register-tiled FP64 for the FP64 factor.
         for (int S0 = 0; S0 < n; S0 += SUPER_W) {
             const int S1 = S0 + SUPER_W < n ? S0 + SUPER_W : n;

@@ -182,10 +182,21 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         rc = resid_norms(ctx, ctx->y, ctx->G, sc.r, sc.b32, &rn, &bn);
         if (rc) return rc;
         const int terms = ctx->mixed_factor != MP_MIXED_AUTO ? ctx->mixed_factor
-                          : n >= MP_MIXED_TF32_FROM       ? MP_MIXED_TF32
+                          : n >= MP_MIXED_FP16_FROM       ? MP_MIXED_FP16
                                                           : MP_MIXED_TF32X3;
         rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, sc.b32, w, true, terms);
         if (rc) return rc;
+        if (terms == MP_MIXED_FP16) {
+            unsigned long long range = 0;
+            if ((rc = check_flags(ctx, FLAG_HALF_RANGE, &range))) return rc;
+            if (range) {  // an operand did not fit FP16: factor J again with TF32 operands
+                if ((rc = fe_j32_from_k(ctx))) return rc;
+                ctx->j32_current = false;
+                if ((rc = resid_norms(ctx, ctx->y, ctx->G, sc.r, sc.b32, &rn, &bn))) return rc;
+                rc = ldlt_factor_solve<float>(ctx, ctx->J32, ld, n, sc.b32, w, true, MP_MIXED_TF32);
+                if (rc) return rc;
+            }
+        }
         cudaEventRecord(ctx->t1.b, ctx->stream);
         k_axpy_f32<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, sc.b32, ctx->y), ++ctx->launches;
         int it = 1;

@@ -22,13 +22,24 @@
 //                      accumulator's "empty" mbarrier.
 // Two accumulators let the epilogue of one tile overlap the MMAs of the next.
 //
-// SPLIT (3xTF32): the operands arrive pre-split by k_split_panel into
-// hi = x rounded to TF32 (11 significant bits) and lo = x - hi (exact in FP32);
-// each tile accumulates hi*hi + hi*lo + lo*hi on the same TMEM accumulator.
-// The dropped lo*lo term is ~2^-22 relative, so the update carries about FP32
-// accuracy instead of TF32's 2^-11, which is what the FP64 refinement of the
-// mixed solve converges against.  Without SPLIT the TMA reads L straight from
-// the factor and W from the panel scratch.
+// Operand modes:
+//   MODE_TF32    the TMA reads L straight from the factor and W from the panel
+//                scratch; one TF32 product a term (2^-11 relative).
+//   MODE_TF32X3  the operands arrive pre-split by k_split_rows into hi = x
+//                rounded to TF32 (11 significant bits) and lo = x - hi (exact
+//                in FP32); each tile accumulates hi*hi + hi*lo + lo*hi on the
+//                same TMEM accumulator.  The dropped lo*lo term is ~2^-22
+//                relative: about FP32 accuracy, three times the MMAs.
+//   MODE_F16     FP16 copies of the operands (k_half_operands), scaled by powers
+//                of two into FP16's range, kind::f16 MMAs with FP32
+//                accumulation, and the epilogue multiplies by the inverse scale.
+//                FP16 keeps TF32's 11 significant bits (rounded to nearest), so
+//                a term is as accurate as MODE_TF32's, while a 128-byte chunk
+//                row carries 64 values instead of 32: half the operand bytes
+//                from L2 per flop, at twice the tensor rate.
+// Every mode's shared-memory chunk rows are 128 bytes (one swizzle row) and an
+// MMA consumes 32 bytes of each row (8 TF32 or 16 FP16 values), so the
+// descriptors and stage layout are the same in all three.
 //
 // Every mbarrier wait is bounded.  A wait that gives up raises a CTA-wide abort
 // flag; every role leaves its loop, the producer and the MMA issuer wait
@@ -37,6 +48,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_fp16.h>
 
 #include "mp_internal.h"
 
@@ -45,11 +57,13 @@ namespace tc {
 
 constexpr int TILE = 128;                   // M: tile rows
 constexpr int TILE_N = 256;                 // N: tile columns
-constexpr int KC = 32;                      // K elements per chunk (one 128-byte swizzle row)
-constexpr int PANEL = 256;                  // panel width: K of a strip update
-constexpr int CHUNK_L = TILE * KC * 4;      // 16 KB: one L operand chunk
-constexpr int CHUNK_W = TILE_N * KC * 4;    // 32 KB: one W operand chunk
-__host__ __device__ constexpr int stages(bool split) { return split ? 2 : 4; }  // 192 KB of stages either way
+enum { MODE_TF32 = 0, MODE_TF32X3 = 1, MODE_F16 = 2 };
+constexpr int KC = 32;                      // FP32 elements per chunk row (one 128-byte swizzle row)
+constexpr int CHUNK_L = TILE * 128;         // 16 KB: one L operand chunk
+constexpr int CHUNK_W = TILE_N * 128;       // 32 KB: one W operand chunk
+// K elements per chunk: one 128-byte row of 4-byte or 2-byte values
+__host__ __device__ constexpr int kc_of(int mode) { return mode == MODE_F16 ? 64 : 32; }
+__host__ __device__ constexpr int stages(int mode) { return mode == MODE_TF32X3 ? 2 : 4; }  // 192 KB of stages
 constexpr int THREADS = 192;                // producer warp, MMA warp, 4 epilogue warps
 constexpr long long SPIN_LIMIT = 1ll << 22;
 
@@ -60,8 +74,10 @@ __device__ __forceinline__ unsigned long long smem_desc(unsigned addr) {
     return (unsigned long long)((addr >> 4) & 0x3FFF) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
 
-// Instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = 256.
+// Instruction descriptors: D F32, A/B TF32 (format 2 of kind::tf32) or F16
+// (format 0 of kind::f16), both K-major, M = 128, N = 256.
 constexpr unsigned IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr unsigned IDESC_F16 = (1u << 4) | (0u << 7) | (0u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
 
 __device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
@@ -107,6 +123,13 @@ __device__ __forceinline__ void mma_tf32(unsigned tmem_d, unsigned long long a, 
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
         ::"r"(tmem_d), "l"(a), "l"(b), "r"(IDESC), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
+        : "memory");
+}
+__device__ __forceinline__ void mma_f16(unsigned tmem_d, unsigned long long a, unsigned long long b, unsigned acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(IDESC_F16), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
         : "memory");
 }
 __device__ __forceinline__ void mma_commit(unsigned long long *bar) {
@@ -166,6 +189,74 @@ __global__ void k_split_rows(const float *__restrict__ src, long long ld, long l
     }
 }
 
+// FP16 operands of a MODE_F16 update: rows [0, nl) of L (pitch ldl) and rows
+// [0, nw) of W (pitch ldw) over K columns (a multiple of 8) into [nl][K] and
+// [nw][K] arrays.  L is scaled by 2^L_EXP, W by 2^e with e set so the largest
+// |d_k| of the K pivots dk lands in [2^4, 2^5) (|W_jk| = |L_jk| |d_k|), and
+// *unscale = 2^-(L_EXP + e); every block finds the same e.  In the factor of a
+// diagonally dominant J every |L_jk| <= 1, so both copies stay at least 2^7
+// below FP16's largest value (65504); a value that would not fit sets
+// FLAG_HALF_RANGE and the caller factors again with TF32 operands.  Values
+// below 2^-14 of the scale lose bits as FP16 subnormals: absolute errors under
+// 2^-25 2^-L_EXP for L and 2^-29 max|d_k| for W, far below the 2^-11 relative
+// rounding of the larger terms.
+constexpr int L_EXP = 8;
+__global__ void __launch_bounds__(256) k_half_operands(const float *__restrict__ L, long long ldl, long long nl,
+                                                       const float *__restrict__ W, long long ldw, long long nw,
+                                                       int K, const float *__restrict__ dk, __half *Lh, __half *Wh,
+                                                       float *unscale, unsigned long long *flags) {
+    __shared__ float sred[8];
+    float m = 0.f;
+    for (int k = threadIdx.x; k < K; k += 256) m = fmaxf(m, fabsf(dk[k]));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = sred[0];
+#pragma unroll
+    for (int w = 1; w < 8; w++) m = fmaxf(m, sred[w]);
+    // floor(log2 m) from the exponent field (m normal); e clamped so 2^e and
+    // 2^-(L_EXP + e) are normal floats
+    int e = 0;
+    if (m >= 1.17549435e-38f && m <= 3.40282347e38f) e = 4 - (int)((__float_as_uint(m) >> 23) & 0xff) + 127;
+    e = e < -100 ? -100 : (e > 100 ? 100 : e);
+    const float sl = (float)(1 << L_EXP), sw = __uint_as_float((unsigned)(127 + e) << 23);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *unscale = __uint_as_float((unsigned)(127 - L_EXP - e) << 23);
+    const int g8 = K / 8;
+    const long long total = (nl + nw) * g8;
+    bool bad = false;
+    for (long long q = blockIdx.x * 256ll + threadIdx.x; q < total; q += (long long)gridDim.x * 256) {
+        long long r = q / g8;
+        const int c = (int)(q - r * g8) * 8;
+        const float *src;
+        __half *dst;
+        float sc;
+        if (r < nl) {
+            src = L + r * ldl + c;
+            dst = Lh + r * K + c;
+            sc = sl;
+        } else {
+            r -= nl;
+            src = W + r * ldw + c;
+            dst = Wh + r * K + c;
+            sc = sw;
+        }
+        const float4 a = __ldg(reinterpret_cast<const float4 *>(src));
+        const float4 b = __ldg(reinterpret_cast<const float4 *>(src) + 1);
+        const float v[8] = {a.x * sc, a.y * sc, a.z * sc, a.w * sc, b.x * sc, b.y * sc, b.z * sc, b.w * sc};
+        uint4 o;
+        unsigned *ow = reinterpret_cast<unsigned *>(&o);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            bad |= fabsf(v[2 * j]) >= 65520.f || fabsf(v[2 * j + 1]) >= 65520.f;
+            const __half2 h = __floats2half2_rn(v[2 * j], v[2 * j + 1]);
+            ow[j] = *reinterpret_cast<const unsigned *>(&h);
+        }
+        *reinterpret_cast<uint4 *>(dst) = o;
+    }
+    if (bad) atomicOr(flags, FLAG_HALF_RANGE);
+}
+
 // A[i][j] -= sum_{k<K} L[i][k] W[j][k] (K = 32*nchunk) for rows from P1 and
 // columns from P1.  colblocks = 0: the 128 x 256 tiles that meet the lower
 // triangle of [P1, n)^2 (the trailing update of a super-panel); colblocks > 0:
@@ -173,14 +264,17 @@ __global__ void k_split_rows(const float *__restrict__ src, long long ld, long l
 // a super-panel), lower parts only.  The L maps cover the rows from P1 (rows
 // past the end read as zero) and load boxes of 128 rows; the W maps cover the
 // output columns' rows and load boxes of 256 rows.
-template <bool SPLIT>
+template <int MODE>
 __global__ void __launch_bounds__(THREADS, 1)
     k_update_tc(const __grid_constant__ CUtensorMap mLh, const __grid_constant__ CUtensorMap mWh,
                 const __grid_constant__ CUtensorMap mLl, const __grid_constant__ CUtensorMap mWl, int n, long long ld,
-                float *A, int P1, long long ntiles, int nchunk, int colblocks, unsigned long long *flags) {
+                float *A, int P1, long long ntiles, int nchunk, int colblocks, const float *unscale,
+                unsigned long long *flags) {
+    constexpr bool SPLIT = MODE == MODE_TF32X3;
+    constexpr int KCE = kc_of(MODE);
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<size_t>(smem_raw) + 1023) & ~size_t(1023));
-    constexpr int STAGES = stages(SPLIT);
+    constexpr int STAGES = stages(MODE);
     // stage: L hi, W hi (, L lo, W lo)
     constexpr unsigned STAGE_BYTES = SPLIT ? 2 * (CHUNK_L + CHUNK_W) : CHUNK_L + CHUNK_W;
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(base + STAGES * STAGE_BYTES);
@@ -231,11 +325,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                     unsigned char *st = base + s * STAGE_BYTES;
                     mbar_expect_tx(&full[s], STAGE_BYTES);
-                    tma_load(st, &mLh, kc * KC, bi * TILE, &full[s]);
-                    tma_load(st + CHUNK_L, &mWh, kc * KC, bj * TILE_N, &full[s]);
+                    tma_load(st, &mLh, kc * KCE, bi * TILE, &full[s]);
+                    tma_load(st + CHUNK_L, &mWh, kc * KCE, bj * TILE_N, &full[s]);
                     if (SPLIT) {
-                        tma_load(st + CHUNK_L + CHUNK_W, &mLl, kc * KC, bi * TILE, &full[s]);
-                        tma_load(st + 2 * CHUNK_L + CHUNK_W, &mWl, kc * KC, bj * TILE_N, &full[s]);
+                        tma_load(st + CHUNK_L + CHUNK_W, &mLl, kc * KCE, bi * TILE, &full[s]);
+                        tma_load(st + 2 * CHUNK_L + CHUNK_W, &mWl, kc * KCE, bj * TILE_N, &full[s]);
                     }
                 }
             }
@@ -269,9 +363,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const unsigned long long dll = smem_desc(saddr(st + CHUNK_L + CHUNK_W));
                     const unsigned long long dwl = smem_desc(saddr(st + 2 * CHUNK_L + CHUNK_W));
 #pragma unroll
-                    for (int kk = 0; kk < KC / 8; kk++) {  // 8 TF32 = 32 B per MMA step: +2 in the descriptor
+                    for (int kk = 0; kk < 4; kk++) {  // 32 B of each row (8 TF32, 16 FP16) per MMA: +2 in the descriptor
                         const unsigned accum = (kc > 0 || kk > 0) ? 1u : 0u;
-                        if (SPLIT) {
+                        if (MODE == MODE_F16) {
+                            mma_f16(d, dl + 2 * kk, dw + 2 * kk, accum);
+                        } else if (SPLIT) {
                             mma_tf32(d, dll + 2 * kk, dw + 2 * kk, accum);
                             mma_tf32(d, dl + 2 * kk, dwl + 2 * kk, 1u);
                             mma_tf32(d, dl + 2 * kk, dw + 2 * kk, 1u);
@@ -297,6 +393,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             // not depend on the MMAs.
             const int q = warp & 3;
             const int r = q * 32 + lane;
+            const float us = MODE == MODE_F16 ? *unscale : 1.0f;  // a power of two: the products stay exact
             long long lt = 0;
             for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
                 int bi, bj;
@@ -344,15 +441,15 @@ __global__ void __launch_bounds__(THREADS, 1)
                                 const long long cg = col + 4 * g;
                                 if (cg + 3 <= row && cg + 3 < n) {
                                     float4 o = cur[cb * 4 + g];
-                                    o.x -= __uint_as_float(v[4 * g]);
-                                    o.y -= __uint_as_float(v[4 * g + 1]);
-                                    o.z -= __uint_as_float(v[4 * g + 2]);
-                                    o.w -= __uint_as_float(v[4 * g + 3]);
+                                    o.x -= us * __uint_as_float(v[4 * g]);
+                                    o.y -= us * __uint_as_float(v[4 * g + 1]);
+                                    o.z -= us * __uint_as_float(v[4 * g + 2]);
+                                    o.w -= us * __uint_as_float(v[4 * g + 3]);
                                     *reinterpret_cast<float4 *>(p + 4 * g) = o;
                                 } else {
 #pragma unroll
                                     for (int j = 0; j < 4; j++)
-                                        if (cg + j <= row && cg + j < n) p[4 * g + j] -= __uint_as_float(v[4 * g + j]);
+                                        if (cg + j <= row && cg + j < n) p[4 * g + j] -= us * __uint_as_float(v[4 * g + j]);
                                 }
                             }
                         }
@@ -375,8 +472,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 }
 
 // operand stages + barriers, TMEM slot, abort flag + 1024-byte alignment slack
-constexpr size_t smem_bytes(bool split) {
-    return (size_t)stages(split) * (split ? 2 * (CHUNK_L + CHUNK_W) : CHUNK_L + CHUNK_W) + 256 + 1024;
+constexpr size_t smem_bytes(int mode) {
+    return (size_t)stages(mode) * (mode == MODE_TF32X3 ? 2 * (CHUNK_L + CHUNK_W) : CHUNK_L + CHUNK_W) + 256 + 1024;
 }
 
 }  // namespace tc

@@ -37,8 +37,8 @@ STATUS = {0: "MP_OK", 1: "MP_ERR_ARG", 2: "MP_ERR_OOM", 3: "MP_ERR_CUDA", 4: "MP
 NONLINEAR, GAUSS_SEIDEL, LAPACK, SPARSE_CG, SPARSE_NEWTON = 0, 1, 2, 3, 4
 FE_DENSE, FE_SPARSE = 0, 1
 FP64, MIXED = 0, 1
-MIXED_AUTO, MIXED_TF32, MIXED_TF32X3 = 0, 1, 3
-MIXED_TF32_FROM = 16384  # MIXED_AUTO: TF32 from this many unknowns (the header's MP_MIXED_TF32_FROM)
+MIXED_AUTO, MIXED_TF32, MIXED_FP16, MIXED_TF32X3 = 0, 1, 2, 3
+MIXED_FP16_FROM = 16384  # MIXED_AUTO: FP16 operands from this many unknowns (the header's MP_MIXED_FP16_FROM)
 WALK_LIMIT_ERROR, WALK_LIMIT_ABSORB = 0, 1
 SCATTER_ATOMIC, SCATTER_FIXED = 0, 1
 ORDER_STORAGE, ORDER_ID = 0, 1
@@ -486,8 +486,9 @@ class Context:
         self._c(lib().mp_set_scatter_mode(self.h, mode))
 
     def set_mixed_factor(self, mode):
-        """MIXED_AUTO (default), MIXED_TF32 or MIXED_TF32X3: tensor-core arithmetic of the
-        mixed-form factorization (AUTO: TF32X3 below 16,384 unknowns, TF32 from there)."""
+        """MIXED_AUTO (default), MIXED_TF32, MIXED_FP16 or MIXED_TF32X3: tensor-core arithmetic
+        of the mixed-form factorization (AUTO: TF32X3 below 16,384 unknowns, FP16 from there;
+        FP16: the trailing updates on scaled FP16 copies of their operands)."""
         self._c(lib().mp_set_mixed_factor(self.h, mode))
 
     def set_sort_period(self, steps):

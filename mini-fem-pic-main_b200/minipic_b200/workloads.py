@@ -183,7 +183,7 @@ def newton_driver(args):
         ctx = mp.Context(deck.mesh)
         if cfg["sphere"]:
             absorb_cavity_walks(ctx)
-        ctx.set_mixed_factor({"auto": mp.MIXED_AUTO, "tf32": mp.MIXED_TF32,
+        ctx.set_mixed_factor({"auto": mp.MIXED_AUTO, "tf32": mp.MIXED_TF32, "fp16": mp.MIXED_FP16,
                               "tf32x3": mp.MIXED_TF32X3}[getattr(args, "mixed_factor", "auto")])
         if getattr(args, "storage", "dense") == "sparse":
             ctx.set_fe_storage(mp.FE_SPARSE)
@@ -216,7 +216,7 @@ def main():
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--sort", type=int, default=0)
     ap.add_argument("--n", type=int, default=0, help="override the mesh's hexes per side (newton driver)")
-    ap.add_argument("--mixed-factor", default="auto", choices=["auto", "tf32", "tf32x3"],
+    ap.add_argument("--mixed-factor", default="auto", choices=["auto", "tf32", "fp16", "tf32x3"],
                     help="tensor-core arithmetic of the mixed-form factorization (newton driver)")
     ap.add_argument("--method", default="lapack", choices=sorted(METHODS), help="newton driver")
     ap.add_argument("--storage", default="dense", choices=["dense", "sparse"], help="newton driver: storage of K")

@@ -6,7 +6,8 @@ compiled code (oracle/_ref):
   switches to its two-level structure (trailing update per super-panel, strip
   updates, ready words over many blocks): the 12^3 Kuhn box (1,859 unknowns)
   and the 20^3 box of the FP64 throughput workload (8,379 unknowns), against
-  dsysv_ (solveLinearLapack, src/FESolver.cpp:528-558).  Bar: y within 1e-9
+  dsysv_ (solveLinearLapack, src/FESolver.cpp:528-558), the mixed form in each
+  of its factor arithmetics (TF32, FP16 operands, 3xTF32).  Bar: y within 1e-9
   relative, a whole computePhi step's potential within 1e-9 relative (FP64)
   and within 1e-8 V (mixed);
 * MoveParticles on the 20^3 box with 2M seeded ions (0.2 hops per
@@ -64,14 +65,17 @@ def test_ldlt_past_one_superpanel_vs_dsysv(tmp_path, n):
     uh_ref = s.get("uh")
     ctx = gpu_context(dk)
     assert ctx.neq == neq
-    for form in (mp.FP64, mp.MIXED):
+    # the mixed form in each tensor-core arithmetic of its factorization
+    for form, mf in ((mp.FP64, mp.MIXED_AUTO), (mp.MIXED, mp.MIXED_AUTO), (mp.MIXED, mp.MIXED_TF32),
+                     (mp.MIXED, mp.MIXED_FP16), (mp.MIXED, mp.MIXED_TF32X3)):
+        ctx.set_mixed_factor(mf)
         ctx.fe_set("d", d0)
         ctx.fe_set("F1", zero)
         ctx.build_f1(den)
         ctx.build_j(mp.LAPACK)
         st = ctx.solve_linear(mp.LAPACK, form, b=G)
         y = ctx.fe_get("y")
-        assert rel_err(y, y_ref) < 1e-9, (form, rel_err(y, y_ref))
+        assert rel_err(y, y_ref) < 1e-9, (form, mf, rel_err(y, y_ref))
         assert st.linear_residual < 1e-12 * max(1.0, np.abs(G).max())
         ctx.fe_set("d", d0)
         ctx.fe_set("F1", zero)
