@@ -291,10 +291,29 @@ __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, in
     }
 }
 
+// kout (or null): the first fused chain step's copy of column block k0 in rows
+// [k0 + kb, jend), [rows][64] (see k_ldlt_step_tc); kb is then 64, so every
+// 16-byte vector of a row is whole and aligned (ld a multiple of 32, k0 of 64).
 template <typename T>
 __global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
-                                                   T *b, unsigned long long *flags) {
+                                                   T *b, unsigned long long *flags, T *kout, int jend) {
     chain_enter();
+    if (kout) {  // at most 3 x 64 rows of 64 values: every load issued before the stores
+        const int k1 = k0 + kb, rows = jend - k1;
+        constexpr int V = 16 / sizeof(T), PER = 3 * NB * NB / V / 256;  // 16-byte vectors a thread
+        using Vec = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+        Vec v[PER];
+#pragma unroll
+        for (int i = 0; i < PER; i++) {
+            const int idx = threadIdx.x + 256 * i, r = idx / (NB / V), c = (idx % (NB / V)) * V;
+            if (r < rows && c < kb) v[i] = *reinterpret_cast<const Vec *>(A + (long long)(k1 + r) * ld + k0 + c);
+        }
+#pragma unroll
+        for (int i = 0; i < PER; i++) {
+            const int idx = threadIdx.x + 256 * i, r = idx / (NB / V), c = (idx % (NB / V)) * V;
+            if (r < rows && c < kb) *reinterpret_cast<Vec *>(kout + (size_t)r * NB + c) = v[i];
+        }
+    }
     diag_block<T>(n, ld, A, k0, kb, dvec, Linv, b, flags);
 }
 
@@ -1389,10 +1408,268 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols_tc(int n, long long ld
     fused_next_diag<float>(n, ld, A, nd, &sL[0][0]);
 }
 
+// One step of the 64-wide chain of the FP32 factor inside a 256-wide panel, in
+// one launch: the panel of block k (rows [k1, n)), the in-panel column update
+// of columns [k1, jend) and the diagonal factor of block k1.  CTA b takes the
+// row block i0 = k1 + 64 b:
+//   W_ik = A_ik Linv_k^T and L_ik = W_ik D_k^-1 (written over A_ik), b_i -= L_ik z_k;
+//   A_ij -= L_ik W_jk^T for each panel column block j0 = k1 + 64 c <= i0, with
+//   W_jk its own for j0 == i0 and otherwise formed again from kin, the copy of
+//   A_jk taken before this launch (the CTA of row block j overwrites A_jk with
+//   L_jk meanwhile); the same arithmetic gives the same W_jk bit for bit;
+//   the updated tiles of column block k1 in rows [k1 + 64, jend) go to kout,
+//   the next step's kin;
+//   CTA 0 then factors block k1 from its updated tile (NextDiag).
+// Against a panel launch followed by a column-update launch, the chain loses a
+// launch and the panel's wait per block: the next diagonal factor starts once
+// CTA 0's own row block is done.  Shared memory: Linv_k, A_ik (then a copied
+// A_jk), L_ik (then the next diagonal tile), W_ik, W_jk, and D_k, z_k and the b
+// sums.
+constexpr size_t STEP_TC_SMEM = sizeof(float) * (5 * NB * MS + 4 * NB);
+template <int TERMS>
+__global__ void __launch_bounds__(256) k_ldlt_step_tc(int n, long long ld, float *A, int k0, int kb,
+                                                      const float *dvec, const float *Linv, float *W, int ldw,
+                                                      float *b, int k1, int jend, const float *kin, float *kout,
+                                                      NextDiag nd) {
+    chain_enter();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float(*sI)[MS] = reinterpret_cast<float(*)[MS]>(smem_raw);
+    float(*sA)[MS] = sI + NB;
+    float(*sL)[MS] = sA + NB;
+    float(*sWo)[MS] = sL + NB;
+    float(*sY)[MS] = sWo + NB;
+    float *sd = reinterpret_cast<float *>(sY + NB);
+    float *sz = sd + NB;
+    float(*sbs)[NB] = reinterpret_cast<float(*)[NB]>(sz + NB);  // [2][64]
+    const int ib = blockIdx.x, i0 = k1 + 64 * ib, t = threadIdx.x;
+    {
+        float va[16], vi[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int idx = q * 256 + t, r = idx >> 6, c = idx & 63, row = i0 + r;
+            va[q] = (row < n && c < kb) ? A[(long long)row * ld + k0 + c] : 0.f;
+            vi[q] = (r < kb && c < kb) ? __ldg(&Linv[r * NB + c]) : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int idx = q * 256 + t;
+            sA[idx >> 6][idx & 63] = va[q];
+            sI[idx >> 6][idx & 63] = vi[q];
+        }
+    }
+    if (t < NB) {
+        sd[t] = t < kb ? dvec[k0 + t] : 1.f;
+        sz[t] = (b && t < kb) ? b[k0 + t] : 0.f;
+    }
+    __syncthreads();
+    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
+    const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
+    {
+        float acc[4][4] = {};
+        warp_mma_64<TERMS>(sA, sI, m0, n0, acc);
+        float bsum[2] = {0.f, 0.f};  // rows m0 + g and m0 + g + 8
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int rr = m0 + g + (e >> 1) * 8, c = n0 + 8 * nt + 2 * tq + (e & 1), row = i0 + rr;
+                const float wv = acc[nt][e];
+                const float lv = wv / sd[c];
+                sWo[rr][c] = wv;
+                sL[rr][c] = lv;
+                if (row < n && c < kb) {
+                    W[(long long)row * ldw + c] = wv;
+                    A[(long long)row * ld + k0 + c] = lv;
+                    bsum[e >> 1] += lv * sz[c];
+                }
+            }
+        if (b) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                float v = bsum[h];
+                v += __shfl_xor_sync(0xffffffffu, v, 1);
+                v += __shfl_xor_sync(0xffffffffu, v, 2);
+                if (tq == 0) sbs[w & 1][m0 + g + 8 * h] = v;
+            }
+        }
+    }
+    __syncthreads();  // sL and sWo complete, sA free
+    if (b && t < NB && i0 + t < n) b[i0 + t] -= sbs[0][t] + sbs[1][t];
+    const int nj = jend > k1 ? (jend - k1 + 63) / 64 : 0;
+    for (int jb = 0; jb < nj && jb <= ib; jb++) {
+        const int j0 = k1 + 64 * jb;
+        const float(*Wj)[MS] = sWo;
+        if (jb != ib) {  // W_jk from the copy of A_jk
+            float va[16];
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
+                va[q] = (j0 + r < jend && c < kb) ? kin[((size_t)jb * NB + r) * NB + c] : 0.f;
+            }
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const int idx = q * 256 + t;
+                sA[idx >> 6][idx & 63] = va[q];
+            }
+            __syncthreads();
+            float accw[4][4] = {};
+            warp_mma_64<TERMS>(sA, sI, m0, n0, accw);
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    sY[m0 + g + (e >> 1) * 8][n0 + 8 * nt + 2 * tq + (e & 1)] = accw[nt][e];
+            __syncthreads();
+            Wj = sY;
+        }
+        float acc[4][4] = {};
+        warp_mma_64<TERMS>(sL, Wj, m0, n0, acc);
+        const bool keep = jb == 0 && owns_next_diag<float>(nd);  // CTA 0: the next diagonal tile, into sA
+        const bool tocopy = jb == 0 && ib >= 1 && i0 < jend;    // the next step's copy of column block k1
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int ii = m0 + g + (e >> 1) * 8, jj = n0 + 8 * nt + 2 * tq + (e & 1), i = i0 + ii, j = j0 + jj;
+                if (i < n && j < jend && j <= i) {
+                    const float v = A[(long long)i * ld + j] - acc[nt][e];
+                    A[(long long)i * ld + j] = v;
+                    if (keep) sA[ii][jj] = v;
+                    if (tocopy) kout[((size_t)(ib - 1) * NB + ii) * NB + jj] = v;
+                }
+            }
+        __syncthreads();  // sA and sY are reused by the next column block
+    }
+    fused_next_diag<float>(n, ld, A, nd, &sA[0][0]);
+}
+
+// The FP64 factor's fused chain step: k_ldlt_step_tc's structure with the
+// products of k_ldlt_panel_dmma / k_ldlt_update_cols_dmma (mma.sync m8n8k4 f64;
+// warp w: rows 16(w/2) .. +15, columns 32(w%2) .. +31 as 2 x 4 tiles of 8 x 8).
+__device__ __forceinline__ void warp_dmma_64(const double (*sa)[MS], const double (*sb)[MS], int m0, int n0,
+                                             double (&acc)[2][4][2]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+#pragma unroll 4
+    for (int kk = 0; kk < NB; kk += 4) {
+        const double a0 = sa[m0 + g][kk + tq], a1 = sa[m0 + 8 + g][kk + tq];
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            const double bv = sb[n0 + 8 * nt + g][kk + tq];
+            dmma_8x8x4(acc[0][nt][0], acc[0][nt][1], a0, bv);
+            dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a1, bv);
+        }
+    }
+}
+constexpr size_t STEP_DMMA_SMEM = sizeof(double) * (5 * NB * MS + 4 * NB);
+__global__ void __launch_bounds__(256) k_ldlt_step_dmma(int n, long long ld, double *A, int k0, int kb,
+                                                        const double *dvec, const double *Linv, double *W, int ldw,
+                                                        double *b, int k1, int jend, const double *kin, double *kout,
+                                                        NextDiag nd) {
+    chain_enter();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double(*sI)[MS] = reinterpret_cast<double(*)[MS]>(smem_raw);
+    double(*sA)[MS] = sI + NB;
+    double(*sL)[MS] = sA + NB;
+    double(*sWo)[MS] = sL + NB;
+    double(*sY)[MS] = sWo + NB;
+    double *sd = reinterpret_cast<double *>(sY + NB);
+    double *sz = sd + NB;
+    double(*sbs)[NB] = reinterpret_cast<double(*)[NB]>(sz + NB);  // [2][64]
+    const int ib = blockIdx.x, i0 = k1 + 64 * ib, t = threadIdx.x;
+    for (int q = 0; q < 16; q++) {
+        const int idx = q * 256 + t, r = idx >> 6, c = idx & 63, row = i0 + r;
+        sA[r][c] = (row < n && c < kb) ? A[(long long)row * ld + k0 + c] : 0.0;
+        sI[r][c] = (r < kb && c < kb) ? __ldg(&Linv[r * NB + c]) : 0.0;
+    }
+    if (t < NB) {
+        sd[t] = t < kb ? dvec[k0 + t] : 1.0;
+        sz[t] = (b && t < kb) ? b[k0 + t] : 0.0;
+    }
+    __syncthreads();
+    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
+    const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
+    {
+        double acc[2][4][2] = {};
+        warp_dmma_64(sA, sI, m0, n0, acc);
+        double bsum[2] = {0.0, 0.0};  // rows m0 + g and m0 + 8 + g
+#pragma unroll
+        for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int rr = m0 + 8 * mi + g, c = n0 + 8 * nt + 2 * tq + e, row = i0 + rr;
+                    const double wv = acc[mi][nt][e];
+                    const double lv = wv / sd[c];
+                    sWo[rr][c] = wv;
+                    sL[rr][c] = lv;
+                    if (row < n && c < kb) {
+                        W[(long long)row * ldw + c] = wv;
+                        A[(long long)row * ld + k0 + c] = lv;
+                        bsum[mi] += lv * sz[c];
+                    }
+                }
+        if (b) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                double v = bsum[h];
+                v += __shfl_xor_sync(0xffffffffu, v, 1);
+                v += __shfl_xor_sync(0xffffffffu, v, 2);
+                if (tq == 0) sbs[w & 1][m0 + 8 * h + g] = v;
+            }
+        }
+    }
+    __syncthreads();
+    if (b && t < NB && i0 + t < n) b[i0 + t] -= sbs[0][t] + sbs[1][t];
+    const int nj = jend > k1 ? (jend - k1 + 63) / 64 : 0;
+    for (int jb = 0; jb < nj && jb <= ib; jb++) {
+        const int j0 = k1 + 64 * jb;
+        const double(*Wj)[MS] = sWo;
+        if (jb != ib) {
+            for (int q = 0; q < 16; q++) {
+                const int idx = q * 256 + t, r = idx >> 6, c = idx & 63;
+                sA[r][c] = (j0 + r < jend && c < kb) ? kin[((size_t)jb * NB + r) * NB + c] : 0.0;
+            }
+            __syncthreads();
+            double accw[2][4][2] = {};
+            warp_dmma_64(sA, sI, m0, n0, accw);
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+                for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                    for (int e = 0; e < 2; e++) sY[m0 + 8 * mi + g][n0 + 8 * nt + 2 * tq + e] = accw[mi][nt][e];
+            __syncthreads();
+            Wj = sY;
+        }
+        double acc[2][4][2] = {};
+        warp_dmma_64(sL, Wj, m0, n0, acc);
+        const bool keep = jb == 0 && owns_next_diag<double>(nd);
+        const bool tocopy = jb == 0 && ib >= 1 && i0 < jend;
+#pragma unroll
+        for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int ii = m0 + 8 * mi + g, jj = n0 + 8 * nt + 2 * tq + e, i = i0 + ii, j = j0 + jj;
+                    if (i < n && j < jend && j <= i) {
+                        const double v = A[(long long)i * ld + j] - acc[mi][nt][e];
+                        A[(long long)i * ld + j] = v;
+                        if (keep) sA[ii][jj] = v;
+                        if (tocopy) kout[((size_t)(ib - 1) * NB + ii) * NB + jj] = v;
+                    }
+                }
+        __syncthreads();
+    }
+    fused_next_diag<double>(n, ld, A, nd, &sA[0][0]);
+}
+
 template <typename T>
 struct LdltWork {
     T *dvec, *W;
     T *s;                    // [NB]; s[0]: the inverse operand scale of an FP16 trailing update
+    T *ktile;                // [2][3][NB][NB] copies of a column block's tiles in a panel (fused chain steps)
     T *Linv;                 // [blocks][NB][NB] inverses of the diagonal blocks' L (the solves use them)
     T *Mc;                   // [4][blocks][NB][NB] coupling blocks: forward, backward at distance 1, then 2
     unsigned long long *ll;  // [2][blocks][2][NB] words the two solves publish their blocks in
@@ -1519,11 +1796,17 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                              (int)tc::smem_bytes(tc::MODE_TF32X3));
         cudaFuncSetAttribute(tc::k_update_tc<tc::MODE_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)tc::smem_bytes(tc::MODE_F16));
+        cudaFuncSetAttribute(tc::k_update_tc_tma<tc::MODE_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tc::smem_bytes_tma());
+        cudaFuncSetAttribute(tc::k_update_tc_tma<tc::MODE_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tc::smem_bytes_tma());
         wavefront_attrs<float>();
         wavefront_attrs<double>();
+        cudaFuncSetAttribute(k_ldlt_step_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)STEP_DMMA_SMEM);
         for (const void *f : {(const void *)k_ldlt_panel_tc<1>, (const void *)k_ldlt_panel_tc<3>,
                               (const void *)k_ldlt_panel_dmma, (const void *)k_ldlt_update_cols_dmma,
-                              (const void *)k_ldlt_update_cols_tc<1>, (const void *)k_ldlt_update_cols_tc<3>})
+                              (const void *)k_ldlt_update_cols_tc<1>, (const void *)k_ldlt_update_cols_tc<3>,
+                              (const void *)k_ldlt_step_tc<1>, (const void *)k_ldlt_step_tc<3>})
             cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         ctx->ldlt_attr = true;
     }
@@ -1535,7 +1818,8 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         int mk;
         if (!diag_done) {
             mk = kt_begin(ctx, MP_KT_DIAG, 0);
-            MP_CUDA(ctx, launch_chain(k_ldlt_diag<T>, dim3(1), 0, st, n, ld, A, k0, kb, w.dvec, Li, b, flags));
+            MP_CUDA(ctx, launch_chain(k_ldlt_diag<T>, dim3(1), 0, st, n, ld, A, k0, kb, w.dvec, Li, b, flags,
+                                      (T *)nullptr, 0));
             ++ctx->launches;
             kt_end(ctx, mk);
         }
@@ -1624,6 +1908,18 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         }
         if (!ok) return fail(ctx, MP_ERR_CUDA, "cuTensorMapEncodeTiled failed for the tensor-core update");
         const int grid = (int)std::min<long long>(ntiles, (long long)ctx->sm_count);
+        if (!split) {  // single-product modes: the old values of A move by TMA
+            CUtensorMap mC;
+            if (!operand_map(&mC, Af, n, ld, tc::TILE, n))
+                return fail(ctx, MP_ERR_CUDA, "cuTensorMapEncodeTiled failed for the tensor-core update");
+            auto kt = mode == tc::MODE_F16 ? tc::k_update_tc_tma<tc::MODE_F16> : tc::k_update_tc_tma<tc::MODE_TF32>;
+            const int mk = kt_begin(ctx, MP_KT_UPDATE, update_flops(R0, C1, K));
+            kt<<<grid, tc::THREADS_TMA, tc::smem_bytes_tma(), st>>>(mLh, mWh, mC, n, R0, ntiles, K / tc::kc_of(mode),
+                                                                     cb, reinterpret_cast<const float *>(w.s), flags),
+                ++ctx->launches;
+            kt_end(ctx, mk);
+            return MP_OK;
+        }
         auto kern = mode == tc::MODE_F16 ? tc::k_update_tc<tc::MODE_F16>
                     : split            ? tc::k_update_tc<tc::MODE_TF32X3>
                                        : tc::k_update_tc<tc::MODE_TF32>;
@@ -1649,9 +1945,45 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             for (int P0 = S0; P0 < S1; P0 += PANEL_W) {
                 const int P1 = P0 + PANEL_W < S1 ? P0 + PANEL_W : S1;
                 bool diag_done = false;
-                for (int k0 = P0; k0 < P1; k0 += NB) {
+                for (int k0 = P0, step = 0; k0 < P1; k0 += NB, step++) {
                     const int kb = P1 - k0 < NB ? P1 - k0 : NB;
                     const int k1 = k0 + kb;
+                    if (w.ktile) {
+                        // fused chain steps: one launch per block (k_ldlt_step_tc / k_ldlt_step_dmma)
+                        T *kin = w.ktile + (size_t)(step & 1) * 3 * NB * NB;
+                        T *kout = w.ktile + (size_t)((step + 1) & 1) * 3 * NB * NB;
+                        T *Li = w.Linv + (size_t)(k0 / NB) * NB * NB;
+                        if (!diag_done) {
+                            const int mk = kt_begin(ctx, MP_KT_DIAG, 0);
+                            MP_CUDA(ctx, launch_chain(k_ldlt_diag<T>, dim3(1), 0, st, n, ld, A, k0, kb, w.dvec, Li, b,
+                                                      flags, k1 < P1 ? kin : (T *)nullptr, P1));
+                            ++ctx->launches;
+                            kt_end(ctx, mk);
+                        }
+                        diag_done = false;
+                        if (k1 < n) {
+                            const int kbn = P1 - k1 < NB ? P1 - k1 : NB;
+                            const NextDiag nd{k1 < P1 ? k1 : 0, k1 < P1 ? kbn : 0, w.dvec,
+                                              w.Linv + (size_t)(k1 / NB) * NB * NB, b, flags};
+                            const int mk = kt_begin(ctx, MP_KT_PANEL, 0);
+                            const dim3 gs((n - k1 + 63) / 64);
+                            if constexpr (std::is_same<T, float>::value) {
+                                MP_CUDA(ctx, launch_chain(tc_terms == 3 ? k_ldlt_step_tc<3> : k_ldlt_step_tc<1>, gs,
+                                                          STEP_TC_SMEM, st, n, ld, A, k0, kb, (const float *)w.dvec,
+                                                          (const float *)Li, w.W + (k0 - S0), (int)SUPER_W, b, k1, P1,
+                                                          (const float *)kin, kout, nd));
+                            } else {
+                                MP_CUDA(ctx, launch_chain(k_ldlt_step_dmma, gs, STEP_DMMA_SMEM, st, n, ld, A, k0, kb,
+                                                          (const double *)w.dvec, (const double *)Li,
+                                                          w.W + (k0 - S0), (int)SUPER_W, b, k1, P1,
+                                                          (const double *)kin, kout, nd));
+                            }
+                            ++ctx->launches;
+                            kt_end(ctx, mk);
+                            diag_done = k1 < P1;
+                        }
+                        continue;
+                    }
                     int rc = diag_and_panel(k0, kb, w.W + (k0 - S0), SUPER_W, diag_done);
                     if (rc) return rc;
                     diag_done = false;

@@ -88,6 +88,8 @@ static int check_flags(mp_ctx *ctx, unsigned long long mask, unsigned long long 
 struct SolveScratch {
     double *dvec64 = nullptr, *W64 = nullptr, *s64 = nullptr, *r = nullptr, *Linv64 = nullptr;
     float *dvec32 = nullptr, *W32 = nullptr, *s32 = nullptr, *b32 = nullptr, *Linv32 = nullptr, *split32 = nullptr;
+    float *kt32 = nullptr;              // [2][3][NB][NB] column-block copies of the fused chain steps
+    double *kt64 = nullptr;
     double *Mc64 = nullptr;             // [2][blocks][NB][NB] coupling blocks (FP64 solves, Gauss-Seidel)
     float *Mc32 = nullptr;              // [4][blocks][NB][NB] coupling blocks (FP32 banded solves)
     unsigned long long *ll = nullptr;   // [2][blocks][2][NB] wavefront words
@@ -97,7 +99,7 @@ struct SolveScratch {
 
 static void release(SolveScratch *s) {
     void *p[] = {s->dvec64, s->W64, s->s64, s->r, s->dvec32, s->W32, s->s32, s->b32,
-                 s->Linv64, s->Linv32, s->Mc64, s->Mc32, s->ll, s->split32};
+                 s->Linv64, s->Linv32, s->Mc64, s->Mc32, s->ll, s->split32, s->kt32, s->kt64};
     for (void *q : p)
         if (q) cudaFree(q);
     *s = SolveScratch();
@@ -127,6 +129,8 @@ static int ensure_scratch(mp_ctx *ctx, SolveScratch **out) {
     MP_CUDA(ctx, cudaMalloc(&s.dvec32, sizeof(float) * (n + 64)));
     MP_CUDA(ctx, cudaMalloc(&s.W32, sizeof(float) * (size_t)(n + NB) * SUPER_W));
     MP_CUDA(ctx, cudaMalloc(&s.s32, sizeof(float) * NB));
+    MP_CUDA(ctx, cudaMalloc(&s.kt32, sizeof(float) * 2 * 3 * NB * NB));
+    MP_CUDA(ctx, cudaMalloc(&s.kt64, sizeof(double) * 2 * 3 * NB * NB));
     MP_CUDA(ctx, cudaMalloc(&s.b32, sizeof(float) * (n + 64)));
     const size_t nblk = (n + NB - 1) / NB;
     MP_CUDA(ctx, cudaMalloc(&s.Linv64, sizeof(double) * nblk * NB * NB));
@@ -159,7 +163,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         if (!ctx->J || !ctx->j_current) return fail(ctx, MP_ERR_STATE, "no current FP64 J (build it first)");
         ctx->j_current = false;  // the factorization overwrites J
         MP_CUDA(ctx, cudaMemcpyAsync(ctx->y, ctx->G, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
-        LdltWork<double> w{sc.dvec64, sc.W64, sc.s64, sc.Linv64, sc.Mc64, sc.ll, nullptr};
+        LdltWork<double> w{sc.dvec64, sc.W64, sc.s64, nullptr, sc.Linv64, sc.Mc64, sc.ll, nullptr};
         rc = ldlt_factor_solve<double>(ctx, ctx->J, ld, n, ctx->y, w, true);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
@@ -176,7 +180,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         if (!ctx->j32_current && (rc = fe_j32_from_k(ctx))) return rc;
         ctx->j32_current = false;
         MP_CUDA(ctx, cudaMemsetAsync(ctx->y, 0, sizeof(double) * n, ctx->stream));
-        LdltWork<float> w{sc.dvec32, sc.W32, sc.s32, sc.Linv32, sc.Mc32, sc.ll, sc.split32};
+        LdltWork<float> w{sc.dvec32, sc.W32, sc.s32, sc.kt32, sc.Linv32, sc.Mc32, sc.ll, sc.split32};
         double rn = 0, bn = 0;
         // r = G (y = 0), in FP32 for the first solve, which also factors J32
         rc = resid_norms(ctx, ctx->y, ctx->G, sc.r, sc.b32, &rn, &bn);

@@ -17,7 +17,8 @@
 //                      tcgen05.commit to the stage's "empty" mbarrier (frees it
 //                      for the producer) and, after a tile's last chunk, to the
 //                      accumulator's "full" mbarrier;
-//   warps 2-5          epilogue: tcgen05.ld of their 32 TMEM lanes (= tile rows),
+//   warps 2-17         epilogue: tcgen05.ld of their 32 TMEM lanes (= tile rows),
+//                      64 columns a warp,
 //                      A[row][col] -= acc for col <= row, then arrive on the
 //                      accumulator's "empty" mbarrier.
 // Two accumulators let the epilogue of one tile overlap the MMAs of the next.
@@ -64,7 +65,8 @@ constexpr int CHUNK_W = TILE_N * 128;       // 32 KB: one W operand chunk
 // K elements per chunk: one 128-byte row of 4-byte or 2-byte values
 __host__ __device__ constexpr int kc_of(int mode) { return mode == MODE_F16 ? 64 : 32; }
 __host__ __device__ constexpr int stages(int mode) { return mode == MODE_TF32X3 ? 2 : 4; }  // 192 KB of stages
-constexpr int THREADS = 192;                // producer warp, MMA warp, 4 epilogue warps
+constexpr int EPI_WARPS = 16;               // epilogue: 4 per TMEM lane quadrant, 64 columns each
+constexpr int THREADS = 64 + 32 * EPI_WARPS; // producer warp, MMA warp, epilogue warps
 constexpr long long SPIN_LIMIT = 1ll << 22;
 
 __device__ __forceinline__ unsigned saddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -117,6 +119,21 @@ __device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, int 
         ::"r"(saddr(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(saddr(bar))
         : "memory");
 }
+
+// 2-D tiled TMA store of a shared-memory box to the map at (x, y); completes
+// in this thread's bulk async-group.  Rows and columns past the map's extent
+// are not written.
+__device__ __forceinline__ void tma_store(const CUtensorMap *map, int x, int y, const void *src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<unsigned long long>(map)),
+                 "r"(x), "r"(y), "r"(saddr(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// generic-proxy writes to shared memory made visible to a following TMA store
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 __device__ __forceinline__ void mma_tf32(unsigned tmem_d, unsigned long long a, unsigned long long b, unsigned acc) {
     asm volatile(
@@ -291,7 +308,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         for (int a = 0; a < 2; a++) {
             mbar_init(&acc_full[a], 1);
-            mbar_init(&acc_empty[a], 4 * 32);
+            mbar_init(&acc_empty[a], EPI_WARPS * 32);
         }
         mbar_init(drain, 1);
         // an earlier launch of this factorization timed out: do nothing more
@@ -386,77 +403,68 @@ __global__ void __launch_bounds__(THREADS, 1)
             while (!mbar_try(drain, 0) && ++spins < SPIN_LIMIT) {
             }
         } else if (warp >= 2) {
-            // ---- epilogue: TMEM lanes 32*(warp%4) .. +31 are this warp's tile rows ----
-            // Each thread owns one tile row and walks its 256 columns in four
-            // quarters of 64: the old values of A for a quarter are loaded one
-            // quarter ahead (the first before the accumulator wait), since they do
-            // not depend on the MMAs.
+            // ---- epilogue: EPI_WARPS warps; warp w reads TMEM lanes 32*(w%4) .. +31
+            // (its tile rows, the lanes a warp may access) and owns columns
+            // 64*((w-2)/4) .. +63 of them.  A thread loads the old values of its
+            // row's 64 columns before it waits for the accumulator (they do not
+            // depend on the MMAs), so 16 loads a thread, 128 KB a CTA, are in
+            // flight behind the next tile's MMAs.
             const int q = warp & 3;
             const int r = q * 32 + lane;
+            const int cq = (warp - 2) >> 2;
             const float us = MODE == MODE_F16 ? *unscale : 1.0f;  // a power of two: the products stay exact
             long long lt = 0;
             for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
                 int bi, bj;
                 tile_of(t, colblocks, bi, bj);
                 const long long row = P1 + (long long)bi * TILE + r;
-                const long long c0 = P1 + (long long)bj * TILE_N;
+                const long long c0 = P1 + (long long)bj * TILE_N + 64 * cq;
                 const bool row_ok = row < n;
-                auto load_quarter = [&](int qq, float4 (&dst)[16]) {
+                float4 cur[16];
 #pragma unroll
-                    for (int g = 0; g < 16; g++) {
-                        const long long col = c0 + 64 * qq + 4 * g;
-                        dst[g] = (row_ok && col + 3 <= row && col + 3 < n)
-                                     ? *reinterpret_cast<const float4 *>(A + row * ld + col)
-                                     : make_float4(0.f, 0.f, 0.f, 0.f);
-                    }
-                };
-                float4 cur[16], nxt[16];
-                load_quarter(0, cur);
+                for (int g = 0; g < 16; g++) {
+                    const long long col = c0 + 4 * g;
+                    cur[g] = (row_ok && col + 3 <= row && col + 3 < n)
+                                 ? *reinterpret_cast<const float4 *>(A + row * ld + col)
+                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
                 const int a = (int)(lt & 1);
                 int ok = 1;
                 if (lane == 0) ok = mbar_wait(&acc_full[a], (unsigned)((lt >> 1) & 1), abort);
                 ok = __shfl_sync(0xffffffffu, ok, 0);
                 if (!ok) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const unsigned taddr = tmem + (unsigned)(a * TILE_N) + ((unsigned)(q * 32) << 16);
+                const unsigned taddr = tmem + (unsigned)(a * TILE_N + 64 * cq) + ((unsigned)(q * 32) << 16);
 #pragma unroll
-                for (int qq = 0; qq < 4; qq++) {
-                    if (qq + 1 < 4) load_quarter(qq + 1, nxt);
+                for (int cb = 0; cb < 4; cb++) {
+                    unsigned v[16];
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+                        "%15}, [%16];"
+                        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                          "=r"(v[14]), "=r"(v[15])
+                        : "r"(taddr + cb * 16));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    const long long col = c0 + 16 * cb;
+                    if (row_ok && col <= row) {
+                        float *p = A + row * ld + col;
 #pragma unroll
-                    for (int cb = 0; cb < 4; cb++) {
-                        unsigned v[16];
-                        asm volatile(
-                            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
-                            "%15}, [%16];"
-                            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                              "=r"(v[14]), "=r"(v[15])
-                            : "r"(taddr + qq * 64 + cb * 16));
-                        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                        const long long col = c0 + 64 * qq + 16 * cb;
-                        if (row_ok && col <= row) {
-                            float *p = A + row * ld + col;
+                        for (int g = 0; g < 4; g++) {
+                            const long long cg = col + 4 * g;
+                            if (cg + 3 <= row && cg + 3 < n) {
+                                float4 o = cur[cb * 4 + g];
+                                o.x -= us * __uint_as_float(v[4 * g]);
+                                o.y -= us * __uint_as_float(v[4 * g + 1]);
+                                o.z -= us * __uint_as_float(v[4 * g + 2]);
+                                o.w -= us * __uint_as_float(v[4 * g + 3]);
+                                *reinterpret_cast<float4 *>(p + 4 * g) = o;
+                            } else {
 #pragma unroll
-                            for (int g = 0; g < 4; g++) {
-                                const long long cg = col + 4 * g;
-                                if (cg + 3 <= row && cg + 3 < n) {
-                                    float4 o = cur[cb * 4 + g];
-                                    o.x -= us * __uint_as_float(v[4 * g]);
-                                    o.y -= us * __uint_as_float(v[4 * g + 1]);
-                                    o.z -= us * __uint_as_float(v[4 * g + 2]);
-                                    o.w -= us * __uint_as_float(v[4 * g + 3]);
-                                    *reinterpret_cast<float4 *>(p + 4 * g) = o;
-                                } else {
-#pragma unroll
-                                    for (int j = 0; j < 4; j++)
-                                        if (cg + j <= row && cg + j < n) p[4 * g + j] -= us * __uint_as_float(v[4 * g + j]);
-                                }
+                                for (int j = 0; j < 4; j++)
+                                    if (cg + j <= row && cg + j < n) p[4 * g + j] -= us * __uint_as_float(v[4 * g + j]);
                             }
                         }
-                    }
-                    if (qq + 1 < 4) {
-#pragma unroll
-                        for (int g = 0; g < 16; g++) cur[g] = nxt[g];
                     }
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -469,6 +477,255 @@ __global__ void __launch_bounds__(THREADS, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
     if (threadIdx.x == 0 && *abort == 1) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
+}
+
+// ---- the same update with the old values of A moved by TMA ----------------------------
+// k_update_tc's epilogue reads and writes A row by row: every warp access
+// touches 32 rows, so L1TEX handles 32 sectors a request and becomes the busiest
+// unit of the SM, which also slows the operand TMA that passes through it.  Here
+// A moves in 128-row x 32-column chunks (16 KB, one 128-byte swizzle row per
+// tile row) through a ring of 4 shared-memory slots:
+//   warp 2 (one lane)  C mover: TMA-loads chunk g into slot g % 4 once the slot's
+//                      previous chunk is done, and TMA-stores that chunk back
+//                      (bulk async-group; its shared-memory reads finish before
+//                      the slot is refilled);
+//   warps 3-6          epilogue: per chunk, tcgen05.ld of 32 accumulator columns
+//                      of their TMEM lanes, old value from the slot (the
+//                      swizzled row of the thread's tile row), new value back
+//                      into the slot, proxy fence, arrive on the slot's "done".
+// Chunks wholly right of column n are neither loaded nor stored.
+// The store writes whole chunks: entries above the diagonal of the trailing
+// matrix get (old - acc) as well.  The factorization reads only the lower
+// triangle of A (diagonal factor, panels, updates, solves), so they are never
+// used; rows and columns past n are neither written nor read (TMA clips them).
+// Three operand stages (144 KB) and the four slots (64 KB) fit one SM.
+constexpr int C_SLOTS = 4;
+constexpr int C_CHUNK = TILE * 128;  // 16 KB: 128 rows x 32 FP32
+constexpr int TMA_EPI_STAGES = 3;
+constexpr int THREADS_TMA = 7 * 32;
+template <int MODE>
+__global__ void __launch_bounds__(THREADS_TMA, 1)
+    k_update_tc_tma(const __grid_constant__ CUtensorMap mL, const __grid_constant__ CUtensorMap mW,
+                    const __grid_constant__ CUtensorMap mC, int n, int P1, long long ntiles, int nchunk,
+                    int colblocks, const float *unscale, unsigned long long *flags) {
+    static_assert(MODE == MODE_TF32 || MODE == MODE_F16, "single-product modes only");
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<size_t>(smem_raw) + 1023) & ~size_t(1023));
+    constexpr int STAGES = TMA_EPI_STAGES;
+    constexpr int KCE = kc_of(MODE);
+    constexpr unsigned STAGE_BYTES = CHUNK_L + CHUNK_W;
+    unsigned char *cslot = base + STAGES * STAGE_BYTES;
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(cslot + C_SLOTS * C_CHUNK);
+    unsigned long long *full = bars, *empty = bars + STAGES, *acc_full = bars + 2 * STAGES,
+                       *acc_empty = bars + 2 * STAGES + 2, *drain = bars + 2 * STAGES + 4,
+                       *c_full = bars + 2 * STAGES + 5, *c_done = c_full + C_SLOTS;
+    unsigned *tmem_slot = reinterpret_cast<unsigned *>(c_done + C_SLOTS);
+    volatile int *abort = reinterpret_cast<volatile int *>(tmem_slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 4 * 32);
+        }
+        mbar_init(drain, 1);
+        for (int s = 0; s < C_SLOTS; s++) {
+            mbar_init(&c_full[s], 1);
+            mbar_init(&c_done[s], 4 * 32);
+        }
+        *abort = (*(volatile unsigned long long *)flags & FLAG_LOOKBACK_TIMEOUT) ? 2 : 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(saddr(tmem_slot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = *tmem_slot;
+
+    if (*abort == 0) {
+        if (warp == 0 && lane == 0) {
+            // ---- operand producer ----
+            long long it = 0;
+            bool ok = true;
+            for (long long t = blockIdx.x; ok && t < ntiles; t += gridDim.x) {
+                int bi, bj;
+                tile_of(t, colblocks, bi, bj);
+                for (int kc = 0; kc < nchunk; kc++, it++) {
+                    const int s = (int)(it % STAGES);
+                    const long long u = it / STAGES;
+                    if (u > 0 && !mbar_wait(&empty[s], (unsigned)((u - 1) & 1), abort)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char *st = base + s * STAGE_BYTES;
+                    mbar_expect_tx(&full[s], STAGE_BYTES);
+                    tma_load(st, &mL, kc * KCE, bi * TILE, &full[s]);
+                    tma_load(st + CHUNK_L, &mW, kc * KCE, bj * TILE_N, &full[s]);
+                }
+            }
+            for (long long k = it - STAGES; k < it; k++) {
+                if (k < 0) continue;
+                const int s = (int)(k % STAGES);
+                long long spins = 0;
+                while (!mbar_try(&full[s], (unsigned)((k / STAGES) & 1)) && ++spins < SPIN_LIMIT) {
+                }
+            }
+        } else if (warp == 1 && lane == 0) {
+            // ---- MMA issuer ----
+            long long it = 0, lt = 0;
+            bool ok = true;
+            for (long long t = blockIdx.x; ok && t < ntiles; t += gridDim.x, lt++) {
+                const int a = (int)(lt & 1);
+                const long long v = lt >> 1;
+                if (v > 0 && !mbar_wait(&acc_empty[a], (unsigned)((v - 1) & 1), abort)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const unsigned d = tmem + (unsigned)(a * TILE_N);
+                for (int kc = 0; kc < nchunk; kc++, it++) {
+                    const int s = (int)(it % STAGES);
+                    if (!mbar_wait(&full[s], (unsigned)((it / STAGES) & 1), abort)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const unsigned char *st = base + s * STAGE_BYTES;
+                    const unsigned long long dl = smem_desc(saddr(st)), dw = smem_desc(saddr(st + CHUNK_L));
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++) {
+                        const unsigned accum = (kc > 0 || kk > 0) ? 1u : 0u;
+                        if (MODE == MODE_F16)
+                            mma_f16(d, dl + 2 * kk, dw + 2 * kk, accum);
+                        else
+                            mma_tf32(d, dl + 2 * kk, dw + 2 * kk, accum);
+                    }
+                    mma_commit(&empty[s]);
+                }
+                if (!ok) break;
+                mma_commit(&acc_full[a]);
+            }
+            mma_commit(drain);
+            long long spins = 0;
+            while (!mbar_try(drain, 0) && ++spins < SPIN_LIMIT) {
+            }
+        } else if (warp == 2 && lane == 0) {
+            // ---- C mover ----
+            int xs[C_SLOTS], ys[C_SLOTS];
+            long long g = 0;
+            bool ok = true;
+            for (long long t = blockIdx.x; ok && t < ntiles; t += gridDim.x) {
+                int bi, bj;
+                tile_of(t, colblocks, bi, bj);
+                for (int c = 0; c < TILE_N / 32; c++, g++) {
+                    const int s = (int)(g % C_SLOTS);
+                    const long long u = g / C_SLOTS;
+                    if (u > 0) {  // the slot's previous chunk: done by the epilogue, stored, read out
+                        if (!mbar_wait(&c_done[s], (unsigned)((u - 1) & 1), abort)) {
+                            ok = false;
+                            break;
+                        }
+                        if (xs[s] < n) {
+                            tma_store(&mC, xs[s], ys[s], cslot + s * C_CHUNK);
+                            bulk_commit();
+                            bulk_wait_read0();
+                        }
+                    }
+                    xs[s] = P1 + bj * TILE_N + 32 * c;
+                    ys[s] = P1 + bi * TILE;
+                    if (xs[s] < n) {
+                        mbar_expect_tx(&c_full[s], C_CHUNK);
+                        tma_load(cslot + s * C_CHUNK, &mC, xs[s], ys[s], &c_full[s]);
+                    } else {  // a chunk wholly right of column n: nothing to move, the epilogue runs on
+                        mbar_arrive(&c_full[s]);
+                    }
+                }
+            }
+            // the ring's last chunks: stored once done; loads of an aborted run landed
+            for (long long k = g - C_SLOTS; k < g; k++) {
+                if (k < 0) continue;
+                const int s = (int)(k % C_SLOTS);
+                if (ok && mbar_wait(&c_done[s], (unsigned)((k / C_SLOTS) & 1), abort)) {
+                    if (xs[s] < n) {
+                        tma_store(&mC, xs[s], ys[s], cslot + s * C_CHUNK);
+                        bulk_commit();
+                    }
+                } else {
+                    ok = false;
+                    long long spins = 0;
+                    while (!mbar_try(&c_full[s], (unsigned)((k / C_SLOTS) & 1)) && ++spins < SPIN_LIMIT) {
+                    }
+                }
+            }
+            bulk_wait0();
+        } else if (warp >= 3) {
+            // ---- epilogue: TMEM lanes 32*(warp%4) .. +31 are this warp's tile rows ----
+            const int q = warp & 3;
+            const int r = q * 32 + lane;
+            const float us = MODE == MODE_F16 ? *unscale : 1.0f;  // a power of two: the products stay exact
+            long long lt = 0, g = 0;
+            bool ok = true;
+            for (long long t = blockIdx.x; ok && t < ntiles; t += gridDim.x, lt++) {
+                const int a = (int)(lt & 1);
+                int w = 1;
+                if (lane == 0) w = mbar_wait(&acc_full[a], (unsigned)((lt >> 1) & 1), abort);
+                if (!__shfl_sync(0xffffffffu, w, 0)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const unsigned taddr = tmem + (unsigned)(a * TILE_N) + ((unsigned)(q * 32) << 16);
+                for (int c = 0; c < TILE_N / 32; c++, g++) {
+                    const int s = (int)(g % C_SLOTS);
+                    int wc = 1;
+                    if (lane == 0) wc = mbar_wait(&c_full[s], (unsigned)((g / C_SLOTS) & 1), abort);
+                    if (!__shfl_sync(0xffffffffu, wc, 0)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned v[32];
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                          "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                          "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                        : "r"(taddr + 32 * c));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    // row r of the slot: 128 bytes, 16-byte unit j stored at j ^ (r % 8) (128-byte swizzle)
+                    unsigned char *rowp = cslot + s * C_CHUNK + r * 128;
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        float4 *p = reinterpret_cast<float4 *>(rowp + ((j ^ (r & 7)) << 4));
+                        float4 o = *p;
+                        o.x -= us * __uint_as_float(v[4 * j]);
+                        o.y -= us * __uint_as_float(v[4 * j + 1]);
+                        o.z -= us * __uint_as_float(v[4 * j + 2]);
+                        o.w -= us * __uint_as_float(v[4 * j + 3]);
+                        *p = o;
+                    }
+                    fence_proxy_async();
+                    mbar_arrive(&c_done[s]);
+                }
+                if (!ok) break;
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                mbar_arrive(&acc_empty[a]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+    if (threadIdx.x == 0 && *abort == 1) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
+}
+// stages, C slots, barriers, TMEM slot, abort flag + 1024-byte alignment slack
+constexpr size_t smem_bytes_tma() {
+    return (size_t)TMA_EPI_STAGES * (CHUNK_L + CHUNK_W) + (size_t)C_SLOTS * C_CHUNK + 256 + 1024;
 }
 
 // operand stages + barriers, TMEM slot, abort flag + 1024-byte alignment slack
