@@ -163,7 +163,7 @@ int fe_solve_ldlt(mp_ctx *ctx, int form, mp_newton_stats *st) {
         if (!ctx->J || !ctx->j_current) return fail(ctx, MP_ERR_STATE, "no current FP64 J (build it first)");
         ctx->j_current = false;  // the factorization overwrites J
         MP_CUDA(ctx, cudaMemcpyAsync(ctx->y, ctx->G, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
-        LdltWork<double> w{sc.dvec64, sc.W64, sc.s64, nullptr, sc.Linv64, sc.Mc64, sc.ll, nullptr};
+        LdltWork<double> w{sc.dvec64, sc.W64, sc.s64, sc.kt64, sc.Linv64, sc.Mc64, sc.ll, nullptr};
         rc = ldlt_factor_solve<double>(ctx, ctx->J, ld, n, ctx->y, w, true);
         if (rc) return rc;
         cudaEventRecord(ctx->t1.b, ctx->stream);
