@@ -77,7 +77,7 @@ KT_NAMES = {mp.KT_PUSH: "push", mp.KT_UPDATE: "trailing_update", mp.KT_DIAG: "di
 KT_KERNEL = {mp.KT_PUSH: {mp.FP64: "k_push_fp64", mp.MIXED: "k_push_mixed"},
              mp.KT_UPDATE: {mp.FP64: "k_update_f64_mma (FP64 mma.sync m8n8k4)", mp.MIXED: "tc::k_update_tc (tcgen05)"},
              mp.KT_DIAG: {mp.FP64: "k_ldlt_diag<double>", mp.MIXED: "k_ldlt_diag<float>"},
-             mp.KT_PANEL: {mp.FP64: "k_ldlt_panel<double>", mp.MIXED: "k_ldlt_panel<float>"},
+             mp.KT_PANEL: {mp.FP64: "k_ldlt_step_dmma", mp.MIXED: "k_ldlt_step_tc"},
              mp.KT_TRSV: {mp.FP64: "k_trsv_ll<double>", mp.MIXED: "k_trsv_ll<float>"}}
 
 

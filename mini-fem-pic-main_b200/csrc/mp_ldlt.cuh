@@ -86,7 +86,16 @@ __device__ __forceinline__ void load4p(const T *p, T *v) {
 //             Linv rows become L_P^-1 (rows) and every later row subtracts
 //             sum_m l_im (that row m); b likewise.  The owners of the step's
 //             columns keep l_im there (L), the pivot owner L_P and D_P.
-// Shared buffers alternate between steps, so one barrier a step suffices.
+// The steps run as a dataflow, not in lock step: every step has its own
+// shared-memory buffers and an mbarrier.  A warp holds two column tiles of all
+// row tiles, so the publishers of step jj are warps 0 .. jj/2 (the columns,
+// the pivot, Linv's rows and b); each of their lanes arrives on the step's
+// mbarrier after its writes, and every thread waits on it before it
+// eliminates.  A warp publishes step jj only after eliminating step jj-1, so
+// the chain from one pivot to the next runs through the warp that owns the
+// next column while the other warps' updates trail behind, instead of the
+// whole CTA meeting at a barrier every step.  Waits are bounded (a wait that
+// gives up raises FLAG_LOOKBACK_TIMEOUT).
 template <typename T>
 __device__ __forceinline__ void ld4s(const T *p, T (&v)[4]) {
     if constexpr (sizeof(T) == 8) {
@@ -107,18 +116,32 @@ __device__ __forceinline__ void st4s(T *p, const T (&v)[4]) {
     }
 }
 
+// One step's published data.
+template <typename T>
+struct __align__(16) DiagStep {
+    T col[NB][4];  // the step's four columns, every row
+    T row[4][NB];  // Linv's rows j0 .. j0+3, every column
+    T piv[4][4];   // the factored pivot block: L_P below the diagonal, D_P on it
+    T rd[4];       // 1 / D_P
+    T bp[4];       // b_j0 .. b_j0+3
+};
+// shared scratch of diag_block: the 16 steps' buffers, then their mbarriers
+template <typename T>
+__host__ __device__ constexpr size_t diag_scratch() {
+    return (size_t)(NB / 4) * sizeof(DiagStep<T>) + (NB / 4) * sizeof(unsigned long long);
+}
+constexpr long long DIAG_SPIN_LIMIT = 1ll << 22;
+
 // The block is read with coherent loads, or from stile (shared memory, row
-// pitch MS) where the in-panel column update of the previous block, whose CTA
-// has just updated the block, hands it over (k_ldlt_update_cols_*, kbn > 0).
-// All 256 threads of the CTA call it.
+// pitch MS) where the chain step that has just updated it hands it over.
+// scratch: diag_scratch<T>() bytes of shared memory, 16-byte aligned.  All 256
+// threads of the CTA call it.
 template <typename T>
 __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv, T *b,
-                                           unsigned long long *flags, const T *stile = nullptr) {
-    __shared__ __align__(16) T scol[2][NB][4];  // the step's four columns, every row
-    __shared__ __align__(16) T srow[2][4][NB];  // Linv's rows j0 .. j0+3, every column
-    __shared__ __align__(16) T spiv[2][4][4];   // the factored pivot block: L_P below the diagonal, D_P on it
-    __shared__ __align__(16) T srd[2][4];       // 1 / D_P
-    __shared__ __align__(16) T sbp[2][4];       // b_j0 .. b_j0+3
+                                           unsigned long long *flags, unsigned char *scratch,
+                                           const T *stile = nullptr) {
+    DiagStep<T> *steps = reinterpret_cast<DiagStep<T> *>(scratch);
+    unsigned long long *pub = reinterpret_cast<unsigned long long *>(steps + NB / 4);
     // a warp holds two column tiles (tc) of all 16 row tiles (ti), so the
     // column-dependent branches of a step (update the block, or Linv) are
     // uniform over a warp
@@ -142,13 +165,16 @@ __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, in
         }
         bb[u] = (b && tc == 0 && r < kb) ? __ldcg(&b[k0 + r]) : T(0);
     }
-    bool singular = false;
+    if (t == 0)
+        for (int jj = 0; jj < NB / 4; jj++) mp::tc::mbar_init(&pub[jj], 32 * (jj / 2 + 1));
+    __syncthreads();
+    bool singular = false, stalled = false;
     for (int jj = 0; jj < NB / 4; jj++) {
-        const int buf = jj & 1;
+        DiagStep<T> &S = steps[jj];
         // ---- publish ----
         if (tc == jj) {
 #pragma unroll
-            for (int u = 0; u < 4; u++) st4s<T>(scol[buf][4 * ti + u], a[u]);
+            for (int u = 0; u < 4; u++) st4s<T>(S.col[4 * ti + u], a[u]);
             if (ti == jj) {
                 T P[4][4], rd[4];
 #pragma unroll
@@ -175,21 +201,23 @@ __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, in
                     }
                 }
 #pragma unroll
-                for (int m = 0; m < 4; m++) st4s<T>(spiv[buf][m], P[m]);
-                st4s<T>(srd[buf], rd);
+                for (int m = 0; m < 4; m++) st4s<T>(S.piv[m], P[m]);
+                st4s<T>(S.rd, rd);
             }
         }
         if (ti == jj) {
 #pragma unroll
-            for (int m = 0; m < 4; m++) st4s<T>(&srow[buf][m][4 * tc], li[m]);
-            if (tc == 0) st4s<T>(sbp[buf], bb);
+            for (int m = 0; m < 4; m++) st4s<T>(&S.row[m][4 * tc], li[m]);
+            if (tc == 0) st4s<T>(S.bp, bb);
         }
-        __syncthreads();
+        if ((t >> 5) <= jj / 2) mp::tc::mbar_arrive(&pub[jj]);  // this warp's part of step jj is written
+        for (long long i = 0; !stalled && !mp::tc::mbar_try(&pub[jj], 0); i++)
+            if (i > DIAG_SPIN_LIMIT) stalled = true;
         // ---- eliminate ----
         T lp[4][4], rd[4];
 #pragma unroll
-        for (int m = 0; m < 4; m++) ld4s<T>(spiv[buf][m], lp[m]);
-        ld4s<T>(srd[buf], rd);
+        for (int m = 0; m < 4; m++) ld4s<T>(S.piv[m], lp[m]);
+        ld4s<T>(S.rd, rd);
         // z = L_P^-1 x (L_P unit lower, from lp's strict lower part)
         auto fwd = [&](const T (&x)[4], T (&z)[4]) {
             z[0] = x[0];
@@ -203,7 +231,7 @@ __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, in
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 T x[4], z[4];
-                ld4s<T>(scol[buf][4 * ti + u], x);
+                ld4s<T>(S.col[4 * ti + u], x);
                 fwd(x, z);
 #pragma unroll
                 for (int m = 0; m < 4; m++) L[u][m] = z[m] * rd[m];
@@ -212,7 +240,7 @@ __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, in
 #pragma unroll
                 for (int v = 0; v < 4; v++) {
                     T x[4], z[4];
-                    ld4s<T>(scol[buf][4 * tc + v], x);
+                    ld4s<T>(S.col[4 * tc + v], x);
                     fwd(x, z);
 #pragma unroll
                     for (int u = 0; u < 4; u++)
@@ -224,7 +252,7 @@ __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, in
         if (tc <= jj) {  // Linv's rows j0.. are zero right of column j0+3
             T R[4][4];
 #pragma unroll
-            for (int m = 0; m < 4; m++) ld4s<T>(&srow[buf][m][4 * tc], R[m]);
+            for (int m = 0; m < 4; m++) ld4s<T>(&S.row[m][4 * tc], R[m]);
 #pragma unroll
             for (int v = 0; v < 4; v++) {
                 R[1][v] = fma(-R[0][v], lp[1][0], R[1][v]);
@@ -247,7 +275,7 @@ __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, in
         }
         if (tc == 0 && ti >= jj) {
             T x[4], z[4];
-            ld4s<T>(sbp[buf], x);
+            ld4s<T>(S.bp, x);
             fwd(x, z);
             if (rowact) {
 #pragma unroll
@@ -274,6 +302,7 @@ __device__ __forceinline__ void diag_block(int n, long long ld, T *A, int k0, in
         }
     }
     if (singular) atomicOr(flags, FLAG_SINGULAR);
+    if (stalled) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
 #pragma unroll
     for (int u = 0; u < 4; u++) {
         const int r = 4 * ti + u;
@@ -298,6 +327,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, int k0, int kb, T *dvec, T *Linv,
                                                    T *b, unsigned long long *flags, T *kout, int jend) {
     chain_enter();
+    extern __shared__ __align__(16) unsigned char smem_raw[];  // diag_scratch<T>()
     if (kout) {  // at most 3 x 64 rows of 64 values: every load issued before the stores
         const int k1 = k0 + kb, rows = jend - k1;
         constexpr int V = 16 / sizeof(T), PER = 3 * NB * NB / V / 256;  // 16-byte vectors a thread
@@ -314,7 +344,7 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int n, long long ld, T *A, in
             if (r < rows && c < kb) *reinterpret_cast<Vec *>(kout + (size_t)r * NB + c) = v[i];
         }
     }
-    diag_block<T>(n, ld, A, k0, kb, dvec, Linv, b, flags);
+    diag_block<T>(n, ld, A, k0, kb, dvec, Linv, b, flags, smem_raw);
 }
 
 // The next block's diagonal factor, run by the CTA of an in-panel column
@@ -329,13 +359,15 @@ template <typename T>
 __device__ __forceinline__ bool owns_next_diag(const NextDiag &nd) {
     return nd.kb > 0 && blockIdx.x == 0 && blockIdx.y == 0;
 }
-// stile: the updated tile in shared memory (row pitch MS), lower part
+// stile: the updated tile in shared memory (row pitch MS), lower part;
+// scratch: diag_scratch<T>() bytes of free shared memory
 template <typename T>
-__device__ __forceinline__ void fused_next_diag(int n, long long ld, T *A, const NextDiag &nd, const T *stile) {
+__device__ __forceinline__ void fused_next_diag(int n, long long ld, T *A, const NextDiag &nd, const T *stile,
+                                                unsigned char *scratch) {
     if (owns_next_diag<T>(nd)) {
         __syncthreads();  // the tile is complete in shared memory
         diag_block<T>(n, ld, A, nd.k0, nd.kb, static_cast<T *>(nd.dvec), static_cast<T *>(nd.Linv),
-                      static_cast<T *>(nd.b), nd.flags, stile);
+                      static_cast<T *>(nd.b), nd.flags, scratch, stile);
     }
 }
 
@@ -1170,244 +1202,6 @@ __device__ __forceinline__ void warp_mma_64(const float (*sa)[MS], const float (
     }
 }
 
-// Panel of the FP32 factor (rows [r0, r0+64) below the diagonal block):
-// W = A_ik Linv^T, L_ik = W D^-1, b_i -= L_ik z_k.  Warp w takes
-// rows 16(w/2) .. +15 and columns 32(w%2) .. +31 of the 64 x 64 product.
-template <int TERMS>
-__global__ void __launch_bounds__(256) k_ldlt_panel_tc(int n, long long ld, float *A, int k0, int kb,
-                                                       const float *dvec, const float *Linv, float *W, int ldw,
-                                                       float *b) {
-    chain_enter();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float(*sA)[MS] = reinterpret_cast<float(*)[MS]>(smem_raw);
-    float(*sI)[MS] = sA + NB;
-    float *sd = reinterpret_cast<float *>(sI + NB);
-    float *sz = sd + NB;
-    float(*sbs)[NB] = reinterpret_cast<float(*)[NB]>(sz + NB);  // [2][64] the two column halves' b sums
-    const int r0 = k0 + kb + blockIdx.x * 64, t = threadIdx.x;
-    {
-        float va[16], vi[16];
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            const int idx = q * 256 + t, r = idx >> 6, c = idx & 63, row = r0 + r;
-            va[q] = (row < n && c < kb) ? A[(long long)row * ld + k0 + c] : 0.f;
-            vi[q] = (r < kb && c < kb) ? __ldg(&Linv[r * NB + c]) : 0.f;
-        }
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            const int idx = q * 256 + t;
-            sA[idx >> 6][idx & 63] = va[q];
-            sI[idx >> 6][idx & 63] = vi[q];
-        }
-    }
-    if (t < NB) {
-        sd[t] = t < kb ? dvec[k0 + t] : 1.f;
-        sz[t] = (b && t < kb) ? b[k0 + t] : 0.f;
-    }
-    __syncthreads();
-    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
-    const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
-    float acc[4][4] = {};
-    warp_mma_64<TERMS>(sA, sI, m0, n0, acc);
-    float bsum[2] = {0.f, 0.f};  // rows m0 + g and m0 + g + 8
-#pragma unroll
-    for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int rr = m0 + g + (e >> 1) * 8, c = n0 + 8 * nt + 2 * tq + (e & 1), row = r0 + rr;
-            if (row < n && c < kb) {
-                const float wv = acc[nt][e];
-                const float lv = wv / sd[c];
-                W[(long long)row * ldw + c] = wv;
-                A[(long long)row * ld + k0 + c] = lv;
-                bsum[e >> 1] += lv * sz[c];
-            }
-        }
-    if (b) {
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            float v = bsum[h];
-            v += __shfl_xor_sync(0xffffffffu, v, 1);
-            v += __shfl_xor_sync(0xffffffffu, v, 2);
-            if (tq == 0) sbs[w & 1][m0 + g + 8 * h] = v;
-        }
-        __syncthreads();
-        if (t < NB && r0 + t < n) b[r0 + t] -= sbs[0][t] + sbs[1][t];
-    }
-}
-
-// Panel of the FP64 factor on the FP64 tensor cores (mma.sync m8n8k4, FP64 in
-// and out): W = A_ik Linv^T, L_ik = W D^-1, b_i -= L_ik z_k.
-// Warp w takes rows 16(w/2) .. +15 and columns 32(w%2) .. +31 of the 64 x 64
-// product: 2 x 4 MMA tiles of 8 x 8.  Shared operands at a pitch of MS = 68
-// doubles (68 = 4 mod 16), so a half-warp's fragment reads hit 16 distinct
-// 8-byte banks.
-__global__ void __launch_bounds__(256) k_ldlt_panel_dmma(int n, long long ld, double *A, int k0, int kb,
-                                                         const double *dvec, const double *Linv, double *W, int ldw,
-                                                         double *b) {
-    chain_enter();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double(*sA)[MS] = reinterpret_cast<double(*)[MS]>(smem_raw);
-    double(*sI)[MS] = sA + NB;
-    double *sd = reinterpret_cast<double *>(sI + NB);
-    double *sz = sd + NB;
-    double(*sbs)[NB] = reinterpret_cast<double(*)[NB]>(sz + NB);  // [2][64] the two column halves' b sums
-    const int r0 = k0 + kb + blockIdx.x * 64, t = threadIdx.x;
-    for (int q = 0; q < 16; q++) {
-        const int idx = q * 256 + t, r = idx >> 6, c = idx & 63, row = r0 + r;
-        sA[r][c] = (row < n && c < kb) ? A[(long long)row * ld + k0 + c] : 0.0;
-        sI[r][c] = (r < kb && c < kb) ? __ldg(&Linv[r * NB + c]) : 0.0;
-    }
-    if (t < NB) {
-        sd[t] = t < kb ? dvec[k0 + t] : 1.0;
-        sz[t] = (b && t < kb) ? b[k0 + t] : 0.0;
-    }
-    __syncthreads();
-    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
-    const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
-    double acc[2][4][2] = {};
-#pragma unroll 4
-    for (int kk = 0; kk < NB; kk += 4) {
-        const double a0 = sA[m0 + g][kk + tq], a1 = sA[m0 + 8 + g][kk + tq];
-#pragma unroll
-        for (int nt = 0; nt < 4; nt++) {
-            const double bv = sI[n0 + 8 * nt + g][kk + tq];
-            dmma_8x8x4(acc[0][nt][0], acc[0][nt][1], a0, bv);
-            dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a1, bv);
-        }
-    }
-    double bsum[2] = {0.0, 0.0};  // rows m0 + g and m0 + 8 + g
-#pragma unroll
-    for (int mi = 0; mi < 2; mi++)
-#pragma unroll
-        for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const int rr = m0 + 8 * mi + g, c = n0 + 8 * nt + 2 * tq + e, row = r0 + rr;
-                if (row < n && c < kb) {
-                    const double wv = acc[mi][nt][e];
-                    const double lv = wv / sd[c];
-                    W[(long long)row * ldw + c] = wv;
-                    A[(long long)row * ld + k0 + c] = lv;
-                    bsum[mi] += lv * sz[c];
-                }
-            }
-    if (b) {
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            double v = bsum[h];
-            v += __shfl_xor_sync(0xffffffffu, v, 1);
-            v += __shfl_xor_sync(0xffffffffu, v, 2);
-            if (tq == 0) sbs[w & 1][m0 + 8 * h + g] = v;
-        }
-        __syncthreads();
-        if (t < NB && r0 + t < n) b[r0 + t] -= sbs[0][t] + sbs[1][t];
-    }
-}
-
-// In-panel column update of the FP64 factor on the FP64 tensor cores
-// (mma.sync m8n8k4): A_ij -= L_ik W_jk^T for the 64 x 64
-// tile (blockIdx.y, blockIdx.x) of rows [k1, n) x columns [k1, jend); the CTA
-// on the next diagonal tile then factors that block.
-__global__ void __launch_bounds__(256) k_ldlt_update_cols_dmma(int n, long long ld, double *A, int k0, int kb,
-                                                               const double *W, int ldw, int k1, int jend,
-                                                               NextDiag nd) {
-    chain_enter();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double(*sL)[MS] = reinterpret_cast<double(*)[MS]>(smem_raw);
-    double(*sW)[MS] = sL + NB;
-    const int i0 = k1 + blockIdx.y * 64, j0 = k1 + blockIdx.x * 64, t = threadIdx.x;
-    if (j0 > i0 + 63 || j0 >= jend) return;  // tile entirely above the diagonal or outside the panel
-    for (int q = 0; q < 16; q++) {
-        const int idx = q * 256 + t, r = idx >> 6, p = idx & 63, ri = i0 + r, rj = j0 + r;
-        sL[r][p] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : 0.0;
-        sW[r][p] = (p < kb && rj < jend) ? __ldg(&W[(long long)rj * ldw + p]) : 0.0;
-    }
-    __syncthreads();
-    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
-    const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
-    double acc[2][4][2] = {};
-#pragma unroll 4
-    for (int kk = 0; kk < NB; kk += 4) {
-        const double a0 = sL[m0 + g][kk + tq], a1 = sL[m0 + 8 + g][kk + tq];
-#pragma unroll
-        for (int nt = 0; nt < 4; nt++) {
-            const double bv = sW[n0 + 8 * nt + g][kk + tq];
-            dmma_8x8x4(acc[0][nt][0], acc[0][nt][1], a0, bv);
-            dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a1, bv);
-        }
-    }
-    // the CTA on the next diagonal tile keeps the updated tile in shared memory
-    // (over sL, once every warp is done with it) for the diagonal factor
-    const bool keep = owns_next_diag<double>(nd);
-    if (keep) __syncthreads();
-#pragma unroll
-    for (int mi = 0; mi < 2; mi++)
-#pragma unroll
-        for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const int ii = m0 + 8 * mi + g, jj = n0 + 8 * nt + 2 * tq + e, i = i0 + ii, j = j0 + jj;
-                if (i < n && j < jend && j <= i) {
-                    const double v = A[(long long)i * ld + j] - acc[mi][nt][e];
-                    A[(long long)i * ld + j] = v;
-                    if (keep) sL[ii][jj] = v;
-                }
-            }
-    fused_next_diag<double>(n, ld, A, nd, &sL[0][0]);
-}
-
-// In-panel column update of the FP32 factor:
-// A_ij -= L_ik W_jk^T for the 64 x 64 tile (blockIdx.y, blockIdx.x) of rows
-// [k1, n) x columns [k1, jend).
-template <int TERMS>
-__global__ void __launch_bounds__(256) k_ldlt_update_cols_tc(int n, long long ld, float *A, int k0, int kb,
-                                                             const float *W, int ldw, int k1, int jend,
-                                                             NextDiag nd) {
-    chain_enter();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float(*sL)[MS] = reinterpret_cast<float(*)[MS]>(smem_raw);
-    float(*sW)[MS] = sL + NB;
-    const int i0 = k1 + blockIdx.y * 64, j0 = k1 + blockIdx.x * 64, t = threadIdx.x;
-    if (j0 > i0 + 63 || j0 >= jend) return;  // tile entirely above the diagonal or outside the panel
-    {
-        float la[16], wa[16];
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            const int idx = q * 256 + t, r = idx >> 6, p = idx & 63, ri = i0 + r, rj = j0 + r;
-            la[q] = (p < kb && ri < n) ? A[(long long)ri * ld + k0 + p] : 0.f;
-            wa[q] = (p < kb && rj < jend) ? __ldg(&W[(long long)rj * ldw + p]) : 0.f;
-        }
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            const int idx = q * 256 + t;
-            sL[idx >> 6][idx & 63] = la[q];
-            sW[idx >> 6][idx & 63] = wa[q];
-        }
-    }
-    __syncthreads();
-    const int w = t >> 5, lane = t & 31, g = lane >> 2, tq = lane & 3;
-    const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1);
-    float acc[4][4] = {};
-    warp_mma_64<TERMS>(sL, sW, m0, n0, acc);
-    // the CTA on the next diagonal tile keeps the updated tile in shared memory
-    // (over sL, once every warp is done with it) for the diagonal factor
-    const bool keep = owns_next_diag<float>(nd);
-    if (keep) __syncthreads();
-#pragma unroll
-    for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int ii = m0 + g + (e >> 1) * 8, jj = n0 + 8 * nt + 2 * tq + (e & 1), i = i0 + ii, j = j0 + jj;
-            if (i < n && j < jend && j <= i) {
-                const float v = A[(long long)i * ld + j] - acc[nt][e];
-                A[(long long)i * ld + j] = v;
-                if (keep) sL[ii][jj] = v;
-            }
-        }
-    fused_next_diag<float>(n, ld, A, nd, &sL[0][0]);
-}
-
 // One step of the 64-wide chain of the FP32 factor inside a 256-wide panel, in
 // one launch: the panel of block k (rows [k1, n)), the in-panel column update
 // of columns [k1, jend) and the diagonal factor of block k1.  CTA b takes the
@@ -1420,9 +1214,9 @@ __global__ void __launch_bounds__(256) k_ldlt_update_cols_tc(int n, long long ld
 //   the updated tiles of column block k1 in rows [k1 + 64, jend) go to kout,
 //   the next step's kin;
 //   CTA 0 then factors block k1 from its updated tile (NextDiag).
-// Against a panel launch followed by a column-update launch, the chain loses a
-// launch and the panel's wait per block: the next diagonal factor starts once
-// CTA 0's own row block is done.  Shared memory: Linv_k, A_ik (then a copied
+// Against a panel launch followed by a column-update launch (the structure it
+// replaced), the chain loses a launch and the panel's wait per block: the next
+// diagonal factor starts once CTA 0's own row block is done.  Shared memory: Linv_k, A_ik (then a copied
 // A_jk), L_ik (then the next diagonal tile), W_ik, W_jk, and D_k, z_k and the b
 // sums.
 constexpr size_t STEP_TC_SMEM = sizeof(float) * (5 * NB * MS + 4 * NB);
@@ -1540,11 +1334,13 @@ __global__ void __launch_bounds__(256) k_ldlt_step_tc(int n, long long ld, float
             }
         __syncthreads();  // sA and sY are reused by the next column block
     }
-    fused_next_diag<float>(n, ld, A, nd, &sA[0][0]);
+    // the diagonal factor's scratch: sWo and sY, free now
+    static_assert(diag_scratch<float>() <= sizeof(float) * 2 * NB * MS, "diagonal scratch");
+    fused_next_diag<float>(n, ld, A, nd, &sA[0][0], reinterpret_cast<unsigned char *>(&sWo[0][0]));
 }
 
 // The FP64 factor's fused chain step: k_ldlt_step_tc's structure with the
-// products of k_ldlt_panel_dmma / k_ldlt_update_cols_dmma (mma.sync m8n8k4 f64;
+// products on the FP64 tensor cores (mma.sync m8n8k4 f64;
 // warp w: rows 16(w/2) .. +15, columns 32(w%2) .. +31 as 2 x 4 tiles of 8 x 8).
 __device__ __forceinline__ void warp_dmma_64(const double (*sa)[MS], const double (*sb)[MS], int m0, int n0,
                                              double (&acc)[2][4][2]) {
@@ -1662,7 +1458,8 @@ __global__ void __launch_bounds__(256) k_ldlt_step_dmma(int n, long long ld, dou
                 }
         __syncthreads();
     }
-    fused_next_diag<double>(n, ld, A, nd, &sA[0][0]);
+    static_assert(diag_scratch<double>() <= sizeof(double) * 2 * NB * MS, "diagonal scratch");
+    fused_next_diag<double>(n, ld, A, nd, &sA[0][0], reinterpret_cast<unsigned char *>(&sWo[0][0]));
 }
 
 template <typename T>
@@ -1781,10 +1578,6 @@ template <typename T>
 int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> w, bool factor,
                       int tc_terms = 0) {
     cudaStream_t st = ctx->stream;
-    const size_t panel_tc_smem = sizeof(float) * (2 * NB * MS + 4 * NB);
-    const size_t panel_dmma_smem = sizeof(double) * (2 * NB * MS + 4 * NB);
-    const size_t cols_dmma_smem = sizeof(double) * 2 * NB * MS;
-    const size_t cols_tc_smem = sizeof(float) * 2 * NB * MS;
     const size_t f64_smem = sizeof(double) * 4 * WKC * WPITCH;
     if (!ctx->ldlt_attr) {  // per context: the attributes belong to the context's device
         const int big = 96 * 1024;
@@ -1803,42 +1596,13 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
         wavefront_attrs<float>();
         wavefront_attrs<double>();
         cudaFuncSetAttribute(k_ldlt_step_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)STEP_DMMA_SMEM);
-        for (const void *f : {(const void *)k_ldlt_panel_tc<1>, (const void *)k_ldlt_panel_tc<3>,
-                              (const void *)k_ldlt_panel_dmma, (const void *)k_ldlt_update_cols_dmma,
-                              (const void *)k_ldlt_update_cols_tc<1>, (const void *)k_ldlt_update_cols_tc<3>,
-                              (const void *)k_ldlt_step_tc<1>, (const void *)k_ldlt_step_tc<3>})
+        cudaFuncSetAttribute(k_ldlt_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)diag_scratch<double>());
+        for (const void *f : {(const void *)k_ldlt_step_tc<1>, (const void *)k_ldlt_step_tc<3>})
             cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         ctx->ldlt_attr = true;
     }
     unsigned long long *flags = ctx->counters + C_FLAGS;
-    // the diagonal factor of block k0 (unless the previous block's in-panel
-    // column update ran it), then the panel below it
-    auto diag_and_panel = [&](int k0, int kb, T *W, int ldw, bool diag_done) -> int {
-        T *Li = w.Linv + (size_t)(k0 / NB) * NB * NB;
-        int mk;
-        if (!diag_done) {
-            mk = kt_begin(ctx, MP_KT_DIAG, 0);
-            MP_CUDA(ctx, launch_chain(k_ldlt_diag<T>, dim3(1), 0, st, n, ld, A, k0, kb, w.dvec, Li, b, flags,
-                                      (T *)nullptr, 0));
-            ++ctx->launches;
-            kt_end(ctx, mk);
-        }
-        int k1 = k0 + kb;
-        if (k1 < n) {
-            mk = kt_begin(ctx, MP_KT_PANEL, 0);
-            const unsigned gp = (n - k1 + 63) / 64;
-            if constexpr (std::is_same<T, float>::value) {
-                MP_CUDA(ctx, launch_chain(tc_terms == 3 ? k_ldlt_panel_tc<3> : k_ldlt_panel_tc<1>, dim3(gp),
-                                          panel_tc_smem, st, n, ld, A, k0, kb, w.dvec, Li, W, ldw, b));
-            } else {
-                MP_CUDA(ctx, launch_chain(k_ldlt_panel_dmma, dim3(gp), panel_dmma_smem, st, n, ld, A, k0, kb, w.dvec,
-                                          Li, W, ldw, b));
-            }
-            ++ctx->launches;
-            kt_end(ctx, mk);
-        }
-        return MP_OK;
-    };
     // algorithmic flops of an update of rows [R0, n) x columns [R0, C1), lower part, depth K
     auto update_flops = [&](int R0, int C1, int K) {
         const double m = n - R0, wcol = C1 - R0;
@@ -1948,62 +1712,40 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
                 for (int k0 = P0, step = 0; k0 < P1; k0 += NB, step++) {
                     const int kb = P1 - k0 < NB ? P1 - k0 : NB;
                     const int k1 = k0 + kb;
-                    if (w.ktile) {
-                        // fused chain steps: one launch per block (k_ldlt_step_tc / k_ldlt_step_dmma)
-                        T *kin = w.ktile + (size_t)(step & 1) * 3 * NB * NB;
-                        T *kout = w.ktile + (size_t)((step + 1) & 1) * 3 * NB * NB;
-                        T *Li = w.Linv + (size_t)(k0 / NB) * NB * NB;
-                        if (!diag_done) {
-                            const int mk = kt_begin(ctx, MP_KT_DIAG, 0);
-                            MP_CUDA(ctx, launch_chain(k_ldlt_diag<T>, dim3(1), 0, st, n, ld, A, k0, kb, w.dvec, Li, b,
-                                                      flags, k1 < P1 ? kin : (T *)nullptr, P1));
-                            ++ctx->launches;
-                            kt_end(ctx, mk);
-                        }
-                        diag_done = false;
-                        if (k1 < n) {
-                            const int kbn = P1 - k1 < NB ? P1 - k1 : NB;
-                            const NextDiag nd{k1 < P1 ? k1 : 0, k1 < P1 ? kbn : 0, w.dvec,
-                                              w.Linv + (size_t)(k1 / NB) * NB * NB, b, flags};
-                            const int mk = kt_begin(ctx, MP_KT_PANEL, 0);
-                            const dim3 gs((n - k1 + 63) / 64);
-                            if constexpr (std::is_same<T, float>::value) {
-                                MP_CUDA(ctx, launch_chain(tc_terms == 3 ? k_ldlt_step_tc<3> : k_ldlt_step_tc<1>, gs,
-                                                          STEP_TC_SMEM, st, n, ld, A, k0, kb, (const float *)w.dvec,
-                                                          (const float *)Li, w.W + (k0 - S0), (int)SUPER_W, b, k1, P1,
-                                                          (const float *)kin, kout, nd));
-                            } else {
-                                MP_CUDA(ctx, launch_chain(k_ldlt_step_dmma, gs, STEP_DMMA_SMEM, st, n, ld, A, k0, kb,
-                                                          (const double *)w.dvec, (const double *)Li,
-                                                          w.W + (k0 - S0), (int)SUPER_W, b, k1, P1,
-                                                          (const double *)kin, kout, nd));
-                            }
-                            ++ctx->launches;
-                            kt_end(ctx, mk);
-                            diag_done = k1 < P1;
-                        }
-                        continue;
+                    // one launch per chain step (k_ldlt_step_tc / k_ldlt_step_dmma): the panel of
+                    // block k0, the in-panel column update and the next block's diagonal factor;
+                    // the first block of a panel is factored alone, which also copies its
+                    // column block's panel tiles for the first step
+                    T *kin = w.ktile + (size_t)(step & 1) * 3 * NB * NB;
+                    T *kout = w.ktile + (size_t)((step + 1) & 1) * 3 * NB * NB;
+                    T *Li = w.Linv + (size_t)(k0 / NB) * NB * NB;
+                    if (!diag_done) {
+                        const int mk = kt_begin(ctx, MP_KT_DIAG, 0);
+                        MP_CUDA(ctx, launch_chain(k_ldlt_diag<T>, dim3(1), diag_scratch<T>(), st, n, ld, A, k0, kb,
+                                                  w.dvec, Li, b, flags, k1 < P1 ? kin : (T *)nullptr, P1));
+                        ++ctx->launches;
+                        kt_end(ctx, mk);
                     }
-                    int rc = diag_and_panel(k0, kb, w.W + (k0 - S0), SUPER_W, diag_done);
-                    if (rc) return rc;
                     diag_done = false;
-                    if (k1 < n && k1 < P1) {
-                        // the update's CTA on the next diagonal tile factors that block
+                    if (k1 < n) {
                         const int kbn = P1 - k1 < NB ? P1 - k1 : NB;
-                        const NextDiag nd{k1, kbn, w.dvec, w.Linv + (size_t)(k1 / NB) * NB * NB, b, flags};
-                        diag_done = true;
-                        dim3 g((P1 - k1 + 63) / 64, (n - k1 + 63) / 64);
+                        const NextDiag nd{k1 < P1 ? k1 : 0, k1 < P1 ? kbn : 0, w.dvec,
+                                          w.Linv + (size_t)(k1 / NB) * NB * NB, b, flags};
                         const int mk = kt_begin(ctx, MP_KT_PANEL, 0);
+                        const dim3 gs((n - k1 + 63) / 64);
                         if constexpr (std::is_same<T, float>::value) {
-                            MP_CUDA(ctx, launch_chain(tc_terms == 3 ? k_ldlt_update_cols_tc<3> : k_ldlt_update_cols_tc<1>,
-                                                      g, cols_tc_smem, st, n, ld, A, k0, kb, w.W + (k0 - S0),
-                                                      SUPER_W, k1, P1, nd));
+                            MP_CUDA(ctx, launch_chain(tc_terms == 3 ? k_ldlt_step_tc<3> : k_ldlt_step_tc<1>, gs,
+                                                      STEP_TC_SMEM, st, n, ld, A, k0, kb, (const float *)w.dvec,
+                                                      (const float *)Li, w.W + (k0 - S0), (int)SUPER_W, b, k1, P1,
+                                                      (const float *)kin, kout, nd));
                         } else {
-                            MP_CUDA(ctx, launch_chain(k_ldlt_update_cols_dmma, g, cols_dmma_smem, st, n, ld, A, k0,
-                                                      kb, w.W + (k0 - S0), SUPER_W, k1, P1, nd));
+                            MP_CUDA(ctx, launch_chain(k_ldlt_step_dmma, gs, STEP_DMMA_SMEM, st, n, ld, A, k0, kb,
+                                                      (const double *)w.dvec, (const double *)Li, w.W + (k0 - S0),
+                                                      (int)SUPER_W, b, k1, P1, (const double *)kin, kout, nd));
                         }
                         ++ctx->launches;
                         kt_end(ctx, mk);
+                        diag_done = k1 < P1;
                     }
                 }
                 if (P1 < S1) {  // a full panel with more of its super-panel to the right
