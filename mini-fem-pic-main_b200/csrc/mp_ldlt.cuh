@@ -661,6 +661,35 @@ __device__ __forceinline__ bool wait_chunk(const unsigned long long *ll, int c, 
     return *ok != 0;
 }
 
+// wait_chunk for up to gmax consecutive blocks c, c + dir, ...: warp 0 waits
+// for block c, then takes the following blocks that are already published
+// (one poll each) into dst + i*NB; returns how many it took (0: the wait gave
+// up).  Behind the front, where the blocks were published long ago, one
+// barrier then covers several blocks.
+template <typename T>
+__device__ __forceinline__ int wait_chunks(const unsigned long long *ll, int c, int dir, int gmax, unsigned epoch,
+                                           T *dst, int backoff, int *cnt, unsigned long long *flags) {
+    if (threadIdx.x < 32) {
+        int got = 0;
+        for (long long spins = 0; spins <= TRSV_SPIN_LIMIT; spins++) {
+            if (ll_try<T>(ll, c, epoch, dst)) {
+                got = 1;
+                break;
+            }
+            if (backoff) __nanosleep(backoff);
+        }
+        if (got)
+            while (got < gmax && ll_try<T>(ll, c + dir * got, epoch, dst + got * NB)) got++;
+        if (threadIdx.x == 0) {
+            *cnt = got;
+            if (!got) atomicOr(flags, FLAG_LOOKBACK_TIMEOUT);
+        }
+    }
+    __syncthreads();
+    return *cnt;
+}
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // The chain's critical wait: every warp polls block c's words itself, so no
 // CTA barrier follows; this lane gets values lane (v0) and lane + 32 (v1).  A
 // wait that gives up raises the error flag and leaves zeros (the caller's
@@ -876,9 +905,13 @@ __global__ void __launch_bounds__(256) k_trsv_ll(int n, long long ld, const T *_
 // Shared memory: the two inverses, C1_b1, C2_b2, C1_b2 ([64][MS] each), the
 // two blocks' partial sums, poll buffers, right-hand sides, x_b1.
 constexpr int BAND_FROM_BLOCKS = 256;
+// far blocks: up to BAND_GROUP published blocks a poll; L's rows of the block
+// BAND_PREFETCH ahead of the one in registers are prefetched into L2 (L does not
+// depend on the front, only the values do)
+constexpr int BAND_GROUP = 4, BAND_PREFETCH = 4;
 template <typename T>
 constexpr size_t band_smem() {
-    return sizeof(T) * (5 * NB * MS + 2 * 16 * (NB + 1) + 5 * NB) + 2 * sizeof(int);
+    return sizeof(T) * (5 * NB * MS + 2 * 16 * (NB + 1) + (2 * BAND_GROUP + 3) * NB) + 2 * sizeof(int);
 }
 
 template <typename T, int DIR>
@@ -893,8 +926,8 @@ __global__ void __launch_bounds__(256, 2)
     T(*sC22)[MS] = sC11 + NB;  // C2 of b2
     T(*sC12)[MS] = sC22 + NB;  // C1 of b2
     T(*spart)[16][NB + 1] = reinterpret_cast<T(*)[16][NB + 1]>(sC12 + NB);  // [2][16][65]
-    T *sx = reinterpret_cast<T *>(spart + 2);                                // [2][NB]
-    T *srhs = sx + 2 * NB;                                                   // [2][NB]
+    T *sx = reinterpret_cast<T *>(spart + 2);                                // [2][BAND_GROUP][NB]
+    T *srhs = sx + 2 * BAND_GROUP * NB;                                      // [2][NB]
     T *sx1 = srhs + 2 * NB;                                                  // [NB]
     int *sok = reinterpret_cast<int *>(sx1 + NB);                            // [2]
     const int nblk = (n + NB - 1) / NB, nband = (nblk + 1) / 2;
@@ -959,33 +992,61 @@ __global__ void __launch_bounds__(256, 2)
                 }
             }
         };
-        bool ok = true;
-        if (nfar > 0) fetch(DIR > 0 ? 0 : nblk - 1);
-        for (int s = 0; s < nfar; s++) {
-            const int j = DIR > 0 ? s : nblk - 1 - s;
-            T *buf = sx + par * NB;
-            ok = wait_chunk<T>(ll, j, epoch, buf, poll_backoff(nfar - s), sok + par, flags);
-            par ^= 1;
-            if (!ok) break;
+        // the lines of L a thread will load for far block j, into L2
+        auto prefetch = [&](int j) {
             if (DIR > 0) {
-#pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    const T xv = buf[q * 16 + k];
-                    acc1 = fma(ap1[k], xv, acc1);
-                    acc2 = fma(ap2[k], xv, acc2);
+                if ((q & 1) == 0) {  // q = 0, 2: the row's two 128-byte lines
+                    if (r < kb1) prefetch_l2(A + (long long)(r01 + r) * ld + j * NB + q * 16);
+                    if (r < kb2) prefetch_l2(A + (long long)(r02 + r) * ld + j * NB + q * 16);
                 }
-            } else {
+            } else if ((c4 & 7) == 0) {  // c4 = 0, 8: each block's two lines of a row
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
-                    const T xe = buf[4 * part + e];
-#pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        a41[k] = fma(ap1[4 * e + k], xe, a41[k]);
-                        a42[k] = fma(ap2[4 * e + k], xe, a42[k]);
+                    const int i = j * NB + 4 * part + e;
+                    if (i < n) {
+                        prefetch_l2(A + (long long)i * ld + r01 + 4 * c4);
+                        if (two) prefetch_l2(A + (long long)i * ld + r02 + 4 * c4);
                     }
                 }
             }
-            if (s + 1 < nfar) fetch(DIR > 0 ? j + 1 : j - 1);
+        };
+        bool ok = true;
+        if (nfar > 0) fetch(DIR > 0 ? 0 : nblk - 1);
+        for (int s = 1; s <= BAND_PREFETCH && s < nfar; s++) prefetch(DIR > 0 ? s : nblk - 1 - s);
+        for (int s = 0; s < nfar;) {
+            T *buf = sx + par * BAND_GROUP * NB;
+            const int gmax = nfar - s < BAND_GROUP ? nfar - s : BAND_GROUP;
+            const int m = wait_chunks<T>(ll, DIR > 0 ? s : nblk - 1 - s, DIR, gmax, epoch, buf,
+                                         poll_backoff(nfar - s), sok + par, flags);
+            par ^= 1;
+            if (m == 0) {
+                ok = false;
+                break;
+            }
+            for (int u = 0; u < m; u++, s++) {
+                const int j = DIR > 0 ? s : nblk - 1 - s;
+                const T *xb = buf + u * NB;
+                if (DIR > 0) {
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        const T xv = xb[q * 16 + k];
+                        acc1 = fma(ap1[k], xv, acc1);
+                        acc2 = fma(ap2[k], xv, acc2);
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const T xe = xb[4 * part + e];
+#pragma unroll
+                        for (int k = 0; k < 4; k++) {
+                            a41[k] = fma(ap1[4 * e + k], xe, a41[k]);
+                            a42[k] = fma(ap2[4 * e + k], xe, a42[k]);
+                        }
+                    }
+                }
+                if (s + 1 < nfar) fetch(DIR > 0 ? j + 1 : j - 1);
+                if (s + 1 + BAND_PREFETCH < nfar) prefetch(DIR > 0 ? j + 1 + BAND_PREFETCH : j - 1 - BAND_PREFETCH);
+            }
         }
         if (DIR > 0) {
             acc1 += __shfl_xor_sync(0xffffffffu, acc1, 1);
