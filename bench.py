@@ -65,9 +65,12 @@ LEGS = ("kuhn20", "nonlinear", "adjoint", "sparse64", "vtk")
 # per kernel, per unit of its algorithmic work; a launch's traffic is scaled by
 # its units (a K = 1,024 trailing update of 55.4 GFLOP moves 444.3 MB in 3xTF32,
 # profiles/k_update_tc_kuhn20_newton.md, and 232.4 MB in TF32,
-# profiles/k_update_tc_tf32_kuhn20_newton.md; profiles/k_push_*_kuhn20_2M.md:
+# profiles/k_update_tc_tf32_kuhn20_newton.md; one of 41.0 GFLOP with FP16
+# operands moves 140.3 MB, profiles/k_update_tc_tma_f16_kuhn20_newton.md;
+# profiles/k_push_*_kuhn20_2M.md:
 # 160.5 MB and 65.1 MB for 1.99M particles, in and out)
 TRAFFIC_PER_UNIT = {("tc3", "update"): 444.3e6 / 55.4e9, ("tc1", "update"): 232.4e6 / 55.4e9,
+                    ("tc2", "update"): 140.3e6 / 41.0e9,
                     ("fp64", "push"): 160.5e6 / (2 * 1.99e6), ("mixed", "push"): 65.1e6 / (2 * 1.99e6)}
 # FP64 tensor-pipe rate implied by one ncu capture of k_update_f64_mma (26.4
 # TFLOP/s at 76.6 % DMMA-pipe activity); this pool's peaks file has no FP64 figure
@@ -192,7 +195,7 @@ def kernel_roofline(ctx, form, pk, step_ms_total, sustained=True, neq=0):
     kname = KT_KERNEL[top][form]
     if top == mp.KT_UPDATE and form == mp.MIXED:
         kname = ("tc::k_update_tc<1> (3xTF32, tcgen05 kind::tf32)" if terms == mp.MIXED_TF32X3 else
-                 "tc::k_update_tc<2> (FP16 operands, tcgen05 kind::f16)")
+                 "tc::k_update_tc_tma<2> (FP16 operands, tcgen05 kind::f16, old values of A moved by TMA)")
     out = {"kernel": kname, "class": KT_NAMES[top], "launches": v["launches"],
            "avg_launch_ms": v["ms"] / max(v["launches"], 1)}
     if top == mp.KT_PUSH:

@@ -2,7 +2,7 @@
 centred r = 0.02 m sphere held at -10 V (371,004 tets, 67,298 nodes, 62,788
 unknowns; the dense FP64 K is 31.6 GB), about 193M O+ ions (spwt 0.05) with a
 tet re-sort every 10 steps, the mixed-precision step (FP32 tet-relative
-particles, 3xTF32 tcgen05 LDL^T with FP64 refinement), the adjoint of K = 10
+particles, tcgen05 LDL^T on FP16 operands with FP64 refinement), the adjoint of K = 10
 push + scatter steps with checkpoints every 5 on the whole population, and the
 FP64 form of the same steps beside it.
 
@@ -113,7 +113,8 @@ def run(args, device, torch, pk):
     keep_m = []
     rm = _steps(c, mp.MIXED, cfg, deck, steps, warmup, torch, device, keep_m)
     out["mixed"] = _summary(rm, c, pk)
-    out["mixed"]["refined_newton"] = "3xTF32 tcgen05 LDL^T, FP64 refinement to ||r|| <= 1e-14 ||G||"
+    out["mixed"]["refined_newton"] = ("tcgen05 LDL^T (FP16-operand trailing updates from %d unknowns, 3xTF32 below), "
+                                      "FP64 refinement to ||r|| <= 1e-14 ||G||" % mp.MIXED_FP16_FROM)
     free, total = torch.cuda.mem_get_info(device)
     out["mixed"]["device_memory_used_GB"] = (total - free) / 1e9
     # adjoint of K push + scatter steps over the whole population, phi held at the last step's
