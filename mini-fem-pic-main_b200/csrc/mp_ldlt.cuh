@@ -758,13 +758,10 @@ __device__ __forceinline__ void load16(const T *p, T (&v)[16]) {
 
 
 // Shared memory of k_trsv_ll: inverse and coupling blocks, partial sums, two
-// poll buffers of TRSV_GROUP blocks, the right-hand side, two poll results.
-// Far blocks are polled up to TRSV_GROUP at a time, and the lines of L a
-// thread loads TRSV_PREFETCH blocks ahead are prefetched into L2.
-constexpr int TRSV_GROUP = 4, TRSV_PREFETCH = 4;
+// poll buffers, the right-hand side, two poll results.
 template <typename T>
 constexpr size_t trsv_smem() {
-    return sizeof(T) * (2 * NB * MS + 16 * (NB + 1) + (2 * TRSV_GROUP + 1) * NB) + 2 * sizeof(int);
+    return sizeof(T) * (2 * NB * MS + 16 * (NB + 1) + 3 * NB) + 2 * sizeof(int);
 }
 
 // DIR = +1: L z = b (unit lower, in place on x); DIR = -1: L^T y = D^-1 z (in
@@ -778,8 +775,8 @@ __global__ void __launch_bounds__(256) k_trsv_ll(int n, long long ld, const T *_
     T(*sI)[MS] = reinterpret_cast<T(*)[MS]>(smem_raw);
     T(*sC)[MS] = sI + NB;
     T(*spart)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(sC + NB);
-    T *sx = reinterpret_cast<T *>(spart + 16);  // [2][TRSV_GROUP][NB]
-    T *srhs = sx + 2 * TRSV_GROUP * NB;
+    T *sx = reinterpret_cast<T *>(spart + 16);  // [2][NB]
+    T *srhs = sx + 2 * NB;
     int *sok = reinterpret_cast<int *>(srhs + NB);  // [2]
     const int nblk = (n + NB - 1) / NB;
     const int t = threadIdx.x;
@@ -821,47 +818,26 @@ __global__ void __launch_bounds__(256) k_trsv_ll(int n, long long ld, const T *_
                 }
             }
         };
-        auto prefetch = [&](int j) {
-            if (DIR > 0) {
-                if ((q & 1) == 0 && r < kb) prefetch_l2(A + (long long)(r0 + r) * ld + j * NB + q * 16);
-            } else if ((c4 & 7) == 0) {
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const int i = j * NB + 4 * part + e;
-                    if (i < n) prefetch_l2(A + (long long)i * ld + r0 + 4 * c4);
-                }
-            }
-        };
         bool ok = true;
         if (nfar > 0) fetch(DIR > 0 ? 0 : nblk - 1);
-        for (int s = 1; s <= TRSV_PREFETCH && s < nfar; s++) prefetch(DIR > 0 ? s : nblk - 1 - s);
-        for (int s = 0; s < nfar;) {
-            T *buf = sx + par * TRSV_GROUP * NB;
-            const int gmax = nfar - s < TRSV_GROUP ? nfar - s : TRSV_GROUP;
-            const int m = wait_chunks<T>(ll, DIR > 0 ? s : nblk - 1 - s, DIR, gmax, epoch, buf,
-                                         poll_backoff(nfar - s), sok + par, flags);
+        for (int s = 0; s < nfar; s++) {
+            const int j = DIR > 0 ? s : nblk - 1 - s;
+            T *buf = sx + par * NB;
+            ok = wait_chunk<T>(ll, j, epoch, buf, poll_backoff(nfar - s), sok + par, flags);
             par ^= 1;
-            if (m == 0) {
-                ok = false;
-                break;
-            }
-            for (int u = 0; u < m; u++, s++) {
-                const int j = DIR > 0 ? s : nblk - 1 - s;
-                const T *xb = buf + u * NB;
-                if (DIR > 0) {
+            if (!ok) break;
+            if (DIR > 0) {
 #pragma unroll
-                    for (int k = 0; k < 16; k++) acc = fma(ap[k], xb[q * 16 + k], acc);
-                } else {
+                for (int k = 0; k < 16; k++) acc = fma(ap[k], buf[q * 16 + k], acc);
+            } else {
 #pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const T xe = xb[4 * part + e];
+                for (int e = 0; e < 4; e++) {
+                    const T xe = buf[4 * part + e];
 #pragma unroll
-                        for (int k = 0; k < 4; k++) acc4[k] = fma(ap[4 * e + k], xe, acc4[k]);
-                    }
+                    for (int k = 0; k < 4; k++) acc4[k] = fma(ap[4 * e + k], xe, acc4[k]);
                 }
-                if (s + 1 < nfar) fetch(DIR > 0 ? j + 1 : j - 1);
-                if (s + 1 + TRSV_PREFETCH < nfar) prefetch(DIR > 0 ? j + 1 + TRSV_PREFETCH : j - 1 - TRSV_PREFETCH);
             }
+            if (s + 1 < nfar) fetch(DIR > 0 ? j + 1 : j - 1);
         }
         if (DIR > 0) {
             acc += __shfl_xor_sync(0xffffffffu, acc, 1);
