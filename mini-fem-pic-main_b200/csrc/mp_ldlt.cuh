@@ -375,95 +375,12 @@ __device__ __forceinline__ void fused_next_diag(int n, long long ld, T *A, const
 // L = A[i][K0 ...] and W rows of pitch ldw (K a multiple of 16).  colblocks = 0:
 // the lower 128x128 tiles of [R0, n)^2 (the trailing update of a super-panel);
 // colblocks > 0: every tile of rows [R0, n) x columns [R0, R0 + 128*colblocks)
-// (a strip inside a super-panel), lower parts only.  256 threads, 8x8
-// accumulators per thread (rows ty + 16u, columns tx + 16v), K streamed in
-// 16-wide chunks through two shared-memory buffers stored k-major (the next
-// chunk is loaded into registers while this one computes).
+// (a strip inside a super-panel), lower parts only.  K streams in 16-wide
+// chunks through two shared-memory buffers stored k-major.
 constexpr int WTILE = 128, WKC = 16;
 
-__global__ void __launch_bounds__(256, 1) k_update_f64(int n, long long ld, double *A, int K0, int K, int R0,
-                                                       const double *__restrict__ W, int ldw, int colblocks) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double(*sL)[WKC][WTILE] = reinterpret_cast<double(*)[WKC][WTILE]>(smem_raw);
-    double(*sW)[WKC][WTILE] = sL + 2;
-    long long bidx = blockIdx.x;
-    int bi, bj;
-    if (colblocks > 0) {
-        bi = (int)(bidx / colblocks);
-        bj = (int)(bidx % colblocks);
-    } else {
-        bi = (int)((sqrt(8.0 * (double)bidx + 1.0) - 1.0) * 0.5);
-        while ((long long)(bi + 1) * (bi + 2) / 2 <= bidx) bi++;
-        while ((long long)bi * (bi + 1) / 2 > bidx) bi--;
-        bj = (int)(bidx - (long long)bi * (bi + 1) / 2);
-    }
-    const long long i0 = R0 + (long long)bi * WTILE, j0 = R0 + (long long)bj * WTILE;
-    if (j0 > i0 + WTILE - 1) return;  // strip tile entirely above the diagonal
-    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-    // loader: row lr of the tile, k half lh (8 values)
-    const int lr = t >> 1, lh = t & 1;
-    const bool lrow = i0 + lr < n, wrow = j0 + lr < n;
-    const double *lsrc = A + (i0 + (lrow ? lr : 0)) * ld + K0 + lh * 8;
-    const double *wsrc = W + (j0 + (wrow ? lr : 0)) * (long long)ldw + lh * 8;
-    double2 pl[4], pw[4];
-    auto fetch = [&](int kc) {
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            pl[e] = lrow ? __ldg(reinterpret_cast<const double2 *>(lsrc + kc * WKC) + e) : make_double2(0.0, 0.0);
-            pw[e] = wrow ? __ldg(reinterpret_cast<const double2 *>(wsrc + kc * WKC) + e) : make_double2(0.0, 0.0);
-        }
-    };
-    auto stash = [&](int buf) {
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            sL[buf][lh * 8 + 2 * e][lr] = pl[e].x;
-            sL[buf][lh * 8 + 2 * e + 1][lr] = pl[e].y;
-            sW[buf][lh * 8 + 2 * e][lr] = pw[e].x;
-            sW[buf][lh * 8 + 2 * e + 1][lr] = pw[e].y;
-        }
-    };
-    double acc[8][8];
-#pragma unroll
-    for (int u = 0; u < 8; u++)
-#pragma unroll
-        for (int v = 0; v < 8; v++) acc[u][v] = 0.0;
-    fetch(0);
-    stash(0);
-    __syncthreads();
-    const int NKC = K / WKC;
-#pragma unroll 1
-    for (int kc = 0; kc < NKC; kc++) {
-        const int buf = kc & 1;
-        if (kc + 1 < NKC) fetch(kc + 1);
-#pragma unroll
-        for (int k = 0; k < WKC; k++) {
-            double a[8], b[8];
-#pragma unroll
-            for (int u = 0; u < 8; u++) a[u] = sL[buf][k][ty + 16 * u];
-#pragma unroll
-            for (int v = 0; v < 8; v++) b[v] = sW[buf][k][tx + 16 * v];
-#pragma unroll
-            for (int u = 0; u < 8; u++)
-#pragma unroll
-                for (int v = 0; v < 8; v++) acc[u][v] = fma(a[u], b[v], acc[u][v]);
-        }
-        if (kc + 1 < NKC) stash(buf ^ 1);
-        __syncthreads();
-    }
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-        const long long row = i0 + ty + 16 * u;
-        if (row >= n) continue;
-#pragma unroll
-        for (int v = 0; v < 8; v++) {
-            const long long col = j0 + tx + 16 * v;
-            if (col < n && col <= row) A[row * ld + col] -= acc[u][v];
-        }
-    }
-}
-
-// The same update on the FP64 tensor cores (mma.sync m8n8k4, FP64 in and out,
-// so the products and sums are FP64 operations as in the SIMT kernel).  Warp w
+// The update runs on the FP64 tensor cores (mma.sync m8n8k4, FP64 in and out,
+// so the products and sums are FP64 operations).  Warp w
 // takes rows 32(w/2) .. +31 and columns 64(w%2) .. +63 of the 128 x 128 tile:
 // 4 x 8 MMA tiles of 8 x 8, 64 accumulators a thread.  Fragments of m8n8k4
 // (g = lane / 4, t = lane % 4): A (row g, k t), B (k t, column g), C (row g,
@@ -1642,14 +1559,9 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
     const size_t f64_smem = sizeof(double) * 4 * WKC * WPITCH;
     if (!ctx->ldlt_attr) {  // per context: the attributes belong to the context's device
         const int big = 96 * 1024;
-        cudaFuncSetAttribute(k_update_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(k_update_f64_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(tc::k_update_tc<tc::MODE_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tc::smem_bytes(tc::MODE_TF32));
         cudaFuncSetAttribute(tc::k_update_tc<tc::MODE_TF32X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)tc::smem_bytes(tc::MODE_TF32X3));
-        cudaFuncSetAttribute(tc::k_update_tc<tc::MODE_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tc::smem_bytes(tc::MODE_F16));
         cudaFuncSetAttribute(tc::k_update_tc_tma<tc::MODE_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)tc::smem_bytes_tma());
         cudaFuncSetAttribute(tc::k_update_tc_tma<tc::MODE_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1745,9 +1657,7 @@ int ldlt_factor_solve(mp_ctx *ctx, T *A, long long ld, int n, T *b, LdltWork<T> 
             kt_end(ctx, mk);
             return MP_OK;
         }
-        auto kern = mode == tc::MODE_F16 ? tc::k_update_tc<tc::MODE_F16>
-                    : split            ? tc::k_update_tc<tc::MODE_TF32X3>
-                                       : tc::k_update_tc<tc::MODE_TF32>;
+        auto kern = tc::k_update_tc<tc::MODE_TF32X3>;  // the single-product modes returned above
         const int mk = kt_begin(ctx, MP_KT_UPDATE, update_flops(R0, C1, K));
         kern<<<grid, tc::THREADS, tc::smem_bytes(mode), st>>>(mLh, mWh, mLl, mWl, n, ld, Af, R0, ntiles,
                                                               K / tc::kc_of(mode), cb,
