@@ -29,6 +29,34 @@ def test_header_and_binding_agree():
     assert declared_symbols() == set(mp.EXPORTED)
 
 
+def header_constants():
+    """Every MP_* constant the header defines, by enum entry or #define."""
+    text = open(os.path.join(ROOT, "include", "minipic_cuda.h")).read()
+    vals = {k: int(v) for k, v in re.findall(r"\b(MP_\w+)\s*=\s*(-?\d+)", text)}
+    vals.update({k: int(v) for k, v in re.findall(r"^#define\s+(MP_\w+)\s+(-?\d+)\s*$", text, re.M)})
+    return vals
+
+
+def test_python_constants_mirror_the_header():
+    h = header_constants()
+    # names the Python package spells the same way without the MP_ prefix
+    same = {k[3:]: v for k, v in h.items() if hasattr(mp, k[3:])}
+    for name in ("MIXED_AUTO", "MIXED_TF32", "MIXED_FP16", "MIXED_TF32X3", "MIXED_FP16_FROM",
+                 "ORDER_STORAGE", "ORDER_ID", "WALK_LIMIT_ERROR", "WALK_LIMIT_ABSORB", "KT_PUSH", "KT_UPDATE"):
+        assert name in same, name
+    for name, v in same.items():
+        assert getattr(mp, name) == v, (name, getattr(mp, name), v)
+    # the forms and storage the package names differently
+    assert (mp.FP64, mp.MIXED) == (h["MP_FORM_FP64"], h["MP_FORM_MIXED"])
+    assert (mp.FE_DENSE, mp.FE_SPARSE) == (h["MP_FE_STORAGE_DENSE"], h["MP_FE_STORAGE_SPARSE"])
+
+
+def test_mixed_factor_arguments_checked():
+    L = mp.lib()
+    for mode in (mp.MIXED_AUTO, mp.MIXED_TF32, mp.MIXED_FP16, mp.MIXED_TF32X3, 4, -1):
+        assert L.mp_set_mixed_factor(None, mode) == 1  # MP_ERR_ARG: no context
+
+
 def test_library_exports_every_declared_symbol():
     L = mp.lib()
     for name in declared_symbols():
